@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Filter-scan benchmark of the B200 query VM.
+
+Workload (one step = one query over one resident table): the 7-column
+benchmark table at 50,000,000 rows held in HBM (seeded synthetic data, ~1.4 GB,
+larger than the 126 MB L2, so no flush is needed between steps) and the scan +
+arithmetic query
+
+    SELECT id, uniformf + normalf5 * 2.5 AS fsum, normali20 / 3 AS idiv,
+           uniformi - normali5 AS isub
+    FROM test WHERE uniformf < c OR normalf20 > d
+
+with c and d taken from the data so the filter keeps 10% of the rows
+(headline); the sweep reports 0.1%, 1%, 10%, 50% and 99%.  The metric is
+filter-scan GB/s of algorithmic bytes: rows x (strides of the columns the
+program reads) + result rows x (result strides).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With --gpus N > 1 (launched by torchrun, one rank per GPU) every rank scans
+its own 50M-row shard (weak scaling) and the ranks all-gather their result
+counts each step, the one exchange the path needs to place every shard's rows
+in global order.  --impl reference times the reference's own CPU VM
+(virginia_multi with every host thread, built from the reference sources) on
+a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+ROWS = 50_000_000
+HEADLINE_SEL = 0.10
+SWEEP = [0.001, 0.01, 0.10, 0.50, 0.99]
+QUERY = ("SELECT id, uniformf + normalf5 * 2.5 AS fsum, normali20 / 3 AS idiv, "
+         "uniformi - normali5 AS isub FROM test WHERE uniformf < {c:.6f} OR normalf20 > {d:.6f}")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def constants(cols, sel):
+    """c and d such that the OR of the two independent conditions, each
+    keeping q of the rows, keeps 1 - (1 - q)^2 = sel of them."""
+    q = 1 - (1 - sel) ** 0.5
+    c = float(np.quantile(cols["uniformf"][:4_000_000], q))
+    d = float(np.quantile(cols["normalf20"][:4_000_000], 1 - q))
+    return c, d
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.device), "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            time.sleep(0.15)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        sm, smax, reasons, power = [], 0.0, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def exchange_counts(n, world):
+    """All-gather each rank's result count; returns this rank's global offset."""
+    if world == 1:
+        return 0, n
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([n], dtype=torch.int64, device="cuda")
+    out = [torch.zeros_like(t) for _ in range(world)]
+    dist.all_gather(out, t)
+    counts = [int(x.item()) for x in out]
+    r = dist.get_rank()
+    return sum(counts[:r]), sum(counts)
+
+
+def pinned_table(n, seed):
+    """The table's columns in pinned host memory (torch) as numpy views."""
+    import torch
+    from virginian_b200 import datagen
+    cols = {}
+    for name in ["id"] + [c for c, _ in datagen.SCHEMA_A]:
+        arr = datagen.column(name, n, seed=seed) if name != "id" else np.arange(n, dtype=np.int32)
+        t = torch.empty(n, dtype={np.dtype(np.int32): torch.int32,
+                                  np.dtype(np.float32): torch.float32}[arr.dtype], pin_memory=True)
+        t.numpy()[:] = arr
+        cols[name] = (t, t.numpy())
+    return cols
+
+
+def cpu_baseline(sql_for, rows, threads, repeat=3):
+    """The reference CPU VM on a bounded sample (same query, same columns)."""
+    from oracle import oracle
+    from virginian_b200 import datagen
+    cols = datagen.table(rows, datagen.SCHEMA_A, seed=0)
+    c, d = constants(cols, HEADLINE_SEL)
+    sql = sql_for(c, d)
+    db = oracle.OracleDB()
+    try:
+        db.create_table("test", datagen.SCHEMA_A)
+        db.insert("test", cols["id"], [cols[x] for x, _ in datagen.SCHEMA_A])
+        r = db.query(sql, mode=1 if threads > 1 else 0, threads=threads, repeat=repeat)
+        out_rows = r.rows
+        secs = r.seconds
+    finally:
+        db.close()
+    alg = rows * 28 + out_rows * 16
+    return alg / secs / 1e9, secs, out_rows
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    rows = 1_000_000
+    from oracle import oracle
+    from virginian_b200 import datagen
+    cols = datagen.table(rows, datagen.SCHEMA_A, seed=0)
+    c, d = constants(cols, HEADLINE_SEL)
+    sql = QUERY.format(c=c, d=d)
+    db = oracle.OracleDB()
+    times = []
+    try:
+        db.create_table("test", datagen.SCHEMA_A)
+        db.insert("test", cols["id"], [cols[x] for x, _ in datagen.SCHEMA_A])
+        out_rows = 0
+        for i in range(args.warmup + args.steps):
+            r = db.query(sql, mode=1, threads=threads, repeat=1)
+            out_rows = r.rows
+            if i >= args.warmup:
+                times.append(r.seconds)
+    finally:
+        db.close()
+    alg = rows * 28 + out_rows * 16
+    total = sum(times)
+    value = alg * len(times) / total / 1e9
+    line = {
+        "impl": "reference", "metric": "filter scan GB/s", "value": round(value, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total / len(times) * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/float32", "data": "synthetic",
+        "config": {"workload": "device-resident filter scan + arithmetic, 10% selectivity",
+                   "rows": rows, "query": sql, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{rows} rows of the same table and query per step, "
+                                   "virginia_multi (src/vm/virginia.c) built from the reference sources"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_b200(args):
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    import virginian_b200 as vb
+    from virginian_b200 import datagen, sql as vsql
+
+    torch.cuda.set_device(local)
+    rows = args.rows
+    pcols = pinned_table(rows, seed=rank)
+    cols = {k: v[1] for k, v in pcols.items()}
+    types = [t for _, t in datagen.SCHEMA_A]
+    cat = vsql.Catalog()
+    cat.add_table("test", datagen.SCHEMA_A)
+
+    def program(sel):
+        c, d = constants(cols, sel)
+        comp = cat.compile(QUERY.format(c=c, d=d))
+        return vb.Program(comp.op_list(), comp.pc, types)
+
+    eng = vb.Engine(local)
+    segs = datagen.segments(cols, datagen.SCHEMA_A)
+    table = vb.Table(eng, types)
+    table.append(segs)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    load_b = None
+
+    def alg_bytes(p, out_rows):
+        return rows * p.info.load_bytes_per_row + out_rows * p.info.out_bytes_per_row
+
+    def timed(p, steps, warmup):
+        for _ in range(warmup):
+            r = table.query(p)
+            n = r.rows
+            r.close()
+        eng.timing(max(steps, 1))
+        barrier(world)
+        torch.cuda.synchronize()
+        l0 = eng.launches
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            r = table.query(p)
+            if world > 1:
+                exchange_counts(r.rows, world)
+            r.close()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = ev0.elapsed_time(ev1)
+        kt = eng.kernel_times(steps)
+        launches = eng.launches - l0
+        err = eng.device_error()
+        if err:
+            raise RuntimeError(f"device error {err}")
+        return n, ms, kt, launches
+
+    # headline
+    p = program(HEADLINE_SEL)
+    with Clocks(local) as clk:
+        out_rows, ms, kt, launches = timed(p, args.steps, args.warmup)
+    ms_max = allreduce_max(ms, world)
+    alg = alg_bytes(p, out_rows)
+    # every rank processes the same number of bytes up to its result rows;
+    # sum the algorithmic bytes over ranks
+    alg_total = alg
+    if world > 1:
+        t = torch.tensor([alg], dtype=torch.float64, device="cuda")
+        import torch.distributed as dist
+        dist.all_reduce(t)
+        alg_total = float(t.item())
+    value = alg_total * args.steps / (ms_max / 1e3) / 1e9
+    kernel_ms = statistics.mean(kt) if kt else None
+    hbm, peak_kind = peaks()
+    achieved = alg / (kernel_ms / 1e3) / 1e9 if kernel_ms else None
+
+    # selectivity sweep (device-resident)
+    sweep = {}
+    for sel in SWEEP:
+        ps = program(sel)
+        n, sms, skt, _ = timed(ps, max(20, args.steps // 5), 2)
+        km = statistics.mean(skt)
+        sweep[f"{sel:g}"] = {"result_rows": n, "ms_per_step": round(sms / max(20, args.steps // 5), 4),
+                             "kernel_ms": round(km, 4),
+                             "gbs": round(alg_bytes(ps, n) / (km / 1e3) / 1e9, 1),
+                             "frac_of_hbm": round(alg_bytes(ps, n) / (km / 1e3) / 1e9 / hbm, 3)}
+
+    # end to end through the C ABI from pinned host buffers
+    info = p.info
+    outs = [torch.empty(max(out_rows, 1) + 1024, dtype={0: torch.int32, 2: torch.float32}[info.out_type[j]],
+                        pin_memory=True) for j in range(info.nout)]
+    import ctypes
+    from virginian_b200._lib import lib as vlib
+    seg_arr, keep = vb._segments(segs, types)
+    ptrs = (ctypes.c_void_p * info.nout)(*[o.data_ptr() for o in outs])
+    nrows = ctypes.c_uint64()
+    e2e_steps = max(3, min(args.steps // 50, 10))
+    vb.check(vlib().virg_gpu_query_host(eng.h, p.h, seg_arr, len(segs), ptrs, out_rows + 1024,
+                                        ctypes.byref(nrows)), "query_host")
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        vb.check(vlib().virg_gpu_query_host(eng.h, p.h, seg_arr, len(segs), ptrs, out_rows + 1024,
+                                            ctypes.byref(nrows)), "query_host")
+        if world > 1:
+            exchange_counts(nrows.value, world)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = allreduce_max(e2e_s, world)
+    assert nrows.value == out_rows
+    e2e_value = alg_total * e2e_steps / e2e_s / 1e9
+    h2d = rows * info.load_bytes_per_row
+    d2h = out_rows * info.out_bytes_per_row
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if args.cpu_baseline and world == 1:
+            v1, s1, _ = cpu_baseline(lambda c, d: QUERY.format(c=c, d=d), args.cpu_rows, 1)
+            cpu = {"value": round(v1, 3), "unit": "GB/s", "cores": 1, "kind": "reference",
+                   "sample": f"{args.cpu_rows} rows of the same table and query, virginia_single "
+                             "(src/vm/virginia.c) built from the reference sources, best of 3"}
+            vm_, sm_, _ = cpu_baseline(lambda c, d: QUERY.format(c=c, d=d), args.cpu_rows,
+                                       os.cpu_count() or 1)
+            cpu_multi = {"value": round(vm_, 3), "unit": "GB/s", "cores": os.cpu_count(),
+                         "kind": "reference", "vm": "virginia_multi"}
+        shape = eng.last_launch()
+        line = {
+            "metric": "filter scan GB/s (% HBM peak)", "value": round(value, 2), "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32/float32", "data": "synthetic",
+            "config": {"workload": "device-resident filter scan + arithmetic (7-column table, "
+                                   "50M rows per GPU, 10% selectivity)",
+                       "rows_per_gpu": rows, "query": QUERY.format(c=constants(cols, 0.1)[0],
+                                                                   d=constants(cols, 0.1)[1]),
+                       "result_rows": out_rows, "l2": "inputs larger than L2 (1.4 GB per step)",
+                       "launch": shape},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+                         "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4) if achieved else None,
+                         "traffic": None, "peak_kind": peak_kind,
+                         "kernel_ms": round(kernel_ms, 4) if kernel_ms else None,
+                         "algorithmic_bytes": alg},
+            "sweep": sweep,
+            "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                    "ms_per_step": round(e2e_s / e2e_steps * 1e3, 3)},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+            line["cpu_multicore"] = cpu_multi
+        print(json.dumps(line))
+    del keep
+    table.close()
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--rows", type=int, default=ROWS)
+    ap.add_argument("--cpu-rows", type=int, default=4_000_000)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,355 @@
+/*
+ * virginian_b200.h - C ABI of the B200 (sm_100a) query VM for Virginian.
+ *
+ * Two groups of entry points:
+ *
+ * 1. The drop-in GPU VM.  virg_vm_gpu and virg_gpu_getsizes have exactly the
+ *    reference's signatures (src/virginian.h:620-622) and replace
+ *    src/vm/vm_gpu.cu in the reference's build.  virg_vm_execute
+ *    (src/vm/execute.c:85-86) calls virg_vm_gpu at OP_Parallel when
+ *    v->use_gpu is set; the reference's host library (tablet slot cache,
+ *    result allocation, reader) stays as it is.
+ *
+ * 2. The engine API (virg_gpu_*): plain pointers and sizes, no reference
+ *    structs except the opcode program itself (virg_op).  It exposes what the
+ *    drop-in is built on: HBM-resident tables, one-launch queries with ordered
+ *    output, host-buffer (end-to-end) queries, streamed execution of
+ *    host-resident tables, batched persistent execution of many queries and a
+ *    continuous-batching serving loop.  None of these has a reference
+ *    counterpart; the reference runs one query per launch sequence.
+ *
+ * Every call returns VIRG_SUCCESS (1) or VIRG_FAIL (0), the reference's
+ * convention (src/virginian.h:118-121); virg_gpu_last_error() gives the
+ * reason for the calling thread's last failure.
+ *
+ * The reference's types below are declared with identical layouts
+ * (src/virginian.h:166-503) so this header can stand alone; when the
+ * reference's virginian.h is included first (it defines VIRGINIAN) the
+ * declarations here are skipped and the reference's own are used.
+ */
+#ifndef VIRGINIAN_B200_H
+#define VIRGINIAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifndef VIRGINIAN
+#include <pthread.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef VIRGINIAN
+/* ---- reference ABI (src/virginian.h), layouts must stay identical ---- */
+#define VIRG_FAIL 0
+#define VIRG_SUCCESS 1
+#define VIRG_MAX_COLUMNS 16
+#define VIRG_MAX_TABLES 16
+#define VIRG_MAX_COLUMN_NAME 16
+#define VIRG_MAX_TABLE_NAME 32
+#define VIRG_MEM_TABLETS 64
+#define VIRG_REGS 16
+#define VIRG_GLOBAL_REGS 16
+#define VIRG_OPS 32
+#define VIRG_VM_TABLES 1
+#define VIRG_ROW_BUFFER 256
+
+/* opcodes, src/virginian.h:166-193 */
+typedef enum {
+	OP_Table = 0, OP_ResultColumn = 1, OP_Parallel = 2, OP_Finish = 3,
+	OP_Column = 4, OP_Rowid = 5, OP_Result = 6, OP_Converge = 7,
+	OP_Invalid = 8, OP_Cast = 9, OP_Integer = 10, OP_Float = 11,
+	OP_Le = 12, OP_Lt = 13, OP_Ge = 14, OP_Gt = 15, OP_Eq = 16, OP_Neq = 17,
+	OP_Add = 18, OP_Sub = 19, OP_Mul = 20, OP_Div = 21,
+	OP_And = 22, OP_Or = 23, OP_Not = 24, OP_Nop = 25
+} virg_ops;
+
+/* value types, src/virginian.h:196-204 */
+typedef enum {
+	VIRG_INT = 0, VIRG_INT64 = 1, VIRG_FLOAT = 2, VIRG_DOUBLE = 3,
+	VIRG_CHAR = 4, VIRG_STRING = 5, VIRG_NULL = 6
+} virg_t;
+
+/* src/virginian.h:227-234 */
+typedef struct {
+	unsigned id;
+	int used;
+	unsigned disk_slot;
+} virg_tablet_info;
+
+/* tablet header, src/virginian.h:251-302 */
+typedef struct {
+	unsigned rows;
+	virg_t key_type;
+	size_t key_stride;
+	size_t key_pointer_stride;
+	unsigned id;
+	unsigned next;
+	int last_tablet;
+	int in_table;
+	unsigned table_id;
+	size_t key_block;
+	size_t key_pointers_block;
+	size_t fixed_block;
+	size_t variable_block;
+	size_t size;
+	unsigned possible_rows;
+	size_t row_stride;
+	unsigned fixed_columns;
+	char fixed_name[VIRG_MAX_COLUMNS][VIRG_MAX_COLUMN_NAME];
+	virg_t fixed_type[VIRG_MAX_COLUMNS];
+	size_t fixed_stride[VIRG_MAX_COLUMNS];
+	size_t fixed_offset[VIRG_MAX_COLUMNS];
+	virg_tablet_info *info;
+} __attribute__((aligned(64))) virg_tablet_meta;
+
+/* opcode argument, src/virginian.h:309-317 */
+typedef union {
+	int i;
+	float f;
+	long long int li;
+	double d;
+	char c;
+	char *s;
+} __attribute__((aligned(8))) virg_var;
+
+/* one opcode, src/virginian.h:327-333 */
+typedef struct {
+	int op;
+	int p1;
+	int p2;
+	int p3;
+	virg_var p4;
+} virg_op;
+
+/* src/virginian.h:341-346 */
+typedef struct virg_result_node_ {
+	unsigned id;
+	struct virg_result_node_ *next;
+} virg_result_node;
+
+/* opcode program + result list, src/virginian.h:356-377 */
+typedef struct {
+	unsigned pc;
+	virg_op stmt[VIRG_OPS];
+	unsigned num_ops;
+	virg_var global_reg[VIRG_GLOBAL_REGS];
+	virg_t type[VIRG_GLOBAL_REGS];
+	unsigned table[VIRG_VM_TABLES];
+	unsigned num_tables;
+	virg_result_node *head_result;
+	virg_result_node *tail_result;
+	float timing1, timing2, timing3;
+} virg_vm;
+
+/* database file state, src/virginian.h:427-458 */
+typedef struct {
+	unsigned num_tablets;
+	unsigned alloced_tablets;
+	unsigned tablet_id_counter;
+	size_t block_size;
+	char tables[VIRG_MAX_TABLES][VIRG_MAX_TABLE_NAME];
+	unsigned first_tablet[VIRG_MAX_TABLES];
+	unsigned last_tablet[VIRG_MAX_TABLES];
+	unsigned write_cursor[VIRG_MAX_TABLES];
+	unsigned table_tablets[VIRG_MAX_TABLES];
+	int table_status[VIRG_MAX_TABLES];
+	virg_tablet_info *tablet_info;
+} virg_db;
+
+/* database state, src/virginian.h:468-503 */
+typedef struct {
+	virg_db db;
+	unsigned tablet_slot_ids[VIRG_MEM_TABLETS];
+	int tablet_slot_status[VIRG_MEM_TABLETS];
+	unsigned tablet_slots_taken;
+	unsigned tablet_slot_counter;
+	virg_tablet_meta *tablet_slots[VIRG_MEM_TABLETS];
+	void *gpu_slots;
+	pthread_mutex_t slot_lock;
+	int dbfd;
+	unsigned threads_per_block;
+	unsigned multi_threads;
+	int use_multi;
+	int use_gpu;
+	int use_stream;
+	int use_mmap;
+} virginian;
+
+/* src/virginian.h:512-523 */
+typedef struct {
+	virginian *v;
+	virg_vm *vm;
+	virg_tablet_meta *tab;
+	virg_tablet_meta *res;
+	unsigned row;
+	unsigned num_rows;
+	unsigned num_tablets;
+	unsigned tablets_proced;
+	pthread_mutex_t tab_lock;
+	pthread_mutex_t res_lock;
+} virg_vm_arg;
+
+/* src/virginian.h:532-541 */
+typedef struct {
+	virg_vm *vm;
+	virg_tablet_meta *res;
+	unsigned row;
+	char buffer[VIRG_ROW_BUFFER];
+} virg_reader;
+#endif /* VIRGINIAN */
+
+/* ======================================================================
+ * 1. Drop-in GPU VM
+ * ====================================================================== */
+
+/*
+ * Replaces virg_vm_gpu (src/virginian.h:620-621, src/vm/vm_gpu.cu:107-578).
+ * Runs the data-parallel section of vm (from vm->pc to its OP_Converge) over
+ * the tablet chain starting at tab[0] and appends result rows to res[0],
+ * allocating further result tablets with virg_vm_allocresult.  Result rows
+ * are in original row order and split across result tablets exactly as the
+ * single-core CPU VM splits them (src/vm/virginia.c:518-524).  On return,
+ * tab[0] and res[0] are the final data and result tablets with one lock each,
+ * as virg_vm_execute's OP_Finish expects (src/vm/execute.c:92-96).
+ * num_tablets = 0 processes the whole chain.  vm->timing1..3 receive the
+ * host-to-device, kernel and device-to-host times in seconds.
+ */
+int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
+	virg_tablet_meta **res, unsigned num_tablets);
+
+/*
+ * Replaces virg_gpu_getsizes (src/virginian.h:622, src/vm/vm_gpu.cu:27-30):
+ * the 15 struct sizes of virg_testsizes (src/virginian.h:553-569) as this
+ * library was compiled, for the host/GPU layout check of
+ * src/test/virgstate.cc:64-80.
+ */
+const size_t *virg_gpu_getsizes(void);
+
+/* ======================================================================
+ * 2. Engine API (no reference counterpart)
+ * ====================================================================== */
+
+typedef struct virg_gpu_engine virg_gpu_engine;
+typedef struct virg_gpu_program virg_gpu_program;
+typedef struct virg_gpu_table virg_gpu_table;
+typedef struct virg_gpu_result virg_gpu_result;
+typedef struct virg_gpu_batch virg_gpu_batch;
+typedef struct virg_serve virg_serve;
+
+/* column types of a table, in the reference's virg_t numbering */
+typedef struct {
+	int key_type;
+	unsigned ncols;
+	int col_type[VIRG_MAX_COLUMNS];
+} virg_gpu_schema;
+
+/* one tablet's columns as plain pointers: rows, the key column (read by
+ * OP_Rowid) and each fixed column (read by OP_Column); host or device memory
+ * depending on the call */
+typedef struct {
+	uint32_t rows;
+	const void *key;
+	const void *col[VIRG_MAX_COLUMNS];
+} virg_gpu_segment;
+
+/* what a compiled program reads and writes */
+typedef struct {
+	unsigned nload;                 /* distinct columns read */
+	int load_column[VIRG_MAX_COLUMNS + 1]; /* column index, -1 = key */
+	unsigned load_bytes_per_row;    /* sum of their strides */
+	unsigned nout;                  /* result columns */
+	int out_type[VIRG_MAX_COLUMNS];
+	unsigned out_stride[VIRG_MAX_COLUMNS];
+	unsigned out_bytes_per_row;
+	unsigned nuops;                 /* interpreted device ops */
+} virg_gpu_program_info;
+
+/* thread-local description of the last failure on this thread */
+const char *virg_gpu_last_error(void);
+
+/* engine: one per device; owns its stream, scratch and caches */
+int virg_gpu_engine_create(int device, virg_gpu_engine **out);
+void virg_gpu_engine_destroy(virg_gpu_engine *e);
+/* the engine's CUDA stream (a cudaStream_t), for event timing by callers */
+void *virg_gpu_engine_stream(virg_gpu_engine *e);
+/* device error word set by bounded waits inside kernels (0 = none); reading
+ * it synchronises the engine stream and clears it */
+int virg_gpu_engine_check(virg_gpu_engine *e, unsigned *device_error);
+/* launch shape: threads per CTA, rows per thread, staging depth, CTAs per
+ * SM; 0 in a field keeps the automatic choice */
+int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
+	unsigned rows_per_thread, unsigned stages, unsigned ctas_per_sm);
+/* record CUDA events around each of the next kernel launches in a ring of
+ * `slots` entries (0 turns it off) */
+int virg_gpu_engine_timing(virg_gpu_engine *e, unsigned slots);
+/* device durations (ms) of up to the last n timed launches, oldest first;
+ * waits for the last one to finish */
+int virg_gpu_engine_kernel_times(virg_gpu_engine *e, float *ms, unsigned n, unsigned *got);
+/* how many kernels the engine has launched since creation */
+unsigned long long virg_gpu_engine_launches(virg_gpu_engine *e);
+/* launch shape chosen for the engine's last launch: shape4 = {threads,
+ * rows per thread, stages, CTAs per SM requested}, grid size, shared memory */
+int virg_gpu_engine_last_launch(virg_gpu_engine *e, unsigned *shape4, unsigned *grid,
+	unsigned *smem);
+
+/* validate and decode the data-parallel section of a reference opcode
+ * program (ops[pc] up to its OP_Converge) for a table schema; host only */
+int virg_gpu_program_create(const virg_op *ops, unsigned num_ops, unsigned pc,
+	const virg_gpu_schema *schema, virg_gpu_program **out);
+int virg_gpu_program_info_get(const virg_gpu_program *p, virg_gpu_program_info *info);
+/* 1 when some still-valid row can read a register its path never set (the
+ * reference CPU VM then reads a stale lane), 0 otherwise */
+int virg_gpu_program_flags(const virg_gpu_program *p);
+void virg_gpu_program_destroy(virg_gpu_program *p);
+
+/* Re-entrant SQL front end.  Emits the same opcode program as the
+ * reference's parser and code generator (src/sql/sql.y:78-240,
+ * src/sql/generate.c:820) for SELECT statements over catalog tables.
+ * ops receives up to VIRG_OPS ops (ResultColumn p4 is left NULL; the names go
+ * to names[k * VIRG_MAX_COLUMN_NAME] for op k), *pc the first op of the
+ * data-parallel section, *table_id the table's catalog index. */
+typedef struct virg_gpu_catalog virg_gpu_catalog;
+int virg_gpu_catalog_create(virg_gpu_catalog **out);
+int virg_gpu_catalog_add_table(virg_gpu_catalog *c, const char *name, int key_type,
+	unsigned ncols, const char *const *col_names, const int *col_types, unsigned *table_id);
+void virg_gpu_catalog_destroy(virg_gpu_catalog *c);
+int virg_gpu_sql_compile(const virg_gpu_catalog *c, const char *sql, virg_op *ops,
+	unsigned *num_ops, unsigned *pc, char *names, unsigned *table_id);
+
+/* HBM-resident table: segments are copied from host (or device) memory into
+ * 256-byte-aligned device columns and stay resident until destroyed */
+int virg_gpu_table_create(virg_gpu_engine *e, const virg_gpu_schema *schema,
+	virg_gpu_table **out);
+int virg_gpu_table_append(virg_gpu_table *t, const virg_gpu_segment *segs,
+	unsigned nsegs);
+uint64_t virg_gpu_table_rows(const virg_gpu_table *t);
+uint64_t virg_gpu_table_bytes(const virg_gpu_table *t);
+void virg_gpu_table_destroy(virg_gpu_table *t);
+
+/* run a program over a resident table; the ordered result stays in HBM.
+ * Asynchronous on the engine stream; virg_gpu_result_rows waits for it. */
+int virg_gpu_query(virg_gpu_engine *e, const virg_gpu_program *p,
+	const virg_gpu_table *t, virg_gpu_result **out);
+int virg_gpu_result_rows(virg_gpu_result *r, uint64_t *rows);
+/* device pointer of result column c (valid until the result is destroyed) */
+const void *virg_gpu_result_column(const virg_gpu_result *r, unsigned c);
+/* copy rows [first, first+count) of every result column to host buffers */
+int virg_gpu_result_download(virg_gpu_result *r, void *const *host_cols,
+	uint64_t first, uint64_t count);
+void virg_gpu_result_destroy(virg_gpu_result *r);
+
+/* end to end: host segments in, host result columns out.  Copies the
+ * referenced columns to the device, runs the program and copies the result
+ * rows back; out_cols[c] must hold `capacity` rows of result column c. */
+int virg_gpu_query_host(virg_gpu_engine *e, const virg_gpu_program *p,
+	const virg_gpu_segment *segs, unsigned nsegs, void *const *out_cols,
+	uint64_t capacity, uint64_t *out_rows);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VIRGINIAN_B200_H */

@@ -1,0 +1,166 @@
+"""Parity of the sm_100a VM with the reference single-core CPU VM (the
+oracle) on the same seeded tables: result streams must be byte-identical and
+in the same order."""
+import numpy as np
+import pytest
+
+import virginian_b200 as vb
+from virginian_b200 import datagen
+from tests.helpers import (CONFIG1, EXTRA, SUITE, assert_same_stream, build_oracle_db, col_types,
+                           config2)
+
+pytestmark = pytest.mark.gpu
+
+TYPES_A = col_types(datagen.SCHEMA_A)
+TYPES_B = col_types(datagen.SCHEMA_B)
+N = 500_000
+
+
+def section_start(vm):
+    return next(k for k in range(vm.num_ops) if vm.stmt[k].op == 2) + 1
+
+
+def program(db, sql, types):
+    vm, _ = db.compile(sql)
+    return vb.Program([vm.stmt[k] for k in range(vm.num_ops)], section_start(vm), types)
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = vb.Engine(0)
+    yield e
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def data_a(oracle_mod, engine):
+    db, cols = build_oracle_db(oracle_mod, N, seed=11)
+    t = vb.Table(engine, TYPES_A)
+    t.append(datagen.segments(cols, datagen.SCHEMA_A))
+    yield db, cols, t
+    t.close()
+    db.close()
+
+
+def run_both(db, t, sql, types):
+    want = db.query(sql).columns
+    p = program(db, sql, types)
+    r = t.query(p)
+    got = r.download()
+    r.close()
+    return got, want, p
+
+
+@pytest.mark.parametrize("sql", SUITE + EXTRA + [CONFIG1])
+def test_resident_query_matches_oracle(data_a, sql, engine):
+    db, _, t = data_a
+    got, want, _ = run_both(db, t, sql, TYPES_A)
+    assert_same_stream(got, want, sql)
+    assert engine.device_error() == 0
+
+
+@pytest.mark.parametrize("sel", [0.001, 0.01, 0.1, 0.5, 0.99])
+def test_config2_selectivity_sweep(data_a, sel):
+    db, cols, t = data_a
+    # c and d from the empirical distributions so the OR of two independent
+    # conditions, each keeping q of the rows, keeps 1 - (1 - q)^2 = sel
+    q = 1 - (1 - sel) ** 0.5
+    c = float(np.quantile(cols["uniformf"], q))
+    d = float(np.quantile(cols["normalf20"], 1 - q))
+    sql = config2(c, d)
+    got, want, _ = run_both(db, t, sql, TYPES_A)
+    assert_same_stream(got, want, sql)
+    frac = got[0].shape[0] / N
+    assert abs(frac - sel) < max(0.02, sel * 0.2)
+
+
+def test_query_host_end_to_end(data_a, engine):
+    db, cols, _ = data_a
+    p = program(db, CONFIG1, TYPES_A)
+    got = engine.query_host(p, datagen.segments(cols, datagen.SCHEMA_A))
+    assert_same_stream(got, db.query(CONFIG1).columns, "query_host")
+
+
+@pytest.mark.parametrize("shape", [(128, 4), (128, 8), (256, 2), (256, 4), (256, 8), (512, 2),
+                                   (512, 4)])
+def test_every_launch_shape(data_a, engine, shape):
+    db, _, t = data_a
+    engine.set_shape(shape[0], shape[1], 2)
+    try:
+        for sql in (CONFIG1, config2(30.0, 20.0), SUITE[8]):
+            got, want, _ = run_both(db, t, sql, TYPES_A)
+            assert_same_stream(got, want, f"{shape} {sql}")
+        assert engine.last_launch()["threads"] == shape[0]
+    finally:
+        engine.set_shape(0, 0, 0, 0)
+
+
+@pytest.mark.parametrize("n", [0, 1, 63, 64, 65, 1023, 1024, 1025, 4097, 70_001])
+def test_edge_sizes(oracle_mod, engine, n):
+    db, cols = build_oracle_db(oracle_mod, n, seed=n)
+    with db:
+        t = vb.Table(engine, TYPES_A)
+        if n:
+            t.append(datagen.segments(cols, datagen.SCHEMA_A))
+        for sql in (CONFIG1, "select id, uniformi from test", SUITE[9]):
+            got, want, _ = run_both(db, t, sql, TYPES_A)
+            assert_same_stream(got, want, f"n={n} {sql}")
+        t.close()
+
+
+def test_ragged_segments(oracle_mod, engine):
+    n = 30_000
+    db, cols = build_oracle_db(oracle_mod, n, seed=5)
+    with db:
+        t = vb.Table(engine, TYPES_A)
+        cuts = [0, 1, 2, 100, 4096, 4097, 9000, 17_777, 30_000]
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            t.append([{"rows": b - a, "key": cols["id"][a:b],
+                       "cols": [cols[c][a:b] for c, _ in datagen.SCHEMA_A]}])
+        for sql in (CONFIG1, SUITE[5], config2(10.0, 10.0)):
+            got, want, _ = run_both(db, t, sql, TYPES_A)
+            assert_same_stream(got, want, sql)
+        t.close()
+
+
+def test_int64_and_double_columns(oracle_mod, engine):
+    n = 300_000
+    db, cols = build_oracle_db(oracle_mod, n, seed=3, schema=datagen.SCHEMA_B)
+    with db:
+        t = vb.Table(engine, TYPES_B)
+        t.append(datagen.segments(cols, datagen.SCHEMA_B, 161_000))
+        for sql in ["select id, uniforml, normald from test where normali20 > 15 and uniformf < 50.0",
+                    "select normald * normald - normald / normald as dd, id from test where normald > 1.5",
+                    "select uniforml + uniforml as l2, uniforml * uniforml as l3 from test where uniforml < uniforml - uniforml",
+                    "select id, normald from test where normald >= normald + normald or uniformi = 3"]:
+            got, want, _ = run_both(db, t, sql, TYPES_B)
+            assert_same_stream(got, want, sql)
+        t.close()
+
+
+def test_float_edge_values(oracle_mod, engine):
+    """Signed zeros, subnormals, infinities and NaN through compares and
+    arithmetic (no flush-to-zero, IEEE division)."""
+    specials = np.array([0.0, -0.0, 1e-45, -1e-45, 1.17549435e-38, 3.4e38, -3.4e38, np.inf, -np.inf,
+                         np.nan, 1.0, -1.0, 0.1, 1e-30], dtype=np.float32)
+    n = 4096
+    rng = np.random.default_rng(9)
+    cols = {"id": np.arange(n, dtype=np.int32)}
+    for name, ty in datagen.SCHEMA_A:
+        if ty == vb.VIRG_FLOAT:
+            cols[name] = rng.choice(specials, size=n).astype(np.float32)
+        else:
+            cols[name] = rng.integers(-3, 3, size=n, dtype=np.int32)
+    db = oracle_mod.OracleDB()
+    with db:
+        db.create_table("test", datagen.SCHEMA_A)
+        db.insert("test", cols["id"], [cols[c] for c, _ in datagen.SCHEMA_A])
+        t = vb.Table(engine, TYPES_A)
+        t.append(datagen.segments(cols, datagen.SCHEMA_A))
+        for sql in ["select id, uniformf / normalf5 as q, normalf20 * uniformf as m from test where uniformf >= normalf5 or normalf20 != normalf20",
+                    "select uniformf - normalf5 as s, normalf20 + normalf20 as a from test where uniformf = 0.0 or normalf5 < 0.0",
+                    "select id, uniformi / normali5 as iq from test where normali5 != 0",
+                    "select normali5 * normali20 - uniformi as z from test"]:
+            got, want, _ = run_both(db, t, sql, TYPES_A)
+            assert_same_stream(got, want, sql)
+        t.close()

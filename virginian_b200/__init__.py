@@ -1,0 +1,246 @@
+"""B200-native query VM for Virginian (sm_100a), Python side.
+
+The product is the C ABI in include/virginian_b200.h, implemented in CUDA in
+``csrc/`` and built into ``libvirginian_b200.so``.  This package wraps it with
+ctypes for tests, benchmarks and Python callers:
+
+* :class:`Engine` - one per device (stream, scratch, caches);
+* :class:`Program` - a validated, decoded data-parallel section of a
+  Virginian opcode program (``virg_op`` array, src/virginian.h:327-377);
+* :class:`Table` - an HBM-resident table made of segments (tablets);
+* :class:`Result` - an ordered, HBM-resident result stream.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import ProgramInfo, Schema, Segment, VirgError, VirgOp, check, lib
+
+# virg_t numbering, src/virginian.h:196-204
+VIRG_INT, VIRG_INT64, VIRG_FLOAT, VIRG_DOUBLE, VIRG_CHAR = 0, 1, 2, 3, 4
+NP_OF = {VIRG_INT: np.int32, VIRG_INT64: np.int64, VIRG_FLOAT: np.float32,
+         VIRG_DOUBLE: np.float64, VIRG_CHAR: np.int8}
+TYPE_OF = {np.dtype(v): k for k, v in NP_OF.items()}
+
+__all__ = ["Engine", "Program", "Table", "Result", "VirgError", "make_schema", "ops_array",
+           "VIRG_INT", "VIRG_INT64", "VIRG_FLOAT", "VIRG_DOUBLE", "VIRG_CHAR", "NP_OF"]
+
+
+def make_schema(col_types: Sequence[int], key_type: int = VIRG_INT) -> Schema:
+    s = Schema()
+    s.key_type = key_type
+    s.ncols = len(col_types)
+    for i, t in enumerate(col_types):
+        s.col_type[i] = t
+    return s
+
+
+def ops_array(ops) -> Tuple[ctypes.Array, int]:
+    """Accepts a ctypes virg_op array/structure sequence or (op,p1,p2,p3,p4) tuples."""
+    n = len(ops)
+    arr = (VirgOp * max(n, 1))()
+    for k, o in enumerate(ops):
+        if isinstance(o, tuple):
+            op, p1, p2, p3 = o[:4]
+            arr[k].op, arr[k].p1, arr[k].p2, arr[k].p3 = op, p1, p2, p3
+            if len(o) > 4:
+                p4 = o[4]
+                if isinstance(p4, float):
+                    arr[k].p4.f = p4
+                else:
+                    arr[k].p4.i = int(p4)
+        else:
+            ctypes.memmove(ctypes.byref(arr[k]), ctypes.byref(o), ctypes.sizeof(VirgOp))
+    return arr, n
+
+
+class Engine:
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().virg_gpu_engine_create(device, ctypes.byref(h)), "engine create")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().virg_gpu_engine_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        return lib().virg_gpu_engine_stream(self.h)
+
+    def set_shape(self, threads: int = 0, rows_per_thread: int = 0, stages: int = 0,
+                  ctas_per_sm: int = 0) -> None:
+        check(lib().virg_gpu_engine_set_shape(self.h, threads, rows_per_thread, stages,
+                                              ctas_per_sm), "set shape")
+
+    def device_error(self) -> int:
+        e = ctypes.c_uint()
+        check(lib().virg_gpu_engine_check(self.h, ctypes.byref(e)), "engine check")
+        return e.value
+
+    def timing(self, slots: int) -> None:
+        """Record events around each of the next launches (ring of `slots`)."""
+        check(lib().virg_gpu_engine_timing(self.h, slots), "engine timing")
+
+    def kernel_times(self, n: int) -> List[float]:
+        """Device milliseconds of up to the last n timed kernel launches."""
+        buf = (ctypes.c_float * max(n, 1))()
+        got = ctypes.c_uint()
+        check(lib().virg_gpu_engine_kernel_times(self.h, buf, n, ctypes.byref(got)), "kernel times")
+        return [buf[i] for i in range(got.value)]
+
+    @property
+    def launches(self) -> int:
+        return int(lib().virg_gpu_engine_launches(self.h))
+
+    def last_launch(self) -> Dict[str, int]:
+        s = (ctypes.c_uint * 4)()
+        g, m = ctypes.c_uint(), ctypes.c_uint()
+        check(lib().virg_gpu_engine_last_launch(self.h, s, ctypes.byref(g), ctypes.byref(m)),
+              "last launch")
+        return {"threads": s[0], "rows_per_thread": s[1], "stages": s[2], "ctas_per_sm": s[3],
+                "grid": g.value, "smem": m.value}
+
+    def query_host(self, program: "Program", segments: Sequence[dict], capacity: Optional[int] = None):
+        """End to end from host arrays: returns the result columns as numpy arrays."""
+        segs, keep = _segments(segments, program.col_types)
+        total = sum(int(s["rows"]) for s in segments)
+        cap = total if capacity is None else capacity
+        info = program.info
+        outs = [np.empty(max(cap, 1), dtype=NP_OF[info.out_type[j]]) for j in range(info.nout)]
+        ptrs = (ctypes.c_void_p * max(1, info.nout))(*[o.ctypes.data for o in outs])
+        rows = ctypes.c_uint64()
+        check(lib().virg_gpu_query_host(self.h, program.h, segs, len(segments), ptrs, cap,
+                                        ctypes.byref(rows)), "query_host")
+        del keep
+        return [o[:rows.value] for o in outs]
+
+
+class Program:
+    def __init__(self, ops, pc: int, col_types: Sequence[int], key_type: int = VIRG_INT):
+        arr, n = ops_array(ops)
+        self.col_types = list(col_types)
+        self.key_type = key_type
+        self.schema = make_schema(col_types, key_type)
+        h = ctypes.c_void_p()
+        check(lib().virg_gpu_program_create(arr, n, pc, ctypes.byref(self.schema), ctypes.byref(h)),
+              "program create")
+        self.h = h
+        self.info = ProgramInfo()
+        check(lib().virg_gpu_program_info_get(self.h, ctypes.byref(self.info)), "program info")
+
+    @property
+    def maybe_undefined(self) -> bool:
+        return lib().virg_gpu_program_flags(self.h) == 1
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().virg_gpu_program_destroy(self.h)
+        except Exception:
+            pass
+
+
+def _segments(segments: Sequence[dict], col_types: Sequence[int]):
+    """Builds virg_gpu_segment structs from dicts {rows, key, cols} of numpy arrays."""
+    arr = (Segment * max(1, len(segments)))()
+    keep = []
+    for i, s in enumerate(segments):
+        arr[i].rows = int(s["rows"])
+        k = s.get("key")
+        if k is not None:
+            k = np.ascontiguousarray(k)
+            keep.append(k)
+            arr[i].key = k.ctypes.data
+        for c, col in enumerate(s["cols"]):
+            if col is None:
+                continue
+            if isinstance(col, int):
+                arr[i].col[c] = col
+                continue
+            col = np.ascontiguousarray(col)
+            if c < len(col_types):
+                assert col.dtype == NP_OF[col_types[c]], (c, col.dtype)
+            keep.append(col)
+            arr[i].col[c] = col.ctypes.data
+    return arr, keep
+
+
+class Table:
+    def __init__(self, engine: Engine, col_types: Sequence[int], key_type: int = VIRG_INT):
+        self.engine = engine
+        self.col_types = list(col_types)
+        self.schema = make_schema(col_types, key_type)
+        h = ctypes.c_void_p()
+        check(lib().virg_gpu_table_create(engine.h, ctypes.byref(self.schema), ctypes.byref(h)),
+              "table create")
+        self.h = h
+
+    def append(self, segments: Sequence[dict]) -> None:
+        segs, keep = _segments(segments, self.col_types)
+        check(lib().virg_gpu_table_append(self.h, segs, len(segments)), "table append")
+        del keep
+
+    @property
+    def rows(self) -> int:
+        return int(lib().virg_gpu_table_rows(self.h))
+
+    @property
+    def nbytes(self) -> int:
+        return int(lib().virg_gpu_table_bytes(self.h))
+
+    def query(self, program: Program) -> "Result":
+        r = ctypes.c_void_p()
+        check(lib().virg_gpu_query(self.engine.h, program.h, self.h, ctypes.byref(r)), "query")
+        return Result(r, program)
+
+    def close(self) -> None:
+        if self.h:
+            lib().virg_gpu_table_destroy(self.h)
+            self.h = None
+
+
+class Result:
+    def __init__(self, h: ctypes.c_void_p, program: Program):
+        self.h = h
+        self.program = program
+
+    @property
+    def rows(self) -> int:
+        n = ctypes.c_uint64()
+        check(lib().virg_gpu_result_rows(self.h, ctypes.byref(n)), "result rows")
+        return n.value
+
+    def column_ptr(self, c: int) -> int:
+        return lib().virg_gpu_result_column(self.h, c)
+
+    def download(self, first: int = 0, count: Optional[int] = None) -> List[np.ndarray]:
+        n = self.rows
+        count = n - first if count is None else count
+        info = self.program.info
+        outs = [np.empty(max(count, 1), dtype=NP_OF[info.out_type[j]]) for j in range(info.nout)]
+        ptrs = (ctypes.c_void_p * max(1, info.nout))(*[o.ctypes.data for o in outs])
+        check(lib().virg_gpu_result_download(self.h, ptrs, first, count), "result download")
+        return [o[:count] for o in outs]
+
+    def close(self) -> None:
+        if self.h:
+            lib().virg_gpu_result_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,120 @@
+"""ctypes bindings of ``libvirginian_b200.so`` (declared in include/virginian_b200.h).
+
+The library is loaded with RTLD_GLOBAL so a Virginian host library loaded
+afterwards binds its ``virg_vm_gpu`` call to it, as the reference's build links
+its GPU VM object into the same archive (src/Makefile:52).  There is no CPU
+fallback: importing fails if the CUDA library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvirginian_b200.so")
+
+VIRG_OPS = 32
+VIRG_MAX_COLUMNS = 16
+
+
+class VirgVar(ctypes.Union):
+    """virg_var, src/virginian.h:309-317."""
+    _fields_ = [("i", ctypes.c_int), ("f", ctypes.c_float), ("li", ctypes.c_longlong),
+                ("d", ctypes.c_double), ("c", ctypes.c_char), ("s", ctypes.c_void_p)]
+
+
+class VirgOp(ctypes.Structure):
+    """virg_op, src/virginian.h:327-333."""
+    _fields_ = [("op", ctypes.c_int), ("p1", ctypes.c_int), ("p2", ctypes.c_int),
+                ("p3", ctypes.c_int), ("p4", VirgVar)]
+
+
+class Schema(ctypes.Structure):
+    _fields_ = [("key_type", ctypes.c_int), ("ncols", ctypes.c_uint),
+                ("col_type", ctypes.c_int * VIRG_MAX_COLUMNS)]
+
+
+class Segment(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_uint32), ("key", ctypes.c_void_p),
+                ("col", ctypes.c_void_p * VIRG_MAX_COLUMNS)]
+
+
+class ProgramInfo(ctypes.Structure):
+    _fields_ = [("nload", ctypes.c_uint), ("load_column", ctypes.c_int * (VIRG_MAX_COLUMNS + 1)),
+                ("load_bytes_per_row", ctypes.c_uint), ("nout", ctypes.c_uint),
+                ("out_type", ctypes.c_int * VIRG_MAX_COLUMNS),
+                ("out_stride", ctypes.c_uint * VIRG_MAX_COLUMNS),
+                ("out_bytes_per_row", ctypes.c_uint), ("nuops", ctypes.c_uint)]
+
+
+def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
+    vp, u, i, u64 = ctypes.c_void_p, ctypes.c_uint, ctypes.c_int, ctypes.c_uint64
+    P = ctypes.POINTER
+    sig = {
+        "virg_gpu_last_error": (ctypes.c_char_p, []),
+        "virg_gpu_getsizes": (P(ctypes.c_size_t), []),
+        "virg_vm_gpu": (i, [vp, vp, vp, vp, u]),
+        "virg_gpu_engine_create": (i, [i, P(vp)]),
+        "virg_gpu_engine_destroy": (None, [vp]),
+        "virg_gpu_engine_stream": (vp, [vp]),
+        "virg_gpu_engine_check": (i, [vp, P(u)]),
+        "virg_gpu_engine_set_shape": (i, [vp, u, u, u, u]),
+        "virg_gpu_engine_launches": (ctypes.c_ulonglong, [vp]),
+        "virg_gpu_engine_timing": (i, [vp, u]),
+        "virg_gpu_engine_kernel_times": (i, [vp, P(ctypes.c_float), u, P(u)]),
+        "virg_gpu_engine_last_launch": (i, [vp, P(u), P(u), P(u)]),
+        "virg_gpu_program_create": (i, [P(VirgOp), u, u, P(Schema), P(vp)]),
+        "virg_gpu_program_info_get": (i, [vp, P(ProgramInfo)]),
+        "virg_gpu_program_flags": (i, [vp]),
+        "virg_gpu_program_destroy": (None, [vp]),
+        "virg_gpu_table_create": (i, [vp, P(Schema), P(vp)]),
+        "virg_gpu_table_append": (i, [vp, P(Segment), u]),
+        "virg_gpu_table_rows": (u64, [vp]),
+        "virg_gpu_table_bytes": (u64, [vp]),
+        "virg_gpu_table_destroy": (None, [vp]),
+        "virg_gpu_query": (i, [vp, vp, vp, P(vp)]),
+        "virg_gpu_result_rows": (i, [vp, P(u64)]),
+        "virg_gpu_result_column": (vp, [vp, u]),
+        "virg_gpu_result_download": (i, [vp, P(vp), u64, u64]),
+        "virg_gpu_result_destroy": (None, [vp]),
+        "virg_gpu_query_host": (i, [vp, vp, P(Segment), u, P(vp), u64, P(u64)]),
+        "virg_gpu_catalog_create": (i, [P(vp)]),
+        "virg_gpu_catalog_add_table": (i, [vp, ctypes.c_char_p, i, u, P(ctypes.c_char_p),
+                                           P(ctypes.c_int), P(u)]),
+        "virg_gpu_catalog_destroy": (None, [vp]),
+        "virg_gpu_sql_compile": (i, [vp, ctypes.c_char_p, P(VirgOp), P(u), P(u), ctypes.c_char_p,
+                                     P(u)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m virginian_b200.build` "
+                "(the VM has no CPU fallback)")
+        _lib = _bind(ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL))
+    return _lib
+
+
+def last_error() -> str:
+    e = lib().virg_gpu_last_error()
+    return e.decode() if e else ""
+
+
+class VirgError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str) -> None:
+    if not rc:
+        raise VirgError(f"{what}: {last_error()}")

@@ -1,0 +1,780 @@
+/*
+ * Host runtime of the B200 query VM: engines, HBM-resident tables, launch
+ * planning and results.
+ *
+ * Device layout.  The reference keeps tablets as 8 MB self-describing blocks
+ * (key column, key-pointer column, fixed columns; src/virginian.h:251-302)
+ * and copies a whole tablet per kernel in its serial mode
+ * (src/vm/vm_gpu.cu:166-168).  Here every resident segment (one tablet's
+ * rows) keeps each column in its own 256-byte-aligned device array padded to
+ * a multiple of 64 rows plus 16, so a tile of any column is one aligned bulk
+ * copy and the 8-byte key-pointer column never crosses the bus.
+ *
+ * Launch planning.  One launch runs any number of queries: their tiles are
+ * numbered query by query, CTAs claim tiles in order, and each query's tiles
+ * chain their look-back through the engine's status words, which carry a
+ * per-launch epoch so the array never needs clearing between launches.
+ */
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "vgpu_engine.h"
+#include "vgpu_util.h"
+#include "engine_internal.h"
+
+namespace vgpu {
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+static int type_bytes(int t)
+{
+	switch (t) {
+	case VT_INT: case VT_FLOAT: return 4;
+	case VT_INT64: case VT_DOUBLE: return 8;
+	case VT_CHAR: return 1;
+	default: return 0;
+	}
+}
+
+#define CUDA_OK(call, what)                                                        \
+	do {                                                                           \
+		cudaError_t e_ = (call);                                                   \
+		if (e_ != cudaSuccess)                                                     \
+			VGPU_FAIL("%s: %s", what, cudaGetErrorString(e_));                      \
+	} while (0)
+
+/* smem bytes a program needs per stage and for its register vectors */
+static void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
+	uint32_t *vec_off, uint32_t *vec_bytes)
+{
+	uint32_t off = 0;
+	for (unsigned i = 0; i < P.nload; i++) {
+		if (load_off)
+			load_off[i] = off;
+		off += (uint32_t)align_up((size_t)tile * P.load_stride[i], 128);
+	}
+	*stage_bytes = off;
+	off = 0;
+	for (unsigned i = 0; i < P.nvec; i++) {
+		if (vec_off)
+			vec_off[i] = off;
+		off += (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
+	}
+	*vec_bytes = off;
+}
+
+static size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes)
+{
+	return kSmemHeader + (size_t)s.stages * stage_bytes + vec_bytes;
+}
+
+int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, Shape *out,
+	size_t *smem_out, uint32_t *stage_out, uint32_t *vec_out)
+{
+	static const unsigned cand[][2] = {{256, 4}, {256, 8}, {128, 8}, {128, 4}, {256, 2}, {512, 2}};
+	const size_t limit = (size_t)e->smem_optin;
+	for (auto &c : cand) {
+		Shape s;
+		s.threads = e->pref.threads ? e->pref.threads : c[0];
+		s.rows_per_thread = e->pref.rows_per_thread ? e->pref.rows_per_thread : c[1];
+		if (!shape_supported(s))
+			VGPU_FAIL("unsupported launch shape %u threads x %u rows", s.threads, s.rows_per_thread);
+		uint32_t stage = 0, vec = 0;
+		for (const Program *P : progs) {
+			uint32_t sb, vb;
+			program_layout(*P, s.tile(), nullptr, &sb, nullptr, &vb);
+			stage = std::max(stage, sb);
+			vec = std::max(vec, vb);
+		}
+		stage = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
+		unsigned st_list[] = {e->pref.stages ? e->pref.stages : 3u, 2u};
+		for (unsigned st : st_list) {
+			s.stages = std::min(st, kMaxStages);
+			size_t smem = smem_for(s, stage, vec);
+			if (smem <= limit) {
+				s.ctas_per_sm = e->pref.ctas_per_sm;
+				*out = s;
+				*smem_out = smem;
+				*stage_out = stage;
+				*vec_out = vec;
+				return 1;
+			}
+		}
+		if (e->pref.threads || e->pref.rows_per_thread)
+			break;
+	}
+	VGPU_FAIL("program needs more shared memory than the device offers");
+}
+
+static int ensure_status(virg_gpu_engine *e, size_t n)
+{
+	if (n <= e->status_cap)
+		return 1;
+	if (e->status)
+		cudaFreeAsync(e->status, e->stream);
+	size_t cap = std::max<size_t>(n, 1 << 16);
+	CUDA_OK(cudaMallocAsync((void **)&e->status, cap * sizeof(uint64_t), e->stream), "status alloc");
+	CUDA_OK(cudaMemsetAsync(e->status, 0, cap * sizeof(uint64_t), e->stream), "status clear");
+	e->status_cap = cap;
+	return 1;
+}
+
+static int ensure_blob(virg_gpu_engine *e, size_t n)
+{
+	if (n <= e->blob_cap)
+		return 1;
+	if (e->blob)
+		cudaFreeAsync(e->blob, e->stream);
+	size_t cap = std::max<size_t>(align_up(n, 4096), 1 << 16);
+	CUDA_OK(cudaMallocAsync(&e->blob, cap, e->stream), "descriptor alloc");
+	e->blob_cap = cap;
+	return 1;
+}
+
+int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing)
+{
+	VGPU_CHECK(!qs.empty(), "no queries");
+	std::vector<const Program *> progs;
+	for (const QueryLaunch &q : qs)
+		progs.push_back(q.prog);
+	Shape shape;
+	size_t smem;
+	uint32_t stage_bytes, vec_bytes;
+	if (!choose_shape(e, progs, &shape, &smem, &stage_bytes, &vec_bytes))
+		return 0;
+	const unsigned tile = shape.tile();
+
+	/* descriptor blob: QDesc[nq] | q_work_prefix[nq+1] | seg_tile_prefix... */
+	const size_t nq = qs.size();
+	size_t off_prefix = align_up(nq * sizeof(QDesc), 16);
+	size_t off_tiles = align_up(off_prefix + (nq + 1) * sizeof(uint64_t), 16);
+	size_t total_tiles_words = 0;
+	for (const QueryLaunch &q : qs)
+		total_tiles_words += q.nsegs + 1;
+	size_t blob_bytes = off_tiles + total_tiles_words * sizeof(uint32_t);
+	e->host_blob.resize(blob_bytes);
+	unsigned char *hb = e->host_blob.data();
+	memset(hb, 0, off_tiles);
+	if (!ensure_blob(e, blob_bytes))
+		return 0;
+	unsigned char *db = static_cast<unsigned char *>(e->blob);
+
+	QDesc *hq = reinterpret_cast<QDesc *>(hb);
+	uint64_t *hprefix = reinterpret_cast<uint64_t *>(hb + off_prefix);
+	uint32_t *htiles = reinterpret_cast<uint32_t *>(hb + off_tiles);
+	uint64_t work = 0;
+	size_t tw = 0;
+	for (size_t i = 0; i < nq; i++) {
+		const QueryLaunch &q = qs[i];
+		QDesc &d = hq[i];
+		d.prog = *q.prog;
+		uint32_t sb, vb;
+		program_layout(*q.prog, tile, d.load_off, &sb, d.vec_off, &vb);
+		d.stage_bytes = sb;
+		d.segs = q.d_segs;
+		d.nsegs = q.nsegs;
+		d.seg_tile_prefix = reinterpret_cast<const uint32_t *>(db + off_tiles + tw * sizeof(uint32_t));
+		uint32_t *pre = htiles + tw;
+		uint64_t t = 0;
+		for (uint32_t s = 0; s < q.nsegs; s++) {
+			pre[s] = (uint32_t)t;
+			t += (q.seg_rows[s] + tile - 1) / tile;
+		}
+		pre[q.nsegs] = (uint32_t)t;
+		tw += q.nsegs + 1;
+		d.work_first = work;
+		d.ntiles = t;
+		hprefix[i] = work;
+		work += t;
+		for (unsigned j = 0; j < q.prog->nout; j++)
+			d.out_ptr[j] = q.out[j];
+		d.capacity = q.capacity;
+		d.total_out = q.d_total;
+		d.block_counts = q.block_counts;
+	}
+	hprefix[nq] = work;
+	VGPU_CHECK(work < 0xFFFFFFF0ull, "too many tiles in one launch (%llu)", (unsigned long long)work);
+
+	e->launches_last = 0;
+	if (work == 0)
+		return 1;
+	if (!ensure_status(e, work))
+		return 0;
+	e->epoch = (e->epoch + 1) & kEpochMask;
+	if (e->epoch == 0) {
+		/* epoch wrapped: stale words could alias the new epoch */
+		CUDA_OK(cudaMemsetAsync(e->status, 0, e->status_cap * sizeof(uint64_t), e->stream), "status");
+		e->epoch = 1;
+	}
+	CUDA_OK(cudaMemcpyAsync(db, hb, blob_bytes, cudaMemcpyHostToDevice, e->stream), "descriptor copy");
+	CUDA_OK(cudaMemsetAsync(e->ctrl, 0, sizeof(unsigned), e->stream), "counter reset");
+
+	KParams kp;
+	kp.queries = reinterpret_cast<const QDesc *>(db);
+	kp.q_work_prefix = reinterpret_cast<const uint64_t *>(db + off_prefix);
+	kp.nq = (uint32_t)nq;
+	kp.total_work = (uint32_t)work;
+	kp.counter = e->ctrl;
+	kp.status = e->status;
+	kp.error = e->ctrl + 1;
+	kp.epoch = e->epoch;
+	kp.nstages = shape.stages;
+	kp.stage_bytes = stage_bytes;
+	kp.stage_area = kSmemHeader;
+	kp.vec_area = (uint32_t)(kSmemHeader + (size_t)shape.stages * stage_bytes);
+
+	int per_sm = (int)shape.ctas_per_sm;
+	if (per_sm == 0 && !occupancy(shape, smem, &per_sm))
+		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+	per_sm = std::max(per_sm, 1);
+	unsigned grid = (unsigned)std::min<uint64_t>(work, (uint64_t)per_sm * e->nsm);
+
+	if (timing && timing->start)
+		cudaEventRecord(timing->start, e->stream);
+	const size_t nring = e->ring_start.size();
+	if (nring)
+		cudaEventRecord(e->ring_start[e->ring_count % nring], e->stream);
+	if (!launch_vm(shape, kp, grid, smem, e->stream))
+		VGPU_FAIL("kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+	if (nring)
+		cudaEventRecord(e->ring_stop[e->ring_count++ % nring], e->stream);
+	if (timing && timing->stop)
+		cudaEventRecord(timing->stop, e->stream);
+	e->launches++;
+	e->launches_last = 1;
+	e->last_shape = shape;
+	e->last_grid = grid;
+	e->last_smem = smem;
+	return 1;
+}
+
+int read_device_error(virg_gpu_engine *e, unsigned *err)
+{
+	unsigned h = 0;
+	CUDA_OK(cudaMemcpyAsync(&h, e->ctrl + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream),
+		"error read");
+	CUDA_OK(cudaStreamSynchronize(e->stream), "stream sync");
+	if (h)
+		CUDA_OK(cudaMemsetAsync(e->ctrl + 1, 0, sizeof(unsigned), e->stream), "error clear");
+	*err = h;
+	return 1;
+}
+
+const char *device_error_text(unsigned code)
+{
+	switch (code) {
+	case DE_LOOKBACK_TIMEOUT: return "look-back wait timed out";
+	case DE_STAGE_TIMEOUT: return "column staging wait timed out";
+	case DE_OUTPUT_OVERFLOW: return "result buffer overflow";
+	case DE_BAD_WORK: return "bad work item";
+	default: return "unknown device error";
+	}
+}
+
+}  // namespace vgpu
+
+using namespace vgpu;
+
+/* ---- engine ------------------------------------------------------------ */
+
+extern "C" int virg_gpu_engine_create(int device, virg_gpu_engine **out)
+{
+	VGPU_CHECK(out != nullptr, "null argument");
+	*out = nullptr;
+	int ndev = 0;
+	CUDA_OK(cudaGetDeviceCount(&ndev), "no CUDA device");
+	VGPU_CHECK(device >= 0 && device < ndev, "device %d not present (%d devices)", device, ndev);
+	CUDA_OK(cudaSetDevice(device), "set device");
+	cudaDeviceProp prop;
+	CUDA_OK(cudaGetDeviceProperties(&prop, device), "device properties");
+	VGPU_CHECK(prop.major == 10, "device %d is sm_%d%d; this library is built for sm_100a", device,
+		prop.major, prop.minor);
+	virg_gpu_engine *e = new virg_gpu_engine();
+	e->device = device;
+	e->nsm = prop.multiProcessorCount;
+	e->smem_optin = (int)prop.sharedMemPerBlockOptin;
+	if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+		cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+		cudaMalloc((void **)&e->ctrl, 64) != cudaSuccess || cudaMemset(e->ctrl, 0, 64) != cudaSuccess) {
+		delete e;
+		VGPU_FAIL("engine setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+	}
+	/* keep freed stream-ordered blocks cached instead of returning them */
+	cudaMemPool_t pool;
+	if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+		uint64_t thr = UINT64_MAX;
+		cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+	}
+	*out = e;
+	return 1;
+}
+
+static void ring_free(virg_gpu_engine *e)
+{
+	for (cudaEvent_t ev : e->ring_start)
+		cudaEventDestroy(ev);
+	for (cudaEvent_t ev : e->ring_stop)
+		cudaEventDestroy(ev);
+	e->ring_start.clear();
+	e->ring_stop.clear();
+	e->ring_count = 0;
+}
+
+extern "C" int virg_gpu_engine_timing(virg_gpu_engine *e, unsigned slots)
+{
+	VGPU_CHECK(e != nullptr, "null engine");
+	std::lock_guard<std::mutex> lk(e->mu);
+	CUDA_OK(cudaSetDevice(e->device), "set device");
+	CUDA_OK(cudaStreamSynchronize(e->stream), "stream sync");
+	ring_free(e);
+	for (unsigned i = 0; i < slots; i++) {
+		cudaEvent_t a, b;
+		CUDA_OK(cudaEventCreate(&a), "event create");
+		CUDA_OK(cudaEventCreate(&b), "event create");
+		e->ring_start.push_back(a);
+		e->ring_stop.push_back(b);
+	}
+	return 1;
+}
+
+extern "C" int virg_gpu_engine_kernel_times(virg_gpu_engine *e, float *ms, unsigned n, unsigned *got)
+{
+	VGPU_CHECK(e != nullptr && ms != nullptr && got != nullptr, "null argument");
+	std::lock_guard<std::mutex> lk(e->mu);
+	const size_t nring = e->ring_start.size();
+	unsigned have = (unsigned)std::min<unsigned long long>(e->ring_count, nring);
+	have = std::min(have, n);
+	*got = 0;
+	if (have == 0)
+		return 1;
+	CUDA_OK(cudaEventSynchronize(e->ring_stop[(e->ring_count - 1) % nring]), "event sync");
+	for (unsigned i = 0; i < have; i++) {
+		const unsigned long long k = e->ring_count - have + i;
+		CUDA_OK(cudaEventElapsedTime(&ms[i], e->ring_start[k % nring], e->ring_stop[k % nring]),
+			"event elapsed");
+	}
+	*got = have;
+	return 1;
+}
+
+extern "C" void virg_gpu_engine_destroy(virg_gpu_engine *e)
+{
+	if (!e)
+		return;
+	cudaSetDevice(e->device);
+	cudaStreamSynchronize(e->stream);
+	ring_free(e);
+	if (e->status)
+		cudaFree(e->status);
+	if (e->blob)
+		cudaFree(e->blob);
+	for (auto &kv : e->scratch)
+		if (kv.second.ptr)
+			cudaFree(kv.second.ptr);
+	cudaFree(e->ctrl);
+	cudaStreamDestroy(e->stream);
+	cudaStreamDestroy(e->copy_stream);
+	delete e;
+}
+
+extern "C" void *virg_gpu_engine_stream(virg_gpu_engine *e) { return e ? (void *)e->stream : nullptr; }
+
+extern "C" int virg_gpu_engine_check(virg_gpu_engine *e, unsigned *device_error)
+{
+	VGPU_CHECK(e != nullptr, "null engine");
+	unsigned err = 0;
+	if (!read_device_error(e, &err))
+		return 0;
+	if (device_error)
+		*device_error = err;
+	return 1;
+}
+
+extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
+	unsigned rows_per_thread, unsigned stages, unsigned ctas_per_sm)
+{
+	VGPU_CHECK(e != nullptr, "null engine");
+	if (threads || rows_per_thread) {
+		Shape s;
+		s.threads = threads ? threads : 256;
+		s.rows_per_thread = rows_per_thread ? rows_per_thread : 4;
+		VGPU_CHECK(shape_supported(s), "unsupported shape %u x %u", s.threads, s.rows_per_thread);
+	}
+	VGPU_CHECK(stages <= kMaxStages, "at most %u stages", kMaxStages);
+	e->pref.threads = threads;
+	e->pref.rows_per_thread = rows_per_thread;
+	e->pref.stages = stages;
+	e->pref.ctas_per_sm = ctas_per_sm;
+	return 1;
+}
+
+extern "C" unsigned long long virg_gpu_engine_launches(virg_gpu_engine *e)
+{
+	return e ? e->launches : 0;
+}
+
+extern "C" int virg_gpu_engine_last_launch(virg_gpu_engine *e, unsigned *shape4, unsigned *grid,
+	unsigned *smem)
+{
+	VGPU_CHECK(e != nullptr, "null engine");
+	if (shape4) {
+		shape4[0] = e->last_shape.threads;
+		shape4[1] = e->last_shape.rows_per_thread;
+		shape4[2] = e->last_shape.stages;
+		shape4[3] = e->last_shape.ctas_per_sm;
+	}
+	if (grid)
+		*grid = e->last_grid;
+	if (smem)
+		*smem = (unsigned)e->last_smem;
+	return 1;
+}
+
+/* ---- resident tables --------------------------------------------------- */
+
+extern "C" int virg_gpu_table_create(virg_gpu_engine *e, const virg_gpu_schema *schema,
+	virg_gpu_table **out)
+{
+	VGPU_CHECK(e != nullptr && schema != nullptr && out != nullptr, "null argument");
+	VGPU_CHECK(schema->ncols <= (unsigned)kMaxCols, "too many columns");
+	for (unsigned c = 0; c < schema->ncols; c++)
+		VGPU_CHECK(type_bytes(schema->col_type[c]) > 0, "column %u: unsupported type %d", c,
+			schema->col_type[c]);
+	virg_gpu_table *t = new virg_gpu_table();
+	t->e = e;
+	t->schema = *schema;
+	*out = t;
+	return 1;
+}
+
+namespace vgpu {
+
+/* rows of device padding per segment column: bulk copies read whole 16-byte
+ * chunks, up to 15 bytes past the last row */
+uint32_t padded_rows(uint32_t rows) { return (uint32_t)align_up(rows, 64) + 16; }
+
+int table_add_segments(virg_gpu_table *t, const virg_gpu_segment *segs, unsigned n,
+	const bool *want_col, bool want_key, cudaStream_t stream)
+{
+	for (unsigned i = 0; i < n; i++) {
+		const virg_gpu_segment &g = segs[i];
+		SegDesc d;
+		memset(&d, 0, sizeof(d));
+		d.rows = g.rows;
+		d.block_base = t->blocks;
+		size_t bytes = 0;
+		const uint32_t pr = padded_rows(g.rows);
+		for (unsigned c = 0; c < t->schema.ncols; c++)
+			if (!want_col || want_col[c])
+				bytes += align_up((size_t)pr * type_bytes(t->schema.col_type[c]), 256);
+		bool key = (want_key || !want_col) && g.key != nullptr;
+		if (key)
+			bytes += align_up((size_t)pr * type_bytes(t->schema.key_type), 256);
+		void *mem = nullptr;
+		if (bytes) {
+			if (t->transient)
+				CUDA_OK(cudaMallocAsync(&mem, bytes, stream), "segment alloc");
+			else
+				CUDA_OK(cudaMalloc(&mem, bytes), "segment alloc");
+			t->allocs.push_back(mem);
+		}
+		unsigned char *p = static_cast<unsigned char *>(mem);
+		for (unsigned c = 0; c < t->schema.ncols; c++) {
+			if (want_col && !want_col[c])
+				continue;
+			const size_t sz = type_bytes(t->schema.col_type[c]);
+			VGPU_CHECK(g.rows == 0 || g.col[c] != nullptr, "segment %u: column %u missing", i, c);
+			if (g.rows)
+				CUDA_OK(cudaMemcpyAsync(p, g.col[c], (size_t)g.rows * sz, cudaMemcpyDefault, stream),
+					"segment copy");
+			d.col[c] = p;
+			p += align_up((size_t)pr * sz, 256);
+		}
+		if (key) {
+			const size_t sz = type_bytes(t->schema.key_type);
+			if (g.rows)
+				CUDA_OK(cudaMemcpyAsync(p, g.key, (size_t)g.rows * sz, cudaMemcpyDefault, stream),
+					"segment key copy");
+			d.col[kKeySlot] = p;
+		} else if (g.rows) {
+			t->segs_without_key++;
+		}
+		t->segs.push_back(d);
+		t->rows += g.rows;
+		t->bytes += bytes;
+		t->blocks += (g.rows + 63) / 64;
+	}
+	t->dirty = true;
+	return 1;
+}
+
+int table_sync_desc(virg_gpu_table *t)
+{
+	if (!t->dirty)
+		return 1;
+	virg_gpu_engine *e = t->e;
+	if (t->d_segs)
+		cudaFreeAsync(t->d_segs, e->stream);
+	t->d_segs = nullptr;
+	if (!t->segs.empty()) {
+		CUDA_OK(cudaMallocAsync((void **)&t->d_segs, t->segs.size() * sizeof(SegDesc), e->stream),
+			"segment table alloc");
+		CUDA_OK(cudaMemcpyAsync(t->d_segs, t->segs.data(), t->segs.size() * sizeof(SegDesc),
+			cudaMemcpyHostToDevice, e->stream), "segment table copy");
+		CUDA_OK(cudaStreamSynchronize(e->stream), "segment table sync");
+	}
+	t->seg_rows.resize(t->segs.size());
+	for (size_t i = 0; i < t->segs.size(); i++)
+		t->seg_rows[i] = t->segs[i].rows;
+	t->dirty = false;
+	return 1;
+}
+
+}  // namespace vgpu
+
+extern "C" int virg_gpu_table_append(virg_gpu_table *t, const virg_gpu_segment *segs, unsigned nsegs)
+{
+	VGPU_CHECK(t != nullptr && (segs != nullptr || nsegs == 0), "null argument");
+	CUDA_OK(cudaSetDevice(t->e->device), "set device");
+	if (!table_add_segments(t, segs, nsegs, nullptr, true, t->e->stream))
+		return 0;
+	CUDA_OK(cudaStreamSynchronize(t->e->stream), "table copy");
+	return table_sync_desc(t);
+}
+
+extern "C" uint64_t virg_gpu_table_rows(const virg_gpu_table *t) { return t ? t->rows : 0; }
+extern "C" uint64_t virg_gpu_table_bytes(const virg_gpu_table *t) { return t ? t->bytes : 0; }
+
+extern "C" void virg_gpu_table_destroy(virg_gpu_table *t)
+{
+	if (!t)
+		return;
+	cudaSetDevice(t->e->device);
+	cudaStreamSynchronize(t->e->stream);
+	for (void *p : t->allocs)
+		cudaFree(p);
+	if (t->d_segs)
+		cudaFree(t->d_segs);
+	delete t;
+}
+
+/* ---- results ----------------------------------------------------------- */
+
+namespace vgpu {
+
+int result_alloc(virg_gpu_engine *e, const Program &P, uint64_t capacity, bool block_counts,
+	uint64_t nblocks, virg_gpu_result **out)
+{
+	virg_gpu_result *r = new virg_gpu_result();
+	r->e = e;
+	r->nout = P.nout;
+	r->capacity = capacity;
+	size_t bytes = 256;  /* total counter */
+	for (unsigned j = 0; j < P.nout; j++) {
+		r->stride[j] = P.out_stride[j];
+		r->type[j] = P.out_type[j];
+		bytes += align_up(std::max<uint64_t>(capacity, 1) * P.out_stride[j], 256);
+	}
+	if (block_counts)
+		bytes += align_up(std::max<uint64_t>(nblocks, 1), 256);
+	if (cudaMallocAsync(&r->mem, bytes, e->stream) != cudaSuccess) {
+		delete r;
+		VGPU_FAIL("result alloc of %zu bytes failed: %s", bytes, cudaGetErrorString(cudaGetLastError()));
+	}
+	unsigned char *p = static_cast<unsigned char *>(r->mem);
+	r->d_total = reinterpret_cast<unsigned long long *>(p);
+	p += 256;
+	for (unsigned j = 0; j < P.nout; j++) {
+		r->out[j] = p;
+		p += align_up(std::max<uint64_t>(capacity, 1) * P.out_stride[j], 256);
+	}
+	r->block_counts = block_counts ? p : nullptr;
+	r->nblocks = nblocks;
+	*out = r;
+	return 1;
+}
+
+}  // namespace vgpu
+
+extern "C" int virg_gpu_query(virg_gpu_engine *e, const virg_gpu_program *p, const virg_gpu_table *t,
+	virg_gpu_result **out)
+{
+	VGPU_CHECK(e != nullptr && p != nullptr && t != nullptr && out != nullptr, "null argument");
+	VGPU_CHECK(t->e == e, "table belongs to another engine");
+	*out = nullptr;
+	CUDA_OK(cudaSetDevice(e->device), "set device");
+	virg_gpu_table *tm = const_cast<virg_gpu_table *>(t);
+	if (!table_sync_desc(tm))
+		return 0;
+	const Program &P = p->prog;
+	for (unsigned i = 0; i < P.nload; i++) {
+		if (P.load_src[i] == kKeySlot)
+			VGPU_CHECK(t->segs_without_key == 0 && type_bytes(t->schema.key_type) == P.load_stride[i],
+				"program reads the key column, which the table does not hold with that type");
+		else
+			VGPU_CHECK(P.load_src[i] < t->schema.ncols &&
+				t->schema.col_type[P.load_src[i]] == (int)P.load_type[i],
+				"program column %u does not match the table schema", P.load_src[i]);
+	}
+	std::lock_guard<std::mutex> lk(e->mu);
+	virg_gpu_result *r;
+	if (!result_alloc(e, P, t->rows, false, 0, &r))
+		return 0;
+	QueryLaunch q;
+	q.prog = &P;
+	q.d_segs = t->d_segs;
+	q.nsegs = (uint32_t)t->segs.size();
+	q.seg_rows = t->seg_rows.data();
+	for (unsigned j = 0; j < P.nout; j++)
+		q.out[j] = r->out[j];
+	q.capacity = t->rows;
+	q.d_total = r->d_total;
+	q.block_counts = nullptr;
+	std::vector<QueryLaunch> qs(1, q);
+	LaunchTiming lt = {e->ev_start, e->ev_stop};
+	if (!run_queries(e, qs, e->timing_enabled ? &lt : nullptr)) {
+		virg_gpu_result_destroy(r);
+		return 0;
+	}
+	r->ntiles_zero = (t->rows == 0);
+	*out = r;
+	return 1;
+}
+
+extern "C" int virg_gpu_result_rows(virg_gpu_result *r, uint64_t *rows)
+{
+	VGPU_CHECK(r != nullptr && rows != nullptr, "null argument");
+	if (!r->have_rows) {
+		virg_gpu_engine *e = r->e;
+		unsigned long long h = 0;
+		if (!r->ntiles_zero)
+			CUDA_OK(cudaMemcpyAsync(&h, r->d_total, sizeof(h), cudaMemcpyDeviceToHost, e->stream),
+				"result count read");
+		unsigned err = 0;
+		if (!read_device_error(e, &err))
+			return 0;
+		VGPU_CHECK(err == 0, "query failed on the device: %s", device_error_text(err));
+		r->rows = h;
+		r->have_rows = true;
+	}
+	*rows = r->rows;
+	return 1;
+}
+
+extern "C" const void *virg_gpu_result_column(const virg_gpu_result *r, unsigned c)
+{
+	return (r && c < r->nout) ? r->out[c] : nullptr;
+}
+
+extern "C" int virg_gpu_result_download(virg_gpu_result *r, void *const *host_cols, uint64_t first,
+	uint64_t count)
+{
+	uint64_t rows;
+	if (!virg_gpu_result_rows(r, &rows))
+		return 0;
+	VGPU_CHECK(first + count <= rows, "rows %llu..%llu past the result (%llu rows)",
+		(unsigned long long)first, (unsigned long long)(first + count), (unsigned long long)rows);
+	virg_gpu_engine *e = r->e;
+	for (unsigned j = 0; j < r->nout; j++)
+		if (count)
+			CUDA_OK(cudaMemcpyAsync(host_cols[j], static_cast<unsigned char *>(r->out[j]) + first * r->stride[j],
+				count * r->stride[j], cudaMemcpyDeviceToHost, e->stream), "result download");
+	CUDA_OK(cudaStreamSynchronize(e->stream), "result download sync");
+	return 1;
+}
+
+extern "C" void virg_gpu_result_destroy(virg_gpu_result *r)
+{
+	if (!r)
+		return;
+	if (r->mem)
+		cudaFreeAsync(r->mem, r->e->stream);
+	delete r;
+}
+
+/* ---- end to end from host buffers -------------------------------------- */
+
+extern "C" int virg_gpu_query_host(virg_gpu_engine *e, const virg_gpu_program *p,
+	const virg_gpu_segment *segs, unsigned nsegs, void *const *out_cols, uint64_t capacity,
+	uint64_t *out_rows)
+{
+	VGPU_CHECK(e != nullptr && p != nullptr && (segs != nullptr || nsegs == 0) && out_rows != nullptr,
+		"null argument");
+	CUDA_OK(cudaSetDevice(e->device), "set device");
+	const Program &P = p->prog;
+	/* stage only the columns the program reads */
+	virg_gpu_table tmp;
+	tmp.e = e;
+	tmp.schema = p->schema;
+	tmp.transient = true;
+	bool want[kMaxCols] = {false};
+	bool want_key = false;
+	for (unsigned i = 0; i < P.nload; i++) {
+		if (P.load_src[i] == kKeySlot)
+			want_key = true;
+		else
+			want[P.load_src[i]] = true;
+	}
+	for (unsigned s = 0; s < nsegs; s++)
+		if (want_key)
+			VGPU_CHECK(segs[s].key != nullptr || segs[s].rows == 0, "segment %u has no key column", s);
+	std::lock_guard<std::mutex> lk(e->mu);
+	int ok = table_add_segments(&tmp, segs, nsegs, want, want_key, e->stream) && table_sync_desc(&tmp);
+	virg_gpu_result *r = nullptr;
+	if (ok)
+		ok = result_alloc(e, P, tmp.rows, false, 0, &r);
+	if (ok) {
+		QueryLaunch q;
+		q.prog = &P;
+		q.d_segs = tmp.d_segs;
+		q.nsegs = (uint32_t)tmp.segs.size();
+		q.seg_rows = tmp.seg_rows.data();
+		for (unsigned j = 0; j < P.nout; j++)
+			q.out[j] = r->out[j];
+		q.capacity = tmp.rows;
+		q.d_total = r->d_total;
+		q.block_counts = nullptr;
+		std::vector<QueryLaunch> qs(1, q);
+		ok = run_queries(e, qs, nullptr);
+		r->ntiles_zero = (tmp.rows == 0);
+	}
+	uint64_t rows = 0;
+	if (ok)
+		ok = virg_gpu_result_rows(r, &rows);
+	if (ok) {
+		*out_rows = rows;
+		uint64_t n = std::min(rows, capacity);
+		for (unsigned j = 0; j < P.nout && n; j++) {
+			cudaError_t ce = cudaMemcpyAsync(out_cols[j], r->out[j], n * r->stride[j],
+				cudaMemcpyDeviceToHost, e->stream);
+			if (ce != cudaSuccess) {
+				set_error("result copy: %s", cudaGetErrorString(ce));
+				ok = 0;
+			}
+		}
+		if (ok && cudaStreamSynchronize(e->stream) != cudaSuccess) {
+			set_error("result copy sync failed");
+			ok = 0;
+		}
+		if (ok && rows > capacity) {
+			set_error("result has %llu rows, the buffers hold %llu", (unsigned long long)rows,
+				(unsigned long long)capacity);
+			ok = 0;
+		}
+	}
+	if (r)
+		virg_gpu_result_destroy(r);
+	for (void *m : tmp.allocs)
+		cudaFreeAsync(m, e->stream);
+	tmp.allocs.clear();
+	if (tmp.d_segs)
+		cudaFreeAsync(tmp.d_segs, e->stream);
+	tmp.d_segs = nullptr;
+	return ok;
+}

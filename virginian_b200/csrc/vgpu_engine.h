@@ -1,0 +1,80 @@
+/* Engine internals shared by the host-side translation units. */
+#ifndef VGPU_ENGINE_H
+#define VGPU_ENGINE_H
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include "../../include/virginian_b200.h"
+#include "vgpu_program.h"
+
+namespace vgpu {
+
+struct ProgramExtra {
+	int maybe_undefined;  /* some row may read a register its path never set */
+	int result_k;         /* program index of the Result op */
+	int converge_k;       /* program index of the Converge op */
+};
+
+int decode_program(const virg_op *ops, unsigned num_ops, unsigned pc,
+	const virg_gpu_schema &schema, Program &P, ProgramExtra &X);
+
+/* launch shape: CTA width, rows per thread, staging depth, CTAs per SM */
+struct Shape {
+	unsigned threads;
+	unsigned rows_per_thread;
+	unsigned stages;
+	unsigned ctas_per_sm;
+	unsigned tile() const { return threads * rows_per_thread; }
+};
+
+/* fixed smem header of the kernel: QDesc copy, barriers, per-stage work
+ * info and the result-scan scratch */
+constexpr unsigned kSmemQDesc = 0;
+constexpr unsigned kMaxStages = 8;
+constexpr unsigned kSmemHeader = 4096;
+
+/* per-stage work item, decoded by the issuing thread */
+struct StageInfo {
+	uint32_t work;      /* global work index, >= total when empty */
+	uint32_t query;
+	uint32_t seg;
+	uint32_t row0;
+	uint32_t nrows;
+	uint32_t pad[3];
+};
+
+/* kernel arguments */
+struct KParams {
+	const QDesc *queries;
+	const uint64_t *q_work_prefix;  /* nq + 1 */
+	uint32_t nq;
+	uint32_t total_work;
+	unsigned *counter;              /* work claim counter, zeroed per launch */
+	uint64_t *status;               /* look-back words, one per work item */
+	unsigned *error;                /* first device error of the launch */
+	uint32_t epoch;
+	uint32_t nstages;
+	uint32_t stage_bytes;           /* stride between stages */
+	uint32_t stage_area;            /* smem offset of stage 0 */
+	uint32_t vec_area;              /* smem offset of the register vectors */
+};
+
+/* host-side launcher implemented in vm_kernel.cu */
+int launch_vm(const Shape &shape, const KParams &kp, unsigned grid, size_t smem,
+	void *stream);
+/* largest dynamic shared memory and resident CTAs for a shape */
+int shape_supported(const Shape &shape);
+int occupancy(const Shape &shape, size_t smem, int *ctas_per_sm);
+
+}  // namespace vgpu
+
+struct virg_gpu_program {
+	vgpu::Program prog;
+	vgpu::ProgramExtra extra;
+	virg_gpu_schema schema;
+};
+
+#endif
