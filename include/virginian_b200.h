@@ -348,6 +348,45 @@ int virg_gpu_query_host(virg_gpu_engine *e, const virg_gpu_program *p,
 	const virg_gpu_segment *segs, unsigned nsegs, void *const *out_cols,
 	uint64_t capacity, uint64_t *out_rows);
 
+/* Streamed execution over host-resident segments (tablets larger than HBM
+ * residency allows): the columns the program reads are copied in chunks of
+ * segs_per_chunk segments (0 = 8) through a ring of device staging buffers on
+ * the engine's copy stream while the VM runs on earlier chunks; the ordered
+ * result stays in HBM.  Segments should be in pinned host memory for the
+ * copies to overlap.  stats (may be NULL) receives the wall time, the time
+ * the copy stream spent copying and the bytes copied. */
+typedef struct {
+	double seconds;
+	double copy_seconds;
+	uint64_t h2d_bytes;
+	unsigned chunks;
+} virg_gpu_stream_stats;
+int virg_gpu_query_streamed(virg_gpu_engine *e, const virg_gpu_program *p,
+	const virg_gpu_segment *segs, unsigned nsegs, unsigned segs_per_chunk,
+	virg_gpu_result **out, virg_gpu_stream_stats *stats);
+
+/* Batched persistent execution: every query added to a batch runs in one
+ * launch of the VM kernel (tiles of all queries in one ordered work list).
+ * A batch owns its descriptors and counters, so virg_gpu_batch_run with
+ * use_graph captures the launch in a CUDA graph once and replays it after.
+ * With autotune on, the first run times the candidate launch shapes on the
+ * batch and caches the fastest in the engine per program-shape key.  Adding
+ * a query after a run rebuilds the batch. */
+int virg_gpu_batch_create(virg_gpu_engine *e, virg_gpu_batch **out);
+int virg_gpu_batch_add(virg_gpu_batch *b, const virg_gpu_program *p, virg_gpu_table *t,
+	unsigned *slot);
+int virg_gpu_batch_set_autotune(virg_gpu_batch *b, int enable);
+int virg_gpu_batch_run(virg_gpu_batch *b, int use_graph);
+/* waits for the last run; fails if the device reported an error */
+int virg_gpu_batch_wait(virg_gpu_batch *b);
+int virg_gpu_batch_rows(virg_gpu_batch *b, unsigned slot, uint64_t *rows);
+const void *virg_gpu_batch_column(const virg_gpu_batch *b, unsigned slot, unsigned c);
+int virg_gpu_batch_download(virg_gpu_batch *b, unsigned slot, void *const *host_cols,
+	uint64_t first, uint64_t count);
+/* shape4 = {threads, rows per thread, stages, grid}; work = tiles */
+int virg_gpu_batch_shape(const virg_gpu_batch *b, unsigned *shape4, uint64_t *work);
+void virg_gpu_batch_destroy(virg_gpu_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,7 @@ NP_OF = {VIRG_INT: np.int32, VIRG_INT64: np.int64, VIRG_FLOAT: np.float32,
          VIRG_DOUBLE: np.float64, VIRG_CHAR: np.int8}
 TYPE_OF = {np.dtype(v): k for k, v in NP_OF.items()}
 
-__all__ = ["Engine", "Program", "Table", "Result", "VirgError", "make_schema", "ops_array",
+__all__ = ["Engine", "Program", "Table", "Result", "Batch", "VirgError", "make_schema", "ops_array",
            "VIRG_INT", "VIRG_INT64", "VIRG_FLOAT", "VIRG_DOUBLE", "VIRG_CHAR", "NP_OF"]
 
 
@@ -244,3 +244,68 @@ class Result:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many (program, table) queries run by one persistent launch."""
+
+    def __init__(self, engine: Engine, autotune: bool = False):
+        self.engine = engine
+        h = ctypes.c_void_p()
+        check(lib().virg_gpu_batch_create(engine.h, ctypes.byref(h)), "batch create")
+        self.h = h
+        self.programs: List[Program] = []
+        if autotune:
+            check(lib().virg_gpu_batch_set_autotune(self.h, 1), "batch autotune")
+
+    def add(self, program: Program, table: Table) -> int:
+        slot = ctypes.c_uint()
+        check(lib().virg_gpu_batch_add(self.h, program.h, table.h, ctypes.byref(slot)), "batch add")
+        self.programs.append(program)
+        return slot.value
+
+    def run(self, graph: bool = True) -> None:
+        check(lib().virg_gpu_batch_run(self.h, 1 if graph else 0), "batch run")
+
+    def wait(self) -> None:
+        check(lib().virg_gpu_batch_wait(self.h), "batch wait")
+
+    def rows(self, slot: int) -> int:
+        n = ctypes.c_uint64()
+        check(lib().virg_gpu_batch_rows(self.h, slot, ctypes.byref(n)), "batch rows")
+        return n.value
+
+    def download(self, slot: int) -> List[np.ndarray]:
+        n = self.rows(slot)
+        info = self.programs[slot].info
+        outs = [np.empty(max(n, 1), dtype=NP_OF[info.out_type[j]]) for j in range(info.nout)]
+        ptrs = (ctypes.c_void_p * max(1, info.nout))(*[o.ctypes.data for o in outs])
+        check(lib().virg_gpu_batch_download(self.h, slot, ptrs, 0, n), "batch download")
+        return [o[:n] for o in outs]
+
+    def shape(self) -> Dict[str, int]:
+        s = (ctypes.c_uint * 4)()
+        w = ctypes.c_uint64()
+        check(lib().virg_gpu_batch_shape(self.h, s, ctypes.byref(w)), "batch shape")
+        return {"threads": s[0], "rows_per_thread": s[1], "stages": s[2], "grid": s[3],
+                "tiles": w.value}
+
+    def close(self) -> None:
+        if self.h:
+            lib().virg_gpu_batch_destroy(self.h)
+            self.h = None
+
+
+def query_streamed(engine: Engine, program: Program, segments: Sequence[dict],
+                   segs_per_chunk: int = 8):
+    """Runs a program over host-resident segments, streaming the columns it
+    reads through a staging ring; returns (Result, stats dict)."""
+    from ._lib import StreamStats
+    segs, keep = _segments(segments, program.col_types)
+    r = ctypes.c_void_p()
+    st = StreamStats()
+    check(lib().virg_gpu_query_streamed(engine.h, program.h, segs, len(segments), segs_per_chunk,
+                                        ctypes.byref(r), ctypes.byref(st)), "query_streamed")
+    del keep
+    return Result(r, program), {"seconds": st.seconds, "copy_seconds": st.copy_seconds,
+                                "h2d_bytes": st.h2d_bytes, "chunks": st.chunks}

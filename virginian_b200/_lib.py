@@ -39,6 +39,11 @@ class Segment(ctypes.Structure):
                 ("col", ctypes.c_void_p * VIRG_MAX_COLUMNS)]
 
 
+class StreamStats(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("copy_seconds", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_uint64), ("chunks", ctypes.c_uint)]
+
+
 class ProgramInfo(ctypes.Structure):
     _fields_ = [("nload", ctypes.c_uint), ("load_column", ctypes.c_int * (VIRG_MAX_COLUMNS + 1)),
                 ("load_bytes_per_row", ctypes.c_uint), ("nout", ctypes.c_uint),
@@ -78,6 +83,17 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_result_download": (i, [vp, P(vp), u64, u64]),
         "virg_gpu_result_destroy": (None, [vp]),
         "virg_gpu_query_host": (i, [vp, vp, P(Segment), u, P(vp), u64, P(u64)]),
+        "virg_gpu_query_streamed": (i, [vp, vp, P(Segment), u, u, P(vp), P(StreamStats)]),
+        "virg_gpu_batch_create": (i, [vp, P(vp)]),
+        "virg_gpu_batch_add": (i, [vp, vp, vp, P(u)]),
+        "virg_gpu_batch_set_autotune": (i, [vp, i]),
+        "virg_gpu_batch_run": (i, [vp, i]),
+        "virg_gpu_batch_wait": (i, [vp]),
+        "virg_gpu_batch_rows": (i, [vp, u, P(u64)]),
+        "virg_gpu_batch_column": (vp, [vp, u, u]),
+        "virg_gpu_batch_download": (i, [vp, u, P(vp), u64, u64]),
+        "virg_gpu_batch_shape": (i, [vp, P(u), P(u64)]),
+        "virg_gpu_batch_destroy": (None, [vp]),
         "virg_gpu_catalog_create": (i, [P(vp)]),
         "virg_gpu_catalog_add_table": (i, [vp, ctypes.c_char_p, i, u, P(ctypes.c_char_p),
                                            P(ctypes.c_int), P(u)]),

@@ -137,34 +137,49 @@ static int ensure_blob(virg_gpu_engine *e, size_t n)
 	return 1;
 }
 
-int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing)
+size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles)
+{
+	const size_t nq = qs.size();
+	*off_prefix = align_up(nq * sizeof(QDesc), 16);
+	*off_tiles = align_up(*off_prefix + (nq + 1) * sizeof(uint64_t), 16);
+	size_t words = 0;
+	for (const QueryLaunch &q : qs)
+		words += q.nsegs + 1;
+	return *off_tiles + words * sizeof(uint32_t);
+}
+
+/* descriptor blob: QDesc[nq] | q_work_prefix[nq+1] | seg_tile_prefix...,
+ * built in host memory with pointers into the device copy at `db` */
+int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Shape *forced,
+	unsigned char *db, Plan &plan)
 {
 	VGPU_CHECK(!qs.empty(), "no queries");
 	std::vector<const Program *> progs;
 	for (const QueryLaunch &q : qs)
 		progs.push_back(q.prog);
-	Shape shape;
-	size_t smem;
-	uint32_t stage_bytes, vec_bytes;
-	if (!choose_shape(e, progs, &shape, &smem, &stage_bytes, &vec_bytes))
+	if (forced) {
+		plan.shape = *forced;
+		uint32_t stage = 0, vec = 0;
+		for (const Program *P : progs) {
+			uint32_t sb, vb;
+			program_layout(*P, forced->tile(), nullptr, &sb, nullptr, &vb);
+			stage = std::max(stage, sb);
+			vec = std::max(vec, vb);
+		}
+		plan.stage_bytes = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
+		plan.vec_bytes = vec;
+		plan.smem = smem_for(plan.shape, plan.stage_bytes, plan.vec_bytes);
+		VGPU_CHECK(plan.smem <= (size_t)e->smem_optin, "shape does not fit shared memory");
+	} else if (!choose_shape(e, progs, &plan.shape, &plan.smem, &plan.stage_bytes, &plan.vec_bytes)) {
 		return 0;
-	const unsigned tile = shape.tile();
-
-	/* descriptor blob: QDesc[nq] | q_work_prefix[nq+1] | seg_tile_prefix... */
+	}
+	const unsigned tile = plan.shape.tile();
 	const size_t nq = qs.size();
-	size_t off_prefix = align_up(nq * sizeof(QDesc), 16);
-	size_t off_tiles = align_up(off_prefix + (nq + 1) * sizeof(uint64_t), 16);
-	size_t total_tiles_words = 0;
-	for (const QueryLaunch &q : qs)
-		total_tiles_words += q.nsegs + 1;
-	size_t blob_bytes = off_tiles + total_tiles_words * sizeof(uint32_t);
-	e->host_blob.resize(blob_bytes);
-	unsigned char *hb = e->host_blob.data();
-	memset(hb, 0, off_tiles);
-	if (!ensure_blob(e, blob_bytes))
-		return 0;
-	unsigned char *db = static_cast<unsigned char *>(e->blob);
-
+	size_t off_prefix, off_tiles;
+	const size_t blob_bytes = plan_blob_bytes(qs, &off_prefix, &off_tiles);
+	plan.blob.assign(blob_bytes, 0);
+	plan.off_prefix = off_prefix;
+	unsigned char *hb = plan.blob.data();
 	QDesc *hq = reinterpret_cast<QDesc *>(hb);
 	uint64_t *hprefix = reinterpret_cast<uint64_t *>(hb + off_prefix);
 	uint32_t *htiles = reinterpret_cast<uint32_t *>(hb + off_tiles);
@@ -197,43 +212,68 @@ int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTi
 		d.capacity = q.capacity;
 		d.total_out = q.d_total;
 		d.block_counts = q.block_counts;
+		d.base_in = q.base_in;
 	}
 	hprefix[nq] = work;
 	VGPU_CHECK(work < 0xFFFFFFF0ull, "too many tiles in one launch (%llu)", (unsigned long long)work);
+	plan.work = work;
+	plan.nq = (uint32_t)nq;
 
+	int per_sm = (int)plan.shape.ctas_per_sm;
+	if (per_sm == 0 && !occupancy(plan.shape, plan.smem, &per_sm))
+		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+	per_sm = std::max(per_sm, 1);
+	plan.grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(work, 1), (uint64_t)per_sm * e->nsm);
+	return 1;
+}
+
+KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter, uint64_t *status,
+	unsigned *error, uint32_t epoch)
+{
+	KParams kp;
+	kp.queries = reinterpret_cast<const QDesc *>(db);
+	kp.q_work_prefix = reinterpret_cast<const uint64_t *>(db + plan.off_prefix);
+	kp.nq = plan.nq;
+	kp.total_work = (uint32_t)plan.work;
+	kp.counter = counter;
+	kp.status = status;
+	kp.error = error;
+	kp.epoch = epoch;
+	kp.nstages = plan.shape.stages;
+	kp.stage_bytes = plan.stage_bytes;
+	kp.stage_area = kSmemHeader;
+	kp.vec_area = (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes);
+	return kp;
+}
+
+int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing)
+{
+	size_t off_prefix, off_tiles;
+	if (!ensure_blob(e, plan_blob_bytes(qs, &off_prefix, &off_tiles)))
+		return 0;
+	unsigned char *db = static_cast<unsigned char *>(e->blob);
+	Plan plan;
+	if (!plan_build(e, qs, nullptr, db, plan))
+		return 0;
 	e->launches_last = 0;
-	if (work == 0)
+	if (plan.work == 0)
 		return 1;
-	if (!ensure_status(e, work))
+	if (!ensure_status(e, plan.work))
 		return 0;
 	e->epoch = (e->epoch + 1) & kEpochMask;
-	if (e->epoch == 0) {
-		/* epoch wrapped: stale words could alias the new epoch */
+	if (e->epoch == 0 || e->epoch == kEpochMask) {
+		/* epoch wrapped: stale words could alias the new epoch; kEpochMask is
+		 * reserved for graph-captured batches */
 		CUDA_OK(cudaMemsetAsync(e->status, 0, e->status_cap * sizeof(uint64_t), e->stream), "status");
 		e->epoch = 1;
 	}
-	CUDA_OK(cudaMemcpyAsync(db, hb, blob_bytes, cudaMemcpyHostToDevice, e->stream), "descriptor copy");
+	CUDA_OK(cudaMemcpyAsync(db, plan.blob.data(), plan.blob.size(), cudaMemcpyHostToDevice, e->stream),
+		"descriptor copy");
 	CUDA_OK(cudaMemsetAsync(e->ctrl, 0, sizeof(unsigned), e->stream), "counter reset");
-
-	KParams kp;
-	kp.queries = reinterpret_cast<const QDesc *>(db);
-	kp.q_work_prefix = reinterpret_cast<const uint64_t *>(db + off_prefix);
-	kp.nq = (uint32_t)nq;
-	kp.total_work = (uint32_t)work;
-	kp.counter = e->ctrl;
-	kp.status = e->status;
-	kp.error = e->ctrl + 1;
-	kp.epoch = e->epoch;
-	kp.nstages = shape.stages;
-	kp.stage_bytes = stage_bytes;
-	kp.stage_area = kSmemHeader;
-	kp.vec_area = (uint32_t)(kSmemHeader + (size_t)shape.stages * stage_bytes);
-
-	int per_sm = (int)shape.ctas_per_sm;
-	if (per_sm == 0 && !occupancy(shape, smem, &per_sm))
-		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
-	per_sm = std::max(per_sm, 1);
-	unsigned grid = (unsigned)std::min<uint64_t>(work, (uint64_t)per_sm * e->nsm);
+	const KParams kp = plan_params(plan, db, e->ctrl, e->status, e->ctrl + 1, e->epoch);
+	const Shape shape = plan.shape;
+	const size_t smem = plan.smem;
+	const unsigned grid = plan.grid;
 
 	if (timing && timing->start)
 		cudaEventRecord(timing->start, e->stream);

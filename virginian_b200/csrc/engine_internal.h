@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -45,6 +46,8 @@ struct virg_gpu_engine {
 	/* ring of (start, stop) events recorded around each kernel launch */
 	std::vector<cudaEvent_t> ring_start, ring_stop;
 	unsigned long long ring_count = 0;
+	/* launch shapes found by batch autotuning, per program-shape key */
+	std::map<std::string, vgpu::Shape> tuned;
 	std::mutex mu;
 };
 
@@ -90,6 +93,7 @@ struct QueryLaunch {
 	uint64_t capacity = 0;
 	unsigned long long *d_total = nullptr;
 	uint8_t *block_counts = nullptr;
+	const unsigned long long *base_in = nullptr;
 };
 
 struct LaunchTiming {
@@ -97,6 +101,23 @@ struct LaunchTiming {
 	cudaEvent_t stop;
 };
 
+/* a launch of one or more queries, ready to issue */
+struct Plan {
+	Shape shape;
+	size_t smem = 0;
+	uint32_t stage_bytes = 0, vec_bytes = 0;
+	std::vector<unsigned char> blob;  /* host copy of the device descriptors */
+	size_t off_prefix = 0;
+	uint64_t work = 0;
+	uint32_t nq = 0;
+	unsigned grid = 0;
+};
+
+size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles);
+int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Shape *forced,
+	unsigned char *db, Plan &plan);
+KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter, uint64_t *status,
+	unsigned *error, uint32_t epoch);
 int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing);
 int read_device_error(virg_gpu_engine *e, unsigned *err);
 const char *device_error_text(unsigned code);

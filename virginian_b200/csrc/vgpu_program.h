@@ -110,6 +110,10 @@ struct alignas(16) QDesc {
 	uint64_t capacity;                /* rows each out column can hold */
 	unsigned long long *total_out;    /* written by the last tile */
 	uint8_t *block_counts;            /* optional: valid rows per 64-row block */
+	/* optional: result rows already written by earlier launches of the same
+	 * query; its first tile starts there */
+	const unsigned long long *base_in;
+	uint64_t pad1;
 };
 
 /* device error codes (written once per launch to the error word) */

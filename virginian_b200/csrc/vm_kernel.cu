@@ -457,7 +457,11 @@ __device__ __forceinline__ bool emit_result(const Ctx &c, const KParams &kp, con
 		uint64_t excl = 0;
 		bool ok = true;
 		if (g == first) {
-			st_release_u64(&kp.status[g], ep | (kFlagPrefix << kStatusFlagShift) | tile_total);
+			/* a query continued from an earlier launch starts at its row count */
+			if (Q.base_in != nullptr)
+				excl = *Q.base_in;
+			st_release_u64(&kp.status[g],
+				ep | (kFlagPrefix << kStatusFlagShift) | ((excl + tile_total) & kStatusValueMask));
 		} else {
 			st_release_u64(&kp.status[g], ep | (kFlagAggregate << kStatusFlagShift) | tile_total);
 			uint64_t j = g - 1;

@@ -43,6 +43,8 @@ def column(name: str, n: int, seed: int = 0, table: int = 0, start: int = 0) -> 
     if name == "id":
         return np.arange(start, start + n, dtype=np.int32)
     ci = names.index(name) + 1
+    if n == 0:
+        return _block(name, np.random.Generator(np.random.Philox(0)), 0)
     block = 1 << 20
     out = []
     b0, b1 = start // block, (start + n + block - 1) // block
