@@ -333,6 +333,12 @@ void virg_gpu_table_destroy(virg_gpu_table *t);
  * Asynchronous on the engine stream; virg_gpu_result_rows waits for it. */
 int virg_gpu_query(virg_gpu_engine *e, const virg_gpu_program *p,
 	const virg_gpu_table *t, virg_gpu_result **out);
+/* time the candidate launch shapes for this program over this table and
+ * cache the fastest in the engine (keyed by program shape and table size
+ * class); later queries with the same key use it.  shape4 (may be NULL)
+ * receives {threads, rows per thread, stages, 0}. */
+int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p,
+	const virg_gpu_table *t, unsigned *shape4);
 int virg_gpu_result_rows(virg_gpu_result *r, uint64_t *rows);
 /* device pointer of result column c (valid until the result is destroyed) */
 const void *virg_gpu_result_column(const virg_gpu_result *r, unsigned c);

@@ -309,3 +309,10 @@ def query_streamed(engine: Engine, program: Program, segments: Sequence[dict],
     del keep
     return Result(r, program), {"seconds": st.seconds, "copy_seconds": st.copy_seconds,
                                 "h2d_bytes": st.h2d_bytes, "chunks": st.chunks}
+
+
+def tune(engine: Engine, program: Program, table: Table) -> Dict[str, int]:
+    """Times the launch shapes for this query and caches the fastest."""
+    s = (ctypes.c_uint * 4)()
+    check(lib().virg_gpu_query_tune(engine.h, program.h, table.h, s), "query tune")
+    return {"threads": s[0], "rows_per_thread": s[1], "stages": s[2]}

@@ -78,6 +78,7 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_table_bytes": (u64, [vp]),
         "virg_gpu_table_destroy": (None, [vp]),
         "virg_gpu_query": (i, [vp, vp, vp, P(vp)]),
+        "virg_gpu_query_tune": (i, [vp, vp, vp, P(u)]),
         "virg_gpu_result_rows": (i, [vp, P(u64)]),
         "virg_gpu_result_column": (vp, [vp, u]),
         "virg_gpu_result_download": (i, [vp, P(vp), u64, u64]),

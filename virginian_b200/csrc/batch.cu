@@ -97,35 +97,6 @@ void batch_release(virg_gpu_batch *b)
 	b->ran = false;
 }
 
-/* the key the tuned shape is cached under: the largest per-row staging and
- * register-vector bytes and program length in the batch, and its size class */
-std::string shape_key(const virg_gpu_batch *b)
-{
-	unsigned ld = 0, vec = 0, nuops = 0, nout = 0;
-	for (auto &it : b->items) {
-		const Program &P = it.p->prog;
-		unsigned l = 0, v = 0;
-		for (unsigned i = 0; i < P.nload; i++)
-			l += P.load_stride[i];
-		for (unsigned i = 0; i < P.nvec; i++)
-			v += P.vec_stride[i];
-		ld = std::max(ld, l);
-		vec = std::max(vec, v);
-		nuops = std::max(nuops, P.nuops);
-		nout = std::max(nout, P.nout);
-	}
-	uint64_t rows = 0;
-	for (auto &it : b->items)
-		rows += it.t->rows;
-	unsigned size_class = 0;
-	while ((1ull << size_class) < rows && size_class < 63)
-		size_class++;
-	char buf[96];
-	snprintf(buf, sizeof(buf), "l%u-v%u-u%u-o%u-q%zu-r%u", ld, vec, nuops, nout, b->items.size(),
-		size_class);
-	return buf;
-}
-
 std::vector<QueryLaunch> launches_of(virg_gpu_batch *b)
 {
 	std::vector<QueryLaunch> qs;
@@ -218,12 +189,12 @@ float time_once(virg_gpu_batch *b)
 int autotune(virg_gpu_batch *b)
 {
 	virg_gpu_engine *e = b->e;
-	const std::string key = shape_key(b);
+	const std::string key = shape_key(launches_of(b));
 	auto hit = e->tuned.find(key);
 	if (hit != e->tuned.end())
 		return build_with(b, &hit->second);
-	static const unsigned cand[][2] = {{128, 4}, {128, 8}, {256, 2}, {256, 4}, {256, 8}, {512, 2},
-		{512, 4}};
+	static const unsigned cand[][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
+		{512, 8}};
 	float best = 1e30f;
 	Shape best_shape = {0, 0, 0, 0};
 	for (auto &c : cand)

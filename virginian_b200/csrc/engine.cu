@@ -50,10 +50,11 @@ static int type_bytes(int t)
 	} while (0)
 
 /* smem bytes a program needs per stage and for its register vectors */
-static void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
+void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
 	uint32_t *vec_off, uint32_t *vec_bytes)
 {
-	uint32_t off = 0;
+	/* a stage: query descriptor + tile info header, then the columns */
+	uint32_t off = kStageHdr;
 	for (unsigned i = 0; i < P.nload; i++) {
 		if (load_off)
 			load_off[i] = off;
@@ -69,16 +70,24 @@ static void program_layout(const Program &P, unsigned tile, uint32_t *load_off, 
 	*vec_bytes = off;
 }
 
-static size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes)
+/* header | stages x stage bytes | register vectors | selection lists */
+size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes)
 {
-	return kSmemHeader + (size_t)s.stages * stage_bytes + vec_bytes;
+	/* register vectors and selection lists (a tile row and a (group, rank)
+	 * tag per entry) are double-buffered: a tile's stores run while the next
+	 * tile is computed */
+	return kSmemHeader + (size_t)s.stages * stage_bytes + 2 * (size_t)vec_bytes +
+		2 * align_up((size_t)s.tile() * 2 * sizeof(uint16_t), 128);
 }
 
 int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, Shape *out,
 	size_t *smem_out, uint32_t *stage_out, uint32_t *vec_out)
 {
-	static const unsigned cand[][2] = {{256, 4}, {256, 8}, {128, 8}, {128, 4}, {256, 2}, {512, 2}};
+	/* first choice: a shape that keeps two CTAs resident per SM, so one CTA's
+	 * barriers and look-back waits overlap the other's work */
+	static const unsigned cand[][2] = {{256, 4}, {128, 8}, {256, 8}, {512, 4}};
 	const size_t limit = (size_t)e->smem_optin;
+	for (int pass = 0; pass < 2; pass++)
 	for (auto &c : cand) {
 		Shape s;
 		s.threads = e->pref.threads ? e->pref.threads : c[0];
@@ -93,11 +102,15 @@ int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, 
 			vec = std::max(vec, vb);
 		}
 		stage = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
-		unsigned st_list[] = {e->pref.stages ? e->pref.stages : 3u, 2u};
+		/* a requested stage count is kept, at one CTA per SM if need be */
+		const unsigned st_list[] = {e->pref.stages ? e->pref.stages : 3u, e->pref.stages ? 0u : 2u};
 		for (unsigned st : st_list) {
+			if (st == 0)
+				continue;
 			s.stages = std::min(st, kMaxStages);
 			size_t smem = smem_for(s, stage, vec);
-			if (smem <= limit) {
+			/* 1 KB of the SM's shared memory is reserved per resident CTA */
+			if (smem <= (pass == 0 ? limit / 2 - 1024 : limit)) {
 				s.ctas_per_sm = e->pref.ctas_per_sm;
 				*out = s;
 				*smem_out = smem;
@@ -135,6 +148,30 @@ static int ensure_blob(virg_gpu_engine *e, size_t n)
 	CUDA_OK(cudaMallocAsync(&e->blob, cap, e->stream), "descriptor alloc");
 	e->blob_cap = cap;
 	return 1;
+}
+
+/* operand descriptors of a query descriptor whose program, load_off and
+ * vec_off are set, for register vectors starting at vec_area */
+void fill_operands(QDesc &d, uint32_t vec_area)
+{
+	const Program &P = d.prog;
+	auto od = [&](uint8_t cls, uint8_t idx) -> uint32_t {
+		if (cls == OC_COL)
+			return OD_STAGE | (uint32_t)(kSmemHeader + d.load_off[idx]);
+		if (cls == OC_VEC)
+			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | (vec_area + d.vec_off[idx]);
+		/* scalars are read from the stage's copy of the descriptor */
+		return OD_SCALAR |
+			(uint32_t)(kSmemHeader + offsetof(QDesc, prog) + offsetof(Program, consts) + idx * 8u);
+	};
+	for (uint32_t k = 0; k < P.nuops; k++) {
+		const UOp &u = P.uops[k];
+		d.od_a[k] = od(u.a_cls, u.a_idx);
+		d.od_b[k] = od(u.b_cls, u.b_idx);
+		d.od_d[k] = od(OC_VEC, u.dst);
+	}
+	for (uint32_t j = 0; j < P.nout; j++)
+		d.od_out[j] = od(P.out_cls[j], P.out_idx[j]);
 }
 
 size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles)
@@ -213,6 +250,7 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		d.total_out = q.d_total;
 		d.block_counts = q.block_counts;
 		d.base_in = q.base_in;
+		fill_operands(d, (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes));
 	}
 	hprefix[nq] = work;
 	VGPU_CHECK(work < 0xFFFFFFF0ull, "too many tiles in one launch (%llu)", (unsigned long long)work);
@@ -243,7 +281,38 @@ KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter
 	kp.stage_bytes = plan.stage_bytes;
 	kp.stage_area = kSmemHeader;
 	kp.vec_area = (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes);
+	kp.vec_bytes = plan.vec_bytes;
+	kp.sel_area = kp.vec_area + 2 * plan.vec_bytes;
 	return kp;
+}
+
+/* the key a tuned launch shape is cached under: the largest per-row staging
+ * and register-vector bytes and program length of the launch's queries, the
+ * number of queries and the size class of the rows they scan */
+std::string shape_key(const std::vector<QueryLaunch> &qs)
+{
+	unsigned ld = 0, vec = 0, nuops = 0, nout = 0;
+	uint64_t rows = 0;
+	for (const QueryLaunch &q : qs) {
+		const Program &P = *q.prog;
+		unsigned l = 0, v = 0;
+		for (unsigned i = 0; i < P.nload; i++)
+			l += P.load_stride[i];
+		for (unsigned i = 0; i < P.nvec; i++)
+			v += P.vec_stride[i];
+		ld = std::max(ld, l);
+		vec = std::max(vec, v);
+		nuops = std::max(nuops, P.nuops);
+		nout = std::max(nout, P.nout);
+		for (uint32_t s = 0; s < q.nsegs; s++)
+			rows += q.seg_rows[s];
+	}
+	unsigned size_class = 0;
+	while ((1ull << size_class) < rows && size_class < 63)
+		size_class++;
+	char buf[96];
+	snprintf(buf, sizeof(buf), "l%u-v%u-u%u-o%u-q%zu-r%u", ld, vec, nuops, nout, qs.size(), size_class);
+	return buf;
 }
 
 int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing)
@@ -253,7 +322,13 @@ int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTi
 		return 0;
 	unsigned char *db = static_cast<unsigned char *>(e->blob);
 	Plan plan;
-	if (!plan_build(e, qs, nullptr, db, plan))
+	const Shape *forced = e->force.threads ? &e->force : nullptr;
+	if (!forced && !e->tuned.empty() && !e->pref.threads) {
+		auto hit = e->tuned.find(shape_key(qs));
+		if (hit != e->tuned.end())
+			forced = &hit->second;
+	}
+	if (!plan_build(e, qs, forced, db, plan))
 		return 0;
 	e->launches_last = 0;
 	if (plan.work == 0)
@@ -424,6 +499,63 @@ extern "C" void virg_gpu_engine_destroy(virg_gpu_engine *e)
 }
 
 extern "C" void *virg_gpu_engine_stream(virg_gpu_engine *e) { return e ? (void *)e->stream : nullptr; }
+
+extern "C" int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p,
+	const virg_gpu_table *t, unsigned *shape4)
+{
+	VGPU_CHECK(e != nullptr && p != nullptr && t != nullptr, "null argument");
+	static const unsigned cand[][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
+		{512, 8}};
+	cudaEvent_t a, z;
+	CUDA_OK(cudaEventCreate(&a), "event");
+	CUDA_OK(cudaEventCreate(&z), "event");
+	float best = 1e30f;
+	Shape best_shape = {0, 0, 0, 0};
+	std::string key;
+	for (auto &c : cand)
+		for (unsigned st = 2; st <= 4; st++) {
+			e->force = Shape{c[0], c[1], st, 0};
+			float t_best = 1e30f;
+			bool ran = true;
+			for (int rep = 0; rep < 3 && ran; rep++) {
+				virg_gpu_result *r = nullptr;
+				cudaEventRecord(a, e->stream);
+				if (!virg_gpu_query(e, p, t, &r)) {
+					ran = false;  /* shape does not fit this program */
+					break;
+				}
+				cudaEventRecord(z, e->stream);
+				uint64_t rows;
+				ran = virg_gpu_result_rows(r, &rows);
+				float ms = 0;
+				cudaEventElapsedTime(&ms, a, z);
+				virg_gpu_result_destroy(r);
+				t_best = std::min(t_best, ms);
+			}
+			if (ran && t_best < best) {
+				best = t_best;
+				best_shape = e->force;
+			}
+		}
+	e->force = Shape{0, 0, 0, 0};
+	cudaEventDestroy(a);
+	cudaEventDestroy(z);
+	VGPU_CHECK(best_shape.threads != 0, "no launch shape fits this program");
+	/* the key of this launch */
+	QueryLaunch q;
+	q.prog = &p->prog;
+	q.nsegs = (uint32_t)t->seg_rows.size();
+	q.seg_rows = t->seg_rows.data();
+	e->tuned[shape_key(std::vector<QueryLaunch>(1, q))] = best_shape;
+	if (shape4) {
+		shape4[0] = best_shape.threads;
+		shape4[1] = best_shape.rows_per_thread;
+		shape4[2] = best_shape.stages;
+		shape4[3] = 0;
+	}
+	set_error("%s", "");
+	return 1;
+}
 
 extern "C" int virg_gpu_engine_check(virg_gpu_engine *e, unsigned *device_error)
 {

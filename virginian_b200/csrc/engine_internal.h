@@ -46,8 +46,9 @@ struct virg_gpu_engine {
 	/* ring of (start, stop) events recorded around each kernel launch */
 	std::vector<cudaEvent_t> ring_start, ring_stop;
 	unsigned long long ring_count = 0;
-	/* launch shapes found by batch autotuning, per program-shape key */
+	/* launch shapes found by autotuning, per program-shape key */
 	std::map<std::string, vgpu::Shape> tuned;
+	vgpu::Shape force = {0, 0, 0, 0};  /* shape under trial while tuning */
 	std::mutex mu;
 };
 
@@ -113,12 +114,17 @@ struct Plan {
 	unsigned grid = 0;
 };
 
+void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
+	uint32_t *vec_off, uint32_t *vec_bytes);
+size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes);
+void fill_operands(QDesc &d, uint32_t vec_area);
 size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles);
 int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Shape *forced,
 	unsigned char *db, Plan &plan);
 KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter, uint64_t *status,
 	unsigned *error, uint32_t epoch);
 int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing);
+std::string shape_key(const std::vector<QueryLaunch> &qs);
 int read_device_error(virg_gpu_engine *e, unsigned *err);
 const char *device_error_text(unsigned code);
 uint32_t padded_rows(uint32_t rows);

@@ -349,6 +349,7 @@ int decode_program(const virg_op *ops, unsigned num_ops, unsigned pc,
 				break;
 			}
 			u.kind = UK_COPYCOL;
+			u.flags = defs[o.p1].size() == 1 ? UF_SINGLE_DEF : 0;
 			u.type = (uint8_t)cur_type[o.p1];
 			u.dst = (uint8_t)slot[o.p1];
 			u.a_cls = OC_COL;
@@ -364,6 +365,7 @@ int decode_program(const virg_op *ops, unsigned num_ops, unsigned pc,
 			}
 			Def d = def_of(o, schema);
 			u.kind = UK_SETCONST;
+			u.flags = defs[o.p1].size() == 1 ? UF_SINGLE_DEF : 0;
 			u.type = (uint8_t)d.type;
 			u.dst = (uint8_t)slot[o.p1];
 			u.a_cls = OC_CONST;
@@ -403,6 +405,7 @@ int decode_program(const virg_op *ops, unsigned num_ops, unsigned pc,
 				u.vjump = o.p4.i != 0;
 			} else if (is_math(o.op)) {
 				u.kind = UK_MATH;
+				u.flags = defs[o.p1].size() == 1 ? UF_SINGLE_DEF : 0;
 				u.sub = (uint8_t)(o.op - OP_Add);
 				u.type = (uint8_t)cur_type[o.p2];
 				u.dst = (uint8_t)slot[o.p1];
@@ -464,6 +467,72 @@ int decode_program(const virg_op *ops, unsigned num_ops, unsigned pc,
 				flow(k + 1, out);
 			if ((is_cmp(o.op) || o.op == OP_Not) && o.p4.i != 0)
 				flow(o.p3, out);
+		}
+	}
+
+	/* filter / projection split.  F is the first op from which the section up
+	 * to Result only loads, sets constants and computes (the code
+	 * generator's result-column block after its condition stub,
+	 * src/sql/generate.c:643-648).  If every jump that keeps a row valid lands
+	 * at or before F, every row valid at Result is active through [F, Result)
+	 * and those ops only matter for valid rows: they run on each warp's
+	 * selection list instead of on every row. */
+	{
+		int F = result_k;
+		for (int k = result_k - 1; k >= (int)pc; k--) {
+			const int op = ops[k].op;
+			if (is_cmp(op) || op == OP_Not || op == OP_Invalid)
+				break;
+			F = k;
+		}
+		for (int k = (int)pc; k < F; k++) {
+			const virg_op &o = ops[k];
+			if ((is_cmp(o.op) || o.op == OP_Not) && o.p4.i != 0 && o.p3 > F)
+				F = result_k;
+		}
+		P.nfilter = 0;
+		while (P.nfilter < P.nuops && P.uops[P.nfilter].kind != UK_RESULT && P.uops[P.nfilter].pc < F)
+			P.nfilter++;
+		/* vectors defined only in the projection are indexed by selection */
+		for (int r = 0; r < kMaxRegs; r++) {
+			if (rclass[r] != RC_VEC)
+				continue;
+			bool only_proj = true;
+			for (int k = (int)pc; k < result_k; k++) {
+				const Def d = def_of(ops[k], schema);
+				if (d.kind != DK_NONE && ops[k].p1 == r && k < F)
+					only_proj = false;
+			}
+			P.vec_compact[slot[r]] = only_proj ? 1 : 0;
+		}
+		X.split_k = F;
+	}
+
+	/* pending-target slots for the filter: rows that jump to pc t wait in a
+	 * slot until the first filter op at or after t; slots are reused */
+	{
+		int slot_target[kMaxSlots];
+		for (int i = 0; i < kMaxSlots; i++)
+			slot_target[i] = -1;
+		for (uint32_t i = 0; i < P.nfilter; i++) {
+			UOp &u = P.uops[i];
+			for (int sl = 0; sl < kMaxSlots; sl++)
+				if (slot_target[sl] >= 0 && slot_target[sl] <= u.pc) {
+					u.join |= (uint8_t)(1u << sl);
+					slot_target[sl] = -1;
+				}
+			if (u.kind != UK_CMP && u.kind != UK_NOT)
+				continue;
+			int use = -1;
+			for (int sl = 0; sl < kMaxSlots; sl++)
+				if (slot_target[sl] == u.target)
+					use = sl;
+			for (int sl = 0; sl < kMaxSlots && use < 0; sl++)
+				if (slot_target[sl] < 0)
+					use = sl;
+			VGPU_CHECK(use >= 0, "more than %d jump targets pending at op %u", kMaxSlots, u.pc);
+			slot_target[use] = u.target;
+			u.tslot = (uint8_t)use;
 		}
 	}
 

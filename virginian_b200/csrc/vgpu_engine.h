@@ -16,6 +16,7 @@ struct ProgramExtra {
 	int maybe_undefined;  /* some row may read a register its path never set */
 	int result_k;         /* program index of the Result op */
 	int converge_k;       /* program index of the Converge op */
+	int split_k;          /* first op of the projection (== result_k if none) */
 };
 
 int decode_program(const virg_op *ops, unsigned num_ops, unsigned pc,
@@ -32,7 +33,7 @@ struct Shape {
 
 /* fixed smem header of the kernel: QDesc copy, barriers, per-stage work
  * info and the result-scan scratch */
-constexpr unsigned kSmemQDesc = 0;
+/* (the kernel's fixed header: barriers, tile offsets, scan scratch) */
 constexpr unsigned kMaxStages = 8;
 constexpr unsigned kSmemHeader = 4096;
 
@@ -45,6 +46,10 @@ struct StageInfo {
 	uint32_t nrows;
 	uint32_t pad[3];
 };
+
+/* every stage starts with a copy of its tile's query descriptor and the tile's
+ * StageInfo, then the staged columns */
+constexpr unsigned kStageHdr = (unsigned)((sizeof(QDesc) + sizeof(StageInfo) + 127) / 128 * 128);
 
 /* kernel arguments */
 struct KParams {
@@ -59,7 +64,9 @@ struct KParams {
 	uint32_t nstages;
 	uint32_t stage_bytes;           /* stride between stages */
 	uint32_t stage_area;            /* smem offset of stage 0 */
-	uint32_t vec_area;              /* smem offset of the register vectors */
+	uint32_t vec_area;              /* smem offset of the register vectors (slot 0) */
+	uint32_t vec_bytes;             /* stride between the two vector slots */
+	uint32_t sel_area;              /* smem offset of the selection lists (2 slots) */
 };
 
 /* host-side launcher implemented in vm_kernel.cu */

@@ -60,9 +60,16 @@ struct UOp {
 	uint8_t pc;       /* program counter of the source op */
 	uint8_t target;   /* jump target (CMP/NOT) */
 	uint8_t vjump;    /* validity kept on jump: p4.i != 0 */
-	uint8_t pad;
-	uint32_t pad2;
+	uint8_t tslot;    /* pending-target slot the jump parks rows in */
+	uint8_t join;     /* slots whose rows become active again at this op */
+	uint8_t flags;    /* UF_* */
+	uint8_t pad0, pad1;
 };
+
+/* the destination register has this single definition, so rows that skip
+ * the op never read it and the store need not be predicated */
+constexpr uint8_t UF_SINGLE_DEF = 1;
+constexpr int kMaxSlots = 8;     /* pending jump targets at any one time */
 
 /* what a decoded program needs; independent of the launch shape */
 struct Program {
@@ -82,7 +89,22 @@ struct Program {
 	/* result columns */
 	uint32_t nout;
 	uint8_t out_cls[kMaxRegs], out_idx[kMaxRegs], out_type[kMaxRegs], out_stride[kMaxRegs];
+	/* uops [0, nfilter) run on every row of a tile (the filter); uops
+	 * [nfilter, nuops - 1) only on the rows still valid (the projection);
+	 * uops[nuops - 1] is the Result */
+	uint32_t nfilter;
+	/* register vectors written only by projection uops are indexed by a
+	 * row's position in its warp's selection list, not by its tile row */
+	uint8_t vec_compact[kMaxRegs];
 };
+
+/* operand descriptor resolved for a launch shape: bits [0,30) are a shared
+ * memory byte offset, bits [30,32) the kind */
+constexpr uint32_t OD_STAGE = 0u << 30;    /* staged column, + stage offset */
+constexpr uint32_t OD_ROWVEC = 1u << 30;   /* register vector by tile row */
+constexpr uint32_t OD_SELVEC = 2u << 30;   /* register vector by selection index */
+constexpr uint32_t OD_SCALAR = 3u << 30;   /* scalar register */
+constexpr uint32_t OD_OFFSET = (1u << 30) - 1;
 
 /* one resident segment (tablet) on the device */
 struct SegDesc {
@@ -98,6 +120,9 @@ struct alignas(16) QDesc {
 	uint32_t load_off[kMaxLoads];
 	uint32_t stage_bytes;
 	uint32_t vec_off[kMaxRegs];
+	/* operand descriptors per uop (a, b, destination) and result column */
+	uint32_t od_a[kMaxOps], od_b[kMaxOps], od_d[kMaxOps];
+	uint32_t od_out[kMaxRegs];
 	/* inputs */
 	const SegDesc *segs;
 	const uint32_t *seg_tile_prefix;  /* nsegs + 1 entries */
