@@ -354,6 +354,23 @@ int virg_gpu_query_host(virg_gpu_engine *e, const virg_gpu_program *p,
 	const virg_gpu_segment *segs, unsigned nsegs, void *const *out_cols,
 	uint64_t capacity, uint64_t *out_rows);
 
+/* No counterpart in the reference.  One program over one segment whose
+ * columns are already in device memory (16-byte aligned, each readable up to
+ * the next multiple of 16 bytes past its last row), writing the result rows,
+ * in the reference's order, to caller-owned device buffers that hold
+ * `capacity` rows each.  It allocates nothing, in device or host memory: for
+ * callers whose allocator owns the device's free memory, or that must not
+ * reach the CUDA allocator on a latency-critical path.  Its scratch is a
+ * fixed device array of about 520 KB, so a segment has at most 67,108,864
+ * rows (2^26); larger ones are refused before any launch.  The first call on
+ * each device (with that device current) looks up the array's address; make
+ * it before any stream capture.  Runs on `stream` (a cudaStream_t, NULL for
+ * the default stream) and waits for it to return the row count in *out_rows.
+ * All calls on a device share the array: calls that overlap in time (other
+ * streams or host threads) race; run them one after another. */
+int virg_gpu_query_prealloc(const virg_gpu_program *p, const virg_gpu_segment *seg,
+	void *const *out_cols, uint64_t capacity, uint64_t *out_rows, void *stream);
+
 /* Streamed execution over host-resident segments (tablets larger than HBM
  * residency allows): the columns the program reads are copied in chunks of
  * segs_per_chunk segments (0 = 8) through a ring of device staging buffers on

@@ -84,6 +84,7 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_result_download": (i, [vp, P(vp), u64, u64]),
         "virg_gpu_result_destroy": (None, [vp]),
         "virg_gpu_query_host": (i, [vp, vp, P(Segment), u, P(vp), u64, P(u64)]),
+        "virg_gpu_query_prealloc": (i, [vp, P(Segment), P(vp), u64, P(u64), vp]),
         "virg_gpu_query_streamed": (i, [vp, vp, P(Segment), u, u, P(vp), P(StreamStats)]),
         "virg_gpu_batch_create": (i, [vp, P(vp)]),
         "virg_gpu_batch_add": (i, [vp, vp, vp, P(u)]),
