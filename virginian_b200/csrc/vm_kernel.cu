@@ -42,7 +42,7 @@ constexpr unsigned kStageSpinLimit = 1u << 24;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
 /* work items claimed per atomic by the producer */
-constexpr unsigned kClaim = 2;
+constexpr unsigned kClaim = 1;
 
 /* shared memory header (kSmemHeader bytes) */
 constexpr unsigned kMaxGroups = 128;  /* R x warps */
