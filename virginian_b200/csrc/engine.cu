@@ -49,9 +49,16 @@ static int type_bytes(int t)
 			VGPU_FAIL("%s: %s", what, cudaGetErrorString(e_));                      \
 	} while (0)
 
-/* smem bytes a program needs per stage and for its register vectors */
+/* smem bytes a program needs per stage and for its register vectors.
+ * Vectors indexed by tile row (written by the filter) get two slots, one per
+ * tile in flight, since a tile's filter runs while the previous tile's rows
+ * are still to be stored; vectors indexed by selection position (written
+ * only by the projection, after the previous tile's stores) get one.  The
+ * vector region of a launch is [row slot 0 | row slot 1 | selection
+ * vectors], sized for the largest of its programs, so that one query's row
+ * slot never overlaps another's selection vectors. */
 void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
-	uint32_t *vec_off, uint32_t *vec_bytes)
+	uint32_t *row_bytes, uint32_t *sel_bytes)
 {
 	/* a stage: query descriptor + tile info header, then the columns */
 	uint32_t off = kStageHdr;
@@ -61,22 +68,59 @@ void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_
 		off += (uint32_t)align_up((size_t)tile * P.load_stride[i], 128);
 	}
 	*stage_bytes = off;
-	off = 0;
+	uint32_t row = 0, sel = 0;
 	for (unsigned i = 0; i < P.nvec; i++) {
-		if (vec_off)
-			vec_off[i] = off;
-		off += (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
+		const uint32_t sz = (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
+		if (P.vec_compact[i])
+			sel += sz;
+		else
+			row += sz;
 	}
-	*vec_bytes = off;
+	*row_bytes = row;
+	*sel_bytes = sel;
+}
+
+/* offsets of a program's vectors in a launch's vector region whose row slots
+ * are row_slot bytes apart */
+void vec_offsets(const Program &P, unsigned tile, uint32_t row_slot, uint32_t *vec_off)
+{
+	uint32_t r = 0, s = 2 * row_slot;
+	for (unsigned i = 0; i < P.nvec; i++) {
+		const uint32_t sz = (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
+		if (P.vec_compact[i]) {
+			vec_off[i] = s;
+			s += sz;
+		} else {
+			vec_off[i] = r;
+			r += sz;
+		}
+	}
+}
+
+/* stage bytes, row-slot bytes and vector-region bytes of a launch */
+void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uint32_t *stage_bytes,
+	uint32_t *row_slot, uint32_t *vec_bytes)
+{
+	uint32_t stage = 0, row = 0, sel = 0;
+	for (const Program *P : progs) {
+		uint32_t sb, rb, vb;
+		program_layout(*P, tile, nullptr, &sb, &rb, &vb);
+		stage = std::max(stage, sb);
+		row = std::max(row, rb);
+		sel = std::max(sel, vb);
+	}
+	*stage_bytes = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
+	*row_slot = row;
+	*vec_bytes = 2 * row + sel;
 }
 
 /* header | stages x stage bytes | register vectors | selection lists */
 size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes)
 {
-	/* register vectors and selection lists (a tile row and a (group, rank)
-	 * tag per entry) are double-buffered: a tile's stores run while the next
-	 * tile is computed */
-	return kSmemHeader + (size_t)s.stages * stage_bytes + 2 * (size_t)vec_bytes +
+	/* the selection lists (a tile row and a (group, rank) tag per entry) are
+	 * double-buffered: a tile's list is built before the previous tile's
+	 * rows are stored */
+	return kSmemHeader + (size_t)s.stages * stage_bytes + (size_t)vec_bytes +
 		2 * align_up((size_t)s.tile() * 2 * sizeof(uint16_t), 128);
 }
 
@@ -94,14 +138,8 @@ int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, 
 		s.rows_per_thread = e->pref.rows_per_thread ? e->pref.rows_per_thread : c[1];
 		if (!shape_supported(s))
 			VGPU_FAIL("unsupported launch shape %u threads x %u rows", s.threads, s.rows_per_thread);
-		uint32_t stage = 0, vec = 0;
-		for (const Program *P : progs) {
-			uint32_t sb, vb;
-			program_layout(*P, s.tile(), nullptr, &sb, nullptr, &vb);
-			stage = std::max(stage, sb);
-			vec = std::max(vec, vb);
-		}
-		stage = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
+		uint32_t stage, row_slot, vec;
+		launch_layout(progs, s.tile(), &stage, &row_slot, &vec);
 		/* a requested stage count is kept, at one CTA per SM if need be */
 		const unsigned st_list[] = {e->pref.stages ? e->pref.stages : 3u, e->pref.stages ? 0u : 2u};
 		for (unsigned st : st_list) {
@@ -150,6 +188,21 @@ static int ensure_blob(virg_gpu_engine *e, size_t n)
 	return 1;
 }
 
+/* the kernel's handler code for a uop */
+static uint32_t op_handler(const UOp &u)
+{
+	switch (u.kind) {
+	case UK_CMP: return H_CMP + u.type * 8u + u.sub;
+	case UK_MATH: return H_MATH + u.type * 4u + u.sub;
+	case UK_NOT: return H_NOT + u.type;
+	case UK_INVALID: return H_INVALID;
+	case UK_SETCONST: return H_SETCONST;
+	case UK_COPYCOL:
+		return (u.type == VT_INT64 || u.type == VT_DOUBLE) ? H_COPY8 : u.type == VT_CHAR ? H_COPY1 : H_COPY4;
+	default: return H_NOP;
+	}
+}
+
 /* operand descriptors of a query descriptor whose program, load_off and
  * vec_off are set, for register vectors starting at vec_area */
 void fill_operands(QDesc &d, uint32_t vec_area)
@@ -166,9 +219,12 @@ void fill_operands(QDesc &d, uint32_t vec_area)
 	};
 	for (uint32_t k = 0; k < P.nuops; k++) {
 		const UOp &u = P.uops[k];
-		d.od_a[k] = od(u.a_cls, u.a_idx);
-		d.od_b[k] = od(u.b_cls, u.b_idx);
-		d.od_d[k] = od(OC_VEC, u.dst);
+		OpRec &r = d.ops[k];
+		r.head = op_handler(u) | ((uint32_t)(u.tslot & 15u) << 8) | (u.vjump ? OPH_VJUMP : 0u) |
+			((u.flags & UF_SINGLE_DEF) ? OPH_SINGLE_DEF : 0u) | ((uint32_t)u.join << 16);
+		r.a = od(u.a_cls, u.a_idx);
+		r.b = od(u.b_cls, u.b_idx);
+		r.d = od(OC_VEC, u.dst);
 	}
 	for (uint32_t j = 0; j < P.nout; j++)
 		d.od_out[j] = od(P.out_cls[j], P.out_idx[j]);
@@ -196,15 +252,8 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		progs.push_back(q.prog);
 	if (forced) {
 		plan.shape = *forced;
-		uint32_t stage = 0, vec = 0;
-		for (const Program *P : progs) {
-			uint32_t sb, vb;
-			program_layout(*P, forced->tile(), nullptr, &sb, nullptr, &vb);
-			stage = std::max(stage, sb);
-			vec = std::max(vec, vb);
-		}
-		plan.stage_bytes = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
-		plan.vec_bytes = vec;
+		uint32_t forced_slot;
+		launch_layout(progs, forced->tile(), &plan.stage_bytes, &forced_slot, &plan.vec_bytes);
 		plan.smem = smem_for(plan.shape, plan.stage_bytes, plan.vec_bytes);
 		VGPU_CHECK(plan.smem <= (size_t)e->smem_optin, "shape does not fit shared memory");
 	} else if (!choose_shape(e, progs, &plan.shape, &plan.smem, &plan.stage_bytes, &plan.vec_bytes)) {
@@ -212,6 +261,8 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 	}
 	const unsigned tile = plan.shape.tile();
 	const size_t nq = qs.size();
+	uint32_t stage_all, row_slot, vec_all;
+	launch_layout(progs, tile, &stage_all, &row_slot, &vec_all);
 	size_t off_prefix, off_tiles;
 	const size_t blob_bytes = plan_blob_bytes(qs, &off_prefix, &off_tiles);
 	plan.blob.assign(blob_bytes, 0);
@@ -226,8 +277,10 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		const QueryLaunch &q = qs[i];
 		QDesc &d = hq[i];
 		d.prog = *q.prog;
-		uint32_t sb, vb;
-		program_layout(*q.prog, tile, d.load_off, &sb, d.vec_off, &vb);
+		uint32_t sb, rb, vb;
+		program_layout(*q.prog, tile, d.load_off, &sb, &rb, &vb);
+		vec_offsets(*q.prog, tile, row_slot, d.vec_off);
+		d.vec_slot = row_slot;
 		d.stage_bytes = sb;
 		d.segs = q.d_segs;
 		d.nsegs = q.nsegs;
@@ -282,7 +335,7 @@ KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter
 	kp.stage_area = kSmemHeader;
 	kp.vec_area = (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes);
 	kp.vec_bytes = plan.vec_bytes;
-	kp.sel_area = kp.vec_area + 2 * plan.vec_bytes;
+	kp.sel_area = kp.vec_area + plan.vec_bytes;
 	return kp;
 }
 

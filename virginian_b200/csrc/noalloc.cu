@@ -112,8 +112,9 @@ int pick_shape(const Program &P, int smem_optin, Shape *shape, size_t *smem, uin
 		for (auto &c : cand)
 			for (unsigned st : {3u, 2u}) {
 				Shape s = {c[0], c[1], st, 0};
-				uint32_t sb, vb;
-				program_layout(P, s.tile(), nullptr, &sb, nullptr, &vb);
+				uint32_t sb, rb, selb;
+				program_layout(P, s.tile(), nullptr, &sb, &rb, &selb);
+				const uint32_t vb = 2 * rb + selb;
 				sb = ((sb < 128 ? 128 : sb) + 127) / 128 * 128;
 				const size_t need = smem_for(s, sb, vb);
 				if (need <= (pass == 0 ? limit / 2 - 1024 : limit)) {
@@ -185,8 +186,10 @@ extern "C" int virg_gpu_query_prealloc(const virg_gpu_program *p, const virg_gpu
 	unsigned char *const db = ds.scratch;
 	QDesc &d = *reinterpret_cast<QDesc *>(hb);
 	d.prog = P;
-	uint32_t sb, vb;
-	program_layout(P, tile, d.load_off, &sb, d.vec_off, &vb);
+	uint32_t sb, rb, selb;
+	program_layout(P, tile, d.load_off, &sb, &rb, &selb);
+	vec_offsets(P, tile, rb, d.vec_off);
+	d.vec_slot = rb;
 	d.stage_bytes = sb;
 	d.segs = reinterpret_cast<const SegDesc *>(db + kOffSeg);
 	d.nsegs = 1;
@@ -238,7 +241,7 @@ extern "C" int virg_gpu_query_prealloc(const virg_gpu_program *p, const virg_gpu
 	kp.stage_area = kSmemHeader;
 	kp.vec_area = vec_area;
 	kp.vec_bytes = vec_bytes;
-	kp.sel_area = vec_area + 2 * vec_bytes;
+	kp.sel_area = vec_area + vec_bytes;
 	int per_sm = 0;
 	if (!occupancy(shape, smem, &per_sm))
 		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));

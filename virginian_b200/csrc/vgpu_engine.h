@@ -64,8 +64,8 @@ struct KParams {
 	uint32_t nstages;
 	uint32_t stage_bytes;           /* stride between stages */
 	uint32_t stage_area;            /* smem offset of stage 0 */
-	uint32_t vec_area;              /* smem offset of the register vectors (slot 0) */
-	uint32_t vec_bytes;             /* stride between the two vector slots */
+	uint32_t vec_area;              /* smem offset of the register-vector region */
+	uint32_t vec_bytes;             /* its size (the largest of the launch's queries) */
 	uint32_t sel_area;              /* smem offset of the selection lists (2 slots) */
 };
 

@@ -106,6 +106,28 @@ constexpr uint32_t OD_SELVEC = 2u << 30;   /* register vector by selection index
 constexpr uint32_t OD_SCALAR = 3u << 30;   /* scalar register */
 constexpr uint32_t OD_OFFSET = (1u << 30) - 1;
 
+/* one interpreted op as the kernel reads it: a single 16-byte record, so a
+ * warp fetches everything an op needs with one shared-memory load.
+ * head: bits [0,8) handler, [8,12) pending-target slot, bit 12 validity kept
+ * on jump, bit 13 single definition, [16,24) slots joined at this op */
+struct alignas(16) OpRec {
+	uint32_t head;
+	uint32_t a, b, d;  /* operand descriptors: source a, source b, destination */
+};
+
+/* handlers: one code per (kind, type, operator) */
+constexpr uint32_t H_NOP = 0;
+constexpr uint32_t H_CMP = 1;        /* + type * 8 + CmpOp      (1..40) */
+constexpr uint32_t H_MATH = 41;      /* + type * 4 + MathOp     (41..60) */
+constexpr uint32_t H_NOT = 61;       /* + type                  (61..65) */
+constexpr uint32_t H_INVALID = 66;
+constexpr uint32_t H_SETCONST = 67;  /* 4-byte Integer/Float */
+constexpr uint32_t H_COPY4 = 68;     /* Column/Rowid copies by element size */
+constexpr uint32_t H_COPY8 = 69;
+constexpr uint32_t H_COPY1 = 70;
+constexpr uint32_t OPH_SINGLE_DEF = 1u << 13;
+constexpr uint32_t OPH_VJUMP = 1u << 12;
+
 /* one resident segment (tablet) on the device */
 struct SegDesc {
 	const void *col[kMaxLoads];  /* fixed columns 0..15, key at kKeySlot */
@@ -120,14 +142,15 @@ struct alignas(16) QDesc {
 	uint32_t load_off[kMaxLoads];
 	uint32_t stage_bytes;
 	uint32_t vec_off[kMaxRegs];
-	/* operand descriptors per uop (a, b, destination) and result column */
-	uint32_t od_a[kMaxOps], od_b[kMaxOps], od_d[kMaxOps];
+	/* the uops as records (handler, operands) and the result columns'
+	 * operand descriptors */
+	OpRec ops[kMaxOps];
 	uint32_t od_out[kMaxRegs];
 	/* inputs */
 	const SegDesc *segs;
 	const uint32_t *seg_tile_prefix;  /* nsegs + 1 entries */
 	uint32_t nsegs;
-	uint32_t pad0;
+	uint32_t vec_slot;                /* distance between the two row-vector slots */
 	uint64_t work_first;              /* global work index of tile 0 */
 	uint64_t ntiles;
 	/* outputs */

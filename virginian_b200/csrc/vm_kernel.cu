@@ -4,22 +4,30 @@
  * Replaces the reference's virginia_gpu (src/vm/vm_gpu.cu:1152-1225), which
  * runs one thread per row with a 16-entry register file in local memory, a
  * switch dispatch per op per thread and atomics for (unordered) result
- * placement.  Here a CTA is a three-role pipeline over tiles of
- * TILE = THREADS x R rows, tied together by mbarriers:
+ * placement.  Here a CTA is a pipeline over tiles of TILE = THREADS x R
+ * rows, tied together by mbarriers, with four roles:
  *
  *  - producer warp: claims work items (one tile of one segment of one query)
- *    from a global counter, in order, and copies the tile's columns plus the
- *    query's descriptor into a ring of shared-memory stages with TMA bulk
- *    copies (cp.async.bulk completing on the stage's full barrier);
+ *    from a global counter, in order, decodes them warp-wide and copies the
+ *    tile's columns (plus the query's descriptor when the stage does not hold
+ *    it) into a ring of shared-memory stages with TMA bulk copies
+ *    (cp.async.bulk completing on the stage's full barrier);
  *  - compute warps: filter every row of the tile (row state as bit masks:
  *    valid, active, and rows parked at pending jump targets), compact each
  *    warp's valid rows into a selection list (__ballot_sync/__popc), run the
  *    projection (result expressions) on listed rows only, then store the
- *    previous tile's rows at their final positions and release its stage;
- *  - sequencer warp: for each tile, scans the (row group, warp) counts and
- *    resolves the tile's position in the query's result with a warp-wide
- *    decoupled look-back over earlier tiles (32 status words per round),
- *    one tile ahead of the stores, so cross-CTA waits overlap computation.
+ *    previous tile's rows at their final positions and release its stage.
+ *    Each op is one 16-byte record fetched with a single shared-memory load
+ *    and dispatched on one handler code; operands are read and written by
+ *    32-bit shared-memory address;
+ *  - scanner warp: scans each tile's (row group, warp) counts and publishes
+ *    the tile's count to the query's look-back words as soon as the ballots
+ *    are done;
+ *  - look-back warp: resolves the tile's position in the query's result with
+ *    a warp-wide decoupled look-back over earlier tiles (32 status words per
+ *    round), one tile ahead of the stores, so cross-CTA waits overlap
+ *    computation.  A tile that directly follows the CTA's previous tile of
+ *    the same query starts where that one ended, with no look-back.
  *
  * Rows land in original row order (the single-core CPU VM's order,
  * src/vm/virginia.c:476-578) with plain stores; no output atomics.
@@ -28,6 +36,7 @@
  * integers wrap as on x86.  Every wait is bounded; on expiry the kernel
  * records an error code and stops instead of hanging.
  */
+#include <cstddef>
 #include <cstdint>
 #include <climits>
 
@@ -41,25 +50,42 @@ namespace vgpu {
 constexpr unsigned kStageSpinLimit = 1u << 24;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
-/* work items claimed per atomic by the producer */
+/* work items claimed per atomic by the producer: one, so tiles that follow
+ * each other in a query are taken, and finished, at about the same time */
 constexpr unsigned kClaim = 1;
+
+/* warps besides the compute warps: scanner, producer, look-back */
+constexpr int kRoleWarps = 3;
 
 /* shared memory header (kSmemHeader bytes) */
 constexpr unsigned kMaxGroups = 128;  /* R x warps */
-constexpr unsigned kOffFull = 0;                           /* mbarrier[kMaxStages] */
-constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;  /* mbarrier[kMaxStages] */
+constexpr unsigned kOffFull = 0;                            /* mbarrier[kMaxStages] */
+constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;   /* mbarrier[kMaxStages] */
 constexpr unsigned kOffCready = kOffEmpty + 8 * kMaxStages; /* mbarrier[2]: counts ready */
-constexpr unsigned kOffOready = kOffCready + 16;           /* mbarrier[2]: offsets ready */
-constexpr unsigned kOffOff = kOffOready + 16;              /* uint64[2]: tile offsets */
-constexpr unsigned kOffFlags = kOffOff + 16;               /* uint32[4]: ok[2], abort */
-constexpr unsigned kOffAgg = kOffFlags + 16;               /* uint64[2]: warps arrived | count */
-constexpr unsigned kOffHeld = kOffAgg + 16;                /* uint32[kMaxStages]: query per stage */
-constexpr unsigned kOffCnt = 256;                          /* uint32[2][kMaxGroups] */
-constexpr unsigned kOffPre = kOffCnt + 8 * kMaxGroups;     /* uint32[2][kMaxGroups] */
+constexpr unsigned kOffSready = kOffCready + 16;            /* mbarrier[2]: scan done */
+constexpr unsigned kOffOready = kOffSready + 16;            /* mbarrier[2]: offsets ready */
+constexpr unsigned kOffOff = kOffOready + 16;               /* uint64[2]: tile offsets */
+constexpr unsigned kOffFlags = kOffOff + 16;                /* uint32[4]: ok[2], abort */
+constexpr unsigned kOffTot = kOffFlags + 16;                /* uint32[2]: tile totals */
+constexpr unsigned kOffHeld = kOffTot + 8;                  /* uint32[kMaxStages]: query per stage */
+constexpr unsigned kOffCnt = 256;                           /* uint32[2][kMaxGroups] */
+constexpr unsigned kOffPre = kOffCnt + 8 * kMaxGroups;      /* uint32[2][kMaxGroups] */
 static_assert(kOffHeld + 4 * kMaxStages <= kOffCnt, "smem header layout");
 static_assert(kOffPre + 8 * kMaxGroups <= kSmemHeader, "smem header overflow");
 static_assert(sizeof(QDesc) % 16 == 0, "QDesc copies in 16-byte chunks");
 static_assert(kStageHdr >= sizeof(QDesc) + sizeof(StageInfo), "stage header too small");
+static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a time");
+
+/* where the fields the compute warps read sit in a stage's descriptor copy */
+constexpr uint32_t kQOps = (uint32_t)offsetof(QDesc, ops);
+constexpr uint32_t kQNFilter = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nfilter));
+constexpr uint32_t kQNUops = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nuops));
+constexpr uint32_t kQNOut = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nout));
+constexpr uint32_t kQOutStride = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, out_stride));
+constexpr uint32_t kQOdOut = (uint32_t)offsetof(QDesc, od_out);
+constexpr uint32_t kQOutPtr = (uint32_t)offsetof(QDesc, out_ptr);
+constexpr uint32_t kQCapacity = (uint32_t)offsetof(QDesc, capacity);
+constexpr uint32_t kQVecSlot = (uint32_t)offsetof(QDesc, vec_slot);
 
 /* ---- PTX wrappers ---------------------------------------------------- */
 
@@ -153,40 +179,151 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const vo
 	return false;
 }
 
-/* ---- operand access ---------------------------------------------------- */
+/* ---- shared-memory access by 32-bit shared address ---------------------
+ * Every tile, register-vector and descriptor access of the compute warps
+ * goes through these, so each is one ld/st.shared.  They are volatile asm:
+ * the compiler keeps them in program order, and the hardware still
+ * pipelines consecutive independent loads. */
 
-/* element i of an operand is at p + i * step (step 0: a broadcast scalar) */
-struct Acc {
-	unsigned char *p;
-	uint32_t step;
-	bool sel;  /* indexed by selection position instead of tile row */
+__device__ __forceinline__ uint32_t lds_u8(uint32_t a)
+{
+	uint32_t v;
+	asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a));
+	return v;
+}
+
+__device__ __forceinline__ uint32_t lds_u16(uint32_t a)
+{
+	uint16_t v;
+	asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+	return v;
+}
+
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a)
+{
+	uint32_t v;
+	asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
+	return v;
+}
+
+__device__ __forceinline__ uint64_t lds_u64(uint32_t a)
+{
+	uint64_t v;
+	asm volatile("ld.shared.b64 %0, [%1];" : "=l"(v) : "r"(a));
+	return v;
+}
+
+__device__ __forceinline__ uint4 lds_v4(uint32_t a)
+{
+	uint4 v;
+	asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+		: "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+	return v;
+}
+
+__device__ __forceinline__ void sts_u8(uint32_t a, uint32_t v)
+{
+	asm volatile("st.shared.u8 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void sts_u16(uint32_t a, uint32_t v)
+{
+	asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"((uint16_t)v) : "memory");
+}
+
+__device__ __forceinline__ void sts_u32(uint32_t a, uint32_t v)
+{
+	asm volatile("st.shared.b32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void sts_u64(uint32_t a, uint64_t v)
+{
+	asm volatile("st.shared.b64 [%0], %1;" ::"r"(a), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void sts_v4(uint32_t a, uint4 v)
+{
+	asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(a), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+		: "memory");
+}
+
+/* typed element access */
+template <typename T>
+struct SM;
+template <>
+struct SM<int32_t> {
+	static __device__ __forceinline__ int32_t ld(uint32_t a) { return (int32_t)lds_u32(a); }
+	static __device__ __forceinline__ void st(uint32_t a, int32_t v) { sts_u32(a, (uint32_t)v); }
+};
+template <>
+struct SM<uint32_t> {
+	static __device__ __forceinline__ uint32_t ld(uint32_t a) { return lds_u32(a); }
+	static __device__ __forceinline__ void st(uint32_t a, uint32_t v) { sts_u32(a, v); }
+};
+template <>
+struct SM<float> {
+	static __device__ __forceinline__ float ld(uint32_t a) { return __uint_as_float(lds_u32(a)); }
+	static __device__ __forceinline__ void st(uint32_t a, float v) { sts_u32(a, __float_as_uint(v)); }
+};
+template <>
+struct SM<long long> {
+	static __device__ __forceinline__ long long ld(uint32_t a) { return (long long)lds_u64(a); }
+	static __device__ __forceinline__ void st(uint32_t a, long long v) { sts_u64(a, (uint64_t)v); }
+};
+template <>
+struct SM<unsigned long long> {
+	static __device__ __forceinline__ unsigned long long ld(uint32_t a) { return lds_u64(a); }
+	static __device__ __forceinline__ void st(uint32_t a, unsigned long long v) { sts_u64(a, v); }
+};
+template <>
+struct SM<double> {
+	static __device__ __forceinline__ double ld(uint32_t a) { return __longlong_as_double((long long)lds_u64(a)); }
+	static __device__ __forceinline__ void st(uint32_t a, double v) { sts_u64(a, (uint64_t)__double_as_longlong(v)); }
+};
+template <>
+struct SM<signed char> {
+	static __device__ __forceinline__ signed char ld(uint32_t a) { return (signed char)lds_u8(a); }
+	static __device__ __forceinline__ void st(uint32_t a, signed char v) { sts_u8(a, (uint32_t)(unsigned char)v); }
+};
+template <>
+struct SM<unsigned char> {
+	static __device__ __forceinline__ unsigned char ld(uint32_t a) { return (unsigned char)lds_u8(a); }
+	static __device__ __forceinline__ void st(uint32_t a, unsigned char v) { sts_u8(a, v); }
 };
 
-/* staged columns and the scalar table live in the stage; register vectors
- * in the tile's vector slot */
-template <typename T>
-__device__ __forceinline__ Acc acc_of(unsigned char *smem, uint32_t od, uint32_t stage_delta,
-	uint32_t vec_delta)
+/* an operand resolved for one tile: element i at addr + i * step (step 0 for
+ * a scalar), indexed by selection position instead of tile row when sel */
+struct Opnd {
+	uint32_t addr;
+	uint32_t step;
+	bool sel;
+};
+
+/* staged columns and scalars (the descriptor's constant table) live in the
+ * tile's stage, row vectors in the tile's row-vector slot, selection
+ * vectors in their single area */
+template <int SIZE>
+__device__ __forceinline__ Opnd opnd(uint32_t od, uint32_t sbase, uint32_t sdelta, uint32_t vdelta)
 {
-	Acc a;
-	const uint32_t kind = od & ~OD_OFFSET;
-	const bool in_stage = kind == OD_STAGE || kind == OD_SCALAR;
-	a.p = smem + (od & OD_OFFSET) + (in_stage ? stage_delta : vec_delta);
-	a.step = kind == OD_SCALAR ? 0u : (uint32_t)sizeof(T);
-	a.sel = kind == OD_SELVEC;
-	return a;
+	const uint32_t kind = od >> 30;
+	Opnd o;
+	o.addr = sbase + (od & OD_OFFSET) +
+		((kind == (OD_STAGE >> 30) || kind == (OD_SCALAR >> 30)) ? sdelta
+			: kind == (OD_ROWVEC >> 30) ? vdelta : 0u);
+	o.step = kind == (OD_SCALAR >> 30) ? 0u : (uint32_t)SIZE;
+	o.sel = kind == (OD_SELVEC >> 30);
+	return o;
 }
 
-template <typename T>
-__device__ __forceinline__ T ld_at(const Acc &a, uint32_t i)
+/* Rows of a tile: thread tid holds R = 4 C rows, in C chunks of 4
+ * consecutive rows; chunk c of thread tid starts at tile row
+ * c * 4 * THREADS + 4 * tid, and row k of the chunk is bit 4 c + k of the
+ * thread's row masks.  One 16-byte shared load fetches a chunk of a 4-byte
+ * column. */
+template <int THREADS>
+__device__ __forceinline__ uint32_t chunk_row(int c, int tid)
 {
-	return *reinterpret_cast<const T *>(a.p + i * a.step);
-}
-
-template <typename T>
-__device__ __forceinline__ void st_at(const Acc &a, uint32_t i, T v)
-{
-	*reinterpret_cast<T *>(a.p + i * a.step) = v;
+	return (uint32_t)(c * 4 * THREADS + 4 * tid);
 }
 
 /* ---- op semantics (src/vm/virginia.c:48-194, :598-680) ------------------ */
@@ -309,174 +446,230 @@ struct RowState {
 	uint32_t pend[kMaxSlots];
 };
 
-struct FCtx {
-	unsigned char *smem;
-	const QDesc *Q;
-	uint32_t stage_delta;
-	uint32_t vec_delta;
-	int tid;
-};
-
 /* rows in `jumped` leave the active set, park in the op's target slot and,
  * for a jump with p4 == 0, stop being valid (src/vm/virginia.c:59-63) */
-__device__ __forceinline__ void take_jump(RowState &st, const UOp &u, uint32_t jumped)
+__device__ __forceinline__ void take_jump(RowState &st, uint32_t head, uint32_t jumped)
 {
 	st.active &= ~jumped;
-	if (!u.vjump)
+	if (!(head & OPH_VJUMP))
 		st.valid &= ~jumped;
+	const uint32_t slot = (head >> 8) & 15u;
 #pragma unroll
 	for (int s = 0; s < kMaxSlots; s++)
-		if (u.tslot == s)
+		if (slot == (uint32_t)s)
 			st.pend[s] |= jumped;
 }
 
-template <typename T, int OP, int THREADS, int R>
-__device__ __forceinline__ void f_cmp(const FCtx &c, const UOp &u, uint32_t k, RowState &st)
+/* element bits <-> values */
+template <typename T>
+__device__ __forceinline__ T from_bits(uint64_t b)
 {
-	const Acc a = acc_of<T>(c.smem, c.Q->od_a[k], c.stage_delta, c.vec_delta);
-	const Acc b = acc_of<T>(c.smem, c.Q->od_b[k], c.stage_delta, c.vec_delta);
-	uint32_t bits = 0;
-	if (b.step == 0) {
-		/* column or vector against a scalar: the common WHERE shape */
-		const T y = ld_at<T>(b, 0);
+	if constexpr (sizeof(T) == 8) {
+		const long long v = (long long)b;
+		return *reinterpret_cast<const T *>(&v);
+	} else if constexpr (sizeof(T) == 4) {
+		const uint32_t v = (uint32_t)b;
+		return *reinterpret_cast<const T *>(&v);
+	} else {
+		const unsigned char v = (unsigned char)b;
+		return *reinterpret_cast<const T *>(&v);
+	}
+}
+
+template <typename T>
+__device__ __forceinline__ uint64_t to_bits(T x)
+{
+	if constexpr (sizeof(T) == 8)
+		return *reinterpret_cast<const unsigned long long *>(&x);
+	else if constexpr (sizeof(T) == 4)
+		return *reinterpret_cast<const uint32_t *>(&x);
+	else
+		return *reinterpret_cast<const unsigned char *>(&x);
+}
+
+/* one chunk (4 consecutive rows) of a column or row vector */
+template <typename T>
+__device__ __forceinline__ void ld_chunk(uint32_t a, T *v)
+{
+	if constexpr (sizeof(T) == 4) {
+		const uint4 q = lds_v4(a);
+		v[0] = from_bits<T>(q.x); v[1] = from_bits<T>(q.y); v[2] = from_bits<T>(q.z); v[3] = from_bits<T>(q.w);
+	} else if constexpr (sizeof(T) == 8) {
+		const uint4 q0 = lds_v4(a), q1 = lds_v4(a + 16);
+		v[0] = from_bits<T>((uint64_t)q0.y << 32 | q0.x);
+		v[1] = from_bits<T>((uint64_t)q0.w << 32 | q0.z);
+		v[2] = from_bits<T>((uint64_t)q1.y << 32 | q1.x);
+		v[3] = from_bits<T>((uint64_t)q1.w << 32 | q1.z);
+	} else {
+		const uint32_t w = lds_u32(a);
+		v[0] = from_bits<T>(w & 0xffu); v[1] = from_bits<T>((w >> 8) & 0xffu);
+		v[2] = from_bits<T>((w >> 16) & 0xffu); v[3] = from_bits<T>(w >> 24);
+	}
+}
+
+template <typename T>
+__device__ __forceinline__ void st_chunk(uint32_t a, const T *v)
+{
+	if constexpr (sizeof(T) == 4) {
+		sts_v4(a, make_uint4((uint32_t)to_bits(v[0]), (uint32_t)to_bits(v[1]), (uint32_t)to_bits(v[2]),
+			(uint32_t)to_bits(v[3])));
+	} else if constexpr (sizeof(T) == 8) {
+		const uint64_t b0 = to_bits(v[0]), b1 = to_bits(v[1]), b2 = to_bits(v[2]), b3 = to_bits(v[3]);
+		sts_v4(a, make_uint4((uint32_t)b0, (uint32_t)(b0 >> 32), (uint32_t)b1, (uint32_t)(b1 >> 32)));
+		sts_v4(a + 16, make_uint4((uint32_t)b2, (uint32_t)(b2 >> 32), (uint32_t)b3, (uint32_t)(b3 >> 32)));
+	} else {
+		sts_u32(a, (uint32_t)(to_bits(v[0]) | to_bits(v[1]) << 8 | to_bits(v[2]) << 16 | to_bits(v[3]) << 24));
+	}
+}
+
+/* the operand's elements for this thread's R rows */
+template <typename T, int THREADS, int R>
+__device__ __forceinline__ void load_rows(const Opnd &o, int tid, T (&v)[R])
+{
+	if (o.step == 0) {
+		const T x = SM<T>::ld(o.addr);
 #pragma unroll
 		for (int r = 0; r < R; r++)
-			bits |= (uint32_t)cmp_eval<T, OP>(ld_at<T>(a, r * THREADS + c.tid), y) << r;
+			v[r] = x;
 	} else {
 #pragma unroll
-		for (int r = 0; r < R; r++) {
-			const uint32_t row = r * THREADS + c.tid;
-			bits |= (uint32_t)cmp_eval<T, OP>(ld_at<T>(a, row), ld_at<T>(b, row)) << r;
-		}
+		for (int c = 0; c < R / 4; c++)
+			ld_chunk<T>(o.addr + chunk_row<THREADS>(c, tid) * (uint32_t)sizeof(T), v + 4 * c);
 	}
-	take_jump(st, u, st.active & bits);
 }
 
+/* store the rows whose bit is set in `mask` (whole chunks at once) */
 template <typename T, int THREADS, int R>
-__device__ __forceinline__ void f_not(const FCtx &c, const UOp &u, uint32_t k, RowState &st)
+__device__ __forceinline__ void store_rows(uint32_t addr, int tid, const T (&v)[R], uint32_t mask)
 {
-	const Acc a = acc_of<T>(c.smem, c.Q->od_a[k], c.stage_delta, c.vec_delta);
+#pragma unroll
+	for (int c = 0; c < R / 4; c++) {
+		const uint32_t a = addr + chunk_row<THREADS>(c, tid) * (uint32_t)sizeof(T);
+		const uint32_t m = (mask >> (4 * c)) & 0xfu;
+		if (m == 0xfu) {
+			st_chunk<T>(a, v + 4 * c);
+		} else if (m) {
+#pragma unroll
+			for (int k = 0; k < 4; k++)
+				if ((m >> k) & 1u)
+					SM<T>::st(a + k * (uint32_t)sizeof(T), v[4 * c + k]);
+		}
+	}
+}
+
+/* per-op arguments of the filter */
+struct FArgs {
+	uint32_t sbase, sd, vd;
+	int tid;
+};
+
+template <typename T, int OP, int THREADS, int R>
+__device__ __forceinline__ void f_cmp(const uint4 &rec, const FArgs &f, RowState &st)
+{
+	T x[R], y[R];
+	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
+	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.z, f.sbase, f.sd, f.vd), f.tid, y);
 	uint32_t bits = 0;
 #pragma unroll
 	for (int r = 0; r < R; r++)
-		bits |= (uint32_t)(ld_at<T>(a, r * THREADS + c.tid) == T(0)) << r;
-	take_jump(st, u, st.active & bits);
+		bits |= (uint32_t)cmp_eval<T, OP>(x[r], y[r]) << r;
+	take_jump(st, rec.x, st.active & bits);
 }
 
-template <typename T, int OP, int THREADS, int R>
-__device__ __forceinline__ void f_math(const FCtx &c, const UOp &u, uint32_t k, const RowState &st)
-{
-	const Acc a = acc_of<T>(c.smem, c.Q->od_a[k], c.stage_delta, c.vec_delta);
-	const Acc b = acc_of<T>(c.smem, c.Q->od_b[k], c.stage_delta, c.vec_delta);
-	const Acc d = acc_of<T>(c.smem, c.Q->od_d[k], c.stage_delta, c.vec_delta);
-	const uint32_t store = (u.flags & UF_SINGLE_DEF) ? 0xffffffffu : st.active;
-#pragma unroll
-	for (int r = 0; r < R; r++) {
-		const uint32_t row = r * THREADS + c.tid;
-		const T z = Math<T, OP>::eval(ld_at<T>(a, row), ld_at<T>(b, row));
-		if ((store >> r) & 1u)
-			st_at<T>(d, row, z);
-	}
-}
-
-/* Integer/Float into a vector register: active rows only */
 template <typename T, int THREADS, int R>
-__device__ __forceinline__ void f_setconst(const FCtx &c, uint32_t k, const RowState &st)
+__device__ __forceinline__ void f_not(const uint4 &rec, const FArgs &f, RowState &st)
 {
-	const Acc a = acc_of<T>(c.smem, c.Q->od_a[k], c.stage_delta, c.vec_delta);
-	const Acc d = acc_of<T>(c.smem, c.Q->od_d[k], c.stage_delta, c.vec_delta);
-	const T v = ld_at<T>(a, 0);
+	T x[R];
+	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
+	uint32_t bits = 0;
 #pragma unroll
 	for (int r = 0; r < R; r++)
-		if ((st.active >> r) & 1u)
-			st_at<T>(d, r * THREADS + c.tid, v);
+		bits |= (uint32_t)(x[r] == T(0)) << r;
+	take_jump(st, rec.x, st.active & bits);
 }
 
-/* Column/Rowid into a vector register: every row (the CPU copies the whole
+/* arithmetic into a register vector: active rows only, unless the register
+ * has this single definition (then no row that skips it reads it) */
+template <typename T, int OP, int THREADS, int R>
+__device__ __forceinline__ void f_math(const uint4 &rec, const FArgs &f, const RowState &st)
+{
+	T x[R], y[R];
+	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
+	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.z, f.sbase, f.sd, f.vd), f.tid, y);
+#pragma unroll
+	for (int r = 0; r < R; r++)
+		x[r] = Math<T, OP>::eval(x[r], y[r]);
+	store_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.w, f.sbase, f.sd, f.vd).addr, f.tid, x,
+		(rec.x & OPH_SINGLE_DEF) ? 0xffffffffu : st.active);
+}
+
+/* Integer/Float into a register vector: active rows only */
+template <int THREADS, int R>
+__device__ __forceinline__ void f_setconst(const uint4 &rec, const FArgs &f, const RowState &st)
+{
+	uint32_t v[R];
+	load_rows<uint32_t, THREADS, R>(opnd<4>(rec.y, f.sbase, f.sd, f.vd), f.tid, v);
+	store_rows<uint32_t, THREADS, R>(opnd<4>(rec.w, f.sbase, f.sd, f.vd).addr, f.tid, v, st.active);
+}
+
+/* Column/Rowid into a register vector: every row (the CPU copies the whole
  * block, src/vm/virginia.c:448) */
 template <typename T, int THREADS, int R>
-__device__ __forceinline__ void f_copycol(const FCtx &c, uint32_t k)
+__device__ __forceinline__ void f_copy(const uint4 &rec, const FArgs &f)
 {
-	const Acc a = acc_of<T>(c.smem, c.Q->od_a[k], c.stage_delta, c.vec_delta);
-	const Acc d = acc_of<T>(c.smem, c.Q->od_d[k], c.stage_delta, c.vec_delta);
-#pragma unroll
-	for (int r = 0; r < R; r++) {
-		const uint32_t row = r * THREADS + c.tid;
-		st_at<T>(d, row, ld_at<T>(a, row));
-	}
+	T x[R];
+	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
+	store_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.w, f.sbase, f.sd, f.vd).addr, f.tid, x, 0xffffffffu);
 }
 
 template <int THREADS, int R>
-__device__ __forceinline__ void filter_op(const FCtx &c, const UOp &u, uint32_t k, RowState &st)
+__device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowState &st)
 {
-	if (u.join) {
+	const uint32_t join = (rec.x >> 16) & 0xffu;
+	if (join) {
 #pragma unroll
 		for (int s = 0; s < kMaxSlots; s++)
-			if ((u.join >> s) & 1u) {
+			if ((join >> s) & 1u) {
 				st.active |= st.pend[s];
 				st.pend[s] = 0;
 			}
 	}
-#define VGPU_CMP_CASES(T, TY)                                                        \
-	case TY * 8 + CO_LE: f_cmp<T, CO_LE, THREADS, R>(c, u, k, st); break;           \
-	case TY * 8 + CO_LT: f_cmp<T, CO_LT, THREADS, R>(c, u, k, st); break;           \
-	case TY * 8 + CO_GE: f_cmp<T, CO_GE, THREADS, R>(c, u, k, st); break;           \
-	case TY * 8 + CO_GT: f_cmp<T, CO_GT, THREADS, R>(c, u, k, st); break;           \
-	case TY * 8 + CO_EQ: f_cmp<T, CO_EQ, THREADS, R>(c, u, k, st); break;           \
-	case TY * 8 + CO_NEQ: f_cmp<T, CO_NEQ, THREADS, R>(c, u, k, st); break;         \
-	case TY * 8 + CO_AND: f_cmp<T, CO_AND, THREADS, R>(c, u, k, st); break;         \
-	case TY * 8 + CO_OR: f_cmp<T, CO_OR, THREADS, R>(c, u, k, st); break;
-#define VGPU_MATH_CASES(T, TY)                                                 \
-	case TY * 8 + MO_ADD: f_math<T, MO_ADD, THREADS, R>(c, u, k, st); break;  \
-	case TY * 8 + MO_SUB: f_math<T, MO_SUB, THREADS, R>(c, u, k, st); break;  \
-	case TY * 8 + MO_MUL: f_math<T, MO_MUL, THREADS, R>(c, u, k, st); break;  \
-	case TY * 8 + MO_DIV: f_math<T, MO_DIV, THREADS, R>(c, u, k, st); break;
-	switch (u.kind) {
-	case UK_CMP:
-		switch (u.type * 8 + u.sub) {
-			VGPU_CMP_CASES(int32_t, VT_INT)
-			VGPU_CMP_CASES(long long, VT_INT64)
-			VGPU_CMP_CASES(float, VT_FLOAT)
-			VGPU_CMP_CASES(double, VT_DOUBLE)
-			VGPU_CMP_CASES(signed char, VT_CHAR)
-		default: break;
-		}
-		break;
-	case UK_MATH:
-		switch (u.type * 8 + u.sub) {
-			VGPU_MATH_CASES(int32_t, VT_INT)
-			VGPU_MATH_CASES(long long, VT_INT64)
-			VGPU_MATH_CASES(float, VT_FLOAT)
-			VGPU_MATH_CASES(double, VT_DOUBLE)
-			VGPU_MATH_CASES(signed char, VT_CHAR)
-		default: break;
-		}
-		break;
-	case UK_NOT:
-		switch (u.type) {
-		case VT_INT: f_not<int32_t, THREADS, R>(c, u, k, st); break;
-		case VT_INT64: f_not<long long, THREADS, R>(c, u, k, st); break;
-		case VT_FLOAT: f_not<float, THREADS, R>(c, u, k, st); break;
-		case VT_DOUBLE: f_not<double, THREADS, R>(c, u, k, st); break;
-		default: f_not<signed char, THREADS, R>(c, u, k, st); break;
-		}
-		break;
-	case UK_INVALID:
-		st.valid &= ~st.active;
-		break;
-	case UK_SETCONST:
-		f_setconst<uint32_t, THREADS, R>(c, k, st);
-		break;
-	case UK_COPYCOL:
-		switch (u.type) {
-		case VT_INT64:
-		case VT_DOUBLE: f_copycol<unsigned long long, THREADS, R>(c, k); break;
-		case VT_CHAR: f_copycol<unsigned char, THREADS, R>(c, k); break;
-		default: f_copycol<uint32_t, THREADS, R>(c, k); break;
-		}
-		break;
-	default:
-		break;
+#define VGPU_CMP_CASES(T, TY)                                                            \
+	case H_CMP + TY * 8 + CO_LE: f_cmp<T, CO_LE, THREADS, R>(rec, f, st); break;        \
+	case H_CMP + TY * 8 + CO_LT: f_cmp<T, CO_LT, THREADS, R>(rec, f, st); break;        \
+	case H_CMP + TY * 8 + CO_GE: f_cmp<T, CO_GE, THREADS, R>(rec, f, st); break;        \
+	case H_CMP + TY * 8 + CO_GT: f_cmp<T, CO_GT, THREADS, R>(rec, f, st); break;        \
+	case H_CMP + TY * 8 + CO_EQ: f_cmp<T, CO_EQ, THREADS, R>(rec, f, st); break;        \
+	case H_CMP + TY * 8 + CO_NEQ: f_cmp<T, CO_NEQ, THREADS, R>(rec, f, st); break;      \
+	case H_CMP + TY * 8 + CO_AND: f_cmp<T, CO_AND, THREADS, R>(rec, f, st); break;      \
+	case H_CMP + TY * 8 + CO_OR: f_cmp<T, CO_OR, THREADS, R>(rec, f, st); break;
+#define VGPU_MATH_CASES(T, TY)                                                        \
+	case H_MATH + TY * 4 + MO_ADD: f_math<T, MO_ADD, THREADS, R>(rec, f, st); break; \
+	case H_MATH + TY * 4 + MO_SUB: f_math<T, MO_SUB, THREADS, R>(rec, f, st); break; \
+	case H_MATH + TY * 4 + MO_MUL: f_math<T, MO_MUL, THREADS, R>(rec, f, st); break; \
+	case H_MATH + TY * 4 + MO_DIV: f_math<T, MO_DIV, THREADS, R>(rec, f, st); break;
+	switch (rec.x & 0xffu) {
+		VGPU_CMP_CASES(int32_t, VT_INT)
+		VGPU_CMP_CASES(long long, VT_INT64)
+		VGPU_CMP_CASES(float, VT_FLOAT)
+		VGPU_CMP_CASES(double, VT_DOUBLE)
+		VGPU_CMP_CASES(signed char, VT_CHAR)
+		VGPU_MATH_CASES(int32_t, VT_INT)
+		VGPU_MATH_CASES(long long, VT_INT64)
+		VGPU_MATH_CASES(float, VT_FLOAT)
+		VGPU_MATH_CASES(double, VT_DOUBLE)
+		VGPU_MATH_CASES(signed char, VT_CHAR)
+	case H_NOT + VT_INT: f_not<int32_t, THREADS, R>(rec, f, st); break;
+	case H_NOT + VT_INT64: f_not<long long, THREADS, R>(rec, f, st); break;
+	case H_NOT + VT_FLOAT: f_not<float, THREADS, R>(rec, f, st); break;
+	case H_NOT + VT_DOUBLE: f_not<double, THREADS, R>(rec, f, st); break;
+	case H_NOT + VT_CHAR: f_not<signed char, THREADS, R>(rec, f, st); break;
+	case H_INVALID: st.valid &= ~st.active; break;
+	case H_SETCONST: f_setconst<THREADS, R>(rec, f, st); break;
+	case H_COPY4: f_copy<uint32_t, THREADS, R>(rec, f); break;
+	case H_COPY8: f_copy<unsigned long long, THREADS, R>(rec, f); break;
+	case H_COPY1: f_copy<unsigned char, THREADS, R>(rec, f); break;
+	default: break;
 	}
 #undef VGPU_CMP_CASES
 #undef VGPU_MATH_CASES
@@ -487,96 +680,75 @@ __device__ __forceinline__ void filter_op(const FCtx &c, const UOp &u, uint32_t 
 /* lane `lane` of a warp handles the warp's selection entries lane + 32 i,
  * i < R; their tile rows are held in registers for the whole projection */
 template <int R>
-struct PCtx {
-	unsigned char *smem;
-	const QDesc *Q;
-	uint32_t stage_delta;
-	uint32_t vec_delta;
-	uint32_t n;            /* entries in the warp's list */
-	uint32_t sel_base;     /* this warp's first selection-vector index */
-	int lane;
-	uint32_t row[R];       /* tile rows of this lane's entries */
+struct PArgs {
+	uint32_t sbase, sd, vd;
+	uint32_t n;     /* entries in the warp's list */
+	uint32_t sel0;  /* selection index of this lane's first entry */
+	uint32_t lane;
+	uint32_t row[R];
 };
 
-template <typename T>
-__device__ __forceinline__ T p_ld(const Acc &a, uint32_t row, uint32_t sidx)
+/* element address of a selection entry */
+__device__ __forceinline__ uint32_t p_addr(const Opnd &o, uint32_t row, uint32_t sidx)
 {
-	return ld_at<T>(a, a.sel ? sidx : row);
-}
-
-template <typename T>
-__device__ __forceinline__ void p_st(const Acc &a, uint32_t row, uint32_t sidx, T v)
-{
-	st_at<T>(a, a.sel ? sidx : row, v);
+	return o.addr + (o.sel ? sidx : row) * o.step;
 }
 
 template <typename T, int OP, int R>
-__device__ __forceinline__ void p_math(const PCtx<R> &c, uint32_t k)
+__device__ __forceinline__ void p_math(const uint4 &rec, const PArgs<R> &c)
 {
-	const Acc a = acc_of<T>(c.smem, c.Q->od_a[k], c.stage_delta, c.vec_delta);
-	const Acc b = acc_of<T>(c.smem, c.Q->od_b[k], c.stage_delta, c.vec_delta);
-	const Acc d = acc_of<T>(c.smem, c.Q->od_d[k], c.stage_delta, c.vec_delta);
+	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
+	const Opnd b = opnd<sizeof(T)>(rec.z, c.sbase, c.sd, c.vd);
+	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
 #pragma unroll
 	for (int i = 0; i < R; i++) {
-		const uint32_t e = c.lane + 32 * i;
-		if (32 * i >= c.n)
+		if (32u * i >= c.n)
 			break;
-		if (e < c.n) {
-			const uint32_t si = c.sel_base + e;
-			p_st<T>(d, c.row[i], si,
-				Math<T, OP>::eval(p_ld<T>(a, c.row[i], si), p_ld<T>(b, c.row[i], si)));
+		if (c.lane + 32u * i < c.n) {
+			const uint32_t si = c.sel0 + 32u * i;
+			const T x = SM<T>::ld(p_addr(a, c.row[i], si));
+			const T y = SM<T>::ld(p_addr(b, c.row[i], si));
+			SM<T>::st(p_addr(d, c.row[i], si), Math<T, OP>::eval(x, y));
 		}
 	}
 }
 
 template <typename T, int R>
-__device__ __forceinline__ void p_copy(const PCtx<R> &c, uint32_t k)
+__device__ __forceinline__ void p_copy(const uint4 &rec, const PArgs<R> &c)
 {
-	const Acc a = acc_of<T>(c.smem, c.Q->od_a[k], c.stage_delta, c.vec_delta);
-	const Acc d = acc_of<T>(c.smem, c.Q->od_d[k], c.stage_delta, c.vec_delta);
+	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
+	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
 #pragma unroll
 	for (int i = 0; i < R; i++) {
-		const uint32_t e = c.lane + 32 * i;
-		if (32 * i >= c.n)
+		if (32u * i >= c.n)
 			break;
-		if (e < c.n) {
-			const uint32_t si = c.sel_base + e;
-			p_st<T>(d, c.row[i], si, p_ld<T>(a, c.row[i], si));
+		if (c.lane + 32u * i < c.n) {
+			const uint32_t si = c.sel0 + 32u * i;
+			SM<T>::st(p_addr(d, c.row[i], si), SM<T>::ld(p_addr(a, c.row[i], si)));
 		}
 	}
 }
 
 template <int R>
-__device__ __forceinline__ void project_op(const PCtx<R> &c, const UOp &u, uint32_t k)
+__device__ __forceinline__ void project_op(const uint4 &rec, const PArgs<R> &c)
 {
-#define VGPU_PMATH_CASES(T, TY)                                      \
-	case TY * 8 + MO_ADD: p_math<T, MO_ADD, R>(c, k); break;        \
-	case TY * 8 + MO_SUB: p_math<T, MO_SUB, R>(c, k); break;        \
-	case TY * 8 + MO_MUL: p_math<T, MO_MUL, R>(c, k); break;        \
-	case TY * 8 + MO_DIV: p_math<T, MO_DIV, R>(c, k); break;
-	switch (u.kind) {
-	case UK_MATH:
-		switch (u.type * 8 + u.sub) {
-			VGPU_PMATH_CASES(int32_t, VT_INT)
-			VGPU_PMATH_CASES(long long, VT_INT64)
-			VGPU_PMATH_CASES(float, VT_FLOAT)
-			VGPU_PMATH_CASES(double, VT_DOUBLE)
-			VGPU_PMATH_CASES(signed char, VT_CHAR)
-		default: break;
-		}
-		break;
-	case UK_SETCONST:
-	case UK_COPYCOL:
-		/* every listed row is active here, so both copy their source */
-		switch (u.type) {
-		case VT_INT64:
-		case VT_DOUBLE: p_copy<unsigned long long, R>(c, k); break;
-		case VT_CHAR: p_copy<unsigned char, R>(c, k); break;
-		default: p_copy<uint32_t, R>(c, k); break;
-		}
-		break;
-	default:
-		break;
+#define VGPU_PMATH_CASES(T, TY)                                             \
+	case H_MATH + TY * 4 + MO_ADD: p_math<T, MO_ADD, R>(rec, c); break;    \
+	case H_MATH + TY * 4 + MO_SUB: p_math<T, MO_SUB, R>(rec, c); break;    \
+	case H_MATH + TY * 4 + MO_MUL: p_math<T, MO_MUL, R>(rec, c); break;    \
+	case H_MATH + TY * 4 + MO_DIV: p_math<T, MO_DIV, R>(rec, c); break;
+	switch (rec.x & 0xffu) {
+		VGPU_PMATH_CASES(int32_t, VT_INT)
+		VGPU_PMATH_CASES(long long, VT_INT64)
+		VGPU_PMATH_CASES(float, VT_FLOAT)
+		VGPU_PMATH_CASES(double, VT_DOUBLE)
+		VGPU_PMATH_CASES(signed char, VT_CHAR)
+	/* every listed row is active here, so constants and columns are copies */
+	case H_SETCONST:
+	case H_COPY4: p_copy<uint32_t, R>(rec, c); break;
+	case H_COPY8: p_copy<unsigned long long, R>(rec, c); break;
+	case H_COPY1: p_copy<unsigned char, R>(rec, c); break;
+	default: break;
 	}
 #undef VGPU_PMATH_CASES
 }
@@ -835,20 +1007,23 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	}
 }
 
-/* ---- sequencer: counts -> tile offsets ----------------------------------- */
+/* ---- scanner: counts -> tile totals and in-tile offsets ------------------ */
 
+/* For each tile: wait for the compute warps' counts, one per 64 rows (a
+ * half of a warp's 128-row chunk), scan them in (chunk, warp, half) = row
+ * order, publish the tile's count to the query's look-back words, record
+ * valid rows per 64-row block when asked, and hand the total to the
+ * look-back warp.  At the end of the CTA's tiles it leaves
+ * the tile index in flags[3] for the look-back warp. */
 template <int THREADS, int R>
-__device__ void sequencer(const KParams &kp, unsigned char *smem, int lane)
+__device__ void scanner(const KParams &kp, unsigned char *smem, int lane)
 {
 	constexpr int NW = THREADS / 32;
-	constexpr int G = R * NW;
+	constexpr int G = R * NW / 2;  /* 64-row groups per tile */
 	constexpr int PER = (G + 31) / 32;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	uint64_t *offs = reinterpret_cast<uint64_t *>(smem + kOffOff);
+	volatile uint32_t *tot = reinterpret_cast<volatile uint32_t *>(smem + kOffTot);
 	const uint32_t nst = kp.nstages;
-	/* the previous tile of this CTA: a tile that directly follows it in the
-	 * same query starts where it ended, with no look-back */
-	uint64_t prev_work = ~0ull, prev_end = 0;
 	for (uint32_t i = 0;; i++) {
 		const uint32_t s = i % nst, q = i & 1u;
 		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + 2))
@@ -856,13 +1031,18 @@ __device__ void sequencer(const KParams &kp, unsigned char *smem, int lane)
 		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
 		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
 		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-		if (si.work >= kp.total_work)
+		if (si.work >= kp.total_work) {
+			__syncwarp();
+			if (lane == 0) {
+				flags[3] = i;
+				mbar_arrive(smem_addr(smem + kOffSready + 8 * q));
+			}
 			return;
+		}
 		if (!mbar_wait(smem_addr(smem + kOffCready + 8 * q), (i >> 1) & 1u, flags + 2))
 			return;
 		const uint32_t *cnt = reinterpret_cast<const uint32_t *>(smem + kOffCnt) + q * kMaxGroups;
 		uint32_t *pre = reinterpret_cast<uint32_t *>(smem + kOffPre) + q * kMaxGroups;
-		/* exclusive scan over groups in (row group, warp) = row order */
 		uint32_t local[PER];
 		uint32_t sum = 0;
 #pragma unroll
@@ -887,6 +1067,52 @@ __device__ void sequencer(const KParams &kp, unsigned char *smem, int lane)
 			run += local[x];
 		}
 		const uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
+		if (lane == 0)
+			publish_count(kp, Q, si.work, tile_total);
+		/* valid rows per 64-row block, for result-tablet splitting on the host */
+		if (Q.block_counts != nullptr) {
+			/* group g covers tile rows 64 g .. 64 g + 63 */
+			for (int g = lane; g < G; g += 32) {
+				const uint32_t local_row = 64u * (uint32_t)g;
+				if (local_row < si.nrows) {
+					const uint64_t blk =
+						(uint64_t)Q.segs[si.seg].block_base + (si.row0 + local_row) / 64;
+					Q.block_counts[blk] = (uint8_t)cnt[g];
+				}
+			}
+		}
+		__syncwarp();
+		if (lane == 0) {
+			tot[q] = tile_total;
+			mbar_arrive(smem_addr(smem + kOffSready + 8 * q));
+		}
+	}
+}
+
+/* ---- look-back warp: tile totals -> result offsets ----------------------- */
+
+template <int THREADS, int R>
+__device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
+{
+	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
+	const volatile uint32_t *tot = reinterpret_cast<const volatile uint32_t *>(smem + kOffTot);
+	uint64_t *offs = reinterpret_cast<uint64_t *>(smem + kOffOff);
+	const uint32_t nst = kp.nstages;
+	/* the previous tile of this CTA: a tile that directly follows it in the
+	 * same query starts where it ended, with no look-back */
+	uint64_t prev_work = ~0ull, prev_end = 0;
+	for (uint32_t i = 0;; i++) {
+		const uint32_t s = i % nst, q = i & 1u;
+		if (!mbar_wait(smem_addr(smem + kOffSready + 8 * q), (i >> 1) & 1u, flags + 2))
+			return;
+		if (flags[3] == i)
+			return;
+		/* the stage still holds tile i: it is released after the tile's
+		 * stores, which wait for this warp */
+		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
+		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
+		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+		const uint32_t tile_total = tot[q];
 		uint64_t excl = 0;
 		bool ok = true;
 		if (si.work == prev_work + 1 && si.work != Q.work_first) {
@@ -900,18 +1126,6 @@ __device__ void sequencer(const KParams &kp, unsigned char *smem, int lane)
 		}
 		prev_work = si.work;
 		prev_end = excl + tile_total;
-		/* valid rows per 64-row block, for result-tablet splitting on the host */
-		if (Q.block_counts != nullptr) {
-			for (int b = lane; b < R * (THREADS / 64); b += 32) {
-				const int r = b / (THREADS / 64), m = b % (THREADS / 64);
-				const uint32_t local_row = r * THREADS + m * 64;
-				if (local_row < si.nrows) {
-					const uint64_t blk =
-						(uint64_t)Q.segs[si.seg].block_base + (si.row0 + local_row) / 64;
-					Q.block_counts[blk] = (uint8_t)(cnt[r * NW + 2 * m] + cnt[r * NW + 2 * m + 1]);
-				}
-			}
-		}
 		__syncwarp();
 		if (lane == 0) {
 			if (!ok)
@@ -932,8 +1146,8 @@ __device__ void sequencer(const KParams &kp, unsigned char *smem, int lane)
 /* ---- compute warps: stores of a finished tile ---------------------------- */
 
 template <int THREADS, int R>
-__device__ __forceinline__ bool store_tile(const KParams &kp, unsigned char *smem, uint32_t p,
-	uint32_t nsel, int warp, int lane)
+__device__ __forceinline__ bool store_tile(const KParams &kp, unsigned char *smem, uint32_t sbase,
+	uint32_t p, uint32_t nsel, int warp, int lane)
 {
 	constexpr int NW = THREADS / 32;
 	constexpr int TILE = THREADS * R;
@@ -943,13 +1157,14 @@ __device__ __forceinline__ bool store_tile(const KParams &kp, unsigned char *sme
 		return false;
 	if (!flags[q])
 		return false;
-	const uint64_t off = reinterpret_cast<const uint64_t *>(smem + kOffOff)[q];
-	const uint32_t *pre = reinterpret_cast<const uint32_t *>(smem + kOffPre) + q * kMaxGroups;
-	const uint32_t stage_delta = s * kp.stage_bytes, vec_delta = q * kp.vec_bytes;
-	const QDesc &Q = *reinterpret_cast<const QDesc *>(smem + kp.stage_area + stage_delta);
-	const uint16_t *list = reinterpret_cast<const uint16_t *>(smem + kp.sel_area) + q * 2 * TILE +
-		warp * 32 * R;
-	const uint16_t *tag = list + TILE;
+	const uint64_t off = lds_u64(sbase + kOffOff + 8 * q);
+	const uint32_t sd = s * kp.stage_bytes;
+	const uint32_t qd = sbase + kp.stage_area + sd;
+	const uint32_t vd = q * lds_u32(qd + kQVecSlot);
+	const uint32_t list = sbase + kp.sel_area + (q * 2 * TILE + warp * 32 * R) * 2;
+	const uint32_t tag = list + TILE * 2;
+	const uint32_t pre = sbase + kOffPre + q * kMaxGroups * 4;
+	const uint64_t cap = lds_u64(qd + kQCapacity);
 	uint32_t row[R];
 	uint64_t pos[R];
 	bool overflow = false;
@@ -958,47 +1173,59 @@ __device__ __forceinline__ bool store_tile(const KParams &kp, unsigned char *sme
 		const uint32_t e = lane + 32 * i;
 		pos[i] = ~0ull;
 		row[i] = 0;
+		if (32u * i >= nsel)
+			continue;
 		if (e < nsel) {
-			row[i] = list[e];
-			const uint32_t t = tag[e];
-			pos[i] = off + pre[(t >> 5) * NW + warp] + (t & 31u);
-			if (pos[i] >= Q.capacity) {
+			row[i] = lds_u16(list + 2 * e);
+			/* tag: chunk and rank within the warp's chunk; the chunk's first
+			 * 64-row group holds its offset in the tile */
+			const uint32_t t = lds_u16(tag + 2 * e);
+			pos[i] = off + lds_u32(pre + 8 * ((t >> 7) * NW + warp)) + (t & 127u);
+			if (pos[i] >= cap) {
 				overflow = true;
 				pos[i] = ~0ull;
 			}
 		}
 	}
-	const uint32_t sel_base = warp * 32 * R;
-	const uint32_t nout = Q.prog.nout;
+	const uint32_t sel0 = warp * 32 * R + lane;
+	const uint32_t nout = lds_u32(qd + kQNOut);
 	for (uint32_t j = 0; j < nout; j++) {
-		const uint32_t od = Q.od_out[j];
-		void *out = Q.out_ptr[j];
-		switch (Q.prog.out_stride[j]) {
+		const uint32_t od = lds_u32(qd + kQOdOut + 4 * j);
+		void *out = reinterpret_cast<void *>(lds_u64(qd + kQOutPtr + 8 * j));
+		switch (lds_u8(qd + kQOutStride + j)) {
 		case 4: {
-			const Acc a = acc_of<uint32_t>(smem, od, stage_delta, vec_delta);
+			const Opnd a = opnd<4>(od, sbase, sd, vd);
 #pragma unroll
-			for (int i = 0; i < R; i++)
+			for (int i = 0; i < R; i++) {
+				if (32u * i >= nsel)
+					break;
 				if (pos[i] != ~0ull)
-					reinterpret_cast<uint32_t *>(out)[pos[i]] =
-						p_ld<uint32_t>(a, row[i], sel_base + lane + 32 * i);
+					reinterpret_cast<uint32_t *>(out)[pos[i]] = lds_u32(p_addr(a, row[i], sel0 + 32 * i));
+			}
 			break;
 		}
 		case 8: {
-			const Acc a = acc_of<unsigned long long>(smem, od, stage_delta, vec_delta);
+			const Opnd a = opnd<8>(od, sbase, sd, vd);
 #pragma unroll
-			for (int i = 0; i < R; i++)
+			for (int i = 0; i < R; i++) {
+				if (32u * i >= nsel)
+					break;
 				if (pos[i] != ~0ull)
 					reinterpret_cast<unsigned long long *>(out)[pos[i]] =
-						p_ld<unsigned long long>(a, row[i], sel_base + lane + 32 * i);
+						lds_u64(p_addr(a, row[i], sel0 + 32 * i));
+			}
 			break;
 		}
 		default: {
-			const Acc a = acc_of<unsigned char>(smem, od, stage_delta, vec_delta);
+			const Opnd a = opnd<1>(od, sbase, sd, vd);
 #pragma unroll
-			for (int i = 0; i < R; i++)
+			for (int i = 0; i < R; i++) {
+				if (32u * i >= nsel)
+					break;
 				if (pos[i] != ~0ull)
 					reinterpret_cast<unsigned char *>(out)[pos[i]] =
-						p_ld<unsigned char>(a, row[i], sel_base + lane + 32 * i);
+						(unsigned char)lds_u8(p_addr(a, row[i], sel0 + 32 * i));
+			}
 			break;
 		}
 		}
@@ -1012,12 +1239,14 @@ __device__ __forceinline__ bool store_tile(const KParams &kp, unsigned char *sme
 }
 
 template <int THREADS, int R>
-__global__ void __launch_bounds__(THREADS + 64) vm_kernel(const KParams kp)
+__global__ void __launch_bounds__(THREADS + 32 * kRoleWarps) vm_kernel(const KParams kp)
 {
 	constexpr int TILE = THREADS * R;
 	constexpr int NW = THREADS / 32;
-	constexpr int G = R * NW;
-	static_assert(R <= 32 && G <= (int)kMaxGroups, "row masks are 32-bit");
+	constexpr int C = R / 4;
+	static_assert(R % 4 == 0 && R <= 32, "rows per thread: whole 4-row chunks, 32-bit row masks");
+	static_assert(R * NW / 2 <= (int)kMaxGroups, "64-row groups per tile");
+	static_assert(TILE <= 65536, "tile rows are 16-bit in the selection lists");
 	extern __shared__ __align__(128) unsigned char smem[];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
@@ -1030,26 +1259,31 @@ __global__ void __launch_bounds__(THREADS + 64) vm_kernel(const KParams kp)
 		}
 		for (uint32_t q = 0; q < 2; q++) {
 			mbar_init(smem_addr(smem + kOffCready + 8 * q), NW);
+			mbar_init(smem_addr(smem + kOffSready + 8 * q), 1);
 			mbar_init(smem_addr(smem + kOffOready + 8 * q), 1);
 		}
 		flags[0] = flags[1] = flags[2] = 0;
-		reinterpret_cast<unsigned long long *>(smem + kOffAgg)[0] = 0ull;
-		reinterpret_cast<unsigned long long *>(smem + kOffAgg)[1] = 0ull;
+		flags[3] = ~0u;
 		for (uint32_t s = 0; s < kMaxStages; s++)
 			reinterpret_cast<uint32_t *>(smem + kOffHeld)[s] = ~0u;
 		fence_mbar_init();
 	}
 	__syncthreads();
+	if (warp == NW) {
+		scanner<THREADS, R>(kp, smem, lane);
+		return;
+	}
 	if (warp == NW + 1) {
 		producer<TILE>(kp, smem, lane);
 		return;
 	}
-	if (warp == NW) {
-		sequencer<THREADS, R>(kp, smem, lane);
+	if (warp == NW + 2) {
+		lookback_warp<THREADS, R>(kp, smem, lane);
 		return;
 	}
 
 	/* compute warps */
+	const uint32_t sbase = smem_addr(smem);
 	uint32_t prev_nsel = 0;
 	uint32_t i = 0;
 	for (;; i++) {
@@ -1061,88 +1295,110 @@ __global__ void __launch_bounds__(THREADS + 64) vm_kernel(const KParams kp)
 			}
 			return;
 		}
-		const uint32_t stage_delta = s * kp.stage_bytes, vec_delta = q * kp.vec_bytes;
-		unsigned char *hdr = smem + kp.stage_area + stage_delta;
-		const QDesc *Q = reinterpret_cast<const QDesc *>(hdr);
-		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-		if (si.work >= kp.total_work)
+		const uint32_t sd = s * kp.stage_bytes;
+		const uint32_t qd = sbase + kp.stage_area + sd;
+		const uint32_t sinfo = qd + (uint32_t)sizeof(QDesc);
+		if (lds_u32(sinfo + offsetof(StageInfo, work)) >= kp.total_work)
 			break;
+		const uint32_t nrows = lds_u32(sinfo + offsetof(StageInfo, nrows));
+		const uint32_t vd = q * lds_u32(qd + kQVecSlot);
 
 		/* ---- filter over every row */
 		RowState st;
 		st.valid = 0;
 #pragma unroll
-		for (int r = 0; r < R; r++)
-			if ((uint32_t)(r * THREADS + tid) < si.nrows)
-				st.valid |= 1u << r;
+		for (int c = 0; c < C; c++)
+#pragma unroll
+			for (int k = 0; k < 4; k++)
+				if (chunk_row<THREADS>(c, tid) + k < nrows)
+					st.valid |= 1u << (4 * c + k);
 		st.active = st.valid;
 #pragma unroll
 		for (int sl = 0; sl < kMaxSlots; sl++)
 			st.pend[sl] = 0;
+		const uint32_t ops = qd + kQOps;
+		const uint32_t nf = lds_u32(qd + kQNFilter);
 		{
-			FCtx fc{smem, Q, stage_delta, vec_delta, tid};
-			const uint32_t nf = Q->prog.nfilter;
-			for (uint32_t k = 0; k < nf; k++)
-				filter_op<THREADS, R>(fc, Q->prog.uops[k], k, st);
+			const FArgs f{sbase, sd, vd, tid};
+			uint4 rec = lds_v4(ops);
+			for (uint32_t k = 0; k < nf; k++) {
+				const uint4 cur = rec;
+				/* the next record's load overlaps this op */
+				rec = lds_v4(ops + 16u * min(k + 1u, (uint32_t)kMaxOps - 1u));
+				filter_op<THREADS, R>(cur, f, st);
+			}
 		}
 
-		/* ---- selection: ballots, this warp's list of valid rows */
-		uint16_t *list = reinterpret_cast<uint16_t *>(smem + kp.sel_area) + q * 2 * TILE +
-			warp * 32 * R;
-		uint16_t *tag = list + TILE;
-		uint32_t *cnt = reinterpret_cast<uint32_t *>(smem + kOffCnt) + q * kMaxGroups;
+		/* ---- selection: this warp's valid rows in row order, per 128-row
+		 * chunk from four bit-plane ballots (row k of each lane's 4) */
+		const uint32_t list = sbase + kp.sel_area + (q * 2 * TILE + warp * 32 * R) * 2;
+		const uint32_t tag = list + TILE * 2;
+		const uint32_t cnt = sbase + kOffCnt + q * kMaxGroups * 4;
 		uint32_t nsel = 0;
 		{
 			const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-			for (int r = 0; r < R; r++) {
-				const uint32_t bal = __ballot_sync(0xffffffffu, (st.valid >> r) & 1u);
-				if ((st.valid >> r) & 1u) {
-					const uint32_t rank = __popc(bal & lt);
-					list[nsel + rank] = (uint16_t)(r * THREADS + tid);
-					/* group and rank: the entry's place in the result */
-					tag[nsel + rank] = (uint16_t)(r * 32 + rank);
+			for (int c = 0; c < C; c++) {
+				const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
+				const uint32_t b0 = __ballot_sync(0xffffffffu, m & 1u);
+				const uint32_t b1 = __ballot_sync(0xffffffffu, m & 2u);
+				const uint32_t b2 = __ballot_sync(0xffffffffu, m & 4u);
+				const uint32_t b3 = __ballot_sync(0xffffffffu, m & 8u);
+				const uint32_t total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+				if (lane == 0) {
+					/* lanes 0-15 hold the chunk's first 64 rows */
+					const uint32_t h0 = __popc(b0 & 0xffffu) + __popc(b1 & 0xffffu) +
+						__popc(b2 & 0xffffu) + __popc(b3 & 0xffffu);
+					sts_u32(cnt + 8 * (c * NW + warp), h0);
+					sts_u32(cnt + 8 * (c * NW + warp) + 4, total - h0);
 				}
-				nsel += __popc(bal);
-				if (lane == 0)
-					cnt[r * NW + warp] = __popc(bal);
+				if (total) {
+					uint32_t rank = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
+					const uint32_t row0 = chunk_row<THREADS>(c, tid);
+#pragma unroll
+					for (int k = 0; k < 4; k++)
+						if ((m >> k) & 1u) {
+							sts_u16(list + 2 * (nsel + rank), row0 + k);
+							/* chunk and rank: the entry's place in the result */
+							sts_u16(tag + 2 * (nsel + rank), ((uint32_t)c << 7) | rank);
+							rank++;
+						}
+				}
+				nsel += total;
 			}
 		}
 		__syncwarp();
-		if (lane == 0) {
-			/* the last warp to add its count publishes the tile's total; the
-			 * counter is next used two tiles on, after the sequencer has
-			 * consumed this tile, so the last warp can clear it */
-			unsigned long long *agg = reinterpret_cast<unsigned long long *>(smem + kOffAgg) + q;
-			const unsigned long long old = atomicAdd(agg, (1ull << 32) | nsel);
-			if ((uint32_t)(old >> 32) == NW - 1) {
-				*agg = 0ull;
-				publish_count(kp, *Q, si.work, (uint32_t)old + nsel);
-			}
+		if (lane == 0)
 			mbar_arrive(smem_addr(smem + kOffCready + 8 * q));
-		}
+
+		/* ---- stores of the previous tile, whose offset is resolved by now;
+		 * before this tile's projection, which reuses the selection vectors */
+		if (i > 0 && !store_tile<THREADS, R>(kp, smem, sbase, i - 1, prev_nsel, warp, lane))
+			return;
+		prev_nsel = nsel;
 
 		/* ---- projection over this warp's selection list */
 		{
-			PCtx<R> pc{smem, Q, stage_delta, vec_delta, nsel, (uint32_t)(warp * 32 * R), lane, {}};
+			PArgs<R> pc;
+			pc.sbase = sbase;
+			pc.sd = sd;
+			pc.vd = vd;
+			pc.n = nsel;
+			pc.sel0 = (uint32_t)(warp * 32 * R + lane);
+			pc.lane = (uint32_t)lane;
 #pragma unroll
 			for (int x = 0; x < R; x++) {
 				const uint32_t e = lane + 32 * x;
-				pc.row[x] = e < nsel ? list[e] : 0u;
+				pc.row[x] = e < nsel ? lds_u16(list + 2 * e) : 0u;
 			}
-			const uint32_t nu = Q->prog.nuops - 1;
-			for (uint32_t k = Q->prog.nfilter; k < nu; k++)
-				project_op<R>(pc, Q->prog.uops[k], k);
+			const uint32_t nu = lds_u32(qd + kQNUops) - 1u;
+			for (uint32_t k = nf; k < nu; k++)
+				project_op<R>(lds_v4(ops + 16u * k), pc);
 		}
 		__syncwarp();
-
-		/* ---- stores of the previous tile, whose offset is resolved by now */
-		if (i > 0 && !store_tile<THREADS, R>(kp, smem, i - 1, prev_nsel, warp, lane))
-			return;
-		prev_nsel = nsel;
 	}
 	if (i > 0)
-		store_tile<THREADS, R>(kp, smem, i - 1, prev_nsel, warp, lane);
+		store_tile<THREADS, R>(kp, smem, sbase, i - 1, prev_nsel, warp, lane);
 }
 
 /* ---- host-side launcher ------------------------------------------------ */
@@ -1153,8 +1409,8 @@ static int launch_t(const KParams &kp, unsigned grid, size_t smem, cudaStream_t 
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	/* THREADS compute threads, the sequencer warp and the producer warp */
-	fn<<<grid, THREADS + 64, smem, stream>>>(kp);
+	/* THREADS compute threads and the scanner, producer and look-back warps */
+	fn<<<grid, THREADS + 32 * kRoleWarps, smem, stream>>>(kp);
 	return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1164,7 +1420,7 @@ static int occ_t(size_t smem, int *ctas)
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 64, smem) == cudaSuccess;
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * kRoleWarps, smem) == cudaSuccess;
 }
 
 #define VGPU_SHAPES(X) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
