@@ -50,13 +50,12 @@ static int type_bytes(int t)
 	} while (0)
 
 /* smem bytes a program needs per stage and for its register vectors.
- * Vectors indexed by tile row (written by the filter) get two slots, one per
- * tile in flight, since a tile's filter runs while the previous tile's rows
- * are still to be stored; vectors indexed by selection position (written
- * only by the projection, after the previous tile's stores) get one.  The
- * vector region of a launch is [row slot 0 | row slot 1 | selection
- * vectors], sized for the largest of its programs, so that one query's row
- * slot never overlaps another's selection vectors. */
+ * Vectors indexed by tile row (written by the filter) get kSlots slots, one
+ * per tile in flight between filter and stores; vectors indexed by
+ * selection position (written and read only by the projection warps) get
+ * one.  The vector region of a launch is [row slots | selection vectors],
+ * sized for the largest of its programs, so that one query's row slot never
+ * overlaps another's selection vectors. */
 void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
 	uint32_t *row_bytes, uint32_t *sel_bytes)
 {
@@ -84,7 +83,7 @@ void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_
  * are row_slot bytes apart */
 void vec_offsets(const Program &P, unsigned tile, uint32_t row_slot, uint32_t *vec_off)
 {
-	uint32_t r = 0, s = 2 * row_slot;
+	uint32_t r = 0, s = kSlots * row_slot;
 	for (unsigned i = 0; i < P.nvec; i++) {
 		const uint32_t sz = (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
 		if (P.vec_compact[i]) {
@@ -111,27 +110,28 @@ void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uin
 	}
 	*stage_bytes = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
 	*row_slot = row;
-	*vec_bytes = 2 * row + sel;
+	*vec_bytes = kSlots * row + sel;
 }
 
 /* header | stages x stage bytes | register vectors | selection lists */
 size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes)
 {
-	/* the selection lists (a tile row and a (group, rank) tag per entry) are
-	 * double-buffered: a tile's list is built before the previous tile's
-	 * rows are stored */
+	/* a selection list (a tile row per selected row) per slot: a tile's list
+	 * is built while earlier tiles' are projected */
 	return kSmemHeader + (size_t)s.stages * stage_bytes + (size_t)vec_bytes +
-		2 * align_up((size_t)s.tile() * 2 * sizeof(uint16_t), 128);
+		kSlots * align_up((size_t)s.tile() * sizeof(uint16_t), 128);
 }
 
 int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, Shape *out,
 	size_t *smem_out, uint32_t *stage_out, uint32_t *vec_out)
 {
-	/* first choice: a shape that keeps two CTAs resident per SM, so one CTA's
-	 * barriers and look-back waits overlap the other's work */
-	static const unsigned cand[][2] = {{256, 4}, {128, 8}, {256, 8}, {512, 4}};
+	/* first choice: one CTA per SM with 2048-row tiles and three stages (a
+	 * tile's fixed costs - claim, look-back, barriers - spread over many
+	 * rows, and loads in flight while two tiles are processed); then
+	 * smaller tiles for programs whose staging does not fit */
+	static const unsigned cand[][2] = {{512, 4}, {256, 8}, {256, 4}, {128, 8}};
 	const size_t limit = (size_t)e->smem_optin;
-	for (int pass = 0; pass < 2; pass++)
+	for (int pass = 1; pass < 2; pass++)
 	for (auto &c : cand) {
 		Shape s;
 		s.threads = e->pref.threads ? e->pref.threads : c[0];
@@ -188,19 +188,23 @@ static int ensure_blob(virg_gpu_engine *e, size_t n)
 	return 1;
 }
 
-/* the kernel's handler code for a uop */
-static uint32_t op_handler(const UOp &u)
+/* the head word of a uop's record (one-hot kind, type and operator) */
+static uint32_t op_head(const UOp &u)
 {
+	uint32_t kind = 0;
 	switch (u.kind) {
-	case UK_CMP: return H_CMP + u.type * 8u + u.sub;
-	case UK_MATH: return H_MATH + u.type * 4u + u.sub;
-	case UK_NOT: return H_NOT + u.type;
-	case UK_INVALID: return H_INVALID;
-	case UK_SETCONST: return H_SETCONST;
-	case UK_COPYCOL:
-		return (u.type == VT_INT64 || u.type == VT_DOUBLE) ? H_COPY8 : u.type == VT_CHAR ? H_COPY1 : H_COPY4;
-	default: return H_NOP;
+	case UK_CMP: kind = OK_CMP; break;
+	case UK_MATH: kind = OK_MATH; break;
+	case UK_NOT: kind = OK_NOT; break;
+	case UK_INVALID: kind = OK_INVALID; break;
+	case UK_SETCONST: kind = OK_SETCONST; break;
+	case UK_COPYCOL: kind = OK_COPY; break;
+	default: break;
 	}
+	const bool has_op = u.kind == UK_CMP || u.kind == UK_MATH;
+	return kind | (1u << (OT_SHIFT + u.type)) | (has_op ? 1u << (OO_SHIFT + u.sub) : 0u) |
+		((uint32_t)(u.tslot & 7u) << OPH_SLOT_SHIFT) | (u.vjump ? OPH_VJUMP : 0u) |
+		((u.flags & UF_SINGLE_DEF) ? OPH_SINGLE_DEF : 0u) | ((uint32_t)u.join << OPH_JOIN_SHIFT);
 }
 
 /* operand descriptors of a query descriptor whose program, load_off and
@@ -220,8 +224,7 @@ void fill_operands(QDesc &d, uint32_t vec_area)
 	for (uint32_t k = 0; k < P.nuops; k++) {
 		const UOp &u = P.uops[k];
 		OpRec &r = d.ops[k];
-		r.head = op_handler(u) | ((uint32_t)(u.tslot & 15u) << 8) | (u.vjump ? OPH_VJUMP : 0u) |
-			((u.flags & UF_SINGLE_DEF) ? OPH_SINGLE_DEF : 0u) | ((uint32_t)u.join << 16);
+		r.head = op_head(u);
 		r.a = od(u.a_cls, u.a_idx);
 		r.b = od(u.b_cls, u.b_idx);
 		r.d = od(OC_VEC, u.dst);

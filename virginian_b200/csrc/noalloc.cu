@@ -114,7 +114,7 @@ int pick_shape(const Program &P, int smem_optin, Shape *shape, size_t *smem, uin
 				Shape s = {c[0], c[1], st, 0};
 				uint32_t sb, rb, selb;
 				program_layout(P, s.tile(), nullptr, &sb, &rb, &selb);
-				const uint32_t vb = 2 * rb + selb;
+				const uint32_t vb = kSlots * rb + selb;
 				sb = ((sb < 128 ? 128 : sb) + 127) / 128 * 128;
 				const size_t need = smem_for(s, sb, vb);
 				if (need <= (pass == 0 ? limit / 2 - 1024 : limit)) {

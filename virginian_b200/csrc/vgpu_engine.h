@@ -49,6 +49,10 @@ struct StageInfo {
 
 /* every stage starts with a copy of its tile's query descriptor and the tile's
  * StageInfo, then the staged columns */
+/* tiles in flight between the filter and the stores of a CTA: slots of the
+ * selection lists, row vectors, counts and offsets */
+constexpr unsigned kSlots = 3;
+
 constexpr unsigned kStageHdr = (unsigned)((sizeof(QDesc) + sizeof(StageInfo) + 127) / 128 * 128);
 
 /* kernel arguments */

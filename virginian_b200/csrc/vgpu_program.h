@@ -107,26 +107,30 @@ constexpr uint32_t OD_SCALAR = 3u << 30;   /* scalar register */
 constexpr uint32_t OD_OFFSET = (1u << 30) - 1;
 
 /* one interpreted op as the kernel reads it: a single 16-byte record, so a
- * warp fetches everything an op needs with one shared-memory load.
- * head: bits [0,8) handler, [8,12) pending-target slot, bit 12 validity kept
- * on jump, bit 13 single definition, [16,24) slots joined at this op */
+ * warp fetches everything an op needs with one shared-memory load */
 struct alignas(16) OpRec {
 	uint32_t head;
 	uint32_t a, b, d;  /* operand descriptors: source a, source b, destination */
 };
 
-/* handlers: one code per (kind, type, operator) */
-constexpr uint32_t H_NOP = 0;
-constexpr uint32_t H_CMP = 1;        /* + type * 8 + CmpOp      (1..40) */
-constexpr uint32_t H_MATH = 41;      /* + type * 4 + MathOp     (41..60) */
-constexpr uint32_t H_NOT = 61;       /* + type                  (61..65) */
-constexpr uint32_t H_INVALID = 66;
-constexpr uint32_t H_SETCONST = 67;  /* 4-byte Integer/Float */
-constexpr uint32_t H_COPY4 = 68;     /* Column/Rowid copies by element size */
-constexpr uint32_t H_COPY8 = 69;
-constexpr uint32_t H_COPY1 = 70;
-constexpr uint32_t OPH_SINGLE_DEF = 1u << 13;
-constexpr uint32_t OPH_VJUMP = 1u << 12;
+/* The head's fields are one-hot, so the kernel picks an op's code with a few
+ * uniform bit-test branches instead of an indirect jump through a table:
+ * bits [0,6) kind, [6,11) operand type (bit OT_SHIFT + VType), [11,19)
+ * operator (bit OO_SHIFT + CmpOp or MathOp), [19,22) pending-target slot,
+ * bit 22 validity kept on jump, bit 23 single definition, [24,32) slots
+ * joined at this op. */
+constexpr uint32_t OK_CMP = 1u << 0;       /* Le..Neq, And, Or */
+constexpr uint32_t OK_MATH = 1u << 1;      /* Add/Sub/Mul/Div */
+constexpr uint32_t OK_NOT = 1u << 2;
+constexpr uint32_t OK_INVALID = 1u << 3;
+constexpr uint32_t OK_SETCONST = 1u << 4;  /* 4-byte Integer/Float */
+constexpr uint32_t OK_COPY = 1u << 5;      /* Column/Rowid into a register vector */
+constexpr uint32_t OT_SHIFT = 6;
+constexpr uint32_t OO_SHIFT = 11;
+constexpr uint32_t OPH_SLOT_SHIFT = 19;
+constexpr uint32_t OPH_VJUMP = 1u << 22;
+constexpr uint32_t OPH_SINGLE_DEF = 1u << 23;
+constexpr uint32_t OPH_JOIN_SHIFT = 24;
 
 /* one resident segment (tablet) on the device */
 struct SegDesc {

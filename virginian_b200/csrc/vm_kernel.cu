@@ -12,27 +12,26 @@
  *    tile's columns (plus the query's descriptor when the stage does not hold
  *    it) into a ring of shared-memory stages with TMA bulk copies
  *    (cp.async.bulk completing on the stage's full barrier);
- *  - compute warps: filter every row of the tile (row state as bit masks:
- *    valid, active, and rows parked at pending jump targets), compact each
- *    warp's valid rows into a selection list (__ballot_sync/__popc), run the
- *    projection (result expressions) on listed rows only, then store the
- *    previous tile's rows at their final positions and release its stage.
- *    Each op is one 16-byte record fetched with a single shared-memory load
- *    and dispatched on one handler code; operands are read and written by
- *    32-bit shared-memory address;
- *  - scanner warp: scans each tile's (row group, warp) counts and publishes
- *    the tile's count to the query's look-back words as soon as the ballots
- *    are done;
+ *  - filter warps (THREADS threads): run the filter ops over every row of the
+ *    tile (row state as bit masks: valid, active, and rows parked at pending
+ *    jump targets; each lane holds R rows in chunks of 4 consecutive rows),
+ *    count valid rows per 64 rows with bit-plane ballots, scan the counts and
+ *    write the tile's selected rows, in row order, to a shared list, then
+ *    publish the tile's count to the query's look-back words;
  *  - look-back warp: resolves the tile's position in the query's result with
  *    a warp-wide decoupled look-back over earlier tiles (32 status words per
- *    round), one tile ahead of the stores, so cross-CTA waits overlap
- *    computation.  A tile that directly follows the CTA's previous tile of
- *    the same query starts where that one ended, with no look-back.
+ *    round); a tile that directly follows the CTA's previous tile of the same
+ *    query starts where that one ended, with no look-back;
+ *  - projection warps: run the projection ops over the tile's list in
+ *    32-entry batches and write each result row to the tile's offset plus
+ *    its list position (coalesced stores), then release the stage.
  *
- * Rows land in original row order (the single-core CPU VM's order,
- * src/vm/virginia.c:476-578) with plain stores; no output atomics.
- * Arithmetic matches the CPU VM bit for bit: float/double use the _rn
- * intrinsics (no FMA contraction, IEEE division) and x86 NaN results,
+ * Each op is one 16-byte record fetched with a single shared-memory load and
+ * dispatched on one handler code; operands are read and written by 32-bit
+ * shared-memory address.  Rows land in original row order (the single-core
+ * CPU VM's order, src/vm/virginia.c:476-578) with plain stores; no output
+ * atomics.  Arithmetic matches the CPU VM bit for bit: float/double use the
+ * _rn intrinsics (no FMA contraction, IEEE division) and x86 NaN results,
  * integers wrap as on x86.  Every wait is bounded; on expiry the kernel
  * records an error code and stops instead of hanging.
  */
@@ -46,32 +45,33 @@
 
 namespace vgpu {
 
-/* bounded waits: iterations of ~100 ns and more, far beyond any real wait */
-constexpr unsigned kStageSpinLimit = 1u << 24;
+/* bounded waits: a stage or offset wait gives up after about a second, far
+ * beyond any real wait; look-back polls after 2^24 rounds of 32-256 ns */
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+constexpr uint32_t kSuspendHintNs = 20000;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
 /* work items claimed per atomic by the producer: one, so tiles that follow
  * each other in a query are taken, and finished, at about the same time */
 constexpr unsigned kClaim = 1;
 
-/* warps besides the compute warps: scanner, producer, look-back */
-constexpr int kRoleWarps = 3;
-
 /* shared memory header (kSmemHeader bytes) */
 constexpr unsigned kMaxGroups = 128;  /* R x warps */
 constexpr unsigned kOffFull = 0;                            /* mbarrier[kMaxStages] */
 constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;   /* mbarrier[kMaxStages] */
-constexpr unsigned kOffCready = kOffEmpty + 8 * kMaxStages; /* mbarrier[2]: counts ready */
-constexpr unsigned kOffSready = kOffCready + 16;            /* mbarrier[2]: scan done */
-constexpr unsigned kOffOready = kOffSready + 16;            /* mbarrier[2]: offsets ready */
-constexpr unsigned kOffOff = kOffOready + 16;               /* uint64[2]: tile offsets */
-constexpr unsigned kOffFlags = kOffOff + 16;                /* uint32[4]: ok[2], abort */
-constexpr unsigned kOffTot = kOffFlags + 16;                /* uint32[2]: tile totals */
-constexpr unsigned kOffHeld = kOffTot + 8;                  /* uint32[kMaxStages]: query per stage */
-constexpr unsigned kOffCnt = 256;                           /* uint32[2][kMaxGroups] */
-constexpr unsigned kOffPre = kOffCnt + 8 * kMaxGroups;      /* uint32[2][kMaxGroups] */
+constexpr unsigned kOffLready = kOffEmpty + 8 * kMaxStages; /* mbarrier[kSlots]: list and count ready */
+constexpr unsigned kOffOready = kOffLready + 8 * kSlots;     /* mbarrier[kSlots]: offset ready */
+constexpr unsigned kOffLfree = kOffOready + 8 * kSlots;      /* mbarrier[kSlots]: projection done */
+constexpr unsigned kOffCdone = kOffLfree + 8 * kSlots;       /* mbarrier[kSlots]: all counts written */
+constexpr unsigned kOffOff = kOffCdone + 8 * kSlots;         /* uint64[kSlots]: tile offsets */
+constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;         /* uint32[8]: ok[kSlots], abort, end tile */
+constexpr unsigned kOffTot = kOffFlags + 32;                 /* uint32[kSlots]: tile totals */
+constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;          /* uint32[kMaxStages]: query per stage */
+constexpr unsigned kOffCnt = 512;                            /* uint32[kSlots][kMaxGroups]: per 64 rows */
+constexpr unsigned kFAbort = 4, kFEnd = 5;                   /* flag words */
+static_assert(kSlots <= kFAbort, "ok flags per slot");
 static_assert(kOffHeld + 4 * kMaxStages <= kOffCnt, "smem header layout");
-static_assert(kOffPre + 8 * kMaxGroups <= kSmemHeader, "smem header overflow");
+static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
 static_assert(sizeof(QDesc) % 16 == 0, "QDesc copies in 16-byte chunks");
 static_assert(kStageHdr >= sizeof(QDesc) + sizeof(StageInfo), "stage header too small");
 static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a time");
@@ -164,19 +164,48 @@ __device__ __forceinline__ void report(unsigned *error, unsigned code)
 	atomicCAS(error, 0u, code);
 }
 
-/* bounded wait for an mbarrier phase; false on timeout or when the CTA's
- * abort flag is set */
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+	uint64_t t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+/* try_wait that suspends the thread until the phase completes or about
+ * hint_ns pass, so a waiting warp takes no issue slots meanwhile */
+__device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t phase, uint32_t hint_ns)
+{
+	uint32_t ok;
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+		"selp.u32 %0, 1, 0, p;\n\t}"
+		: "=r"(ok)
+		: "r"(bar), "r"(phase), "r"(hint_ns)
+		: "memory");
+	return ok != 0;
+}
+
+/* bounded wait for an mbarrier phase; false on timeout (about a second) or
+ * when the CTA's abort flag (a shared-memory word, if given) is set */
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const volatile uint32_t *abort)
 {
-	for (unsigned i = 0; i < kStageSpinLimit; i++) {
-		if (mbar_try_wait(bar, phase))
+	if (mbar_try_wait(bar, phase))
+		return true;
+	const uint32_t abort_addr = abort ? smem_addr(const_cast<const uint32_t *>(abort)) : 0u;
+	const uint64_t t0 = globaltimer_ns();
+	for (;;) {
+		if (mbar_try_wait_hint(bar, phase, kSuspendHintNs))
 			return true;
-		if (abort && *abort)
+		if (abort_addr) {
+			uint32_t v;
+			asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(abort_addr));
+			if (v)
+				return false;
+		}
+		if (globaltimer_ns() - t0 > kWaitLimitNs)
 			return false;
-		if (i > 8)
-			__nanosleep(i < 64 ? 32 : 128);
 	}
-	return false;
 }
 
 /* ---- shared-memory access by 32-bit shared address ---------------------
@@ -453,7 +482,7 @@ __device__ __forceinline__ void take_jump(RowState &st, uint32_t head, uint32_t 
 	st.active &= ~jumped;
 	if (!(head & OPH_VJUMP))
 		st.valid &= ~jumped;
-	const uint32_t slot = (head >> 8) & 15u;
+	const uint32_t slot = (head >> OPH_SLOT_SHIFT) & 7u;
 #pragma unroll
 	for (int s = 0; s < kMaxSlots; s++)
 		if (slot == (uint32_t)s)
@@ -622,10 +651,40 @@ __device__ __forceinline__ void f_copy(const uint4 &rec, const FArgs &f)
 	store_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.w, f.sbase, f.sd, f.vd).addr, f.tid, x, 0xffffffffu);
 }
 
+/* operand type and operator tests on a record head */
+__device__ __forceinline__ bool h_type(uint32_t h, int t) { return (h >> (OT_SHIFT + t)) & 1u; }
+__device__ __forceinline__ bool h_op(uint32_t h, int o) { return (h >> (OO_SHIFT + o)) & 1u; }
+
+template <typename T, int THREADS, int R>
+__device__ __forceinline__ void f_cmp_any(const uint4 &rec, const FArgs &f, RowState &st)
+{
+	const uint32_t h = rec.x;
+	if (h_op(h, CO_LT)) f_cmp<T, CO_LT, THREADS, R>(rec, f, st);
+	else if (h_op(h, CO_GT)) f_cmp<T, CO_GT, THREADS, R>(rec, f, st);
+	else if (h_op(h, CO_LE)) f_cmp<T, CO_LE, THREADS, R>(rec, f, st);
+	else if (h_op(h, CO_GE)) f_cmp<T, CO_GE, THREADS, R>(rec, f, st);
+	else if (h_op(h, CO_EQ)) f_cmp<T, CO_EQ, THREADS, R>(rec, f, st);
+	else if (h_op(h, CO_NEQ)) f_cmp<T, CO_NEQ, THREADS, R>(rec, f, st);
+	else if (h_op(h, CO_AND)) f_cmp<T, CO_AND, THREADS, R>(rec, f, st);
+	else f_cmp<T, CO_OR, THREADS, R>(rec, f, st);
+}
+
+template <typename T, int THREADS, int R>
+__device__ __forceinline__ void f_math_any(const uint4 &rec, const FArgs &f, const RowState &st)
+{
+	const uint32_t h = rec.x;
+	if (h_op(h, MO_ADD)) f_math<T, MO_ADD, THREADS, R>(rec, f, st);
+	else if (h_op(h, MO_SUB)) f_math<T, MO_SUB, THREADS, R>(rec, f, st);
+	else if (h_op(h, MO_MUL)) f_math<T, MO_MUL, THREADS, R>(rec, f, st);
+	else f_math<T, MO_DIV, THREADS, R>(rec, f, st);
+}
+
+/* one filter op: kind, then type, then operator, each by bit tests */
 template <int THREADS, int R>
 __device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowState &st)
 {
-	const uint32_t join = (rec.x >> 16) & 0xffu;
+	const uint32_t h = rec.x;
+	const uint32_t join = h >> OPH_JOIN_SHIFT;
 	if (join) {
 #pragma unroll
 		for (int s = 0; s < kMaxSlots; s++)
@@ -634,123 +693,107 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowS
 				st.pend[s] = 0;
 			}
 	}
-#define VGPU_CMP_CASES(T, TY)                                                            \
-	case H_CMP + TY * 8 + CO_LE: f_cmp<T, CO_LE, THREADS, R>(rec, f, st); break;        \
-	case H_CMP + TY * 8 + CO_LT: f_cmp<T, CO_LT, THREADS, R>(rec, f, st); break;        \
-	case H_CMP + TY * 8 + CO_GE: f_cmp<T, CO_GE, THREADS, R>(rec, f, st); break;        \
-	case H_CMP + TY * 8 + CO_GT: f_cmp<T, CO_GT, THREADS, R>(rec, f, st); break;        \
-	case H_CMP + TY * 8 + CO_EQ: f_cmp<T, CO_EQ, THREADS, R>(rec, f, st); break;        \
-	case H_CMP + TY * 8 + CO_NEQ: f_cmp<T, CO_NEQ, THREADS, R>(rec, f, st); break;      \
-	case H_CMP + TY * 8 + CO_AND: f_cmp<T, CO_AND, THREADS, R>(rec, f, st); break;      \
-	case H_CMP + TY * 8 + CO_OR: f_cmp<T, CO_OR, THREADS, R>(rec, f, st); break;
-#define VGPU_MATH_CASES(T, TY)                                                        \
-	case H_MATH + TY * 4 + MO_ADD: f_math<T, MO_ADD, THREADS, R>(rec, f, st); break; \
-	case H_MATH + TY * 4 + MO_SUB: f_math<T, MO_SUB, THREADS, R>(rec, f, st); break; \
-	case H_MATH + TY * 4 + MO_MUL: f_math<T, MO_MUL, THREADS, R>(rec, f, st); break; \
-	case H_MATH + TY * 4 + MO_DIV: f_math<T, MO_DIV, THREADS, R>(rec, f, st); break;
-	switch (rec.x & 0xffu) {
-		VGPU_CMP_CASES(int32_t, VT_INT)
-		VGPU_CMP_CASES(long long, VT_INT64)
-		VGPU_CMP_CASES(float, VT_FLOAT)
-		VGPU_CMP_CASES(double, VT_DOUBLE)
-		VGPU_CMP_CASES(signed char, VT_CHAR)
-		VGPU_MATH_CASES(int32_t, VT_INT)
-		VGPU_MATH_CASES(long long, VT_INT64)
-		VGPU_MATH_CASES(float, VT_FLOAT)
-		VGPU_MATH_CASES(double, VT_DOUBLE)
-		VGPU_MATH_CASES(signed char, VT_CHAR)
-	case H_NOT + VT_INT: f_not<int32_t, THREADS, R>(rec, f, st); break;
-	case H_NOT + VT_INT64: f_not<long long, THREADS, R>(rec, f, st); break;
-	case H_NOT + VT_FLOAT: f_not<float, THREADS, R>(rec, f, st); break;
-	case H_NOT + VT_DOUBLE: f_not<double, THREADS, R>(rec, f, st); break;
-	case H_NOT + VT_CHAR: f_not<signed char, THREADS, R>(rec, f, st); break;
-	case H_INVALID: st.valid &= ~st.active; break;
-	case H_SETCONST: f_setconst<THREADS, R>(rec, f, st); break;
-	case H_COPY4: f_copy<uint32_t, THREADS, R>(rec, f); break;
-	case H_COPY8: f_copy<unsigned long long, THREADS, R>(rec, f); break;
-	case H_COPY1: f_copy<unsigned char, THREADS, R>(rec, f); break;
-	default: break;
+	if (h & OK_CMP) {
+		if (h_type(h, VT_FLOAT)) f_cmp_any<float, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_INT)) f_cmp_any<int32_t, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_DOUBLE)) f_cmp_any<double, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_INT64)) f_cmp_any<long long, THREADS, R>(rec, f, st);
+		else f_cmp_any<signed char, THREADS, R>(rec, f, st);
+	} else if (h & OK_INVALID) {
+		st.valid &= ~st.active;
+	} else if (h & OK_MATH) {
+		if (h_type(h, VT_FLOAT)) f_math_any<float, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_INT)) f_math_any<int32_t, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_DOUBLE)) f_math_any<double, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_INT64)) f_math_any<long long, THREADS, R>(rec, f, st);
+		else f_math_any<signed char, THREADS, R>(rec, f, st);
+	} else if (h & OK_NOT) {
+		if (h_type(h, VT_FLOAT)) f_not<float, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_INT)) f_not<int32_t, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_DOUBLE)) f_not<double, THREADS, R>(rec, f, st);
+		else if (h_type(h, VT_INT64)) f_not<long long, THREADS, R>(rec, f, st);
+		else f_not<signed char, THREADS, R>(rec, f, st);
+	} else if (h & OK_SETCONST) {
+		f_setconst<THREADS, R>(rec, f, st);
+	} else if (h & OK_COPY) {
+		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) f_copy<unsigned long long, THREADS, R>(rec, f);
+		else if (h_type(h, VT_CHAR)) f_copy<unsigned char, THREADS, R>(rec, f);
+		else f_copy<uint32_t, THREADS, R>(rec, f);
 	}
-#undef VGPU_CMP_CASES
-#undef VGPU_MATH_CASES
 }
 
-/* ---- projection: only the rows in the warp's selection list ------------- */
+/* ---- projection: the tile's selected rows, in row order ------------------
+ * The projection warps share the tile's list: warp p takes the 32-entry
+ * batches p, p + P, p + 2 P, ...; entry e is selection index e and its
+ * result row lands at the tile's offset + e. */
 
-/* lane `lane` of a warp handles the warp's selection entries lane + 32 i,
- * i < R; their tile rows are held in registers for the whole projection */
-template <int R>
 struct PArgs {
 	uint32_t sbase, sd, vd;
-	uint32_t n;     /* entries in the warp's list */
-	uint32_t sel0;  /* selection index of this lane's first entry */
-	uint32_t lane;
-	uint32_t row[R];
+	uint32_t list;   /* smem address of the tile's list of tile rows (u16) */
+	uint32_t n;      /* entries */
+	uint32_t e0;     /* this lane's first entry */
+	uint32_t step;   /* entries between this lane's entries: 32 P */
 };
 
-/* element address of a selection entry */
-__device__ __forceinline__ uint32_t p_addr(const Opnd &o, uint32_t row, uint32_t sidx)
+/* element address of a list entry */
+__device__ __forceinline__ uint32_t p_addr(const Opnd &o, uint32_t row, uint32_t e)
 {
-	return o.addr + (o.sel ? sidx : row) * o.step;
+	return o.addr + (o.sel ? e : row) * o.step;
 }
 
-template <typename T, int OP, int R>
-__device__ __forceinline__ void p_math(const uint4 &rec, const PArgs<R> &c)
+template <typename T, int OP>
+__device__ __forceinline__ void p_math(const uint4 &rec, const PArgs &c)
 {
 	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
 	const Opnd b = opnd<sizeof(T)>(rec.z, c.sbase, c.sd, c.vd);
 	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
-#pragma unroll
-	for (int i = 0; i < R; i++) {
-		if (32u * i >= c.n)
-			break;
-		if (c.lane + 32u * i < c.n) {
-			const uint32_t si = c.sel0 + 32u * i;
-			const T x = SM<T>::ld(p_addr(a, c.row[i], si));
-			const T y = SM<T>::ld(p_addr(b, c.row[i], si));
-			SM<T>::st(p_addr(d, c.row[i], si), Math<T, OP>::eval(x, y));
-		}
+	for (uint32_t e = c.e0; e < c.n; e += c.step) {
+		const uint32_t row = lds_u16(c.list + 2 * e);
+		const T x = SM<T>::ld(p_addr(a, row, e));
+		const T y = SM<T>::ld(p_addr(b, row, e));
+		SM<T>::st(p_addr(d, row, e), Math<T, OP>::eval(x, y));
 	}
 }
 
-template <typename T, int R>
-__device__ __forceinline__ void p_copy(const uint4 &rec, const PArgs<R> &c)
+template <typename T>
+__device__ __forceinline__ void p_copy(const uint4 &rec, const PArgs &c)
 {
 	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
 	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
-#pragma unroll
-	for (int i = 0; i < R; i++) {
-		if (32u * i >= c.n)
-			break;
-		if (c.lane + 32u * i < c.n) {
-			const uint32_t si = c.sel0 + 32u * i;
-			SM<T>::st(p_addr(d, c.row[i], si), SM<T>::ld(p_addr(a, c.row[i], si)));
-		}
+	for (uint32_t e = c.e0; e < c.n; e += c.step) {
+		const uint32_t row = lds_u16(c.list + 2 * e);
+		SM<T>::st(p_addr(d, row, e), SM<T>::ld(p_addr(a, row, e)));
 	}
 }
 
-template <int R>
-__device__ __forceinline__ void project_op(const uint4 &rec, const PArgs<R> &c)
+template <typename T>
+__device__ __forceinline__ void p_math_any(const uint4 &rec, const PArgs &c)
 {
-#define VGPU_PMATH_CASES(T, TY)                                             \
-	case H_MATH + TY * 4 + MO_ADD: p_math<T, MO_ADD, R>(rec, c); break;    \
-	case H_MATH + TY * 4 + MO_SUB: p_math<T, MO_SUB, R>(rec, c); break;    \
-	case H_MATH + TY * 4 + MO_MUL: p_math<T, MO_MUL, R>(rec, c); break;    \
-	case H_MATH + TY * 4 + MO_DIV: p_math<T, MO_DIV, R>(rec, c); break;
-	switch (rec.x & 0xffu) {
-		VGPU_PMATH_CASES(int32_t, VT_INT)
-		VGPU_PMATH_CASES(long long, VT_INT64)
-		VGPU_PMATH_CASES(float, VT_FLOAT)
-		VGPU_PMATH_CASES(double, VT_DOUBLE)
-		VGPU_PMATH_CASES(signed char, VT_CHAR)
-	/* every listed row is active here, so constants and columns are copies */
-	case H_SETCONST:
-	case H_COPY4: p_copy<uint32_t, R>(rec, c); break;
-	case H_COPY8: p_copy<unsigned long long, R>(rec, c); break;
-	case H_COPY1: p_copy<unsigned char, R>(rec, c); break;
-	default: break;
+	const uint32_t h = rec.x;
+	if (h_op(h, MO_ADD)) p_math<T, MO_ADD>(rec, c);
+	else if (h_op(h, MO_SUB)) p_math<T, MO_SUB>(rec, c);
+	else if (h_op(h, MO_MUL)) p_math<T, MO_MUL>(rec, c);
+	else p_math<T, MO_DIV>(rec, c);
+}
+
+/* one projection op: arithmetic, or a copy (every listed row is active
+ * here, so constants and columns are copies) */
+__device__ __forceinline__ void project_op(const uint4 &rec, const PArgs &c)
+{
+	const uint32_t h = rec.x;
+	if (h & OK_MATH) {
+		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, c);
+		else if (h_type(h, VT_INT)) p_math_any<int32_t>(rec, c);
+		else if (h_type(h, VT_DOUBLE)) p_math_any<double>(rec, c);
+		else if (h_type(h, VT_INT64)) p_math_any<long long>(rec, c);
+		else p_math_any<signed char>(rec, c);
+	} else if (h & OK_SETCONST) {
+		p_copy<uint32_t>(rec, c);
+	} else if (h & OK_COPY) {
+		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) p_copy<unsigned long long>(rec, c);
+		else if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, c);
+		else p_copy<uint32_t>(rec, c);
 	}
-#undef VGPU_PMATH_CASES
 }
 
 /* ---- ordered placement ------------------------------------------------- */
@@ -785,54 +828,94 @@ __device__ __forceinline__ void publish_count(const KParams &kp, const QDesc &Q,
 		st_status(&kp.status[g], ep | (kFlagAggregate << kStatusFlagShift) | tile_total);
 }
 
-/* find the rows written by the query's earlier tiles and publish this
- * tile's inclusive prefix.  Each round reads 32 predecessors' status words;
- * it stops at the nearest one that carries an inclusive prefix.  Returns
- * false if a predecessor never published (bounded wait). */
-__device__ bool lookback(const KParams &kp, const QDesc &Q, uint64_t g, uint32_t tile_total,
+/* Rows written by the query's tiles before tile g (its exclusive prefix):
+ * walks back over earlier tiles' status words, kLookbackPerLane per lane
+ * per round, summing aggregates up to the nearest inclusive prefix.  The
+ * caller's own latest tile of the query (known, the index `known` with
+ * inclusive prefix `known_end`, or none when known < the query's first
+ * tile) is a prefix that needs no load, so the walk never passes it.  It
+ * needs only the predecessors, so it runs while tile g itself is still being
+ * filtered.  Returns false if a predecessor never published (bounded wait). */
+constexpr int kLookbackPerLane = 4;
+
+__device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int64_t known, uint64_t known_end,
 	int lane, uint64_t *excl_out)
 {
-	const uint64_t first = Q.work_first;
-	const uint64_t ep = (uint64_t)kp.epoch << kStatusEpochShift;
-	if (g == first) {
+	constexpr int W = 32 * kLookbackPerLane;
+	const int64_t first = (int64_t)Q.work_first;
+	if ((int64_t)g == first) {
 		*excl_out = query_base(Q);
 		return true;
 	}
+	/* indices below `floor` are not read: the query's start, or the known
+	 * prefix (read as a stop) */
+	const int64_t floor = known >= first ? known : first;
 	uint64_t excl = 0;
 	int64_t j = (int64_t)g - 1;
 	unsigned spins = 0;
 	while (true) {
-		const int64_t idx = j - lane;
-		const bool inrange = idx >= (int64_t)first;
-		uint64_t v = 0;
-		bool ready = !inrange;
-		if (inrange) {
-			v = ld_status(&kp.status[idx]);
-			ready = (v >> kStatusEpochShift) == kp.epoch && ((v >> kStatusFlagShift) & 3u);
+		uint64_t v[kLookbackPerLane];
+		uint32_t stopbits = 0, wait = 0;
+#pragma unroll
+		for (int x = 0; x < kLookbackPerLane; x++) {
+			const int64_t idx = j - (lane * kLookbackPerLane + x);
+			if (idx < floor || idx == known) {
+				/* a stop: the known prefix, or nothing before the query */
+				v[x] = (idx == known) ? (known_end & kStatusValueMask) : 0ull;
+				stopbits |= 1u << x;
+			} else {
+				v[x] = ld_status(&kp.status[idx]);
+			}
 		}
-		while (!__all_sync(0xffffffffu, ready)) {
+		/* wait until every loaded word carries this launch's epoch and a flag */
+		while (true) {
+			wait = 0;
+#pragma unroll
+			for (int x = 0; x < kLookbackPerLane; x++)
+				if (!((stopbits >> x) & 1u)) {
+					const bool rx = (v[x] >> kStatusEpochShift) == kp.epoch && ((v[x] >> kStatusFlagShift) & 3u);
+					if (!rx)
+						wait |= 1u << x;
+					else if (((v[x] >> kStatusFlagShift) & 3u) == kFlagPrefix)
+						stopbits |= 1u << x;
+				}
+			/* only words before the window's nearest stop are needed */
+			const uint32_t sm = __ballot_sync(0xffffffffu, stopbits != 0);
+			const int stop_lane = sm ? __ffs(sm) - 1 : 32;
+			const uint32_t need = lane < stop_lane ? 0xffffffffu
+				: lane == stop_lane ? ((stopbits & (0u - stopbits)) - 1u) : 0u;
+			const uint32_t blocking = wait & need;
+			if (__all_sync(0xffffffffu, blocking == 0))
+				break;
 			if (++spins > kLookbackSpinLimit)
 				return false;
 			__nanosleep(spins < 64 ? 32 : 256);
-			if (!ready) {
-				v = ld_status(&kp.status[idx]);
-				ready = (v >> kStatusEpochShift) == kp.epoch && ((v >> kStatusFlagShift) & 3u);
-			}
+#pragma unroll
+			for (int x = 0; x < kLookbackPerLane; x++)
+				if ((blocking >> x) & 1u)
+					v[x] = ld_status(&kp.status[j - (lane * kLookbackPerLane + x)]);
 		}
-		const bool is_prefix = !inrange || ((v >> kStatusFlagShift) & 3u) == kFlagPrefix;
-		const uint32_t pm = __ballot_sync(0xffffffffu, is_prefix);
-		const uint64_t val = inrange ? (v & kStatusValueMask) : 0ull;
+		/* the nearest stop over the whole window: the first lane with one,
+		 * then that lane's first */
+		const int xs = stopbits ? __ffs(stopbits) - 1 : kLookbackPerLane;
+		const uint32_t pm = __ballot_sync(0xffffffffu, stopbits != 0);
+		uint64_t part = 0;
 		if (pm) {
 			const int stop = __ffs(pm) - 1;
-			excl += warp_sum_u64(lane <= stop ? val : 0ull);
+			const int xstop = __shfl_sync(0xffffffffu, xs, stop);
+#pragma unroll
+			for (int x = 0; x < kLookbackPerLane; x++)
+				if (lane < stop || (lane == stop && x <= xstop))
+					part += v[x] & kStatusValueMask;
+			excl += warp_sum_u64(part);
 			break;
 		}
-		excl += warp_sum_u64(val);
-		j -= 32;
+#pragma unroll
+		for (int x = 0; x < kLookbackPerLane; x++)
+			part += v[x] & kStatusValueMask;
+		excl += warp_sum_u64(part);
+		j -= W;
 	}
-	if (lane == 0)
-		st_status(&kp.status[g],
-			ep | (kFlagPrefix << kStatusFlagShift) | ((excl + tile_total) & kStatusValueMask));
 	*excl_out = excl;
 	return true;
 }
@@ -930,7 +1013,7 @@ __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, ProdQ
 template <int TILE>
 __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 {
-	const volatile uint32_t *abort = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags) + 2;
+	const volatile uint32_t *abort = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags) + kFAbort;
 	uint32_t *held = reinterpret_cast<uint32_t *>(smem + kOffHeld);
 	const uint32_t nst = kp.nstages;
 	ProdQuery pq;
@@ -1007,88 +1090,6 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	}
 }
 
-/* ---- scanner: counts -> tile totals and in-tile offsets ------------------ */
-
-/* For each tile: wait for the compute warps' counts, one per 64 rows (a
- * half of a warp's 128-row chunk), scan them in (chunk, warp, half) = row
- * order, publish the tile's count to the query's look-back words, record
- * valid rows per 64-row block when asked, and hand the total to the
- * look-back warp.  At the end of the CTA's tiles it leaves
- * the tile index in flags[3] for the look-back warp. */
-template <int THREADS, int R>
-__device__ void scanner(const KParams &kp, unsigned char *smem, int lane)
-{
-	constexpr int NW = THREADS / 32;
-	constexpr int G = R * NW / 2;  /* 64-row groups per tile */
-	constexpr int PER = (G + 31) / 32;
-	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	volatile uint32_t *tot = reinterpret_cast<volatile uint32_t *>(smem + kOffTot);
-	const uint32_t nst = kp.nstages;
-	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst, q = i & 1u;
-		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + 2))
-			return;
-		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
-		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-		if (si.work >= kp.total_work) {
-			__syncwarp();
-			if (lane == 0) {
-				flags[3] = i;
-				mbar_arrive(smem_addr(smem + kOffSready + 8 * q));
-			}
-			return;
-		}
-		if (!mbar_wait(smem_addr(smem + kOffCready + 8 * q), (i >> 1) & 1u, flags + 2))
-			return;
-		const uint32_t *cnt = reinterpret_cast<const uint32_t *>(smem + kOffCnt) + q * kMaxGroups;
-		uint32_t *pre = reinterpret_cast<uint32_t *>(smem + kOffPre) + q * kMaxGroups;
-		uint32_t local[PER];
-		uint32_t sum = 0;
-#pragma unroll
-		for (int x = 0; x < PER; x++) {
-			const int gi = lane * PER + x;
-			local[x] = gi < G ? cnt[gi] : 0u;
-			sum += local[x];
-		}
-		uint32_t incl = sum;
-#pragma unroll
-		for (int d = 1; d < 32; d <<= 1) {
-			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
-			if (lane >= d)
-				incl += v;
-		}
-		uint32_t run = incl - sum;
-#pragma unroll
-		for (int x = 0; x < PER; x++) {
-			const int gi = lane * PER + x;
-			if (gi < G)
-				pre[gi] = run;
-			run += local[x];
-		}
-		const uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
-		if (lane == 0)
-			publish_count(kp, Q, si.work, tile_total);
-		/* valid rows per 64-row block, for result-tablet splitting on the host */
-		if (Q.block_counts != nullptr) {
-			/* group g covers tile rows 64 g .. 64 g + 63 */
-			for (int g = lane; g < G; g += 32) {
-				const uint32_t local_row = 64u * (uint32_t)g;
-				if (local_row < si.nrows) {
-					const uint64_t blk =
-						(uint64_t)Q.segs[si.seg].block_base + (si.row0 + local_row) / 64;
-					Q.block_counts[blk] = (uint8_t)cnt[g];
-				}
-			}
-		}
-		__syncwarp();
-		if (lane == 0) {
-			tot[q] = tile_total;
-			mbar_arrive(smem_addr(smem + kOffSready + 8 * q));
-		}
-	}
-}
-
 /* ---- look-back warp: tile totals -> result offsets ----------------------- */
 
 template <int THREADS, int R>
@@ -1102,40 +1103,48 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 	 * same query starts where it ended, with no look-back */
 	uint64_t prev_work = ~0ull, prev_end = 0;
 	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst, q = i & 1u;
-		if (!mbar_wait(smem_addr(smem + kOffSready + 8 * q), (i >> 1) & 1u, flags + 2))
+		const uint32_t s = i % nst, q = i % kSlots;
+		/* the tile's data has landed: its work item is known, so the walk
+		 * over earlier tiles starts while the filter warps run */
+		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort))
 			return;
-		if (flags[3] == i)
-			return;
-		/* the stage still holds tile i: it is released after the tile's
-		 * stores, which wait for this warp */
+		/* the stage holds tile i until the tile's stores, which wait for
+		 * this warp */
 		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
 		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
 		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-		const uint32_t tile_total = tot[q];
+		if (si.work >= kp.total_work)
+			return;
 		uint64_t excl = 0;
 		bool ok = true;
-		if (si.work == prev_work + 1 && si.work != Q.work_first) {
+		const bool follows = si.work == prev_work + 1 && si.work != Q.work_first;
+		if (follows)
 			excl = prev_end;
-			if (lane == 0)
-				st_status(&kp.status[si.work],
-					((uint64_t)kp.epoch << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
-					((excl + tile_total) & kStatusValueMask));
-		} else {
-			ok = lookback(kp, Q, si.work, tile_total, lane, &excl);
-		}
+		else
+			ok = lookback_excl(kp, Q, si.work, prev_work == ~0ull ? -1 : (int64_t)prev_work, prev_end, lane, &excl);
+		/* the tile's own count */
+		if (ok && !mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
+			return;
+		const uint32_t tile_total = ok ? tot[q] : 0u;
 		prev_work = si.work;
 		prev_end = excl + tile_total;
 		__syncwarp();
 		if (lane == 0) {
-			if (!ok)
+			if (!ok) {
 				report(kp.error, DE_LOOKBACK_TIMEOUT);
-			else if (si.work == Q.work_first + Q.ntiles - 1)
-				*Q.total_out = excl + tile_total;
+			} else {
+				/* the inclusive prefix (a query's first tile published its own) */
+				if (si.work != Q.work_first)
+					st_status(&kp.status[si.work],
+						((uint64_t)kp.epoch << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
+						((excl + tile_total) & kStatusValueMask));
+				if (si.work == Q.work_first + Q.ntiles - 1)
+					*Q.total_out = excl + tile_total;
+			}
 			offs[q] = excl;
 			flags[q] = ok ? 1u : 0u;
 			if (!ok)
-				flags[2] = 1u;
+				flags[kFAbort] = 1u;
 			mbar_arrive(smem_addr(smem + kOffOready + 8 * q));
 		}
 		if (!ok)
@@ -1143,109 +1152,102 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 	}
 }
 
-/* ---- compute warps: stores of a finished tile ---------------------------- */
+/* ---- projection warps: projection and ordered stores of each tile -------- */
 
-template <int THREADS, int R>
-__device__ __forceinline__ bool store_tile(const KParams &kp, unsigned char *smem, uint32_t sbase,
-	uint32_t p, uint32_t nsel, int warp, int lane)
+template <int THREADS, int R, int P>
+__device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int lane)
 {
-	constexpr int NW = THREADS / 32;
 	constexpr int TILE = THREADS * R;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	const uint32_t s = p % kp.nstages, q = p & 1u;
-	if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (p >> 1) & 1u, flags + 2))
-		return false;
-	if (!flags[q])
-		return false;
-	const uint64_t off = lds_u64(sbase + kOffOff + 8 * q);
-	const uint32_t sd = s * kp.stage_bytes;
-	const uint32_t qd = sbase + kp.stage_area + sd;
-	const uint32_t vd = q * lds_u32(qd + kQVecSlot);
-	const uint32_t list = sbase + kp.sel_area + (q * 2 * TILE + warp * 32 * R) * 2;
-	const uint32_t tag = list + TILE * 2;
-	const uint32_t pre = sbase + kOffPre + q * kMaxGroups * 4;
-	const uint64_t cap = lds_u64(qd + kQCapacity);
-	uint32_t row[R];
-	uint64_t pos[R];
-	bool overflow = false;
-#pragma unroll
-	for (int i = 0; i < R; i++) {
-		const uint32_t e = lane + 32 * i;
-		pos[i] = ~0ull;
-		row[i] = 0;
-		if (32u * i >= nsel)
-			continue;
-		if (e < nsel) {
-			row[i] = lds_u16(list + 2 * e);
-			/* tag: chunk and rank within the warp's chunk; the chunk's first
-			 * 64-row group holds its offset in the tile */
-			const uint32_t t = lds_u16(tag + 2 * e);
-			pos[i] = off + lds_u32(pre + 8 * ((t >> 7) * NW + warp)) + (t & 127u);
-			if (pos[i] >= cap) {
-				overflow = true;
-				pos[i] = ~0ull;
+	const uint32_t sbase = smem_addr(smem);
+	const uint32_t nst = kp.nstages;
+	for (uint32_t i = 0;; i++) {
+		const uint32_t s = i % nst, q = i % kSlots;
+		if (!mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+			if (lane == 0 && !flags[kFAbort]) {
+				report(kp.error, DE_STAGE_TIMEOUT);
+				flags[kFAbort] = 1u;
 			}
+			return;
+		}
+		if (flags[kFEnd] == i)
+			return;
+		const uint32_t sd = s * kp.stage_bytes;
+		const uint32_t qd = sbase + kp.stage_area + sd;
+		PArgs c;
+		c.sbase = sbase;
+		c.sd = sd;
+		c.vd = q * lds_u32(qd + kQVecSlot);
+		c.list = sbase + kp.sel_area + q * TILE * 2;
+		c.n = lds_u32(sbase + kOffTot + 4 * q);
+		c.e0 = 32u * (uint32_t)pw + (uint32_t)lane;
+		c.step = 32u * P;
+		const uint32_t ops = qd + kQOps;
+		if (c.e0 - (uint32_t)lane < c.n) {
+			const uint32_t nu = lds_u32(qd + kQNUops) - 1u;
+			for (uint32_t k = lds_u32(qd + kQNFilter); k < nu; k++)
+				project_op(lds_v4(ops + 16u * k), c);
+		}
+
+		/* ---- stores at the tile's offset, once the look-back resolved it */
+		if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
+			return;
+		if (!flags[q])
+			return;
+		const uint64_t off = lds_u64(sbase + kOffOff + 8 * q);
+		if (c.e0 - (uint32_t)lane < c.n) {
+			const uint64_t cap = lds_u64(qd + kQCapacity);
+			bool overflow = false;
+			const uint32_t nout = lds_u32(qd + kQNOut);
+			for (uint32_t j = 0; j < nout; j++) {
+				const uint32_t od = lds_u32(qd + kQOdOut + 4 * j);
+				unsigned char *out = reinterpret_cast<unsigned char *>(lds_u64(qd + kQOutPtr + 8 * j));
+				const uint32_t stride = lds_u8(qd + kQOutStride + j);
+				const Opnd a = stride == 8 ? opnd<8>(od, sbase, sd, c.vd)
+					: stride == 4 ? opnd<4>(od, sbase, sd, c.vd) : opnd<1>(od, sbase, sd, c.vd);
+				for (uint32_t e = c.e0; e < c.n; e += c.step) {
+					const uint64_t pos = off + e;
+					if (pos >= cap) {
+						overflow = true;
+						break;
+					}
+					const uint32_t at = p_addr(a, lds_u16(c.list + 2 * e), e);
+					if (stride == 4)
+						reinterpret_cast<uint32_t *>(out)[pos] = lds_u32(at);
+					else if (stride == 8)
+						reinterpret_cast<unsigned long long *>(out)[pos] = lds_u64(at);
+					else
+						out[pos] = (unsigned char)lds_u8(at);
+				}
+			}
+			if (overflow)
+				report(kp.error, DE_OUTPUT_OVERFLOW);
+		}
+		__syncwarp();
+		if (lane == 0) {
+			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
+			mbar_arrive(smem_addr(smem + kOffLfree + 8 * q));
 		}
 	}
-	const uint32_t sel0 = warp * 32 * R + lane;
-	const uint32_t nout = lds_u32(qd + kQNOut);
-	for (uint32_t j = 0; j < nout; j++) {
-		const uint32_t od = lds_u32(qd + kQOdOut + 4 * j);
-		void *out = reinterpret_cast<void *>(lds_u64(qd + kQOutPtr + 8 * j));
-		switch (lds_u8(qd + kQOutStride + j)) {
-		case 4: {
-			const Opnd a = opnd<4>(od, sbase, sd, vd);
-#pragma unroll
-			for (int i = 0; i < R; i++) {
-				if (32u * i >= nsel)
-					break;
-				if (pos[i] != ~0ull)
-					reinterpret_cast<uint32_t *>(out)[pos[i]] = lds_u32(p_addr(a, row[i], sel0 + 32 * i));
-			}
-			break;
-		}
-		case 8: {
-			const Opnd a = opnd<8>(od, sbase, sd, vd);
-#pragma unroll
-			for (int i = 0; i < R; i++) {
-				if (32u * i >= nsel)
-					break;
-				if (pos[i] != ~0ull)
-					reinterpret_cast<unsigned long long *>(out)[pos[i]] =
-						lds_u64(p_addr(a, row[i], sel0 + 32 * i));
-			}
-			break;
-		}
-		default: {
-			const Opnd a = opnd<1>(od, sbase, sd, vd);
-#pragma unroll
-			for (int i = 0; i < R; i++) {
-				if (32u * i >= nsel)
-					break;
-				if (pos[i] != ~0ull)
-					reinterpret_cast<unsigned char *>(out)[pos[i]] =
-						(unsigned char)lds_u8(p_addr(a, row[i], sel0 + 32 * i));
-			}
-			break;
-		}
-		}
-	}
-	if (overflow)
-		report(kp.error, DE_OUTPUT_OVERFLOW);
-	__syncwarp();
-	if (lane == 0)
-		mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
-	return true;
 }
 
+/* projection warps per CTA: half the filter warps, 1 to 4 */
+template <int THREADS>
+struct ProjWarps {
+	static constexpr int value = THREADS / 64 < 1 ? 1 : THREADS / 64 > 4 ? 4 : THREADS / 64;
+};
+
 template <int THREADS, int R>
-__global__ void __launch_bounds__(THREADS + 32 * kRoleWarps) vm_kernel(const KParams kp)
+__global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)) vm_kernel(const KParams kp)
 {
 	constexpr int TILE = THREADS * R;
 	constexpr int NW = THREADS / 32;
 	constexpr int C = R / 4;
+	constexpr int P = ProjWarps<THREADS>::value;
+	constexpr int G = 2 * C * NW;          /* 64-row groups per tile */
+	constexpr int PER = (G + 31) / 32;
 	static_assert(R % 4 == 0 && R <= 32, "rows per thread: whole 4-row chunks, 32-bit row masks");
-	static_assert(R * NW / 2 <= (int)kMaxGroups, "64-row groups per tile");
+	static_assert(G <= (int)kMaxGroups, "64-row groups per tile");
 	static_assert(TILE <= 65536, "tile rows are 16-bit in the selection lists");
 	extern __shared__ __align__(128) unsigned char smem[];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1255,51 +1257,63 @@ __global__ void __launch_bounds__(THREADS + 32 * kRoleWarps) vm_kernel(const KPa
 	if (tid == 0) {
 		for (uint32_t s = 0; s < nst; s++) {
 			mbar_init(smem_addr(smem + kOffFull + 8 * s), 1);
-			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), NW);
+			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), P);
 		}
-		for (uint32_t q = 0; q < 2; q++) {
-			mbar_init(smem_addr(smem + kOffCready + 8 * q), NW);
-			mbar_init(smem_addr(smem + kOffSready + 8 * q), 1);
+		for (uint32_t q = 0; q < kSlots; q++) {
+			mbar_init(smem_addr(smem + kOffLready + 8 * q), NW);
 			mbar_init(smem_addr(smem + kOffOready + 8 * q), 1);
+			mbar_init(smem_addr(smem + kOffLfree + 8 * q), P);
+			mbar_init(smem_addr(smem + kOffCdone + 8 * q), NW);
 		}
-		flags[0] = flags[1] = flags[2] = 0;
-		flags[3] = ~0u;
+		for (int x = 0; x < 8; x++)
+			flags[x] = 0;
+		flags[kFEnd] = ~0u;
 		for (uint32_t s = 0; s < kMaxStages; s++)
 			reinterpret_cast<uint32_t *>(smem + kOffHeld)[s] = ~0u;
 		fence_mbar_init();
 	}
 	__syncthreads();
 	if (warp == NW) {
-		scanner<THREADS, R>(kp, smem, lane);
-		return;
-	}
-	if (warp == NW + 1) {
 		producer<TILE>(kp, smem, lane);
 		return;
 	}
-	if (warp == NW + 2) {
+	if (warp == NW + 1) {
 		lookback_warp<THREADS, R>(kp, smem, lane);
 		return;
 	}
+	if (warp >= NW + 2) {
+		proj_warps<THREADS, R, P>(kp, smem, warp - (NW + 2), lane);
+		return;
+	}
 
-	/* compute warps */
+	/* filter warps */
 	const uint32_t sbase = smem_addr(smem);
-	uint32_t prev_nsel = 0;
-	uint32_t i = 0;
-	for (;; i++) {
-		const uint32_t s = i % nst, q = i & 1u;
-		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + 2)) {
-			if (lane == 0 && !flags[2]) {
+	for (uint32_t i = 0;; i++) {
+		const uint32_t s = i % nst, q = i % kSlots;
+		/* the list and row-vector slot q are free once the projection of
+		 * tile i - kSlots is done */
+		bool ok = i < kSlots ||
+			mbar_wait(smem_addr(smem + kOffLfree + 8 * q), ((i - kSlots) / kSlots) & 1u, flags + kFAbort);
+		ok = ok && mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort);
+		if (!ok) {
+			if (lane == 0 && !flags[kFAbort]) {
 				report(kp.error, DE_STAGE_TIMEOUT);
-				flags[2] = 1u;
+				flags[kFAbort] = 1u;
 			}
 			return;
 		}
 		const uint32_t sd = s * kp.stage_bytes;
 		const uint32_t qd = sbase + kp.stage_area + sd;
 		const uint32_t sinfo = qd + (uint32_t)sizeof(QDesc);
-		if (lds_u32(sinfo + offsetof(StageInfo, work)) >= kp.total_work)
-			break;
+		if (lds_u32(sinfo + offsetof(StageInfo, work)) >= kp.total_work) {
+			/* no more tiles: tell the look-back and projection warps */
+			__syncwarp();
+			if (lane == 0) {
+				flags[kFEnd] = i;
+				mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
+			}
+			return;
+		}
 		const uint32_t nrows = lds_u32(sinfo + offsetof(StageInfo, nrows));
 		const uint32_t vd = q * lds_u32(qd + kQVecSlot);
 
@@ -1316,9 +1330,9 @@ __global__ void __launch_bounds__(THREADS + 32 * kRoleWarps) vm_kernel(const KPa
 #pragma unroll
 		for (int sl = 0; sl < kMaxSlots; sl++)
 			st.pend[sl] = 0;
-		const uint32_t ops = qd + kQOps;
-		const uint32_t nf = lds_u32(qd + kQNFilter);
 		{
+			const uint32_t ops = qd + kQOps;
+			const uint32_t nf = lds_u32(qd + kQNFilter);
 			const FArgs f{sbase, sd, vd, tid};
 			uint4 rec = lds_v4(ops);
 			for (uint32_t k = 0; k < nf; k++) {
@@ -1329,76 +1343,104 @@ __global__ void __launch_bounds__(THREADS + 32 * kRoleWarps) vm_kernel(const KPa
 			}
 		}
 
-		/* ---- selection: this warp's valid rows in row order, per 128-row
-		 * chunk from four bit-plane ballots (row k of each lane's 4) */
-		const uint32_t list = sbase + kp.sel_area + (q * 2 * TILE + warp * 32 * R) * 2;
-		const uint32_t tag = list + TILE * 2;
+		/* ---- counts per 64 rows, from four bit-plane ballots per 128-row
+		 * chunk of the warp (row k of each lane's 4) */
 		const uint32_t cnt = sbase + kOffCnt + q * kMaxGroups * 4;
-		uint32_t nsel = 0;
-		{
-			const uint32_t lt = (1u << lane) - 1u;
+		const uint32_t lt = (1u << lane) - 1u;
+		uint32_t rank[C], total[C];
 #pragma unroll
-			for (int c = 0; c < C; c++) {
-				const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
-				const uint32_t b0 = __ballot_sync(0xffffffffu, m & 1u);
-				const uint32_t b1 = __ballot_sync(0xffffffffu, m & 2u);
-				const uint32_t b2 = __ballot_sync(0xffffffffu, m & 4u);
-				const uint32_t b3 = __ballot_sync(0xffffffffu, m & 8u);
-				const uint32_t total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
-				if (lane == 0) {
-					/* lanes 0-15 hold the chunk's first 64 rows */
-					const uint32_t h0 = __popc(b0 & 0xffffu) + __popc(b1 & 0xffffu) +
-						__popc(b2 & 0xffffu) + __popc(b3 & 0xffffu);
-					sts_u32(cnt + 8 * (c * NW + warp), h0);
-					sts_u32(cnt + 8 * (c * NW + warp) + 4, total - h0);
-				}
-				if (total) {
-					uint32_t rank = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
-					const uint32_t row0 = chunk_row<THREADS>(c, tid);
-#pragma unroll
-					for (int k = 0; k < 4; k++)
-						if ((m >> k) & 1u) {
-							sts_u16(list + 2 * (nsel + rank), row0 + k);
-							/* chunk and rank: the entry's place in the result */
-							sts_u16(tag + 2 * (nsel + rank), ((uint32_t)c << 7) | rank);
-							rank++;
-						}
-				}
-				nsel += total;
+		for (int c = 0; c < C; c++) {
+			const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
+			const uint32_t b0 = __ballot_sync(0xffffffffu, m & 1u);
+			const uint32_t b1 = __ballot_sync(0xffffffffu, m & 2u);
+			const uint32_t b2 = __ballot_sync(0xffffffffu, m & 4u);
+			const uint32_t b3 = __ballot_sync(0xffffffffu, m & 8u);
+			total[c] = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+			rank[c] = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
+			if (lane == 0) {
+				/* lanes 0-15 hold the chunk's first 64 rows */
+				const uint32_t h0 = __popc(b0 & 0xffffu) + __popc(b1 & 0xffffu) + __popc(b2 & 0xffffu) +
+					__popc(b3 & 0xffffu);
+				sts_u32(cnt + 8 * (c * NW + warp), h0);
+				sts_u32(cnt + 8 * (c * NW + warp) + 4, total[c] - h0);
 			}
 		}
 		__syncwarp();
 		if (lane == 0)
-			mbar_arrive(smem_addr(smem + kOffCready + 8 * q));
-
-		/* ---- stores of the previous tile, whose offset is resolved by now;
-		 * before this tile's projection, which reuses the selection vectors */
-		if (i > 0 && !store_tile<THREADS, R>(kp, smem, sbase, i - 1, prev_nsel, warp, lane))
-			return;
-		prev_nsel = nsel;
-
-		/* ---- projection over this warp's selection list */
-		{
-			PArgs<R> pc;
-			pc.sbase = sbase;
-			pc.sd = sd;
-			pc.vd = vd;
-			pc.n = nsel;
-			pc.sel0 = (uint32_t)(warp * 32 * R + lane);
-			pc.lane = (uint32_t)lane;
-#pragma unroll
-			for (int x = 0; x < R; x++) {
-				const uint32_t e = lane + 32 * x;
-				pc.row[x] = e < nsel ? lds_u16(list + 2 * e) : 0u;
+			mbar_arrive(smem_addr(smem + kOffCdone + 8 * q));
+		if (!mbar_wait(smem_addr(smem + kOffCdone + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+			if (lane == 0 && !flags[kFAbort]) {
+				report(kp.error, DE_STAGE_TIMEOUT);
+				flags[kFAbort] = 1u;
 			}
-			const uint32_t nu = lds_u32(qd + kQNUops) - 1u;
-			for (uint32_t k = nf; k < nu; k++)
-				project_op<R>(lds_v4(ops + 16u * k), pc);
+			return;
+		}
+
+		/* ---- every warp scans the tile's counts: (chunk, warp, half) is row
+		 * order, so a chunk's rows start at the sum of the counts before it */
+		uint32_t loc[PER], lane_pre[PER];
+		uint32_t sum = 0;
+#pragma unroll
+		for (int x = 0; x < PER; x++) {
+			const int g = lane * PER + x;
+			loc[x] = g < G ? lds_u32(cnt + 4 * g) : 0u;
+			lane_pre[x] = sum;
+			sum += loc[x];
+		}
+		uint32_t incl = sum;
+#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+			if (lane >= d)
+				incl += v;
+		}
+		const uint32_t ex = incl - sum;
+		const uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
+
+		/* ---- the tile-ordered list of selected rows */
+		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
+#pragma unroll
+		for (int c = 0; c < C; c++) {
+			const uint32_t g = 2u * (uint32_t)(c * NW + warp);
+			uint32_t v = 0;
+#pragma unroll
+			for (int x = 0; x < PER; x++)
+				if ((uint32_t)x == g % PER)
+					v = ex + lane_pre[x];
+			const uint32_t base = __shfl_sync(0xffffffffu, v, (int)(g / PER));
+			if (total[c]) {
+				const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
+				uint32_t at = base + rank[c];
+				const uint32_t row0 = chunk_row<THREADS>(c, tid);
+#pragma unroll
+				for (int k = 0; k < 4; k++)
+					if ((m >> k) & 1u)
+						sts_u16(list + 2 * at++, row0 + k);
+			}
+		}
+
+		/* ---- the tile's count: to the look-back words and the other roles */
+		if (warp == 0) {
+			const unsigned char *hdr = smem + kp.stage_area + sd;
+			const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
+			if (lane == 0) {
+				publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
+				sts_u32(sbase + kOffTot + 4 * q, tile_total);
+			}
+			/* valid rows per 64-row block, for result-tablet splitting on the
+			 * host: group g covers tile rows 64 g .. 64 g + 63 */
+			if (Q.block_counts != nullptr) {
+				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+				for (int g = lane; g < G; g += 32)
+					if (64u * (uint32_t)g < si.nrows)
+						Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
+							(uint8_t)lds_u32(cnt + 4 * g);
+			}
 		}
 		__syncwarp();
+		if (lane == 0)
+			mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
 	}
-	if (i > 0)
-		store_tile<THREADS, R>(kp, smem, sbase, i - 1, prev_nsel, warp, lane);
 }
 
 /* ---- host-side launcher ------------------------------------------------ */
@@ -1409,8 +1451,8 @@ static int launch_t(const KParams &kp, unsigned grid, size_t smem, cudaStream_t 
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	/* THREADS compute threads and the scanner, producer and look-back warps */
-	fn<<<grid, THREADS + 32 * kRoleWarps, smem, stream>>>(kp);
+	/* THREADS filter threads, the producer and look-back warps and the projection warps */
+	fn<<<grid, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem, stream>>>(kp);
 	return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1420,7 +1462,7 @@ static int occ_t(size_t smem, int *ctas)
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * kRoleWarps, smem) == cudaSuccess;
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem) == cudaSuccess;
 }
 
 #define VGPU_SHAPES(X) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
