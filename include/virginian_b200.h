@@ -410,6 +410,60 @@ int virg_gpu_batch_download(virg_gpu_batch *b, unsigned slot, void *const *host_
 int virg_gpu_batch_shape(const virg_gpu_batch *b, unsigned *shape4, uint64_t *work);
 void virg_gpu_batch_destroy(virg_gpu_batch *b);
 
+/* Serving loop (no reference counterpart; the reference runs one query per
+ * launch sequence, src/vm/execute.c:85-86).  A scheduler thread keeps one
+ * persistent VM kernel running over the engine's resident tables and folds
+ * submitted queries into it while it runs (continuous batching): queries are
+ * admitted in arrival order while the result budget has room for their
+ * estimated result size, their descriptors are uploaded and published to
+ * the running kernel through a doorbell in host-mapped memory, and the
+ * kernel reports each finished query in a completion record.  A query whose
+ * rows exceed its estimate is admitted again with its exact row count.
+ * Results stay in the result budget's device memory until released.  Tables
+ * must not be appended to while queries over them are in flight. */
+typedef struct {
+	uint64_t result_budget_bytes;    /* device memory for results (0: 20 GB) */
+	unsigned max_queries;            /* queries per kernel session (0: 4096) */
+	unsigned idle_us;                /* end an idle session after this long (0: 2000) */
+	unsigned max_load_bytes_per_row; /* staged column bytes a program may read (0: 32) */
+	unsigned max_row_vector_bytes;   /* filter register-vector bytes per row (0: 16) */
+	unsigned max_sel_vector_bytes;   /* projection register-vector bytes per row (0: 48) */
+	unsigned wait_limit_ms;          /* bound of the kernel's waits (0: 60000) */
+} virg_serve_config;
+
+typedef struct {
+	int done;                        /* rows are stored */
+	uint64_t rows;
+	unsigned readmits;               /* admissions after an estimate proved short */
+	double queue_us;                 /* submission to (last) admission */
+	double latency_us;               /* submission to completion seen by the host */
+} virg_serve_status;
+
+typedef struct {
+	unsigned sessions;               /* kernel sessions launched */
+	unsigned long long admitted, readmitted;
+	unsigned long long pending, inflight;
+	unsigned long long arena_used;   /* result bytes reserved */
+	unsigned device_error;           /* first device error of any session */
+	unsigned shape[4];               /* threads, rows per thread, stages, grid */
+} virg_serve_counters;
+
+int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cfg, virg_serve **out);
+/* queue a query; estimated_rows 0 reserves the bound (the table's rows) */
+int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_gpu_table *t,
+	uint64_t estimated_rows, uint64_t *ticket);
+/* a query's state; wait_ms < 0 waits for completion, > 0 up to that long */
+int virg_serve_poll(virg_serve *s, uint64_t ticket, int wait_ms, virg_serve_status *st);
+/* copy a completed query's rows to host buffers, one per result column */
+int virg_serve_download(virg_serve *s, uint64_t ticket, void *const *host_cols);
+/* device pointer of result column c of a completed query */
+const void *virg_serve_column(virg_serve *s, uint64_t ticket, unsigned c);
+/* free a completed query's result memory */
+int virg_serve_release(virg_serve *s, uint64_t ticket);
+int virg_serve_stats(virg_serve *s, virg_serve_counters *c);
+/* stops the scheduler and the running session */
+void virg_serve_destroy(virg_serve *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,7 @@ NP_OF = {VIRG_INT: np.int32, VIRG_INT64: np.int64, VIRG_FLOAT: np.float32,
          VIRG_DOUBLE: np.float64, VIRG_CHAR: np.int8}
 TYPE_OF = {np.dtype(v): k for k, v in NP_OF.items()}
 
-__all__ = ["Engine", "Program", "Table", "Result", "Batch", "VirgError", "make_schema", "ops_array",
+__all__ = ["Engine", "Program", "Table", "Result", "Batch", "Serve", "VirgError", "make_schema", "ops_array",
            "VIRG_INT", "VIRG_INT64", "VIRG_FLOAT", "VIRG_DOUBLE", "VIRG_CHAR", "NP_OF"]
 
 
@@ -293,6 +293,67 @@ class Batch:
     def close(self) -> None:
         if self.h:
             lib().virg_gpu_batch_destroy(self.h)
+            self.h = None
+
+
+class Serve:
+    """Serving loop: queries folded into one running persistent kernel
+    (continuous batching), admitted by estimated result memory."""
+
+    def __init__(self, engine: Engine, result_budget_bytes: int = 0, max_queries: int = 0,
+                 idle_us: int = 0, max_load_bytes_per_row: int = 0, max_row_vector_bytes: int = 0,
+                 max_sel_vector_bytes: int = 0, wait_limit_ms: int = 0):
+        from ._lib import ServeConfig
+        cfg = ServeConfig(result_budget_bytes, max_queries, idle_us, max_load_bytes_per_row,
+                          max_row_vector_bytes, max_sel_vector_bytes, wait_limit_ms)
+        h = ctypes.c_void_p()
+        check(lib().virg_serve_create(engine.h, ctypes.byref(cfg), ctypes.byref(h)), "serve create")
+        self.h = h
+        self.engine = engine
+        self._programs: Dict[int, Program] = {}
+
+    def submit(self, program: Program, table: Table, estimated_rows: int = 0) -> int:
+        t = ctypes.c_uint64()
+        check(lib().virg_serve_submit(self.h, program.h, table.h, estimated_rows, ctypes.byref(t)),
+              "serve submit")
+        self._programs[t.value] = program
+        return t.value
+
+    def poll(self, ticket: int, wait_ms: int = 0) -> Dict[str, float]:
+        from ._lib import ServeStatus
+        st = ServeStatus()
+        check(lib().virg_serve_poll(self.h, ticket, wait_ms, ctypes.byref(st)), "serve poll")
+        return {"done": bool(st.done), "rows": st.rows, "readmits": st.readmits,
+                "queue_us": st.queue_us, "latency_us": st.latency_us}
+
+    def wait(self, ticket: int) -> Dict[str, float]:
+        return self.poll(ticket, -1)
+
+    def download(self, ticket: int) -> List[np.ndarray]:
+        n = self.wait(ticket)["rows"]
+        info = self._programs[ticket].info
+        outs = [np.empty(max(n, 1), dtype=NP_OF[info.out_type[j]]) for j in range(info.nout)]
+        ptrs = (ctypes.c_void_p * max(1, info.nout))(*[o.ctypes.data for o in outs])
+        check(lib().virg_serve_download(self.h, ticket, ptrs), "serve download")
+        return [o[:n] for o in outs]
+
+    def release(self, ticket: int) -> None:
+        check(lib().virg_serve_release(self.h, ticket), "serve release")
+        self._programs.pop(ticket, None)
+
+    def stats(self) -> Dict[str, int]:
+        from ._lib import ServeCounters
+        c = ServeCounters()
+        check(lib().virg_serve_stats(self.h, ctypes.byref(c)), "serve stats")
+        return {"sessions": c.sessions, "admitted": c.admitted, "readmitted": c.readmitted,
+                "pending": c.pending, "inflight": c.inflight, "arena_used": c.arena_used,
+                "device_error": c.device_error,
+                "shape": {"threads": c.shape[0], "rows_per_thread": c.shape[1], "stages": c.shape[2],
+                          "grid": c.shape[3]}}
+
+    def close(self) -> None:
+        if self.h:
+            lib().virg_serve_destroy(self.h)
             self.h = None
 
 

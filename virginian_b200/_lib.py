@@ -44,6 +44,25 @@ class StreamStats(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("chunks", ctypes.c_uint)]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("result_budget_bytes", ctypes.c_uint64), ("max_queries", ctypes.c_uint),
+                ("idle_us", ctypes.c_uint), ("max_load_bytes_per_row", ctypes.c_uint),
+                ("max_row_vector_bytes", ctypes.c_uint), ("max_sel_vector_bytes", ctypes.c_uint),
+                ("wait_limit_ms", ctypes.c_uint)]
+
+
+class ServeStatus(ctypes.Structure):
+    _fields_ = [("done", ctypes.c_int), ("rows", ctypes.c_uint64), ("readmits", ctypes.c_uint),
+                ("queue_us", ctypes.c_double), ("latency_us", ctypes.c_double)]
+
+
+class ServeCounters(ctypes.Structure):
+    _fields_ = [("sessions", ctypes.c_uint), ("admitted", ctypes.c_ulonglong),
+                ("readmitted", ctypes.c_ulonglong), ("pending", ctypes.c_ulonglong),
+                ("inflight", ctypes.c_ulonglong), ("arena_used", ctypes.c_ulonglong),
+                ("device_error", ctypes.c_uint), ("shape", ctypes.c_uint * 4)]
+
+
 class ProgramInfo(ctypes.Structure):
     _fields_ = [("nload", ctypes.c_uint), ("load_column", ctypes.c_int * (VIRG_MAX_COLUMNS + 1)),
                 ("load_bytes_per_row", ctypes.c_uint), ("nout", ctypes.c_uint),
@@ -96,6 +115,14 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_batch_download": (i, [vp, u, P(vp), u64, u64]),
         "virg_gpu_batch_shape": (i, [vp, P(u), P(u64)]),
         "virg_gpu_batch_destroy": (None, [vp]),
+        "virg_serve_create": (i, [vp, P(ServeConfig), P(vp)]),
+        "virg_serve_submit": (i, [vp, vp, vp, u64, P(u64)]),
+        "virg_serve_poll": (i, [vp, u64, ctypes.c_int, P(ServeStatus)]),
+        "virg_serve_download": (i, [vp, u64, P(vp)]),
+        "virg_serve_column": (vp, [vp, u64, u]),
+        "virg_serve_release": (i, [vp, u64]),
+        "virg_serve_stats": (i, [vp, P(ServeCounters)]),
+        "virg_serve_destroy": (None, [vp]),
         "virg_gpu_catalog_create": (i, [P(vp)]),
         "virg_gpu_catalog_add_table": (i, [vp, ctypes.c_char_p, i, u, P(ctypes.c_char_p),
                                            P(ctypes.c_int), P(u)]),

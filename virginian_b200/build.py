@@ -17,8 +17,8 @@ LIB = os.path.join(HERE, "libvirginian_b200.so")
 BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["vm_kernel.cu", "engine.cu", "batch.cu", "stream.cu", "dropin.cu", "noalloc.cu", "program.cpp",
-           "sqlc.cpp"]
+SOURCES = ["vm_kernel.cu", "engine.cu", "batch.cu", "stream.cu", "dropin.cu", "noalloc.cu", "serve.cu",
+           "program.cpp", "sqlc.cpp"]
 EXTRA_SOURCES: List[str] = []
 
 FLAGS = [

@@ -55,6 +55,23 @@ constexpr unsigned kSlots = 3;
 
 constexpr unsigned kStageHdr = (unsigned)((sizeof(QDesc) + sizeof(StageInfo) + 127) / 128 * 128);
 
+/* serving-session control, in host-mapped memory written by the host:
+ * published queries and work items (a query's descriptor is complete before
+ * it is counted here) and the stop request */
+struct ServeCtl {
+	unsigned long long avail;  /* (queries << 40) | work items */
+	unsigned stop;             /* no more work after `avail` */
+	unsigned pad;
+};
+constexpr unsigned long long kAvailWorkMask = (1ull << 40) - 1;
+
+/* per-query completion record, in host-mapped memory: rows, then `seq`
+ * (the query's index + 1) once every tile's rows are stored */
+struct ServeRec {
+	unsigned long long rows;
+	unsigned long long seq;
+};
+
 /* kernel arguments */
 struct KParams {
 	const QDesc *queries;
@@ -71,6 +88,16 @@ struct KParams {
 	uint32_t vec_area;              /* smem offset of the register-vector region */
 	uint32_t vec_bytes;             /* its size (the largest of the launch's queries) */
 	uint32_t sel_area;              /* smem offset of the selection lists (2 slots) */
+	/* look-back words: word idx & status_mask, tagged epoch + (idx >> status_shift);
+	 * a launch with a word per work item uses ~0 and 63 (one tag) */
+	unsigned long long status_mask = ~0ull;
+	uint32_t status_shift = 63;
+	uint32_t wait_limit_ms = 1000;  /* bound of every wait of the kernel's warps */
+	/* serving sessions only (null otherwise): the work list grows while the
+	 * kernel runs; finished queries are reported in recs */
+	const ServeCtl *serve = nullptr;
+	ServeRec *recs = nullptr;
+	unsigned *done_tiles = nullptr; /* stored tiles per query */
 };
 
 /* host-side launcher implemented in vm_kernel.cu */

@@ -45,10 +45,13 @@
 
 namespace vgpu {
 
-/* bounded waits: a stage or offset wait gives up after about a second, far
- * beyond any real wait; look-back polls after 2^24 rounds of 32-256 ns */
-constexpr uint64_t kWaitLimitNs = 1000000000ull;
+/* bounded waits: a stage or offset wait gives up after the launch's limit
+ * (a second by default), far beyond any real wait; look-back polls after
+ * 2^24 rounds of 32-256 ns */
 constexpr uint32_t kSuspendHintNs = 20000;
+
+/* flag words of a CTA: ok per slot, then abort, end tile, -, wait limit */
+constexpr unsigned kFAbortSlot = 4;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
 /* work items claimed per atomic by the producer: one, so tiles that follow
@@ -68,7 +71,7 @@ constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;         /* uint32[8]: ok[kS
 constexpr unsigned kOffTot = kOffFlags + 32;                 /* uint32[kSlots]: tile totals */
 constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;          /* uint32[kMaxStages]: query per stage */
 constexpr unsigned kOffCnt = 512;                            /* uint32[kSlots][kMaxGroups]: per 64 rows */
-constexpr unsigned kFAbort = 4, kFEnd = 5;                   /* flag words */
+constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
 static_assert(kSlots <= kFAbort, "ok flags per slot");
 static_assert(kOffHeld + 4 * kMaxStages <= kOffCnt, "smem header layout");
 static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
@@ -186,13 +189,21 @@ __device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t phase,
 	return ok != 0;
 }
 
-/* bounded wait for an mbarrier phase; false on timeout (about a second) or
- * when the CTA's abort flag (a shared-memory word, if given) is set */
+/* bounded wait for an mbarrier phase; false on timeout or when the CTA's
+ * abort flag (a shared-memory word, if given) is set.  The bound is the
+ * launch's wait limit, which the CTA keeps in the last of its flag words
+ * (the abort flag's neighbours); a second without an abort flag. */
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const volatile uint32_t *abort)
 {
 	if (mbar_try_wait(bar, phase))
 		return true;
 	const uint32_t abort_addr = abort ? smem_addr(const_cast<const uint32_t *>(abort)) : 0u;
+	uint64_t limit_ns = 1000000000ull;
+	if (abort_addr) {
+		uint32_t ms;
+		asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(ms) : "r"(abort_addr + 4 * (7 - kFAbortSlot)));
+		limit_ns = (uint64_t)ms * 1000000ull;
+	}
 	const uint64_t t0 = globaltimer_ns();
 	for (;;) {
 		if (mbar_try_wait_hint(bar, phase, kSuspendHintNs))
@@ -203,7 +214,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const vo
 			if (v)
 				return false;
 		}
-		if (globaltimer_ns() - t0 > kWaitLimitNs)
+		if (globaltimer_ns() - t0 > limit_ns)
 			return false;
 	}
 }
@@ -806,6 +817,17 @@ __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v)
 	return v;
 }
 
+/* a work item's look-back word and the tag its words carry in this launch */
+__device__ __forceinline__ uint64_t *status_at(const KParams &kp, uint64_t idx)
+{
+	return kp.status + (idx & kp.status_mask);
+}
+
+__device__ __forceinline__ uint64_t status_tag(const KParams &kp, uint64_t idx)
+{
+	return (uint64_t)((kp.epoch + (uint32_t)(idx >> kp.status_shift)) & kEpochMask);
+}
+
 /* rows the query wrote before its first tile: nonzero only for a query
  * continued from an earlier launch */
 __device__ __forceinline__ uint64_t query_base(const QDesc &Q)
@@ -820,12 +842,12 @@ __device__ __forceinline__ uint64_t query_base(const QDesc &Q)
 __device__ __forceinline__ void publish_count(const KParams &kp, const QDesc &Q, uint64_t g,
 	uint32_t tile_total)
 {
-	const uint64_t ep = (uint64_t)kp.epoch << kStatusEpochShift;
+	const uint64_t ep = status_tag(kp, g) << kStatusEpochShift;
 	if (g == Q.work_first)
-		st_status(&kp.status[g], ep | (kFlagPrefix << kStatusFlagShift) |
+		st_status(status_at(kp, g), ep | (kFlagPrefix << kStatusFlagShift) |
 			((query_base(Q) + tile_total) & kStatusValueMask));
 	else
-		st_status(&kp.status[g], ep | (kFlagAggregate << kStatusFlagShift) | tile_total);
+		st_status(status_at(kp, g), ep | (kFlagAggregate << kStatusFlagShift) | tile_total);
 }
 
 /* Rows written by the query's tiles before tile g (its exclusive prefix):
@@ -864,7 +886,7 @@ __device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int
 				v[x] = (idx == known) ? (known_end & kStatusValueMask) : 0ull;
 				stopbits |= 1u << x;
 			} else {
-				v[x] = ld_status(&kp.status[idx]);
+				v[x] = ld_status(status_at(kp, (uint64_t)idx));
 			}
 		}
 		/* wait until every loaded word carries this launch's epoch and a flag */
@@ -873,7 +895,9 @@ __device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int
 #pragma unroll
 			for (int x = 0; x < kLookbackPerLane; x++)
 				if (!((stopbits >> x) & 1u)) {
-					const bool rx = (v[x] >> kStatusEpochShift) == kp.epoch && ((v[x] >> kStatusFlagShift) & 3u);
+					const uint64_t idx = (uint64_t)(j - (lane * kLookbackPerLane + x));
+					const bool rx = (v[x] >> kStatusEpochShift) == status_tag(kp, idx) &&
+						((v[x] >> kStatusFlagShift) & 3u);
 					if (!rx)
 						wait |= 1u << x;
 					else if (((v[x] >> kStatusFlagShift) & 3u) == kFlagPrefix)
@@ -893,7 +917,7 @@ __device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int
 #pragma unroll
 			for (int x = 0; x < kLookbackPerLane; x++)
 				if ((blocking >> x) & 1u)
-					v[x] = ld_status(&kp.status[j - (lane * kLookbackPerLane + x)]);
+					v[x] = ld_status(status_at(kp, (uint64_t)(j - (lane * kLookbackPerLane + x))));
 		}
 		/* the nearest stop over the whole window: the first lane with one,
 		 * then that lane's first */
@@ -962,16 +986,16 @@ struct ProdItem {
  * in increasing order, so the query and segment searches start at the
  * previous item's. */
 template <int TILE>
-__device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, ProdQuery &pq, ProdItem &it,
-	int lane)
+__device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint64_t total, uint32_t nq,
+	ProdQuery &pq, ProdItem &it, int lane)
 {
 	it.w = w;
 	it.bytes = 0;
 	it.src = nullptr;
-	if (w >= kp.total_work)
+	if (w >= total)
 		return;
 	if (pq.Q == nullptr || w >= pq.end) {
-		const uint32_t qi = warp_search(kp.q_work_prefix, pq.Q ? pq.qi : 0u, kp.nq, w, lane);
+		const uint32_t qi = warp_search(kp.q_work_prefix, pq.Q ? pq.qi : 0u, nq, w, lane);
 		const QDesc *Q = kp.queries + qi;
 		pq.Q = Q;
 		pq.qi = qi;
@@ -1009,13 +1033,24 @@ __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, ProdQ
  * decodes the next item while those copies run.  Claiming one item ahead,
  * not a whole ring ahead, keeps claimed tiles from idling while other CTAs'
  * look-backs wait for their counts.  An invalid claim (past the end of the
- * work list) is announced without data and ends the CTA's pipeline. */
+ * work list) is announced without data and ends the CTA's pipeline.
+ *
+ * In a serving session the work list grows: a claim past the published
+ * work waits for the host's doorbell (or its stop request), and each
+ * released stage counts its tile as stored; the tile that completes a
+ * query writes the query's completion record. */
 template <int TILE>
 __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 {
 	const volatile uint32_t *abort = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags) + kFAbort;
 	uint32_t *held = reinterpret_cast<uint32_t *>(smem + kOffHeld);
 	const uint32_t nst = kp.nstages;
+	const bool serving = kp.serve != nullptr;
+	/* published work and queries: fixed for a launch, growing (from none)
+	 * in a serving session, whose kp.total_work only marks the end item */
+	uint64_t total = serving ? 0ull : kp.total_work;
+	uint32_t nq = serving ? 0u : kp.nq;
+	uint32_t pend = 0;  /* serving: stages whose tile is issued but not yet counted */
 	ProdQuery pq;
 	pq.Q = nullptr;
 	pq.qi = 0;
@@ -1031,8 +1066,79 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		left--;
 		return next++;
 	};
+	/* serving: the tile of stage s is stored; the query's last one reports */
+	auto count_stored = [&](uint32_t s) {
+		const uint32_t qi = held[s];
+		__threadfence();
+		const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
+		const QDesc *Q = kp.queries + qi;
+		if (done == (unsigned)Q->ntiles) {
+			__threadfence();
+			const unsigned long long rows = *reinterpret_cast<volatile unsigned long long *>(Q->total_out);
+			volatile ServeRec *r = kp.recs + qi;
+			r->rows = rows;
+			__threadfence_system();
+			r->seq = (unsigned long long)qi + 1ull;
+		}
+	};
+	/* serving: wait for the tiles issued in iterations lo..hi to be stored
+	 * and count them (lane 0) */
+	auto drain = [&](uint32_t lo, uint32_t hi) {
+		for (uint32_t kk = lo; kk <= hi; kk++) {
+			const uint32_t s = kk % nst;
+			if ((pend >> s) & 1u) {
+				if (!mbar_wait(smem_addr(smem + kOffEmpty + 8 * s), (kk / nst) & 1u, abort))
+					return false;
+				count_stored(s);
+				pend &= ~(1u << s);
+			}
+		}
+		return true;
+	};
+	/* the next work item: in a serving session a claim past the published
+	 * work waits (bounded) for the doorbell; ~0 ends the pipeline */
+	auto next_item = [&](uint32_t issued_k) -> uint32_t {
+		const uint32_t w = claim();
+		if (!serving || w < total)
+			return w;
+		uint64_t t0 = 0;
+		int ok = 1;
+		unsigned nap = 1000;  /* ns between doorbell polls, growing while idle */
+		for (;;) {
+			unsigned long long a = 0;
+			unsigned stop = 0;
+			if (lane == 0) {
+				if (issued_k != ~0u && pend)
+					ok = drain(issued_k + 1 > nst ? issued_k + 1 - nst : 0u, issued_k) ? 1 : 0;
+				a = *reinterpret_cast<const volatile unsigned long long *>(&kp.serve->avail);
+				stop = *reinterpret_cast<const volatile unsigned *>(&kp.serve->stop);
+			}
+			ok = __shfl_sync(0xffffffffu, ok, 0);
+			a = __shfl_sync(0xffffffffu, a, 0);
+			stop = __shfl_sync(0xffffffffu, stop, 0);
+			total = a & kAvailWorkMask;
+			nq = (uint32_t)(a >> 40);
+			if (w < total)
+				return w;
+			if (stop || !ok)
+				return ~0u;
+			if (t0 == 0)
+				t0 = globaltimer_ns();
+			else if (globaltimer_ns() - t0 > (uint64_t)kp.wait_limit_ms * 1000000ull) {
+				if (lane == 0)
+					report(kp.error, DE_STAGE_TIMEOUT);
+				return ~0u;
+			}
+			__nanosleep(nap);
+			nap = nap < 16000 ? nap * 2 : nap;
+		}
+	};
 	ProdItem it;
-	decode_item<TILE>(kp, claim(), pq, it, lane);
+	{
+		/* claim first: next_item updates total and nq */
+		const uint32_t w = next_item(~0u);
+		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
+	}
 	uint32_t k = 0;
 	for (;; k++) {
 		const uint32_t s = k % nst, j = k / nst;
@@ -1044,42 +1150,59 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 				ok = mbar_wait(empty, (j - 1) & 1u, abort);
 				if (!ok && !*abort)
 					report(kp.error, DE_STAGE_TIMEOUT);
+				if (ok && serving && ((pend >> s) & 1u)) {
+					count_stored(s);
+					pend &= ~(1u << s);
+				}
 			}
 			if (!__shfl_sync(0xffffffffu, ok, 0))
 				break;
 		}
 		unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
+		bool end = it.w >= total;
+		if (!end && pq.Q == nullptr) {
+			/* a work item without a decoded query: never copy from it */
+			if (lane == 0)
+				report(kp.error, DE_BAD_WORK);
+			end = true;
+		}
 		if (lane == 0) {
 			StageInfo si;
-			si.work = it.w;
+			si.work = end ? ~0u : it.w;
 			si.query = pq.qi;
 			si.seg = it.seg;
 			si.row0 = it.row0;
 			si.nrows = it.nrows;
 			*reinterpret_cast<StageInfo *>(hdr + sizeof(QDesc)) = si;
 		}
-		if (it.w >= kp.total_work) {
+		if (end) {
+			/* serving: every issued tile is counted before the CTA ends */
+			if (serving && lane == 0 && k > 0)
+				drain(k > nst ? k - nst : 0u, k - 1);
 			__syncwarp();
 			if (lane == 0)
 				mbar_arrive(full);
 			return;
 		}
 		const bool copy_desc = held[s] != pq.qi;
-		const uint32_t total = __reduce_add_sync(0xffffffffu, it.bytes) +
+		const uint32_t bytes = __reduce_add_sync(0xffffffffu, it.bytes) +
 			(copy_desc ? (uint32_t)sizeof(QDesc) : 0u);
 		__syncwarp();
 		if (lane == 0) {
 			held[s] = pq.qi;
+			pend |= 1u << s;
 			fence_proxy_async_smem();
-			mbar_arrive_expect_tx(full, total);
+			mbar_arrive_expect_tx(full, bytes);
 		}
+		pend = __shfl_sync(0xffffffffu, pend, 0);
 		__syncwarp();
 		const uint32_t base = smem_addr(hdr);
 		if (it.bytes)
 			bulk_load(base + pq.off, it.src, it.bytes, full);
 		if (copy_desc && lane == 31)
 			bulk_load(base, pq.Q, (uint32_t)sizeof(QDesc), full);
-		decode_item<TILE>(kp, claim(), pq, it, lane);
+		const uint32_t w = next_item(k);
+		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
 	}
 	/* abandoned: wait (bounded) for the copies already issued so none lands
 	 * after the CTA exits */
@@ -1135,8 +1258,8 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 			} else {
 				/* the inclusive prefix (a query's first tile published its own) */
 				if (si.work != Q.work_first)
-					st_status(&kp.status[si.work],
-						((uint64_t)kp.epoch << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
+					st_status(status_at(kp, si.work),
+						(status_tag(kp, si.work) << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
 						((excl + tile_total) & kStatusValueMask));
 				if (si.work == Q.work_first + Q.ntiles - 1)
 					*Q.total_out = excl + tile_total;
@@ -1220,7 +1343,9 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 						out[pos] = (unsigned char)lds_u8(at);
 				}
 			}
-			if (overflow)
+			/* a serving session reports rows beyond capacity in the
+			 * query's completion record instead */
+			if (overflow && kp.serve == nullptr)
 				report(kp.error, DE_OUTPUT_OVERFLOW);
 		}
 		__syncwarp();
@@ -1268,6 +1393,7 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		for (int x = 0; x < 8; x++)
 			flags[x] = 0;
 		flags[kFEnd] = ~0u;
+		flags[kFWaitMs] = kp.wait_limit_ms;
 		for (uint32_t s = 0; s < kMaxStages; s++)
 			reinterpret_cast<uint32_t *>(smem + kOffHeld)[s] = ~0u;
 		fence_mbar_init();
