@@ -193,6 +193,305 @@ def cpu_baseline(sql_for, rows, threads, repeat=3):
     return alg / secs / 1e9, secs, out_rows
 
 
+# ---- batched, serving and streamed workloads --------------------------------
+
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    print(f"[bench {time.perf_counter() - _T0:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+def _accept_for(cat, types, layout=None):
+    """compiles, decodes cleanly and, for the serving loop, fits its layout"""
+    import virginian_b200 as vb
+
+    def ok(q):
+        try:
+            c = cat.compile(q)
+            p = vb.Program(c.op_list(), c.pc, types)
+        except vb.VirgError:
+            return False
+        if p.maybe_undefined:
+            return False
+        if layout:
+            i = p.info
+            return (i.load_bytes_per_row <= layout[0] and i.row_vector_bytes <= layout[1]
+                    and i.sel_vector_bytes <= layout[2])
+        return True
+    return ok
+
+
+def _device_tables(eng, sizes, seed0):
+    """Resident tables of the benchmark schema generated on the GPU."""
+    import torch
+    import virginian_b200 as vb
+    from virginian_b200 import datagen
+    types = [t for _, t in datagen.SCHEMA_A]
+    tables = []
+    for i, n in enumerate(sizes):
+        segs, keep = datagen.device_table(int(n), datagen.SCHEMA_A, seed=seed0 + i)
+        t = vb.Table(eng, types)
+        t.append(segs)
+        del segs, keep
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        tables.append(t)
+    return tables
+
+
+def _queries(n, seed, ntables, layout=None):
+    import virginian_b200 as vb
+    from virginian_b200 import datagen, querygen, sql as vsql
+    types = [t for _, t in datagen.SCHEMA_A]
+    check = vsql.Catalog()
+    check.add_table("test", datagen.SCHEMA_A)
+    qs = querygen.generate(n, seed=seed, accept=_accept_for(check, types, layout))
+    rng = np.random.default_rng(seed + 1)
+    out = []
+    for q, k in zip(qs, rng.integers(0, ntables, size=n)):
+        c = check.compile(q)
+        out.append((q, int(k), vb.Program(c.op_list(), c.pc, types)))
+    return out
+
+
+def bench_batched(eng, reps=5):
+    """256 generated queries over 64 resident tables of log-uniform size in
+    [10k, 20M] rows: one persistent graph-replayed launch (autotuned shape)
+    against one launch per query, results compared."""
+    import virginian_b200 as vb
+    rng = np.random.default_rng(404)
+    sizes = np.exp(rng.uniform(np.log(1e4), np.log(2e7), size=64)).astype(np.int64)
+    tables = _device_tables(eng, sizes, 1000)
+    log("batched: tables ready")
+    work = _queries(256, 77, len(tables))
+    log("batched: per-query path")
+    # one launch per query (the result count read back after each)
+    for q, k, p in work[:8]:
+        r = tables[k].query(p)
+        _ = r.rows
+        r.close()
+    t0 = time.perf_counter()
+    per_rows = []
+    for q, k, p in work:
+        r = tables[k].query(p)
+        per_rows.append(r.rows)
+        r.close()
+    per_s = time.perf_counter() - t0
+    log("batched: batch path")
+    b = vb.Batch(eng, autotune=True)
+    for q, k, p in work:
+        b.add(p, tables[k])
+    b.run(graph=True)  # autotunes the shape, captures the graph
+    b.wait()
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        b.run(graph=True)
+        b.wait()
+        times.append(time.perf_counter() - t0)
+    batch_s = statistics.median(times)
+    rows_equal = all(b.rows(i) == per_rows[i] for i in range(len(work)))
+    sample = np.random.default_rng(5).choice(len(work), size=24, replace=False)
+    bytes_equal = True
+    for i in sample:
+        q, k, p = work[int(i)]
+        r = tables[k].query(p)
+        a, c = r.download(), b.download(int(i))
+        r.close()
+        bytes_equal = bytes_equal and all(np.array_equal(x.view(np.uint8), y.view(np.uint8)) for x, y in zip(a, c))
+    shape = b.shape()
+    b.close()
+    total_rows = int(sizes.sum())
+    for t in tables:
+        t.close()
+    return {"workload": "256 generated queries (predicate trees of depth 1-4, 1-5 result columns) over 64 "
+                        "resident tables, rows log-uniform in [1e4, 2e7]",
+            "tables": 64, "queries": len(work), "table_rows": total_rows,
+            "batched_qps": round(len(work) / batch_s, 1), "per_query_qps": round(len(work) / per_s, 1),
+            "speedup": round(per_s / batch_s, 2), "batched_ms": round(batch_s * 1e3, 3),
+            "per_query_ms": round(per_s * 1e3, 3), "result_rows": int(sum(per_rows)),
+            "rows_equal": bool(rows_equal), "bytes_equal_sample": bool(bytes_equal),
+            "sample_checked": int(len(sample)), "shape": shape,
+            "launches": {"batched_per_rep": 1, "per_query": len(work)}}
+
+
+def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
+    """The serving loop over 32 resident tables (~40 GB, 10M-200M rows each):
+    Poisson arrivals of generated queries at each rate, latency from arrival
+    to completion seen by the host, against serial one-launch-per-query
+    execution of the same arrival sequence."""
+    import virginian_b200 as vb
+    rng = np.random.default_rng(505)
+    raw = np.exp(rng.uniform(np.log(1e7), np.log(2e8), size=32))
+    sizes = np.clip(raw * (1.43e9 / raw.sum()), 1e7, 2e8).astype(np.int64)
+    tables = _device_tables(eng, sizes, 2000)
+    log("serving: tables ready")
+    layout = (32, 16, 48)
+    work = _queries(per_rate, 88, len(tables), layout)
+    srv = vb.Serve(eng, result_budget_bytes=20 << 30, max_load_bytes_per_row=layout[0],
+                   max_row_vector_bytes=layout[1], max_sel_vector_bytes=layout[2])
+    # warm: one query through each path
+    t = srv.submit(work[0][2], tables[work[0][1]])
+    srv.wait(t, timeout_s=120)
+    srv.release(t)
+    r = tables[work[0][1]].query(work[0][2])
+    _ = r.rows
+    r.close()
+    out = {}
+    exact = True
+    import threading
+    for ri, rate in enumerate(rates):
+        # the same queries at every rate; only the arrival process differs
+        chunk = work[:per_rate]
+        log(f"serving: rate {rate}")
+        gaps = np.random.default_rng(600 + ri).exponential(1.0 / rate, size=len(chunk))
+        arrivals = np.cumsum(gaps) - gaps[0]
+        # a client thread consumes results as they complete and releases
+        # their memory, while arrivals keep coming
+        tickets, lag = [None] * len(chunk), [0.0] * len(chunk)
+        lat, done_at, kept, errors = [0.0] * len(chunk), [0.0] * len(chunk), [], []
+        ready = threading.Semaphore(0)
+
+        def consume():
+            try:
+                for n in range(len(chunk)):
+                    ready.acquire()
+                    st = srv.wait(tickets[n], timeout_s=120)
+                    lat[n] = lag[n] * 1e3 + st["latency_us"] / 1e3
+                    done_at[n] = arrivals[n] + lat[n] / 1e3
+                    if ri == 0 and n < 6:
+                        kept.append((n, srv.download(tickets[n])))
+                    srv.release(tickets[n])
+            except Exception as ex:  # surfaced after the join
+                errors.append(ex)
+
+        th = threading.Thread(target=consume)
+        th.start()
+        t0 = time.perf_counter()
+        for n, ((q, k, p), at) in enumerate(zip(chunk, arrivals)):
+            # wait for the arrival without holding the interpreter lock, so
+            # the client thread keeps consuming results meanwhile
+            while time.perf_counter() - t0 < at:
+                time.sleep(0)
+            lag[n] = time.perf_counter() - t0 - at
+            tickets[n] = srv.submit(p, tables[k])
+            ready.release()
+        th.join()
+        if errors:
+            raise errors[0]
+        serve_span = max(done_at) - arrivals[0]
+        for n, c in kept:
+            q, k, p = chunk[n]
+            r = tables[k].query(p)
+            a = r.download()
+            r.close()
+            exact = exact and all(np.array_equal(x.view(np.uint8), y.view(np.uint8)) for x, y in zip(a, c))
+        # serial: one launch per query, in arrival order
+        log(f"serving: serial at rate {rate}")
+        slat = []
+        t0 = time.perf_counter()
+        for (q, k, p), at in zip(chunk, arrivals):
+            while time.perf_counter() - t0 < at:
+                pass
+            r = tables[k].query(p)
+            _ = r.rows
+            r.close()
+            slat.append((time.perf_counter() - t0 - at) * 1e3)
+        serial_span = time.perf_counter() - t0
+        out[str(rate)] = {
+            "queries": len(chunk), "offered_qps": rate,
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "sustained_qps": round(len(chunk) / serve_span, 1),
+            "serial_p50_ms": round(float(np.percentile(slat, 50)), 3),
+            "serial_p99_ms": round(float(np.percentile(slat, 99)), 3),
+            "serial_qps": round(len(chunk) / serial_span, 1),
+            "submit_lag_p99_ms": round(float(np.percentile(lag, 99)) * 1e3, 3)}
+    st = srv.stats()
+    srv.close()
+    total_rows = int(sizes.sum())
+    for t in tables:
+        t.close()
+    return {"workload": "32 resident tables (rows log-uniform in [1e7, 2e8], %.1f GB), generated queries, "
+                        "Poisson arrivals; latency from arrival to completion seen by the host" %
+                        (total_rows * 28 / 1e9),
+            "table_rows": total_rows, "result_budget_gb": 20, "rates": out,
+            "mix_equals_alone_sample": bool(exact), "sessions": st["sessions"],
+            "readmitted": st["readmitted"], "shape": st["shape"]}
+
+
+STREAM_QUERY = ("SELECT id, uniformi, uniforml, normald FROM test "
+                "WHERE normali20 > 15 AND uniformf < 50.0")
+
+
+def bench_streamed(eng, rows=400_000_000, chunk=25_000_000):
+    """400M rows of the 9-column schema in pinned host memory, streamed
+    through the staging ring, against the same query on the table resident
+    in HBM."""
+    import torch
+    import virginian_b200 as vb
+    from virginian_b200 import datagen, sql as vsql
+    schema = datagen.SCHEMA_B
+    types = [t for _, t in schema]
+    names = ["id"] + [c for c, _ in schema]
+    dt = {"id": torch.int32, "uniformi": torch.int32, "normali5": torch.int32, "normali20": torch.int32,
+          "uniformf": torch.float32, "normalf5": torch.float32, "normalf20": torch.float32,
+          "uniforml": torch.int64, "normald": torch.float64}
+    host = {nm: torch.empty(rows, dtype=dt[nm], pin_memory=True) for nm in names}
+    for a in range(0, rows, chunk):
+        b = min(rows, a + chunk)
+        segs, keep = datagen.device_table(b - a, schema, seed=3000 + a // chunk, seg_rows=b - a)
+        for nm, tsr in zip(names, keep):
+            host[nm][a:b].copy_(tsr)
+        if a:
+            host["id"][a:b] += a
+        del segs, keep
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    log("streamed: host data ready")
+    seg_rows = 161_000 * 8
+    segs = [{"rows": min(rows, a + seg_rows) - a,
+             "key": host["id"][a:].data_ptr(),
+             "cols": [host[c][a:].data_ptr() for c, _ in schema]} for a in range(0, rows, seg_rows)]
+    cat = vsql.Catalog()
+    cat.add_table("test", schema)
+    c = cat.compile(STREAM_QUERY)
+    p = vb.Program(c.op_list(), c.pc, types)
+    r, st0 = vb.query_streamed(eng, p, segs, 4)
+    r.close()
+    runs = []
+    for _ in range(3):
+        r, st = vb.query_streamed(eng, p, segs, 4)
+        n = r.rows
+        r.close()
+        runs.append(st)
+    best = min(runs, key=lambda x: x["seconds"])
+    # the same query on the table resident in HBM
+    log("streamed: resident comparison")
+    t = vb.Table(eng, types)
+    t.append(segs)
+    eng.timing(5)
+    for _ in range(2):
+        rr = t.query(p)
+        _ = rr.rows
+        rr.close()
+    for _ in range(5):
+        rr = t.query(p)
+        nres = rr.rows
+        rr.close()
+    kms = statistics.median(eng.kernel_times(5))
+    t.close()
+    alg = rows * p.info.load_bytes_per_row + n * p.info.out_bytes_per_row
+    del host
+    return {"workload": "400M rows of the 9-column schema (%.1f GB) in pinned host memory; %s" %
+                        (rows * 48 / 1e9, STREAM_QUERY),
+            "rows": rows, "result_rows": int(n), "h2d_bytes": int(best["h2d_bytes"]),
+            "seconds": round(best["seconds"], 4),
+            "host_link_gbs": round(best["h2d_bytes"] / best["seconds"] / 1e9, 2),
+            "scan_gbs_streamed": round(alg / best["seconds"] / 1e9, 2),
+            "resident_kernel_ms": round(kms, 3), "scan_gbs_resident": round(alg / (kms / 1e3) / 1e9, 1),
+            "rows_equal": bool(nres == n)}
+
+
 def run_reference(args):
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -245,6 +544,7 @@ def run_b200(args):
 
     torch.cuda.set_device(local)
     rows = args.rows
+    log(f"headline: generating {rows} rows")
     pcols = pinned_table(rows, seed=rank)
     cols = {k: v[1] for k, v in pcols.items()}
     types = [t for _, t in datagen.SCHEMA_A]
@@ -296,6 +596,7 @@ def run_b200(args):
         return n, ms, kt, launches
 
     # headline
+    log("headline: table resident, timing")
     p = program(HEADLINE_SEL)
     with Clocks(local) as clk:
         out_rows, ms, kt, launches = timed(p, args.steps, args.warmup)
@@ -315,6 +616,7 @@ def run_b200(args):
     achieved = alg / (kernel_ms / 1e3) / 1e9 if kernel_ms else None
 
     # selectivity sweep (device-resident)
+    log("sweep")
     sweep = {}
     for sel in SWEEP:
         ps = program(sel)
@@ -326,6 +628,7 @@ def run_b200(args):
                              "frac_of_hbm": round(alg_bytes(ps, n) / (km / 1e3) / 1e9 / hbm, 3)}
 
     # end to end through the C ABI from pinned host buffers
+    log("e2e")
     info = p.info
     outs = [torch.empty(max(out_rows, 1) + 1024, dtype={0: torch.int32, 2: torch.float32}[info.out_type[j]],
                         pin_memory=True) for j in range(info.nout)]
@@ -355,6 +658,7 @@ def run_b200(args):
     if rank == 0:
         cpu = None
         if args.cpu_baseline and world == 1:
+            log("cpu baseline")
             v1, s1, _ = cpu_baseline(lambda c, d: QUERY.format(c=c, d=d), args.cpu_rows, 1)
             cpu = {"value": round(v1, 3), "unit": "GB/s", "cores": 1, "kind": "reference",
                    "sample": f"{args.cpu_rows} rows of the same table and query, virginia_single "
@@ -391,9 +695,21 @@ def run_b200(args):
         if cpu:
             line["cpu_baseline"] = cpu
             line["cpu_multicore"] = cpu_multi
-        print(json.dumps(line))
     del keep
     table.close()
+    # the other workloads: one GPU, rank 0 (the sharded path covers the scan)
+    if rank == 0 and world == 1:
+        sections = [x for x in args.sections.split(",") if x]
+        for name, fn in (("batched", bench_batched), ("serving", bench_serving),
+                         ("streamed", bench_streamed)):
+            if name in sections:
+                log(name)
+                try:
+                    line[name] = fn(eng)
+                except Exception as ex:  # report, keep the headline line
+                    line[name] = {"error": f"{type(ex).__name__}: {ex}"}
+    if rank == 0:
+        print(json.dumps(line))
     eng.close()
     if world > 1:
         import torch.distributed as dist
@@ -409,6 +725,8 @@ def main():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--cpu-rows", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--sections", default="batched,serving,streamed",
+                    help="workloads besides the headline scan (comma list; empty for none)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

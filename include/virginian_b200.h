@@ -265,6 +265,8 @@ typedef struct {
 	unsigned out_stride[VIRG_MAX_COLUMNS];
 	unsigned out_bytes_per_row;
 	unsigned nuops;                 /* interpreted device ops */
+	unsigned row_vector_bytes;      /* per row: register vectors the filter writes */
+	unsigned sel_vector_bytes;      /* per row: register vectors only the projection writes */
 } virg_gpu_program_info;
 
 /* thread-local description of the last failure on this thread */

@@ -159,7 +159,9 @@ def _segments(segments: Sequence[dict], col_types: Sequence[int]):
     for i, s in enumerate(segments):
         arr[i].rows = int(s["rows"])
         k = s.get("key")
-        if k is not None:
+        if isinstance(k, int):
+            arr[i].key = k
+        elif k is not None:
             k = np.ascontiguousarray(k)
             keep.append(k)
             arr[i].key = k.ctypes.data
@@ -326,8 +328,15 @@ class Serve:
         return {"done": bool(st.done), "rows": st.rows, "readmits": st.readmits,
                 "queue_us": st.queue_us, "latency_us": st.latency_us}
 
-    def wait(self, ticket: int) -> Dict[str, float]:
-        return self.poll(ticket, -1)
+    def wait(self, ticket: int, timeout_s: float = 600.0) -> Dict[str, float]:
+        import time
+        deadline = time.monotonic() + timeout_s
+        while True:
+            st = self.poll(ticket, 100)
+            if st["done"]:
+                return st
+            if time.monotonic() > deadline:
+                raise VirgError(f"serve wait: query {ticket} not done after {timeout_s} s: {self.stats()}")
 
     def download(self, ticket: int) -> List[np.ndarray]:
         n = self.wait(ticket)["rows"]

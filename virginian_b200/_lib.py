@@ -68,7 +68,8 @@ class ProgramInfo(ctypes.Structure):
                 ("load_bytes_per_row", ctypes.c_uint), ("nout", ctypes.c_uint),
                 ("out_type", ctypes.c_int * VIRG_MAX_COLUMNS),
                 ("out_stride", ctypes.c_uint * VIRG_MAX_COLUMNS),
-                ("out_bytes_per_row", ctypes.c_uint), ("nuops", ctypes.c_uint)]
+                ("out_bytes_per_row", ctypes.c_uint), ("nuops", ctypes.c_uint),
+                ("row_vector_bytes", ctypes.c_uint), ("sel_vector_bytes", ctypes.c_uint)]
 
 
 def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:

@@ -466,6 +466,21 @@ void scheduler(virg_serve *s)
 			std::unique_lock<std::mutex> lk(s->mu);
 			if (s->running && !s->inflight.empty() && harvest(s))
 				busy = true;
+			/* a session kernel that ended with queries still in flight (a
+			 * device error ended it) fails the loop */
+			if (s->running && !s->inflight.empty() && cudaStreamQuery(s->kstream) != cudaErrorNotReady) {
+				harvest(s);
+				if (!s->inflight.empty()) {
+					unsigned err = 0;
+					cudaMemcpy(&err, s->d_ctrl + 1, sizeof(err), cudaMemcpyDeviceToHost);
+					char buf[160];
+					snprintf(buf, sizeof(buf), "the serving kernel ended with %zu queries in flight (device error %u: %s)",
+						s->inflight.size(), err, device_error_text(err));
+					s->fail = buf;
+					s->running = false;
+					busy = true;
+				}
+			}
 			/* a session that cannot take the next query ends once drained */
 			if (s->running && !s->pending.empty() && s->inflight.empty() &&
 				(s->nq >= s->cfg.max_queries || s->work >= kSessionWorkLimit / 2 ||

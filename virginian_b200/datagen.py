@@ -98,3 +98,39 @@ def segments(cols: Dict[str, np.ndarray], schema: Sequence[Tuple[str, int]],
         out.append({"rows": e - s, "key": cols["id"][s:e],
                     "cols": [cols[name][s:e] for name, _ in schema]})
     return out
+
+
+def device_table(n: int, schema: Sequence[Tuple[str, int]] = SCHEMA_A, seed: int = 0,
+                 seg_rows: int = TABLET_ROWS_A, device: str = "cuda"):
+    """A table of n rows generated on the GPU with torch, for workloads too
+    large to generate on the host (tens of GB): the same column
+    distributions as column(), from torch's own seeded generator, so the
+    bytes differ from the host generator's.  Returns (segments with device
+    pointers, tensors to keep alive while they are used)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    cols = {"id": torch.arange(n, dtype=torch.int32, device=device)}
+    for name, _ in schema:
+        if name == "uniformi":
+            t = torch.floor(torch.rand(n, generator=g, device=device) * 100).to(torch.int32)
+        elif name in ("normali5", "normali20"):
+            sd = 5.0 if name == "normali5" else 20.0
+            t = torch.round(torch.randn(n, generator=g, device=device) * sd).to(torch.int32)
+        elif name == "uniformf":
+            t = torch.rand(n, generator=g, device=device) * 100.0
+        elif name in ("normalf5", "normalf20"):
+            t = torch.randn(n, generator=g, device=device) * (5.0 if name == "normalf5" else 20.0)
+        elif name == "uniforml":
+            t = torch.randint(-(2 ** 63), 2 ** 63 - 1, (n,), generator=g, device=device, dtype=torch.int64)
+        elif name == "normald":
+            t = torch.randn(n, generator=g, device=device, dtype=torch.float64)
+        else:
+            raise ValueError(name)
+        cols[name] = t.contiguous()
+    segs = []
+    for a in range(0, n, seg_rows):
+        b = min(n, a + seg_rows)
+        segs.append({"rows": b - a, "key": cols["id"][a:].data_ptr(),
+                     "cols": [cols[c][a:].data_ptr() for c, _ in schema]})
+    return segs, list(cols.values())
