@@ -146,17 +146,11 @@ def barrier(world):
 
 
 def exchange_counts(n, world):
-    """All-gather each rank's result count; returns this rank's global offset."""
+    """Each rank's first row in the global result (virginian_b200.shard)."""
     if world == 1:
         return 0, n
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([n], dtype=torch.int64, device="cuda")
-    out = [torch.zeros_like(t) for _ in range(world)]
-    dist.all_gather(out, t)
-    counts = [int(x.item()) for x in out]
-    r = dist.get_rank()
-    return sum(counts[:r]), sum(counts)
+    from virginian_b200 import shard
+    return shard.exchange_counts(n, device="cuda")
 
 
 def pinned_table(n, seed):
