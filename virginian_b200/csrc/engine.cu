@@ -59,12 +59,16 @@ static int type_bytes(int t)
 void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
 	uint32_t *row_bytes, uint32_t *sel_bytes)
 {
-	/* a stage: query descriptor + tile info header, then the columns */
+	/* a stage: query descriptor + tile info header, then the columns the
+	 * filter reads (load_off 0: not staged, the projection gathers it) */
+	const uint32_t staged = staged_loads(P);
 	uint32_t off = kStageHdr;
 	for (unsigned i = 0; i < P.nload; i++) {
+		const bool st = (staged >> i) & 1u;
 		if (load_off)
-			load_off[i] = off;
-		off += (uint32_t)align_up((size_t)tile * P.load_stride[i], 128);
+			load_off[i] = st ? off : 0u;
+		if (st)
+			off += (uint32_t)align_up((size_t)tile * P.load_stride[i], 128);
 	}
 	*stage_bytes = off;
 	uint32_t row = 0, sel = 0;
@@ -212,25 +216,52 @@ static uint32_t op_head(const UOp &u)
 void fill_operands(QDesc &d, uint32_t vec_area)
 {
 	const Program &P = d.prog;
-	auto od = [&](uint8_t cls, uint8_t idx) -> uint32_t {
+	/* filter uops read staged columns and the stage's copy of the
+	 * descriptor's constants, by shared-memory offset */
+	auto od_filter = [&](uint8_t cls, uint8_t idx) -> uint32_t {
 		if (cls == OC_COL)
 			return OD_STAGE | (uint32_t)(kSmemHeader + d.load_off[idx]);
 		if (cls == OC_VEC)
 			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | (vec_area + d.vec_off[idx]);
-		/* scalars are read from the stage's copy of the descriptor */
 		return OD_SCALAR |
 			(uint32_t)(kSmemHeader + offsetof(QDesc, prog) + offsetof(Program, consts) + idx * 8u);
+	};
+	/* projection uops and result columns run after the tile's stage is
+	 * released: columns by load index (gathered from the segment's column
+	 * in device memory), constants by index (from the descriptor in device
+	 * memory) */
+	auto od_proj = [&](uint8_t cls, uint8_t idx) -> uint32_t {
+		if (cls == OC_COL)
+			return OD_STAGE | idx;
+		if (cls == OC_VEC)
+			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | (vec_area + d.vec_off[idx]);
+		return OD_SCALAR | idx;
 	};
 	for (uint32_t k = 0; k < P.nuops; k++) {
 		const UOp &u = P.uops[k];
 		OpRec &r = d.ops[k];
 		r.head = op_head(u);
+		auto od = [&](uint8_t cls, uint8_t idx) { return k < P.nfilter ? od_filter(cls, idx) : od_proj(cls, idx); };
 		r.a = od(u.a_cls, u.a_idx);
 		r.b = od(u.b_cls, u.b_idx);
 		r.d = od(OC_VEC, u.dst);
 	}
 	for (uint32_t j = 0; j < P.nout; j++)
-		d.od_out[j] = od(P.out_cls[j], P.out_idx[j]);
+		d.od_out[j] = od_proj(P.out_cls[j], P.out_idx[j]);
+}
+
+/* loads read by filter uops: only these are staged in shared memory */
+uint32_t staged_loads(const Program &P)
+{
+	uint32_t m = 0;
+	for (uint32_t k = 0; k < P.nfilter; k++) {
+		const UOp &u = P.uops[k];
+		if (u.a_cls == OC_COL)
+			m |= 1u << u.a_idx;
+		if (u.b_cls == OC_COL)
+			m |= 1u << u.b_idx;
+	}
+	return m;
 }
 
 size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles)

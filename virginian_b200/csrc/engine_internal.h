@@ -121,6 +121,7 @@ void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uin
 	uint32_t *row_slot, uint32_t *vec_bytes);
 size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes);
 void fill_operands(QDesc &d, uint32_t vec_area);
+uint32_t staged_loads(const Program &P);
 size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles);
 int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Shape *forced,
 	unsigned char *db, Plan &plan);

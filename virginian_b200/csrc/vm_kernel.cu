@@ -9,22 +9,28 @@
  *
  *  - producer warp: claims work items (one tile of one segment of one query)
  *    from a global counter, in order, decodes them warp-wide and copies the
- *    tile's columns (plus the query's descriptor when the stage does not hold
- *    it) into a ring of shared-memory stages with TMA bulk copies
- *    (cp.async.bulk completing on the stage's full barrier);
+ *    columns the filter reads (plus the query's descriptor when the stage
+ *    does not hold it) into a ring of shared-memory stages with TMA bulk
+ *    copies (cp.async.bulk completing on the stage's full barrier);
  *  - filter warps (THREADS threads): run the filter ops over every row of the
  *    tile (row state as bit masks: valid, active, and rows parked at pending
  *    jump targets; each lane holds R rows in chunks of 4 consecutive rows),
  *    count valid rows per 64 rows with bit-plane ballots, scan the counts and
  *    write the tile's selected rows, in row order, to a shared list, then
- *    publish the tile's count to the query's look-back words;
+ *    publish the tile's count to the query's look-back words and release
+ *    the stage: the list and the tile's row vectors sit in one of kSlots
+ *    slots, so the next tiles' copies and filters run while this one's
+ *    projection waits for its offset;
  *  - look-back warp: resolves the tile's position in the query's result with
  *    a warp-wide decoupled look-back over earlier tiles (32 status words per
  *    round); a tile that directly follows the CTA's previous tile of the same
  *    query starts where that one ended, with no look-back;
  *  - projection warps: run the projection ops over the tile's list in
- *    32-entry batches and write each result row to the tile's offset plus
- *    its list position (coalesced stores), then release the stage.
+ *    32-entry batches, gathering the columns they read from device memory
+ *    at the selected rows only (late materialization: a selective query
+ *    reads only the sectors that hold selected rows), and write each result
+ *    row to the tile's offset plus its list position (coalesced stores),
+ *    then release the slot.
  *
  * Each op is one 16-byte record fetched with a single shared-memory load and
  * dispatched on one handler code; operands are read and written by 32-bit
@@ -70,10 +76,13 @@ constexpr unsigned kOffOff = kOffCdone + 8 * kSlots;         /* uint64[kSlots]: 
 constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;         /* uint32[8]: ok[kSlots], abort, end tile */
 constexpr unsigned kOffTot = kOffFlags + 32;                 /* uint32[kSlots]: tile totals */
 constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;          /* uint32[kMaxStages]: query per stage */
+constexpr unsigned kOffSlotInfo = 336;                       /* uint32[kSlots][4]: query, segment, first row */
+constexpr unsigned kOffPCount = kOffSlotInfo + 16 * kSlots;  /* uint32[kSlots]: projection warps done (serving) */
 constexpr unsigned kOffCnt = 512;                            /* uint32[kSlots][kMaxGroups]: per 64 rows */
 constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
 static_assert(kSlots <= kFAbort, "ok flags per slot");
-static_assert(kOffHeld + 4 * kMaxStages <= kOffCnt, "smem header layout");
+static_assert(kOffHeld + 4 * kMaxStages <= kOffSlotInfo, "smem header layout");
+static_assert(kOffPCount + 4 * kSlots <= kOffCnt, "smem header layout");
 static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
 static_assert(sizeof(QDesc) % 16 == 0, "QDesc copies in 16-byte chunks");
 static_assert(kStageHdr >= sizeof(QDesc) + sizeof(StageInfo), "stage header too small");
@@ -82,12 +91,6 @@ static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a
 /* where the fields the compute warps read sit in a stage's descriptor copy */
 constexpr uint32_t kQOps = (uint32_t)offsetof(QDesc, ops);
 constexpr uint32_t kQNFilter = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nfilter));
-constexpr uint32_t kQNUops = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nuops));
-constexpr uint32_t kQNOut = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nout));
-constexpr uint32_t kQOutStride = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, out_stride));
-constexpr uint32_t kQOdOut = (uint32_t)offsetof(QDesc, od_out);
-constexpr uint32_t kQOutPtr = (uint32_t)offsetof(QDesc, out_ptr);
-constexpr uint32_t kQCapacity = (uint32_t)offsetof(QDesc, capacity);
 constexpr uint32_t kQVecSlot = (uint32_t)offsetof(QDesc, vec_slot);
 
 /* ---- PTX wrappers ---------------------------------------------------- */
@@ -160,6 +163,17 @@ __device__ __forceinline__ uint64_t ld_status(const uint64_t *p)
 __device__ __forceinline__ void st_status(uint64_t *p, uint64_t v)
 {
 	asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+/* the serving doorbell, with acquire semantics: descriptors, work prefixes
+ * and tile prefixes the host wrote before ringing it are seen by every
+ * later load of this CTA (ordered through its mbarriers), even where a load
+ * of a neighbouring entry had cached their lines before the host wrote them */
+__device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long *p)
+{
+	unsigned long long v;
+	asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
 }
 
 __device__ __forceinline__ void report(unsigned *error, unsigned code)
@@ -734,46 +748,94 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowS
 }
 
 /* ---- projection: the tile's selected rows, in row order ------------------
- * The projection warps share the tile's list: warp p takes the 32-entry
- * batches p, p + P, p + 2 P, ...; entry e is selection index e and its
- * result row lands at the tile's offset + e. */
+ * The projection runs after the tile's stage is released, on the tile's
+ * list and row-vector slot: columns are gathered from the segment in device
+ * memory by tile row (only the selected rows' sectors are read) and
+ * constants come from the query's descriptor in device memory.  The
+ * projection warps share the list: warp p takes the 32-entry batches p,
+ * p + P, p + 2 P, ...; entry e is selection index e and its result row
+ * lands at the tile's offset + e. */
 
 struct PArgs {
-	uint32_t sbase, sd, vd;
-	uint32_t list;   /* smem address of the tile's list of tile rows (u16) */
-	uint32_t n;      /* entries */
-	uint32_t e0;     /* this lane's first entry */
-	uint32_t step;   /* entries between this lane's entries: 32 P */
+	uint32_t sbase;     /* shared memory base address */
+	uint32_t vd;        /* the slot's offset in the row-vector area */
+	uint32_t list;      /* smem address of the tile's list of tile rows (u16) */
+	uint32_t n;         /* entries */
+	uint32_t e0;        /* this lane's first entry */
+	uint32_t step;      /* entries between this lane's entries: 32 P */
+	const QDesc *gq;    /* the query's descriptor in device memory */
+	uint64_t colbase;   /* lane i: column i's address of the tile's row 0 */
 };
 
-/* element address of a list entry */
-__device__ __forceinline__ uint32_t p_addr(const Opnd &o, uint32_t row, uint32_t e)
+/* a projection operand: a column in device memory, a row vector (by tile
+ * row), a selection vector (by entry) or a constant */
+struct POp {
+	uint32_t kind;
+	uint32_t saddr;
+	const unsigned char *gaddr;
+	uint64_t bits;
+};
+
+/* resolves an operand descriptor; every lane of the warp calls it */
+__device__ __forceinline__ POp popnd(uint32_t od, const PArgs &c)
 {
-	return o.addr + (o.sel ? e : row) * o.step;
+	POp o;
+	o.kind = od >> 30;
+	const uint32_t off = od & OD_OFFSET;
+	const uint64_t col = __shfl_sync(0xffffffffu, c.colbase, (int)(off & 31u));
+	o.gaddr = reinterpret_cast<const unsigned char *>(col);
+	o.saddr = c.sbase + off + (o.kind == (OD_ROWVEC >> 30) ? c.vd : 0u);
+	o.bits = o.kind == (OD_SCALAR >> 30) ? c.gq->prog.consts[off % kMaxRegs] : 0ull;
+	return o;
+}
+
+template <typename T>
+__device__ __forceinline__ T ldg_elem(const unsigned char *p)
+{
+	if constexpr (sizeof(T) == 8)
+		return from_bits<T>((uint64_t)__ldg(reinterpret_cast<const unsigned long long *>(p)));
+	else if constexpr (sizeof(T) == 4)
+		return from_bits<T>((uint64_t)__ldg(reinterpret_cast<const unsigned int *>(p)));
+	else
+		return from_bits<T>((uint64_t)__ldg(reinterpret_cast<const unsigned char *>(p)));
+}
+
+template <typename T>
+__device__ __forceinline__ T pget(const POp &o, uint32_t row, uint32_t e)
+{
+	if (o.kind == (OD_STAGE >> 30))
+		return ldg_elem<T>(o.gaddr + (size_t)row * sizeof(T));
+	if (o.kind == (OD_ROWVEC >> 30))
+		return SM<T>::ld(o.saddr + row * (uint32_t)sizeof(T));
+	if (o.kind == (OD_SELVEC >> 30))
+		return SM<T>::ld(o.saddr + e * (uint32_t)sizeof(T));
+	return from_bits<T>(o.bits);
+}
+
+/* destinations are register vectors */
+template <typename T>
+__device__ __forceinline__ void pput(const POp &o, uint32_t row, uint32_t e, T v)
+{
+	SM<T>::st(o.saddr + (o.kind == (OD_SELVEC >> 30) ? e : row) * (uint32_t)sizeof(T), v);
 }
 
 template <typename T, int OP>
 __device__ __forceinline__ void p_math(const uint4 &rec, const PArgs &c)
 {
-	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
-	const Opnd b = opnd<sizeof(T)>(rec.z, c.sbase, c.sd, c.vd);
-	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
+	const POp a = popnd(rec.y, c), b = popnd(rec.z, c), d = popnd(rec.w, c);
 	for (uint32_t e = c.e0; e < c.n; e += c.step) {
 		const uint32_t row = lds_u16(c.list + 2 * e);
-		const T x = SM<T>::ld(p_addr(a, row, e));
-		const T y = SM<T>::ld(p_addr(b, row, e));
-		SM<T>::st(p_addr(d, row, e), Math<T, OP>::eval(x, y));
+		pput<T>(d, row, e, Math<T, OP>::eval(pget<T>(a, row, e), pget<T>(b, row, e)));
 	}
 }
 
 template <typename T>
 __device__ __forceinline__ void p_copy(const uint4 &rec, const PArgs &c)
 {
-	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
-	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
+	const POp a = popnd(rec.y, c), d = popnd(rec.w, c);
 	for (uint32_t e = c.e0; e < c.n; e += c.step) {
 		const uint32_t row = lds_u16(c.list + 2 * e);
-		SM<T>::st(p_addr(d, row, e), SM<T>::ld(p_addr(a, row, e)));
+		pput<T>(d, row, e, pget<T>(a, row, e));
 	}
 }
 
@@ -805,6 +867,20 @@ __device__ __forceinline__ void project_op(const uint4 &rec, const PArgs &c)
 		else if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, c);
 		else p_copy<uint32_t>(rec, c);
 	}
+}
+
+/* one result column of the tile's entries, at the tile's offset; false if a
+ * row lies beyond the buffers' capacity */
+template <typename T>
+__device__ __forceinline__ bool p_store(const POp &a, const PArgs &c, T *out, uint64_t off, uint64_t cap)
+{
+	for (uint32_t e = c.e0; e < c.n; e += c.step) {
+		const uint64_t pos = off + e;
+		if (pos >= cap)
+			return false;
+		out[pos] = pget<T>(a, lds_u16(c.list + 2 * e), e);
+	}
+	return true;
 }
 
 /* ---- ordered placement ------------------------------------------------- */
@@ -860,13 +936,13 @@ __device__ __forceinline__ void publish_count(const KParams &kp, const QDesc &Q,
  * filtered.  Returns false if a predecessor never published (bounded wait). */
 constexpr int kLookbackPerLane = 4;
 
-__device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int64_t known, uint64_t known_end,
-	int lane, uint64_t *excl_out)
+__device__ bool lookback_excl(const KParams &kp, uint64_t work_first, uint64_t base, uint64_t g,
+	int64_t known, uint64_t known_end, int lane, uint64_t *excl_out)
 {
 	constexpr int W = 32 * kLookbackPerLane;
-	const int64_t first = (int64_t)Q.work_first;
+	const int64_t first = (int64_t)work_first;
 	if ((int64_t)g == first) {
-		*excl_out = query_base(Q);
+		*excl_out = base;
 		return true;
 	}
 	/* indices below `floor` are not read: the query's start, or the known
@@ -1020,25 +1096,24 @@ __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint6
 	it.seg = s;
 	it.row0 = row0;
 	it.nrows = min((uint32_t)TILE, sd->rows - row0);
-	if ((uint32_t)lane < pq.nload) {
+	/* only the columns the filter reads are staged (load_off != 0) */
+	if ((uint32_t)lane < pq.nload && pq.off != 0) {
 		it.src = static_cast<const unsigned char *>(sd->col[pq.src]) + (size_t)row0 * pq.stride;
 		it.bytes = (it.nrows * pq.stride + 15u) & ~15u;
 	}
 }
 
-/* The producer warp fills the ring of stages.  Once the compute warps
- * released a stage it announces the decoded work item and issues its copies
- * (lane i copies column i; the query descriptor only when the stage does
- * not hold it already), then claims (kClaim per atomic, in order) and
- * decodes the next item while those copies run.  Claiming one item ahead,
- * not a whole ring ahead, keeps claimed tiles from idling while other CTAs'
- * look-backs wait for their counts.  An invalid claim (past the end of the
- * work list) is announced without data and ends the CTA's pipeline.
- *
- * In a serving session the work list grows: a claim past the published
- * work waits for the host's doorbell (or its stop request), and each
- * released stage counts its tile as stored; the tile that completes a
- * query writes the query's completion record. */
+/* The producer warp fills the ring of stages.  Once the filter warps and the
+ * look-back warp released a stage it announces the decoded work item and
+ * issues its copies (lane i copies column i if the filter reads it; the
+ * query descriptor only when the stage does not hold it already), then
+ * claims (kClaim per atomic, in order) and decodes the next item while
+ * those copies run.  Claiming one item ahead, not a whole ring ahead, keeps
+ * claimed tiles from idling while other CTAs' look-backs wait for their
+ * counts.  An invalid claim (past the end of the work list) is announced
+ * without data and ends the CTA's pipeline.  In a serving session the work
+ * list grows: a claim past the published work waits (bounded) for the
+ * host's doorbell or its stop request. */
 template <int TILE>
 __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 {
@@ -1050,7 +1125,6 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	 * in a serving session, whose kp.total_work only marks the end item */
 	uint64_t total = serving ? 0ull : kp.total_work;
 	uint32_t nq = serving ? 0u : kp.nq;
-	uint32_t pend = 0;  /* serving: stages whose tile is issued but not yet counted */
 	ProdQuery pq;
 	pq.Q = nullptr;
 	pq.qi = 0;
@@ -1066,61 +1140,27 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		left--;
 		return next++;
 	};
-	/* serving: the tile of stage s is stored; the query's last one reports */
-	auto count_stored = [&](uint32_t s) {
-		const uint32_t qi = held[s];
-		__threadfence();
-		const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
-		const QDesc *Q = kp.queries + qi;
-		if (done == (unsigned)Q->ntiles) {
-			__threadfence();
-			const unsigned long long rows = *reinterpret_cast<volatile unsigned long long *>(Q->total_out);
-			volatile ServeRec *r = kp.recs + qi;
-			r->rows = rows;
-			__threadfence_system();
-			r->seq = (unsigned long long)qi + 1ull;
-		}
-	};
-	/* serving: wait for the tiles issued in iterations lo..hi to be stored
-	 * and count them (lane 0) */
-	auto drain = [&](uint32_t lo, uint32_t hi) {
-		for (uint32_t kk = lo; kk <= hi; kk++) {
-			const uint32_t s = kk % nst;
-			if ((pend >> s) & 1u) {
-				if (!mbar_wait(smem_addr(smem + kOffEmpty + 8 * s), (kk / nst) & 1u, abort))
-					return false;
-				count_stored(s);
-				pend &= ~(1u << s);
-			}
-		}
-		return true;
-	};
-	/* the next work item: in a serving session a claim past the published
-	 * work waits (bounded) for the doorbell; ~0 ends the pipeline */
-	auto next_item = [&](uint32_t issued_k) -> uint32_t {
+	/* the next work item; ~0 ends the pipeline */
+	auto next_item = [&]() -> uint32_t {
 		const uint32_t w = claim();
 		if (!serving || w < total)
 			return w;
 		uint64_t t0 = 0;
-		int ok = 1;
 		unsigned nap = 1000;  /* ns between doorbell polls, growing while idle */
 		for (;;) {
 			unsigned long long a = 0;
 			unsigned stop = 0;
 			if (lane == 0) {
-				if (issued_k != ~0u && pend)
-					ok = drain(issued_k + 1 > nst ? issued_k + 1 - nst : 0u, issued_k) ? 1 : 0;
-				a = *reinterpret_cast<const volatile unsigned long long *>(&kp.serve->avail);
+				a = ld_acquire_sys(&kp.serve->avail);
 				stop = *reinterpret_cast<const volatile unsigned *>(&kp.serve->stop);
 			}
-			ok = __shfl_sync(0xffffffffu, ok, 0);
 			a = __shfl_sync(0xffffffffu, a, 0);
 			stop = __shfl_sync(0xffffffffu, stop, 0);
 			total = a & kAvailWorkMask;
 			nq = (uint32_t)(a >> 40);
 			if (w < total)
 				return w;
-			if (stop || !ok)
+			if (stop)
 				return ~0u;
 			if (t0 == 0)
 				t0 = globaltimer_ns();
@@ -1136,7 +1176,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	ProdItem it;
 	{
 		/* claim first: next_item updates total and nq */
-		const uint32_t w = next_item(~0u);
+		const uint32_t w = next_item();
 		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
 	}
 	uint32_t k = 0;
@@ -1150,10 +1190,6 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 				ok = mbar_wait(empty, (j - 1) & 1u, abort);
 				if (!ok && !*abort)
 					report(kp.error, DE_STAGE_TIMEOUT);
-				if (ok && serving && ((pend >> s) & 1u)) {
-					count_stored(s);
-					pend &= ~(1u << s);
-				}
 			}
 			if (!__shfl_sync(0xffffffffu, ok, 0))
 				break;
@@ -1176,9 +1212,6 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 			*reinterpret_cast<StageInfo *>(hdr + sizeof(QDesc)) = si;
 		}
 		if (end) {
-			/* serving: every issued tile is counted before the CTA ends */
-			if (serving && lane == 0 && k > 0)
-				drain(k > nst ? k - nst : 0u, k - 1);
 			__syncwarp();
 			if (lane == 0)
 				mbar_arrive(full);
@@ -1190,18 +1223,16 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		__syncwarp();
 		if (lane == 0) {
 			held[s] = pq.qi;
-			pend |= 1u << s;
 			fence_proxy_async_smem();
 			mbar_arrive_expect_tx(full, bytes);
 		}
-		pend = __shfl_sync(0xffffffffu, pend, 0);
 		__syncwarp();
 		const uint32_t base = smem_addr(hdr);
 		if (it.bytes)
 			bulk_load(base + pq.off, it.src, it.bytes, full);
 		if (copy_desc && lane == 31)
 			bulk_load(base, pq.Q, (uint32_t)sizeof(QDesc), full);
-		const uint32_t w = next_item(k);
+		const uint32_t w = next_item();
 		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
 	}
 	/* abandoned: wait (bounded) for the copies already issued so none lands
@@ -1231,20 +1262,26 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 		 * over earlier tiles starts while the filter warps run */
 		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort))
 			return;
-		/* the stage holds tile i until the tile's stores, which wait for
-		 * this warp */
 		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
 		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
 		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
 		if (si.work >= kp.total_work)
 			return;
+		/* what this warp needs of the stage, before releasing its share */
+		const uint64_t first = Q.work_first, last = Q.work_first + Q.ntiles - 1;
+		unsigned long long *const total_out = Q.total_out;
+		const uint64_t base = query_base(Q);
+		__syncwarp();
+		if (lane == 0)
+			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
 		uint64_t excl = 0;
 		bool ok = true;
-		const bool follows = si.work == prev_work + 1 && si.work != Q.work_first;
+		const bool follows = si.work == prev_work + 1 && si.work != first;
 		if (follows)
 			excl = prev_end;
 		else
-			ok = lookback_excl(kp, Q, si.work, prev_work == ~0ull ? -1 : (int64_t)prev_work, prev_end, lane, &excl);
+			ok = lookback_excl(kp, first, base, si.work, prev_work == ~0ull ? -1 : (int64_t)prev_work,
+				prev_end, lane, &excl);
 		/* the tile's own count */
 		if (ok && !mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
 			return;
@@ -1257,12 +1294,12 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 				report(kp.error, DE_LOOKBACK_TIMEOUT);
 			} else {
 				/* the inclusive prefix (a query's first tile published its own) */
-				if (si.work != Q.work_first)
+				if (si.work != first)
 					st_status(status_at(kp, si.work),
 						(status_tag(kp, si.work) << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
 						((excl + tile_total) & kStatusValueMask));
-				if (si.work == Q.work_first + Q.ntiles - 1)
-					*Q.total_out = excl + tile_total;
+				if (si.work == last)
+					*total_out = excl + tile_total;
 			}
 			offs[q] = excl;
 			flags[q] = ok ? 1u : 0u;
@@ -1275,17 +1312,14 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 	}
 }
 
-/* ---- projection warps: projection and ordered stores of each tile -------- */
-
 template <int THREADS, int R, int P>
 __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int lane)
 {
 	constexpr int TILE = THREADS * R;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
 	const uint32_t sbase = smem_addr(smem);
-	const uint32_t nst = kp.nstages;
 	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst, q = i % kSlots;
+		const uint32_t q = i % kSlots;
 		if (!mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
 			if (lane == 0 && !flags[kFAbort]) {
 				report(kp.error, DE_STAGE_TIMEOUT);
@@ -1295,21 +1329,36 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 		}
 		if (flags[kFEnd] == i)
 			return;
-		const uint32_t sd = s * kp.stage_bytes;
-		const uint32_t qd = sbase + kp.stage_area + sd;
+		/* the tile: query, segment and first row, left by the filter warps */
+		const uint32_t qi = lds_u32(sbase + kOffSlotInfo + 16 * q);
+		const uint32_t seg = lds_u32(sbase + kOffSlotInfo + 16 * q + 4);
+		const uint32_t row0 = lds_u32(sbase + kOffSlotInfo + 16 * q + 8);
+		/* plain loads, not the read-only path: a serving session's host
+		 * writes descriptors while the kernel runs */
+		const QDesc *gq = kp.queries + qi;
 		PArgs c;
 		c.sbase = sbase;
-		c.sd = sd;
-		c.vd = q * lds_u32(qd + kQVecSlot);
+		c.vd = q * gq->vec_slot;
 		c.list = sbase + kp.sel_area + q * TILE * 2;
 		c.n = lds_u32(sbase + kOffTot + 4 * q);
 		c.e0 = 32u * (uint32_t)pw + (uint32_t)lane;
 		c.step = 32u * P;
-		const uint32_t ops = qd + kQOps;
-		if (c.e0 - (uint32_t)lane < c.n) {
-			const uint32_t nu = lds_u32(qd + kQNUops) - 1u;
-			for (uint32_t k = lds_u32(qd + kQNFilter); k < nu; k++)
-				project_op(lds_v4(ops + 16u * k), c);
+		c.gq = gq;
+		c.colbase = 0;
+		const bool mine = c.e0 - (uint32_t)lane < c.n;
+		if (mine) {
+			const uint32_t nload = gq->prog.nload;
+			if ((uint32_t)lane < nload) {
+				const SegDesc *sd = gq->segs + seg;
+				const uint32_t src = gq->prog.load_src[lane];
+				const uint32_t stride = gq->prog.load_stride[lane];
+				c.colbase = reinterpret_cast<uint64_t>(sd->col[src]) + (uint64_t)row0 * stride;
+			}
+			const uint32_t nu = gq->prog.nuops - 1u;
+			for (uint32_t k = gq->prog.nfilter; k < nu; k++) {
+				const uint4 rec = *reinterpret_cast<const uint4 *>(&gq->ops[k]);
+				project_op(rec, c);
+			}
 		}
 
 		/* ---- stores at the tile's offset, once the look-back resolved it */
@@ -1318,39 +1367,49 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 		if (!flags[q])
 			return;
 		const uint64_t off = lds_u64(sbase + kOffOff + 8 * q);
-		if (c.e0 - (uint32_t)lane < c.n) {
-			const uint64_t cap = lds_u64(qd + kQCapacity);
-			bool overflow = false;
-			const uint32_t nout = lds_u32(qd + kQNOut);
+		if (mine) {
+			const uint64_t cap = gq->capacity;
+			bool ok = true;
+			const uint32_t nout = gq->prog.nout;
 			for (uint32_t j = 0; j < nout; j++) {
-				const uint32_t od = lds_u32(qd + kQOdOut + 4 * j);
-				unsigned char *out = reinterpret_cast<unsigned char *>(lds_u64(qd + kQOutPtr + 8 * j));
-				const uint32_t stride = lds_u8(qd + kQOutStride + j);
-				const Opnd a = stride == 8 ? opnd<8>(od, sbase, sd, c.vd)
-					: stride == 4 ? opnd<4>(od, sbase, sd, c.vd) : opnd<1>(od, sbase, sd, c.vd);
-				for (uint32_t e = c.e0; e < c.n; e += c.step) {
-					const uint64_t pos = off + e;
-					if (pos >= cap) {
-						overflow = true;
-						break;
-					}
-					const uint32_t at = p_addr(a, lds_u16(c.list + 2 * e), e);
-					if (stride == 4)
-						reinterpret_cast<uint32_t *>(out)[pos] = lds_u32(at);
-					else if (stride == 8)
-						reinterpret_cast<unsigned long long *>(out)[pos] = lds_u64(at);
-					else
-						out[pos] = (unsigned char)lds_u8(at);
-				}
+				const POp a = popnd(gq->od_out[j], c);
+				void *out = gq->out_ptr[j];
+				const uint32_t stride = gq->prog.out_stride[j];
+				if (stride == 4)
+					ok &= p_store<uint32_t>(a, c, static_cast<uint32_t *>(out), off, cap);
+				else if (stride == 8)
+					ok &= p_store<unsigned long long>(a, c, static_cast<unsigned long long *>(out), off, cap);
+				else
+					ok &= p_store<unsigned char>(a, c, static_cast<unsigned char *>(out), off, cap);
 			}
 			/* a serving session reports rows beyond capacity in the
 			 * query's completion record instead */
-			if (overflow && kp.serve == nullptr)
+			if (!ok && kp.serve == nullptr)
 				report(kp.error, DE_OUTPUT_OVERFLOW);
 		}
 		__syncwarp();
 		if (lane == 0) {
-			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
+			if (kp.serve != nullptr) {
+				/* serving: the last projection warp to store the tile counts
+				 * it; the query's last tile writes its completion record */
+				__threadfence();
+				uint32_t before;
+				asm volatile("atom.shared.add.u32 %0, [%1], 1;"
+					: "=r"(before) : "r"(sbase + kOffPCount + 4 * q) : "memory");
+				if (before == (uint32_t)P - 1u) {
+					sts_u32(sbase + kOffPCount + 4 * q, 0u);
+					const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
+					if (done == (unsigned)gq->ntiles) {
+						__threadfence();
+						const unsigned long long rows =
+							*reinterpret_cast<volatile unsigned long long *>(gq->total_out);
+						volatile ServeRec *r = kp.recs + qi;
+						r->rows = rows;
+						__threadfence_system();
+						r->seq = (unsigned long long)qi + 1ull;
+					}
+				}
+			}
 			mbar_arrive(smem_addr(smem + kOffLfree + 8 * q));
 		}
 	}
@@ -1382,7 +1441,9 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 	if (tid == 0) {
 		for (uint32_t s = 0; s < nst; s++) {
 			mbar_init(smem_addr(smem + kOffFull + 8 * s), 1);
-			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), P);
+			/* a stage is free once the filter warps and the look-back warp
+			 * are done with it; the projection reads only the slot */
+			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), NW + 1);
 		}
 		for (uint32_t q = 0; q < kSlots; q++) {
 			mbar_init(smem_addr(smem + kOffLready + 8 * q), NW);
@@ -1392,6 +1453,8 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		}
 		for (int x = 0; x < 8; x++)
 			flags[x] = 0;
+		for (uint32_t q = 0; q < kSlots; q++)
+			reinterpret_cast<uint32_t *>(smem + kOffPCount)[q] = 0;
 		flags[kFEnd] = ~0u;
 		flags[kFWaitMs] = kp.wait_limit_ms;
 		for (uint32_t s = 0; s < kMaxStages; s++)
@@ -1552,6 +1615,11 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 			if (lane == 0) {
 				publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
 				sts_u32(sbase + kOffTot + 4 * q, tile_total);
+				/* what the projection needs of the stage, which is released
+				 * before it runs */
+				sts_u32(sbase + kOffSlotInfo + 16 * q, lds_u32(sinfo + offsetof(StageInfo, query)));
+				sts_u32(sbase + kOffSlotInfo + 16 * q + 4, lds_u32(sinfo + offsetof(StageInfo, seg)));
+				sts_u32(sbase + kOffSlotInfo + 16 * q + 8, lds_u32(sinfo + offsetof(StageInfo, row0)));
 			}
 			/* valid rows per 64-row block, for result-tablet splitting on the
 			 * host: group g covers tile rows 64 g .. 64 g + 63 */
@@ -1564,8 +1632,10 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 			}
 		}
 		__syncwarp();
-		if (lane == 0)
+		if (lane == 0) {
 			mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
+			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
+		}
 	}
 }
 
