@@ -5,31 +5,31 @@
  * runs one thread per row with a 16-entry register file in local memory, a
  * switch dispatch per op per thread and atomics for (unordered) result
  * placement.  Here a CTA is a pipeline over tiles of TILE = THREADS x R
- * rows, tied together by mbarriers, with four roles:
+ * rows, tied together by mbarriers, with five roles:
  *
  *  - producer warp: claims work items (one tile of one segment of one query)
  *    from a global counter, in order, decodes them warp-wide and copies the
- *    columns the filter reads (plus the query's descriptor when the stage
- *    does not hold it) into a ring of shared-memory stages with TMA bulk
- *    copies (cp.async.bulk completing on the stage's full barrier);
+ *    tile's columns (plus the query's descriptor when the stage does not
+ *    hold it) into a ring of shared-memory stages with TMA bulk copies
+ *    (cp.async.bulk completing on the stage's full barrier);
  *  - filter warps (THREADS threads): run the filter ops over every row of the
  *    tile (row state as bit masks: valid, active, and rows parked at pending
  *    jump targets; each lane holds R rows in chunks of 4 consecutive rows),
  *    count valid rows per 64 rows with bit-plane ballots, scan the counts and
- *    write the tile's selected rows, in row order, to a shared list, then
- *    publish the tile's count to the query's look-back words and release
- *    the stage: the list and the tile's row vectors sit in one of kSlots
- *    slots, so the next tiles' copies and filters run while this one's
- *    projection waits for its offset;
+ *    write the tile's selected rows, in row order, to the list of one of
+ *    kSlots slots, then publish the tile's count to the query's look-back
+ *    words;
  *  - look-back warp: resolves the tile's position in the query's result with
  *    a warp-wide decoupled look-back over earlier tiles (32 status words per
  *    round); a tile that directly follows the CTA's previous tile of the same
  *    query starts where that one ended, with no look-back;
  *  - projection warps: run the projection ops over the tile's list in
- *    32-entry batches, gathering the columns they read from device memory
- *    at the selected rows only (late materialization: a selective query
- *    reads only the sectors that hold selected rows), and write each result
- *    row to the tile's offset plus its list position (coalesced stores),
+ *    32-entry batches, with results (and a copy of every other result
+ *    column) in the slot by list position, then release the stage: no stage
+ *    waits for a look-back, so copies and filters of the next tiles run
+ *    while up to kSlots tiles wait for their offsets;
+ *  - store warps: once the offset is known, write each result row from the
+ *    slot to the tile's offset plus its list position (coalesced stores),
  *    then release the slot.
  *
  * Each op is one 16-byte record fetched with a single shared-memory load and
@@ -60,30 +60,27 @@ constexpr uint32_t kSuspendHintNs = 20000;
 constexpr unsigned kFAbortSlot = 4;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
-/* work items claimed per atomic by the producer: one, so tiles that follow
- * each other in a query are taken, and finished, at about the same time */
-constexpr unsigned kClaim = 1;
-
 /* shared memory header (kSmemHeader bytes) */
-constexpr unsigned kMaxGroups = 128;  /* R x warps */
-constexpr unsigned kOffFull = 0;                            /* mbarrier[kMaxStages] */
-constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;   /* mbarrier[kMaxStages] */
-constexpr unsigned kOffLready = kOffEmpty + 8 * kMaxStages; /* mbarrier[kSlots]: list and count ready */
-constexpr unsigned kOffOready = kOffLready + 8 * kSlots;     /* mbarrier[kSlots]: offset ready */
-constexpr unsigned kOffLfree = kOffOready + 8 * kSlots;      /* mbarrier[kSlots]: projection done */
-constexpr unsigned kOffCdone = kOffLfree + 8 * kSlots;       /* mbarrier[kSlots]: all counts written */
-constexpr unsigned kOffOff = kOffCdone + 8 * kSlots;         /* uint64[kSlots]: tile offsets */
-constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;         /* uint32[8]: ok[kSlots], abort, end tile */
-constexpr unsigned kOffTot = kOffFlags + 32;                 /* uint32[kSlots]: tile totals */
-constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;          /* uint32[kMaxStages]: query per stage */
-constexpr unsigned kOffSlotInfo = 336;                       /* uint32[kSlots][4]: query, segment, first row */
-constexpr unsigned kOffPCount = kOffSlotInfo + 16 * kSlots;  /* uint32[kSlots]: projection warps done (serving) */
-constexpr unsigned kOffCnt = 512;                            /* uint32[kSlots][kMaxGroups]: per 64 rows */
+constexpr unsigned kOffFull = 0;                              /* mbarrier[kMaxStages]: data landed */
+constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;     /* mbarrier[kMaxStages]: stage free */
+constexpr unsigned kOffCdone = kOffEmpty + 8 * kMaxStages;    /* mbarrier[kMaxStages]: counts written */
+constexpr unsigned kOffFready = kOffCdone + 8 * kMaxStages;   /* mbarrier[kMaxStages]: filter done */
+constexpr unsigned kOffSready = kOffFready + 8 * kMaxStages;  /* mbarrier[kMaxStages]: tile total known */
+constexpr unsigned kOffLfree = kOffSready + 8 * kMaxStages;   /* mbarrier[kSlots]: stores done */
+constexpr unsigned kOffCready = kOffLfree + 8 * kSlots;       /* mbarrier[kSlots]: projection done */
+constexpr unsigned kOffOready = kOffCready + 8 * kSlots;      /* mbarrier[kSlots]: offset ready */
+constexpr unsigned kOffOff = kOffOready + 8 * kSlots;         /* uint64[kSlots]: tile offsets */
+constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;          /* uint32[8]: ok[kSlots], abort, end tile */
+constexpr unsigned kOffTot = kOffFlags + 32;                  /* uint32[kSlots]: tile totals */
+constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;           /* uint32[kMaxStages]: query per stage */
+constexpr unsigned kOffSlotInfo = 512;                        /* uint32[kSlots][4]: query, segment, first row */
+constexpr unsigned kOffPCount = kOffSlotInfo + 16 * kSlots;   /* uint32[kSlots]: store warps done (serving) */
+constexpr unsigned kOffLbuilt = 576;                          /* mbarrier[kSlots]: list written */
 constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
 static_assert(kSlots <= kFAbort, "ok flags per slot");
 static_assert(kOffHeld + 4 * kMaxStages <= kOffSlotInfo, "smem header layout");
-static_assert(kOffPCount + 4 * kSlots <= kOffCnt, "smem header layout");
-static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
+static_assert(kOffPCount + 4 * kSlots <= kOffLbuilt, "smem header layout");
+static_assert(kOffLbuilt + 8 * kSlots <= kSmemHeader, "smem header overflow");
 static_assert(sizeof(QDesc) % 16 == 0, "QDesc copies in 16-byte chunks");
 static_assert(kStageHdr >= sizeof(QDesc) + sizeof(StageInfo), "stage header too small");
 static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a time");
@@ -92,6 +89,7 @@ static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a
 constexpr uint32_t kQOps = (uint32_t)offsetof(QDesc, ops);
 constexpr uint32_t kQNFilter = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nfilter));
 constexpr uint32_t kQVecSlot = (uint32_t)offsetof(QDesc, vec_slot);
+constexpr uint32_t kQOpEnd = (uint32_t)offsetof(QDesc, op_end);
 
 /* ---- PTX wrappers ---------------------------------------------------- */
 
@@ -233,6 +231,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const vo
 	}
 }
 
+/* a wait that gave up: the first role to give up records the error and
+ * stops the CTA's other roles (an abort already set is not reported again) */
+__device__ __forceinline__ void give_up(const KParams &kp, volatile uint32_t *flags, int lane)
+{
+	if (lane == 0 && !flags[kFAbortSlot]) {
+		report(kp.error, DE_STAGE_TIMEOUT);
+		flags[kFAbortSlot] = 1u;
+	}
+}
+
 /* ---- shared-memory access by 32-bit shared address ---------------------
  * Every tile, register-vector and descriptor access of the compute warps
  * goes through these, so each is one ld/st.shared.  They are volatile asm:
@@ -353,17 +361,15 @@ struct Opnd {
 	bool sel;
 };
 
-/* staged columns and scalars (the descriptor's constant table) live in the
- * tile's stage, row vectors in the tile's row-vector slot, selection
- * vectors in their single area */
+/* staged columns, scalars (the descriptor's constant table) and register
+ * vectors by tile row live in the tile's stage, register vectors by
+ * selection position in the tile's slot */
 template <int SIZE>
 __device__ __forceinline__ Opnd opnd(uint32_t od, uint32_t sbase, uint32_t sdelta, uint32_t vdelta)
 {
 	const uint32_t kind = od >> 30;
 	Opnd o;
-	o.addr = sbase + (od & OD_OFFSET) +
-		((kind == (OD_STAGE >> 30) || kind == (OD_SCALAR >> 30)) ? sdelta
-			: kind == (OD_ROWVEC >> 30) ? vdelta : 0u);
+	o.addr = sbase + (od & OD_OFFSET) + (kind == (OD_SELVEC >> 30) ? vdelta : sdelta);
 	o.step = kind == (OD_SCALAR >> 30) ? 0u : (uint32_t)SIZE;
 	o.sel = kind == (OD_SELVEC >> 30);
 	return o;
@@ -748,94 +754,50 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowS
 }
 
 /* ---- projection: the tile's selected rows, in row order ------------------
- * The projection runs after the tile's stage is released, on the tile's
- * list and row-vector slot: columns are gathered from the segment in device
- * memory by tile row (only the selected rows' sectors are read) and
- * constants come from the query's descriptor in device memory.  The
- * projection warps share the list: warp p takes the 32-entry batches p,
- * p + P, p + 2 P, ...; entry e is selection index e and its result row
- * lands at the tile's offset + e. */
+ * The projection warps run the projection ops over the tile's list while
+ * the tile is still staged, writing results into the tile's slot indexed by
+ * selection position (register vectors the projection writes, and a copy of
+ * every other result column), and then release the stage: the stores wait
+ * for the tile's offset on the slot alone.  The warps share the list: warp p
+ * takes the 32-entry batches p, p + P, p + 2 P, ...; entry e is selection
+ * index e and its result row lands at the tile's offset + e. */
 
 struct PArgs {
-	uint32_t sbase;     /* shared memory base address */
-	uint32_t vd;        /* the slot's offset in the row-vector area */
-	uint32_t list;      /* smem address of the tile's list of tile rows (u16) */
-	uint32_t n;         /* entries */
-	uint32_t e0;        /* this lane's first entry */
-	uint32_t step;      /* entries between this lane's entries: 32 P */
-	const QDesc *gq;    /* the query's descriptor in device memory */
-	uint64_t colbase;   /* lane i: column i's address of the tile's row 0 */
+	uint32_t sbase, sd, vd;
+	uint32_t list;   /* smem address of the tile's list of tile rows (u16) */
+	uint32_t n;      /* entries */
+	uint32_t e0;     /* this lane's first entry */
+	uint32_t step;   /* entries between this lane's entries: 32 P */
 };
 
-/* a projection operand: a column in device memory, a row vector (by tile
- * row), a selection vector (by entry) or a constant */
-struct POp {
-	uint32_t kind;
-	uint32_t saddr;
-	const unsigned char *gaddr;
-	uint64_t bits;
-};
-
-/* resolves an operand descriptor; every lane of the warp calls it */
-__device__ __forceinline__ POp popnd(uint32_t od, const PArgs &c)
+/* element address of a list entry */
+__device__ __forceinline__ uint32_t p_addr(const Opnd &o, uint32_t row, uint32_t e)
 {
-	POp o;
-	o.kind = od >> 30;
-	const uint32_t off = od & OD_OFFSET;
-	const uint64_t col = __shfl_sync(0xffffffffu, c.colbase, (int)(off & 31u));
-	o.gaddr = reinterpret_cast<const unsigned char *>(col);
-	o.saddr = c.sbase + off + (o.kind == (OD_ROWVEC >> 30) ? c.vd : 0u);
-	o.bits = o.kind == (OD_SCALAR >> 30) ? c.gq->prog.consts[off % kMaxRegs] : 0ull;
-	return o;
-}
-
-template <typename T>
-__device__ __forceinline__ T ldg_elem(const unsigned char *p)
-{
-	if constexpr (sizeof(T) == 8)
-		return from_bits<T>((uint64_t)__ldg(reinterpret_cast<const unsigned long long *>(p)));
-	else if constexpr (sizeof(T) == 4)
-		return from_bits<T>((uint64_t)__ldg(reinterpret_cast<const unsigned int *>(p)));
-	else
-		return from_bits<T>((uint64_t)__ldg(reinterpret_cast<const unsigned char *>(p)));
-}
-
-template <typename T>
-__device__ __forceinline__ T pget(const POp &o, uint32_t row, uint32_t e)
-{
-	if (o.kind == (OD_STAGE >> 30))
-		return ldg_elem<T>(o.gaddr + (size_t)row * sizeof(T));
-	if (o.kind == (OD_ROWVEC >> 30))
-		return SM<T>::ld(o.saddr + row * (uint32_t)sizeof(T));
-	if (o.kind == (OD_SELVEC >> 30))
-		return SM<T>::ld(o.saddr + e * (uint32_t)sizeof(T));
-	return from_bits<T>(o.bits);
-}
-
-/* destinations are register vectors */
-template <typename T>
-__device__ __forceinline__ void pput(const POp &o, uint32_t row, uint32_t e, T v)
-{
-	SM<T>::st(o.saddr + (o.kind == (OD_SELVEC >> 30) ? e : row) * (uint32_t)sizeof(T), v);
+	return o.addr + (o.sel ? e : row) * o.step;
 }
 
 template <typename T, int OP>
 __device__ __forceinline__ void p_math(const uint4 &rec, const PArgs &c)
 {
-	const POp a = popnd(rec.y, c), b = popnd(rec.z, c), d = popnd(rec.w, c);
+	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
+	const Opnd b = opnd<sizeof(T)>(rec.z, c.sbase, c.sd, c.vd);
+	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
 	for (uint32_t e = c.e0; e < c.n; e += c.step) {
 		const uint32_t row = lds_u16(c.list + 2 * e);
-		pput<T>(d, row, e, Math<T, OP>::eval(pget<T>(a, row, e), pget<T>(b, row, e)));
+		const T x = SM<T>::ld(p_addr(a, row, e));
+		const T y = SM<T>::ld(p_addr(b, row, e));
+		SM<T>::st(p_addr(d, row, e), Math<T, OP>::eval(x, y));
 	}
 }
 
 template <typename T>
 __device__ __forceinline__ void p_copy(const uint4 &rec, const PArgs &c)
 {
-	const POp a = popnd(rec.y, c), d = popnd(rec.w, c);
+	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
+	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
 	for (uint32_t e = c.e0; e < c.n; e += c.step) {
 		const uint32_t row = lds_u16(c.list + 2 * e);
-		pput<T>(d, row, e, pget<T>(a, row, e));
+		SM<T>::st(p_addr(d, row, e), SM<T>::ld(p_addr(a, row, e)));
 	}
 }
 
@@ -850,7 +812,8 @@ __device__ __forceinline__ void p_math_any(const uint4 &rec, const PArgs &c)
 }
 
 /* one projection op: arithmetic, or a copy (every listed row is active
- * here, so constants and columns are copies) */
+ * here, so constants and columns are copies; result columns that are not
+ * projection vectors are copied into the slot the same way) */
 __device__ __forceinline__ void project_op(const uint4 &rec, const PArgs &c)
 {
 	const uint32_t h = rec.x;
@@ -869,16 +832,17 @@ __device__ __forceinline__ void project_op(const uint4 &rec, const PArgs &c)
 	}
 }
 
-/* one result column of the tile's entries, at the tile's offset; false if a
- * row lies beyond the buffers' capacity */
+/* one result column of the tile's entries, from the slot to the tile's
+ * offset; false if a row lies beyond the buffers' capacity */
 template <typename T>
-__device__ __forceinline__ bool p_store(const POp &a, const PArgs &c, T *out, uint64_t off, uint64_t cap)
+__device__ __forceinline__ bool store_column(uint32_t src, uint32_t e0, uint32_t n, uint32_t step, T *out,
+	uint64_t off, uint64_t cap)
 {
-	for (uint32_t e = c.e0; e < c.n; e += c.step) {
+	for (uint32_t e = e0; e < n; e += step) {
 		const uint64_t pos = off + e;
 		if (pos >= cap)
 			return false;
-		out[pos] = pget<T>(a, lds_u16(c.list + 2 * e), e);
+		out[pos] = SM<T>::ld(src + e * (uint32_t)sizeof(T));
 	}
 	return true;
 }
@@ -1049,6 +1013,10 @@ struct ProdQuery {
 	const uint32_t *tile_prefix;
 	uint32_t nsegs, nload, qi, seg_hint;
 	uint32_t src, stride, off;   /* this lane's column */
+	/* the current segment: its tiles [seg_t0, seg_t1) of the query, rows,
+	 * and this lane's column in it; seg ~0 when none */
+	uint32_t seg, seg_t0, seg_t1, seg_rows;
+	const unsigned char *colp;
 };
 
 /* one decoded work item; src and bytes are this lane's column copy */
@@ -1060,7 +1028,8 @@ struct ProdItem {
 
 /* decode work item w with the whole producer warp.  A CTA claims work items
  * in increasing order, so the query and segment searches start at the
- * previous item's. */
+ * previous item's, and an item in the previous item's segment needs no
+ * load at all. */
 template <int TILE>
 __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint64_t total, uint32_t nq,
 	ProdQuery &pq, ProdItem &it, int lane)
@@ -1082,38 +1051,46 @@ __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint6
 		pq.nsegs = Q->nsegs;
 		pq.nload = Q->prog.nload;
 		pq.seg_hint = 0;
+		pq.seg = ~0u;
 		if (lane < kMaxLoads) {
 			pq.src = Q->prog.load_src[lane];
 			pq.stride = Q->prog.load_stride[lane];
 			pq.off = Q->load_off[lane];
 		}
 	}
-	const uint64_t t = w - pq.first;
-	const uint32_t s = warp_search(pq.tile_prefix, pq.seg_hint, pq.nsegs, t, lane);
-	pq.seg_hint = s;
-	const SegDesc *sd = pq.segs + s;
-	const uint32_t row0 = (uint32_t)(t - pq.tile_prefix[s]) * TILE;
-	it.seg = s;
+	const uint32_t t = (uint32_t)(w - pq.first);
+	if (pq.seg == ~0u || t >= pq.seg_t1) {
+		const uint32_t s = warp_search(pq.tile_prefix, pq.seg_hint, pq.nsegs, t, lane);
+		const SegDesc *sd = pq.segs + s;
+		pq.seg_hint = s;
+		pq.seg = s;
+		pq.seg_t0 = pq.tile_prefix[s];
+		pq.seg_t1 = pq.tile_prefix[s + 1];
+		pq.seg_rows = sd->rows;
+		if ((uint32_t)lane < pq.nload)
+			pq.colp = static_cast<const unsigned char *>(sd->col[pq.src]);
+	}
+	const uint32_t row0 = (t - pq.seg_t0) * TILE;
+	it.seg = pq.seg;
 	it.row0 = row0;
-	it.nrows = min((uint32_t)TILE, sd->rows - row0);
-	/* only the columns the filter reads are staged (load_off != 0) */
-	if ((uint32_t)lane < pq.nload && pq.off != 0) {
-		it.src = static_cast<const unsigned char *>(sd->col[pq.src]) + (size_t)row0 * pq.stride;
+	it.nrows = min((uint32_t)TILE, pq.seg_rows - row0);
+	if ((uint32_t)lane < pq.nload) {
+		it.src = pq.colp + (size_t)row0 * pq.stride;
 		it.bytes = (it.nrows * pq.stride + 15u) & ~15u;
 	}
 }
 
-/* The producer warp fills the ring of stages.  Once the filter warps and the
- * look-back warp released a stage it announces the decoded work item and
- * issues its copies (lane i copies column i if the filter reads it; the
- * query descriptor only when the stage does not hold it already), then
- * claims (kClaim per atomic, in order) and decodes the next item while
- * those copies run.  Claiming one item ahead, not a whole ring ahead, keeps
- * claimed tiles from idling while other CTAs' look-backs wait for their
- * counts.  An invalid claim (past the end of the work list) is announced
- * without data and ends the CTA's pipeline.  In a serving session the work
- * list grows: a claim past the published work waits (bounded) for the
- * host's doorbell or its stop request. */
+/* The producer warp fills the ring of stages.  Once the projection warps
+ * and the look-back warp released a stage it announces the decoded work
+ * item and issues its copies (lane i copies column i; the query descriptor
+ * only when the stage does not hold it already), then takes the next claim
+ * (in order, with the one after it already in flight) and decodes it while
+ * those copies run.  Claiming a couple of items ahead, not a whole ring
+ * ahead, keeps claimed tiles from idling while other CTAs' look-backs wait
+ * for their counts.  An invalid claim (past the end of the work list) is
+ * announced without data and ends the CTA's pipeline.  In a serving session
+ * the work list grows: a claim past the published work waits (bounded) for
+ * the host's doorbell or its stop request. */
 template <int TILE>
 __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 {
@@ -1128,17 +1105,21 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	ProdQuery pq;
 	pq.Q = nullptr;
 	pq.qi = 0;
-	uint32_t next = 0, left = 0;
+	/* claims: one atomic in flight (lane 0) while the previous claim's item
+	 * is decoded and issued, so its round trip is off the per-tile path */
+	uint32_t inflight = 0;
+	bool have = false;
 	auto claim = [&]() -> uint32_t {
-		if (left == 0) {
-			uint32_t v = 0;
-			if (lane == 0)
-				v = atomicAdd(kp.counter, kClaim);
-			next = __shfl_sync(0xffffffffu, v, 0);
-			left = kClaim;
+		uint32_t v = 0;
+		if (lane == 0) {
+			if (!have) {
+				inflight = atomicAdd(kp.counter, 1u);
+				have = true;
+			}
+			v = inflight;
+			inflight = atomicAdd(kp.counter, 1u);
 		}
-		left--;
-		return next++;
+		return __shfl_sync(0xffffffffu, v, 0);
 	};
 	/* the next work item; ~0 ends the pipeline */
 	auto next_item = [&]() -> uint32_t {
@@ -1250,7 +1231,6 @@ template <int THREADS, int R>
 __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 {
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	const volatile uint32_t *tot = reinterpret_cast<const volatile uint32_t *>(smem + kOffTot);
 	uint64_t *offs = reinterpret_cast<uint64_t *>(smem + kOffOff);
 	const uint32_t nst = kp.nstages;
 	/* the previous tile of this CTA: a tile that directly follows it in the
@@ -1258,49 +1238,62 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 	uint64_t prev_work = ~0ull, prev_end = 0;
 	for (uint32_t i = 0;; i++) {
 		const uint32_t s = i % nst, q = i % kSlots;
-		/* the tile's data has landed: its work item is known, so the walk
-		 * over earlier tiles starts while the filter warps run */
-		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort))
+		/* the tile's data has landed: its work item is known */
+		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
+			give_up(kp, flags, lane);
 			return;
+		}
 		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
 		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-		if (si.work >= kp.total_work)
+		const volatile StageInfo &si = *reinterpret_cast<const volatile StageInfo *>(hdr + sizeof(QDesc));
+		const uint32_t work = si.work;
+		if (work >= kp.total_work)
 			return;
-		/* what this warp needs of the stage, before releasing its share */
 		const uint64_t first = Q.work_first, last = Q.work_first + Q.ntiles - 1;
 		unsigned long long *const total_out = Q.total_out;
 		const uint64_t base = query_base(Q);
+		/* the tile's own count, left in the stage by the filter; then the
+		 * stage is released as far as this warp goes, before the walk over
+		 * other CTAs' tiles */
+		if (!mbar_wait(smem_addr(smem + kOffSready + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
+			give_up(kp, flags, lane);
+			return;
+		}
+		const uint32_t count = si.total;
 		__syncwarp();
 		if (lane == 0)
 			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
 		uint64_t excl = 0;
 		bool ok = true;
-		const bool follows = si.work == prev_work + 1 && si.work != first;
+		const bool follows = work == prev_work + 1 && work != first;
 		if (follows)
 			excl = prev_end;
 		else
-			ok = lookback_excl(kp, first, base, si.work, prev_work == ~0ull ? -1 : (int64_t)prev_work,
-				prev_end, lane, &excl);
-		/* the tile's own count */
-		if (ok && !mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
-			return;
-		const uint32_t tile_total = ok ? tot[q] : 0u;
-		prev_work = si.work;
+			ok = lookback_excl(kp, first, base, work, prev_work == ~0ull ? -1 : (int64_t)prev_work, prev_end,
+				lane, &excl);
+		const uint32_t tile_total = ok ? count : 0u;
+		prev_work = work;
 		prev_end = excl + tile_total;
-		__syncwarp();
 		if (lane == 0) {
 			if (!ok) {
 				report(kp.error, DE_LOOKBACK_TIMEOUT);
 			} else {
 				/* the inclusive prefix (a query's first tile published its own) */
-				if (si.work != first)
-					st_status(status_at(kp, si.work),
-						(status_tag(kp, si.work) << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
+				if (work != first)
+					st_status(status_at(kp, work),
+						(status_tag(kp, work) << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
 						((excl + tile_total) & kStatusValueMask));
-				if (si.work == last)
+				if (work == last)
 					*total_out = excl + tile_total;
 			}
+		}
+		/* the slot's offset: free once the tile's projection is done, which
+		 * waited for the stores of the slot's previous tile */
+		if (!mbar_wait(smem_addr(smem + kOffCready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+			give_up(kp, flags, lane);
+			return;
+		}
+		if (lane == 0) {
 			offs[q] = excl;
 			flags[q] = ok ? 1u : 0u;
 			if (!ok)
@@ -1312,15 +1305,142 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 	}
 }
 
+/* projection warps: build the tile's list of selected rows from the
+ * filter's ballots, run the projection ops over it into the tile's slot,
+ * then give the stage back to the producer */
 template <int THREADS, int R, int P>
 __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int lane)
 {
 	constexpr int TILE = THREADS * R;
+	constexpr int NW = THREADS / 32;
+	constexpr int C = R / 4;
+	constexpr int G = 2 * C * NW;          /* 64-row groups per tile */
+	constexpr int PER = (G + 31) / 32;
+	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
+	const uint32_t sbase = smem_addr(smem);
+	const uint32_t nst = kp.nstages;
+	for (uint32_t i = 0;; i++) {
+		const uint32_t s = i % nst, q = i % kSlots;
+		bool ok = mbar_wait(smem_addr(smem + kOffFready + 8 * s), (i / nst) & 1u, flags + kFAbort);
+		/* the slot is free once the stores of its previous tile are done.
+		 * The end of the tiles waits for it too: its arrival on the slot's
+		 * projection barrier must not complete a phase that the look-back
+		 * warp still has to see for the slot's previous tile. */
+		ok = ok && (i < kSlots ||
+			mbar_wait(smem_addr(smem + kOffLfree + 8 * q), ((i - kSlots) / kSlots) & 1u, flags + kFAbort));
+		if (!ok) {
+			if (lane == 0 && !flags[kFAbort]) {
+				report(kp.error, DE_STAGE_TIMEOUT);
+				flags[kFAbort] = 1u;
+			}
+			return;
+		}
+		if (flags[kFEnd] == i) {
+			/* no more tiles: tell the store warps */
+			__syncwarp();
+			if (lane == 0)
+				mbar_arrive(smem_addr(smem + kOffCready + 8 * q));
+			return;
+		}
+		const uint32_t sd = s * kp.stage_bytes;
+		const uint32_t qd = sbase + kp.stage_area + sd;
+		const uint32_t sinfo = qd + (uint32_t)sizeof(QDesc);
+		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
+
+		/* ---- the list: every warp scans the group counts ((chunk, warp,
+		 * half) is row order); warp p writes the rows of chunks p, p + P, ... */
+		const uint32_t cnt = qd + kStageCnt;
+		uint32_t lane_pre[PER];
+		uint32_t sum = 0;
+#pragma unroll
+		for (int x = 0; x < PER; x++) {
+			const int g = lane * PER + x;
+			lane_pre[x] = sum;
+			sum += g < G ? lds_u32(cnt + 4 * g) : 0u;
+		}
+		uint32_t incl = sum;
+#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+			if (lane >= d)
+				incl += v;
+		}
+		const uint32_t ex = incl - sum;
+		const uint32_t lt = (1u << lane) - 1u;
+		for (int ch = pw; ch < C * NW; ch += P) {
+			const uint32_t g = 2u * (uint32_t)ch;
+			uint32_t v = 0;
+#pragma unroll
+			for (int x = 0; x < PER; x++)
+				if ((uint32_t)x == g % PER)
+					v = ex + lane_pre[x];
+			const uint32_t base = __shfl_sync(0xffffffffu, v, (int)(g / PER));
+			const uint4 b = lds_v4(qd + kStageMasks + 16u * (uint32_t)ch);
+			const uint32_t m = ((b.x >> lane) & 1u) | (((b.y >> lane) & 1u) << 1) | (((b.z >> lane) & 1u) << 2) |
+				(((b.w >> lane) & 1u) << 3);
+			if (m) {
+				uint32_t at = base + __popc(b.x & lt) + __popc(b.y & lt) + __popc(b.z & lt) + __popc(b.w & lt);
+				/* chunk c of filter warp w: tile rows c * 4 * THREADS + 128 w + 4 lane + k */
+				const uint32_t row0 = (uint32_t)(ch / NW) * 4u * THREADS + 128u * (uint32_t)(ch % NW) + 4u * lane;
+#pragma unroll
+				for (int k = 0; k < 4; k++)
+					if ((m >> k) & 1u)
+						sts_u16(list + 2 * at++, row0 + k);
+			}
+		}
+		/* every projection warp reads entries the others wrote (a bounded
+		 * rendezvous of the projection warps) */
+		__syncwarp();
+		if (lane == 0)
+			mbar_arrive(smem_addr(smem + kOffLbuilt + 8 * q));
+		if (!mbar_wait(smem_addr(smem + kOffLbuilt + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+			if (lane == 0 && !flags[kFAbort]) {
+				report(kp.error, DE_STAGE_TIMEOUT);
+				flags[kFAbort] = 1u;
+			}
+			return;
+		}
+
+		PArgs c;
+		c.sbase = sbase;
+		c.sd = sd;
+		c.vd = q * lds_u32(qd + kQVecSlot);
+		c.list = list;
+		c.n = lds_u32(sinfo + offsetof(StageInfo, total));
+		c.e0 = 32u * (uint32_t)pw + (uint32_t)lane;
+		c.step = 32u * P;
+		const uint32_t ops = qd + kQOps;
+		if (c.e0 - (uint32_t)lane < c.n) {
+			const uint32_t end = lds_u32(qd + kQOpEnd);
+			for (uint32_t k = lds_u32(qd + kQNFilter); k < end; k++)
+				project_op(lds_v4(ops + 16u * k), c);
+		}
+		if (pw == 0 && lane == 0) {
+			/* what the store warps need, after the stage is released */
+			sts_u32(sbase + kOffTot + 4 * q, c.n);
+			sts_u32(sbase + kOffSlotInfo + 16 * q, lds_u32(sinfo + offsetof(StageInfo, query)));
+			sts_u32(sbase + kOffSlotInfo + 16 * q + 4, lds_u32(sinfo + offsetof(StageInfo, seg)));
+			sts_u32(sbase + kOffSlotInfo + 16 * q + 8, lds_u32(sinfo + offsetof(StageInfo, row0)));
+		}
+		__syncwarp();
+		if (lane == 0) {
+			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
+			mbar_arrive(smem_addr(smem + kOffCready + 8 * q));
+		}
+	}
+}
+
+/* store warps: once the tile's projection is done and the look-back
+ * resolved its offset, its result columns go from the slot to device
+ * memory at offset + entry (coalesced), and the slot is released */
+template <int THREADS, int R, int S>
+__device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int lane)
+{
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
 	const uint32_t sbase = smem_addr(smem);
 	for (uint32_t i = 0;; i++) {
 		const uint32_t q = i % kSlots;
-		if (!mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+		if (!mbar_wait(smem_addr(smem + kOffCready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
 			if (lane == 0 && !flags[kFAbort]) {
 				report(kp.error, DE_STAGE_TIMEOUT);
 				flags[kFAbort] = 1u;
@@ -1329,58 +1449,38 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 		}
 		if (flags[kFEnd] == i)
 			return;
-		/* the tile: query, segment and first row, left by the filter warps */
-		const uint32_t qi = lds_u32(sbase + kOffSlotInfo + 16 * q);
-		const uint32_t seg = lds_u32(sbase + kOffSlotInfo + 16 * q + 4);
-		const uint32_t row0 = lds_u32(sbase + kOffSlotInfo + 16 * q + 8);
-		/* plain loads, not the read-only path: a serving session's host
-		 * writes descriptors while the kernel runs */
-		const QDesc *gq = kp.queries + qi;
-		PArgs c;
-		c.sbase = sbase;
-		c.vd = q * gq->vec_slot;
-		c.list = sbase + kp.sel_area + q * TILE * 2;
-		c.n = lds_u32(sbase + kOffTot + 4 * q);
-		c.e0 = 32u * (uint32_t)pw + (uint32_t)lane;
-		c.step = 32u * P;
-		c.gq = gq;
-		c.colbase = 0;
-		const bool mine = c.e0 - (uint32_t)lane < c.n;
-		if (mine) {
-			const uint32_t nload = gq->prog.nload;
-			if ((uint32_t)lane < nload) {
-				const SegDesc *sd = gq->segs + seg;
-				const uint32_t src = gq->prog.load_src[lane];
-				const uint32_t stride = gq->prog.load_stride[lane];
-				c.colbase = reinterpret_cast<uint64_t>(sd->col[src]) + (uint64_t)row0 * stride;
-			}
-			const uint32_t nu = gq->prog.nuops - 1u;
-			for (uint32_t k = gq->prog.nfilter; k < nu; k++) {
-				const uint4 rec = *reinterpret_cast<const uint4 *>(&gq->ops[k]);
-				project_op(rec, c);
-			}
-		}
-
-		/* ---- stores at the tile's offset, once the look-back resolved it */
-		if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
+		if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+			give_up(kp, flags, lane);
 			return;
+		}
 		if (!flags[q])
 			return;
 		const uint64_t off = lds_u64(sbase + kOffOff + 8 * q);
-		if (mine) {
+		const uint32_t n = lds_u32(sbase + kOffTot + 4 * q);
+		const uint32_t qi = lds_u32(sbase + kOffSlotInfo + 16 * q);
+		/* the stage is gone: the result columns' fields come from the
+		 * descriptor in device memory (plain loads, not the read-only path:
+		 * a serving session's host writes descriptors while the kernel
+		 * runs) */
+		const QDesc *gq = kp.queries + qi;
+		const uint32_t e0 = 32u * (uint32_t)sw + (uint32_t)lane;
+		if (e0 - (uint32_t)lane < n) {
+			const uint32_t vd = q * gq->vec_slot;
 			const uint64_t cap = gq->capacity;
-			bool ok = true;
 			const uint32_t nout = gq->prog.nout;
+			bool ok = true;
 			for (uint32_t j = 0; j < nout; j++) {
-				const POp a = popnd(gq->od_out[j], c);
+				const uint32_t src = sbase + (gq->od_out[j] & OD_OFFSET) + vd;
 				void *out = gq->out_ptr[j];
 				const uint32_t stride = gq->prog.out_stride[j];
 				if (stride == 4)
-					ok &= p_store<uint32_t>(a, c, static_cast<uint32_t *>(out), off, cap);
+					ok &= store_column<uint32_t>(src, e0, n, 32u * S, static_cast<uint32_t *>(out), off, cap);
 				else if (stride == 8)
-					ok &= p_store<unsigned long long>(a, c, static_cast<unsigned long long *>(out), off, cap);
+					ok &= store_column<unsigned long long>(src, e0, n, 32u * S,
+						static_cast<unsigned long long *>(out), off, cap);
 				else
-					ok &= p_store<unsigned char>(a, c, static_cast<unsigned char *>(out), off, cap);
+					ok &= store_column<unsigned char>(src, e0, n, 32u * S, static_cast<unsigned char *>(out),
+						off, cap);
 			}
 			/* a serving session reports rows beyond capacity in the
 			 * query's completion record instead */
@@ -1390,13 +1490,13 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 		__syncwarp();
 		if (lane == 0) {
 			if (kp.serve != nullptr) {
-				/* serving: the last projection warp to store the tile counts
-				 * it; the query's last tile writes its completion record */
+				/* serving: the last store warp to finish the tile counts it;
+				 * the query's last tile writes its completion record */
 				__threadfence();
 				uint32_t before;
 				asm volatile("atom.shared.add.u32 %0, [%1], 1;"
 					: "=r"(before) : "r"(sbase + kOffPCount + 4 * q) : "memory");
-				if (before == (uint32_t)P - 1u) {
+				if (before == (uint32_t)S - 1u) {
 					sts_u32(sbase + kOffPCount + 4 * q, 0u);
 					const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
 					if (done == (unsigned)gq->ntiles) {
@@ -1415,24 +1515,30 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 	}
 }
 
-/* projection warps per CTA: half the filter warps, 1 to 4 */
+/* projection warps per CTA: half the filter warps, 1 to 4; store warps:
+ * half the projection warps, at least 1 */
 template <int THREADS>
 struct ProjWarps {
 	static constexpr int value = THREADS / 64 < 1 ? 1 : THREADS / 64 > 4 ? 4 : THREADS / 64;
 };
+template <int THREADS>
+struct StoreWarps {
+	static constexpr int value = ProjWarps<THREADS>::value / 2 < 1 ? 1 : ProjWarps<THREADS>::value / 2;
+};
 
 template <int THREADS, int R>
-__global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)) vm_kernel(const KParams kp)
+__global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value))
+vm_kernel(const KParams kp)
 {
-	constexpr int TILE = THREADS * R;
 	constexpr int NW = THREADS / 32;
 	constexpr int C = R / 4;
 	constexpr int P = ProjWarps<THREADS>::value;
+	constexpr int S = StoreWarps<THREADS>::value;
 	constexpr int G = 2 * C * NW;          /* 64-row groups per tile */
 	constexpr int PER = (G + 31) / 32;
 	static_assert(R % 4 == 0 && R <= 32, "rows per thread: whole 4-row chunks, 32-bit row masks");
 	static_assert(G <= (int)kMaxGroups, "64-row groups per tile");
-	static_assert(TILE <= 65536, "tile rows are 16-bit in the selection lists");
+	static_assert(THREADS * R <= 65536, "tile rows are 16-bit in the selection lists");
 	extern __shared__ __align__(128) unsigned char smem[];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
@@ -1441,15 +1547,18 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 	if (tid == 0) {
 		for (uint32_t s = 0; s < nst; s++) {
 			mbar_init(smem_addr(smem + kOffFull + 8 * s), 1);
-			/* a stage is free once the filter warps and the look-back warp
-			 * are done with it; the projection reads only the slot */
-			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), NW + 1);
+			/* a stage is free once the projection warps and the look-back
+			 * warp are done with it */
+			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), P + 1);
+			mbar_init(smem_addr(smem + kOffCdone + 8 * s), NW);
+			mbar_init(smem_addr(smem + kOffFready + 8 * s), 1);
+			mbar_init(smem_addr(smem + kOffSready + 8 * s), 1);
 		}
 		for (uint32_t q = 0; q < kSlots; q++) {
-			mbar_init(smem_addr(smem + kOffLready + 8 * q), NW);
+			mbar_init(smem_addr(smem + kOffLfree + 8 * q), S);
+			mbar_init(smem_addr(smem + kOffCready + 8 * q), P);
 			mbar_init(smem_addr(smem + kOffOready + 8 * q), 1);
-			mbar_init(smem_addr(smem + kOffLfree + 8 * q), P);
-			mbar_init(smem_addr(smem + kOffCdone + 8 * q), NW);
+			mbar_init(smem_addr(smem + kOffLbuilt + 8 * q), P);
 		}
 		for (int x = 0; x < 8; x++)
 			flags[x] = 0;
@@ -1463,11 +1572,15 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 	}
 	__syncthreads();
 	if (warp == NW) {
-		producer<TILE>(kp, smem, lane);
+		producer<THREADS * R>(kp, smem, lane);
 		return;
 	}
 	if (warp == NW + 1) {
 		lookback_warp<THREADS, R>(kp, smem, lane);
+		return;
+	}
+	if (warp >= NW + 2 + P) {
+		store_warps<THREADS, R, S>(kp, smem, warp - (NW + 2 + P), lane);
 		return;
 	}
 	if (warp >= NW + 2) {
@@ -1475,16 +1588,12 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		return;
 	}
 
-	/* filter warps */
+	/* filter warps: they wait for data only, so a tile's count is
+	 * published as soon as its columns have landed */
 	const uint32_t sbase = smem_addr(smem);
 	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst, q = i % kSlots;
-		/* the list and row-vector slot q are free once the projection of
-		 * tile i - kSlots is done */
-		bool ok = i < kSlots ||
-			mbar_wait(smem_addr(smem + kOffLfree + 8 * q), ((i - kSlots) / kSlots) & 1u, flags + kFAbort);
-		ok = ok && mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort);
-		if (!ok) {
+		const uint32_t s = i % nst;
+		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
 			if (lane == 0 && !flags[kFAbort]) {
 				report(kp.error, DE_STAGE_TIMEOUT);
 				flags[kFAbort] = 1u;
@@ -1495,16 +1604,15 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		const uint32_t qd = sbase + kp.stage_area + sd;
 		const uint32_t sinfo = qd + (uint32_t)sizeof(QDesc);
 		if (lds_u32(sinfo + offsetof(StageInfo, work)) >= kp.total_work) {
-			/* no more tiles: tell the look-back and projection warps */
-			__syncwarp();
-			if (lane == 0) {
+			/* no more tiles: tell the projection warps (and through them the
+			 * store warps) */
+			if (warp == 0 && lane == 0) {
 				flags[kFEnd] = i;
-				mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
+				mbar_arrive(smem_addr(smem + kOffFready + 8 * s));
 			}
 			return;
 		}
 		const uint32_t nrows = lds_u32(sinfo + offsetof(StageInfo, nrows));
-		const uint32_t vd = q * lds_u32(qd + kQVecSlot);
 
 		/* ---- filter over every row */
 		RowState st;
@@ -1522,7 +1630,7 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		{
 			const uint32_t ops = qd + kQOps;
 			const uint32_t nf = lds_u32(qd + kQNFilter);
-			const FArgs f{sbase, sd, vd, tid};
+			const FArgs f{sbase, sd, 0u, tid};
 			uint4 rec = lds_v4(ops);
 			for (uint32_t k = 0; k < nf; k++) {
 				const uint4 cur = rec;
@@ -1532,11 +1640,9 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 			}
 		}
 
-		/* ---- counts per 64 rows, from four bit-plane ballots per 128-row
-		 * chunk of the warp (row k of each lane's 4) */
-		const uint32_t cnt = sbase + kOffCnt + q * kMaxGroups * 4;
-		const uint32_t lt = (1u << lane) - 1u;
-		uint32_t rank[C], total[C];
+		/* ---- four bit-plane ballots per 128-row chunk of the warp (row k of
+		 * each lane's 4) and the valid rows per 64 rows, into the stage */
+		const uint32_t cnt = qd + kStageCnt;
 #pragma unroll
 		for (int c = 0; c < C; c++) {
 			const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
@@ -1544,97 +1650,57 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 			const uint32_t b1 = __ballot_sync(0xffffffffu, m & 2u);
 			const uint32_t b2 = __ballot_sync(0xffffffffu, m & 4u);
 			const uint32_t b3 = __ballot_sync(0xffffffffu, m & 8u);
-			total[c] = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
-			rank[c] = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
 			if (lane == 0) {
 				/* lanes 0-15 hold the chunk's first 64 rows */
+				const uint32_t total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
 				const uint32_t h0 = __popc(b0 & 0xffffu) + __popc(b1 & 0xffffu) + __popc(b2 & 0xffffu) +
 					__popc(b3 & 0xffffu);
+				sts_v4(qd + kStageMasks + 16u * (uint32_t)(c * NW + warp), make_uint4(b0, b1, b2, b3));
 				sts_u32(cnt + 8 * (c * NW + warp), h0);
-				sts_u32(cnt + 8 * (c * NW + warp) + 4, total[c] - h0);
+				sts_u32(cnt + 8 * (c * NW + warp) + 4, total - h0);
 			}
 		}
 		__syncwarp();
 		if (lane == 0)
-			mbar_arrive(smem_addr(smem + kOffCdone + 8 * q));
-		if (!mbar_wait(smem_addr(smem + kOffCdone + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+			mbar_arrive(smem_addr(smem + kOffCdone + 8 * s));
+		if (warp != 0)
+			continue;
+
+		/* ---- warp 0: the tile's count, to the look-back words and the
+		 * other roles */
+		if (!mbar_wait(smem_addr(smem + kOffCdone + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
 			if (lane == 0 && !flags[kFAbort]) {
 				report(kp.error, DE_STAGE_TIMEOUT);
 				flags[kFAbort] = 1u;
 			}
 			return;
 		}
-
-		/* ---- every warp scans the tile's counts: (chunk, warp, half) is row
-		 * order, so a chunk's rows start at the sum of the counts before it */
-		uint32_t loc[PER], lane_pre[PER];
 		uint32_t sum = 0;
 #pragma unroll
 		for (int x = 0; x < PER; x++) {
 			const int g = lane * PER + x;
-			loc[x] = g < G ? lds_u32(cnt + 4 * g) : 0u;
-			lane_pre[x] = sum;
-			sum += loc[x];
+			sum += g < G ? lds_u32(cnt + 4 * g) : 0u;
 		}
-		uint32_t incl = sum;
-#pragma unroll
-		for (int d = 1; d < 32; d <<= 1) {
-			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
-			if (lane >= d)
-				incl += v;
+		const uint32_t tile_total = __reduce_add_sync(0xffffffffu, sum);
+		const unsigned char *hdr = smem + kp.stage_area + sd;
+		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
+		if (lane == 0) {
+			publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
+			sts_u32(sinfo + offsetof(StageInfo, total), tile_total);
 		}
-		const uint32_t ex = incl - sum;
-		const uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
-
-		/* ---- the tile-ordered list of selected rows */
-		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
-#pragma unroll
-		for (int c = 0; c < C; c++) {
-			const uint32_t g = 2u * (uint32_t)(c * NW + warp);
-			uint32_t v = 0;
-#pragma unroll
-			for (int x = 0; x < PER; x++)
-				if ((uint32_t)x == g % PER)
-					v = ex + lane_pre[x];
-			const uint32_t base = __shfl_sync(0xffffffffu, v, (int)(g / PER));
-			if (total[c]) {
-				const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
-				uint32_t at = base + rank[c];
-				const uint32_t row0 = chunk_row<THREADS>(c, tid);
-#pragma unroll
-				for (int k = 0; k < 4; k++)
-					if ((m >> k) & 1u)
-						sts_u16(list + 2 * at++, row0 + k);
-			}
-		}
-
-		/* ---- the tile's count: to the look-back words and the other roles */
-		if (warp == 0) {
-			const unsigned char *hdr = smem + kp.stage_area + sd;
-			const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-			if (lane == 0) {
-				publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
-				sts_u32(sbase + kOffTot + 4 * q, tile_total);
-				/* what the projection needs of the stage, which is released
-				 * before it runs */
-				sts_u32(sbase + kOffSlotInfo + 16 * q, lds_u32(sinfo + offsetof(StageInfo, query)));
-				sts_u32(sbase + kOffSlotInfo + 16 * q + 4, lds_u32(sinfo + offsetof(StageInfo, seg)));
-				sts_u32(sbase + kOffSlotInfo + 16 * q + 8, lds_u32(sinfo + offsetof(StageInfo, row0)));
-			}
-			/* valid rows per 64-row block, for result-tablet splitting on the
-			 * host: group g covers tile rows 64 g .. 64 g + 63 */
-			if (Q.block_counts != nullptr) {
-				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-				for (int g = lane; g < G; g += 32)
-					if (64u * (uint32_t)g < si.nrows)
-						Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
-							(uint8_t)lds_u32(cnt + 4 * g);
-			}
+		/* valid rows per 64-row block, for result-tablet splitting on the
+		 * host: group g covers tile rows 64 g .. 64 g + 63 */
+		if (Q.block_counts != nullptr) {
+			const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+			for (int g = lane; g < G; g += 32)
+				if (64u * (uint32_t)g < si.nrows)
+					Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
+						(uint8_t)lds_u32(cnt + 4 * g);
 		}
 		__syncwarp();
 		if (lane == 0) {
-			mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
-			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
+			mbar_arrive(smem_addr(smem + kOffSready + 8 * s));
+			mbar_arrive(smem_addr(smem + kOffFready + 8 * s));
 		}
 	}
 }
@@ -1647,8 +1713,8 @@ static int launch_t(const KParams &kp, unsigned grid, size_t smem, cudaStream_t 
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	/* THREADS filter threads, the producer and look-back warps and the projection warps */
-	fn<<<grid, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem, stream>>>(kp);
+	/* THREADS filter threads, the producer and look-back warps, the projection and store warps */
+	fn<<<grid, THREADS + 32 * (2 + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem, stream>>>(kp);
 	return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1658,10 +1724,10 @@ static int occ_t(size_t smem, int *ctas)
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem) == cudaSuccess;
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (2 + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem) == cudaSuccess;
 }
 
-#define VGPU_SHAPES(X) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
+#define VGPU_SHAPES(X) X(128, 4) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
 
 int shape_supported(const Shape &s)
 {
