@@ -198,7 +198,7 @@ int autotune(virg_gpu_batch *b)
 	float best = 1e30f;
 	Shape best_shape = {0, 0, 0, 0};
 	for (auto &c : cand)
-		for (unsigned st = 2; st <= 4; st++) {
+		for (unsigned st : {kSlots}) {
 			Shape s = {c[0], c[1], st, 0};
 			set_error("%s", "");
 			if (!build_with(b, &s))

@@ -129,7 +129,8 @@ int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, 
 		uint32_t stage, slot, vec;
 		launch_layout(progs, s.tile(), &stage, &slot, &vec);
 		/* a requested stage count is kept, at one CTA per SM if need be */
-		const unsigned st_list[] = {e->pref.stages ? e->pref.stages : 3u, e->pref.stages ? 0u : 2u};
+		/* as many stages as slots: the kernel has a look-back warp per stage */
+		const unsigned st_list[] = {kSlots};
 		for (unsigned st : st_list) {
 			if (st == 0)
 				continue;
@@ -575,7 +576,7 @@ extern "C" int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p
 	Shape best_shape = {0, 0, 0, 0};
 	std::string key;
 	for (auto &c : cand)
-		for (unsigned st = 2; st <= 4; st++) {
+		for (unsigned st : {kSlots}) {
 			e->force = Shape{c[0], c[1], st, 0};
 			float t_best = 1e30f;
 			bool ran = true;
@@ -640,7 +641,7 @@ extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 		s.rows_per_thread = rows_per_thread ? rows_per_thread : 4;
 		VGPU_CHECK(shape_supported(s), "unsupported shape %u x %u", s.threads, s.rows_per_thread);
 	}
-	VGPU_CHECK(stages <= kMaxStages, "at most %u stages", kMaxStages);
+	VGPU_CHECK(stages == 0 || stages == kSlots, "the kernel runs %u stages", kSlots);
 	e->pref.threads = threads;
 	e->pref.rows_per_thread = rows_per_thread;
 	e->pref.stages = stages;

@@ -110,7 +110,7 @@ int pick_shape(const Program &P, int smem_optin, Shape *shape, size_t *smem, uin
 	const size_t limit = (size_t)smem_optin;
 	for (int pass = 0; pass < 2; pass++)
 		for (auto &c : cand)
-			for (unsigned st : {3u, 2u}) {
+			for (unsigned st : {kSlots}) {
 				Shape s = {c[0], c[1], st, 0};
 				uint32_t sb, lb;
 				program_layout(P, s.tile(), nullptr, nullptr, nullptr, &sb, &lb);

@@ -199,7 +199,7 @@ int serve_layout(virg_serve *s)
 			kStageHdr + (size_t)tile * (s->cfg.max_load_bytes_per_row + s->cfg.max_row_vector_bytes), 128);
 		const uint32_t slot = (uint32_t)align_up((size_t)tile * s->cfg.max_sel_vector_bytes, 128);
 		const uint32_t vec = kSlots * slot;
-		for (unsigned st : {3u, 2u}) {
+		for (unsigned st : {kSlots}) {
 			sh.stages = st;
 			const size_t need = smem_for(sh, stage, vec);
 			if (need <= limit) {

@@ -58,6 +58,8 @@ constexpr uint32_t kSuspendHintNs = 20000;
 
 /* flag words of a CTA: ok per slot, then abort, end tile, -, wait limit */
 constexpr unsigned kFAbortSlot = 4;
+/* look-back warps per CTA: one per stage and slot */
+constexpr unsigned kLookbackWarps = 3;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
 /* shared memory header (kSmemHeader bytes) */
@@ -78,6 +80,8 @@ constexpr unsigned kOffPCount = kOffSlotInfo + 16 * kSlots;   /* uint32[kSlots]:
 constexpr unsigned kOffLbuilt = 576;                          /* mbarrier[kSlots]: list written */
 constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
 static_assert(kSlots <= kFAbort, "ok flags per slot");
+static_assert(kLookbackWarps == kSlots, "a look-back warp per slot");
+static_assert(kFEnd == 5 && kFWaitMs == 7, "flag words read by the waits");
 static_assert(kOffHeld + 4 * kMaxStages <= kOffSlotInfo, "smem header layout");
 static_assert(kOffPCount + 4 * kSlots <= kOffLbuilt, "smem header layout");
 static_assert(kOffLbuilt + 8 * kSlots <= kSmemHeader, "smem header overflow");
@@ -228,6 +232,26 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const vo
 		}
 		if (globaltimer_ns() - t0 > limit_ns)
 			return false;
+	}
+}
+
+/* a bounded wait for tile i's phase that also ends (2) once the tiles are
+ * known to end before tile i; 1 when the phase completed, 0 on abort or
+ * time-out */
+__device__ __forceinline__ int mbar_wait_or_end(uint32_t bar, uint32_t phase, const volatile uint32_t *flags,
+	uint32_t i)
+{
+	const uint64_t limit_ns = (uint64_t)flags[7] * 1000000ull;
+	const uint64_t t0 = globaltimer_ns();
+	for (;;) {
+		if (mbar_try_wait_hint(bar, phase, 1000u))
+			return 1;
+		if (flags[kFAbortSlot])
+			return 0;
+		if (flags[5] <= i)
+			return 2;
+		if (globaltimer_ns() - t0 > limit_ns)
+			return 0;
 	}
 }
 
@@ -1227,19 +1251,29 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 
 /* ---- look-back warp: tile totals -> result offsets ----------------------- */
 
+/* Look-back warps: kLookbackWarps of them, warp k taking the tiles
+ * k, k + kLookbackWarps, ... of the CTA.  A launch has as many stages as
+ * slots and look-back warps, so warp k owns stage k and slot k and meets
+ * their barriers' phases in order; the walks over earlier tiles of several
+ * tiles run at the same time. */
 template <int THREADS, int R>
-__device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
+__device__ void lookback_warp(const KParams &kp, unsigned char *smem, int k, int lane)
 {
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
 	uint64_t *offs = reinterpret_cast<uint64_t *>(smem + kOffOff);
 	const uint32_t nst = kp.nstages;
-	/* the previous tile of this CTA: a tile that directly follows it in the
-	 * same query starts where it ended, with no look-back */
+	/* this warp's previous tile: a later tile of the same query can stop its
+	 * walk there, and a tile that directly follows it starts where it
+	 * ended, with no look-back */
 	uint64_t prev_work = ~0ull, prev_end = 0;
-	for (uint32_t i = 0;; i++) {
+	for (uint32_t i = (uint32_t)k;; i += kLookbackWarps) {
 		const uint32_t s = i % nst, q = i % kSlots;
-		/* the tile's data has landed: its work item is known */
-		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
+		/* the tile's data has landed (its work item is known), or the tiles
+		 * ended before it */
+		const int got = mbar_wait_or_end(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags, i);
+		if (got == 2)
+			return;
+		if (got == 0) {
 			give_up(kp, flags, lane);
 			return;
 		}
@@ -1305,11 +1339,14 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 	}
 }
 
-/* projection warps: build the tile's list of selected rows from the
- * filter's ballots, run the projection ops over it into the tile's slot,
- * then give the stage back to the producer */
+/* projection warps: kSlots teams of PT warps, team t taking the tiles t,
+ * t + kSlots, ... (it owns stage t and slot t and meets their barriers'
+ * phases in order), so the projections of different tiles run at the same
+ * time.  A team builds the tile's list of selected rows from the filter's
+ * ballots, runs the projection ops over it into the tile's slot, then gives
+ * the stage back to the producer. */
 template <int THREADS, int R, int P>
-__device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int lane)
+__device__ void proj_warps(const KParams &kp, unsigned char *smem, int team, int pw, int lane)
 {
 	constexpr int TILE = THREADS * R;
 	constexpr int NW = THREADS / 32;
@@ -1319,27 +1356,19 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
 	const uint32_t sbase = smem_addr(smem);
 	const uint32_t nst = kp.nstages;
-	for (uint32_t i = 0;; i++) {
+	for (uint32_t i = (uint32_t)team;; i += kSlots) {
 		const uint32_t s = i % nst, q = i % kSlots;
-		bool ok = mbar_wait(smem_addr(smem + kOffFready + 8 * s), (i / nst) & 1u, flags + kFAbort);
-		/* the slot is free once the stores of its previous tile are done.
-		 * The end of the tiles waits for it too: its arrival on the slot's
-		 * projection barrier must not complete a phase that the look-back
-		 * warp still has to see for the slot's previous tile. */
-		ok = ok && (i < kSlots ||
+		/* the filter is done with the tile, or the tiles ended before it */
+		const int got = mbar_wait_or_end(smem_addr(smem + kOffFready + 8 * s), (i / nst) & 1u, flags, i);
+		/* the end of the tiles (no arrival: the slot's store warp and
+		 * look-back warp see the end themselves) */
+		if (got == 2 || (got == 1 && flags[kFEnd] == i))
+			return;
+		/* the slot is free once the stores of its previous tile are done */
+		const bool ok = got == 1 && (i < kSlots ||
 			mbar_wait(smem_addr(smem + kOffLfree + 8 * q), ((i - kSlots) / kSlots) & 1u, flags + kFAbort));
 		if (!ok) {
-			if (lane == 0 && !flags[kFAbort]) {
-				report(kp.error, DE_STAGE_TIMEOUT);
-				flags[kFAbort] = 1u;
-			}
-			return;
-		}
-		if (flags[kFEnd] == i) {
-			/* no more tiles: tell the store warps */
-			__syncwarp();
-			if (lane == 0)
-				mbar_arrive(smem_addr(smem + kOffCready + 8 * q));
+			give_up(kp, flags, lane);
 			return;
 		}
 		const uint32_t sd = s * kp.stage_bytes;
@@ -1348,7 +1377,8 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
 
 		/* ---- the list: every warp scans the group counts ((chunk, warp,
-		 * half) is row order); warp p writes the rows of chunks p, p + P, ... */
+		 * half) is row order); warp p of the team writes the rows of chunks
+		 * p, p + P, ... */
 		const uint32_t cnt = qd + kStageCnt;
 		uint32_t lane_pre[PER];
 		uint32_t sum = 0;
@@ -1388,18 +1418,18 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 						sts_u16(list + 2 * at++, row0 + k);
 			}
 		}
-		/* every projection warp reads entries the others wrote (a bounded
-		 * rendezvous of the projection warps) */
-		__syncwarp();
-		if (lane == 0)
-			mbar_arrive(smem_addr(smem + kOffLbuilt + 8 * q));
-		if (!mbar_wait(smem_addr(smem + kOffLbuilt + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
-			if (lane == 0 && !flags[kFAbort]) {
-				report(kp.error, DE_STAGE_TIMEOUT);
-				flags[kFAbort] = 1u;
+		/* every warp of the team reads entries the others wrote (a bounded
+		 * rendezvous of the team) */
+		if (P > 1) {
+			__syncwarp();
+			if (lane == 0)
+				mbar_arrive(smem_addr(smem + kOffLbuilt + 8 * q));
+			if (!mbar_wait(smem_addr(smem + kOffLbuilt + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+				give_up(kp, flags, lane);
+				return;
 			}
-			return;
 		}
+		__syncwarp();
 
 		PArgs c;
 		c.sbase = sbase;
@@ -1430,25 +1460,24 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 	}
 }
 
-/* store warps: once the tile's projection is done and the look-back
- * resolved its offset, its result columns go from the slot to device
- * memory at offset + entry (coalesced), and the slot is released */
+/* store warps: one per slot.  Once the tile's projection is done and the
+ * look-back resolved its offset, its result columns go from the slot to
+ * device memory at offset + entry (coalesced), and the slot is released */
 template <int THREADS, int R, int S>
 __device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int lane)
 {
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
 	const uint32_t sbase = smem_addr(smem);
-	for (uint32_t i = 0;; i++) {
+	/* store warp q owns slot q: the tiles q, q + kSlots, ... */
+	for (uint32_t i = (uint32_t)sw;; i += kSlots) {
 		const uint32_t q = i % kSlots;
-		if (!mbar_wait(smem_addr(smem + kOffCready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
-			if (lane == 0 && !flags[kFAbort]) {
-				report(kp.error, DE_STAGE_TIMEOUT);
-				flags[kFAbort] = 1u;
-			}
+		const int got = mbar_wait_or_end(smem_addr(smem + kOffCready + 8 * q), (i / kSlots) & 1u, flags, i);
+		if (got == 2)
+			return;
+		if (got == 0) {
+			give_up(kp, flags, lane);
 			return;
 		}
-		if (flags[kFEnd] == i)
-			return;
 		if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
 			give_up(kp, flags, lane);
 			return;
@@ -1463,8 +1492,8 @@ __device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int 
 		 * a serving session's host writes descriptors while the kernel
 		 * runs) */
 		const QDesc *gq = kp.queries + qi;
-		const uint32_t e0 = 32u * (uint32_t)sw + (uint32_t)lane;
-		if (e0 - (uint32_t)lane < n) {
+		const uint32_t e0 = (uint32_t)lane;
+		if (n) {
 			const uint32_t vd = q * gq->vec_slot;
 			const uint64_t cap = gq->capacity;
 			const uint32_t nout = gq->prog.nout;
@@ -1474,12 +1503,12 @@ __device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int 
 				void *out = gq->out_ptr[j];
 				const uint32_t stride = gq->prog.out_stride[j];
 				if (stride == 4)
-					ok &= store_column<uint32_t>(src, e0, n, 32u * S, static_cast<uint32_t *>(out), off, cap);
+					ok &= store_column<uint32_t>(src, e0, n, 32u, static_cast<uint32_t *>(out), off, cap);
 				else if (stride == 8)
-					ok &= store_column<unsigned long long>(src, e0, n, 32u * S,
+					ok &= store_column<unsigned long long>(src, e0, n, 32u,
 						static_cast<unsigned long long *>(out), off, cap);
 				else
-					ok &= store_column<unsigned char>(src, e0, n, 32u * S, static_cast<unsigned char *>(out),
+					ok &= store_column<unsigned char>(src, e0, n, 32u, static_cast<unsigned char *>(out),
 						off, cap);
 			}
 			/* a serving session reports rows beyond capacity in the
@@ -1490,24 +1519,18 @@ __device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int 
 		__syncwarp();
 		if (lane == 0) {
 			if (kp.serve != nullptr) {
-				/* serving: the last store warp to finish the tile counts it;
-				 * the query's last tile writes its completion record */
+				/* serving: the tile is stored; the query's last tile writes
+				 * its completion record */
 				__threadfence();
-				uint32_t before;
-				asm volatile("atom.shared.add.u32 %0, [%1], 1;"
-					: "=r"(before) : "r"(sbase + kOffPCount + 4 * q) : "memory");
-				if (before == (uint32_t)S - 1u) {
-					sts_u32(sbase + kOffPCount + 4 * q, 0u);
-					const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
-					if (done == (unsigned)gq->ntiles) {
-						__threadfence();
-						const unsigned long long rows =
-							*reinterpret_cast<volatile unsigned long long *>(gq->total_out);
-						volatile ServeRec *r = kp.recs + qi;
-						r->rows = rows;
-						__threadfence_system();
-						r->seq = (unsigned long long)qi + 1ull;
-					}
+				const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
+				if (done == (unsigned)gq->ntiles) {
+					__threadfence();
+					const unsigned long long rows =
+						*reinterpret_cast<volatile unsigned long long *>(gq->total_out);
+					volatile ServeRec *r = kp.recs + qi;
+					r->rows = rows;
+					__threadfence_system();
+					r->seq = (unsigned long long)qi + 1ull;
 				}
 			}
 			mbar_arrive(smem_addr(smem + kOffLfree + 8 * q));
@@ -1515,19 +1538,23 @@ __device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int 
 	}
 }
 
-/* projection warps per CTA: half the filter warps, 1 to 4; store warps:
- * half the projection warps, at least 1 */
+/* projection warps per team: two from 256 filter threads on, else one;
+ * kSlots teams.  Store warps: one per slot. */
+template <int THREADS>
+struct TeamWarps {
+	static constexpr int value = THREADS >= 256 ? 2 : 1;
+};
 template <int THREADS>
 struct ProjWarps {
-	static constexpr int value = THREADS / 64 < 1 ? 1 : THREADS / 64 > 4 ? 4 : THREADS / 64;
+	static constexpr int value = (int)kSlots * TeamWarps<THREADS>::value;
 };
 template <int THREADS>
 struct StoreWarps {
-	static constexpr int value = ProjWarps<THREADS>::value / 2 < 1 ? 1 : ProjWarps<THREADS>::value / 2;
+	static constexpr int value = (int)kSlots;
 };
 
 template <int THREADS, int R>
-__global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value))
+__global__ void __launch_bounds__(THREADS + 32 * (1 + kLookbackWarps + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), 1)
 vm_kernel(const KParams kp)
 {
 	constexpr int NW = THREADS / 32;
@@ -1547,18 +1574,18 @@ vm_kernel(const KParams kp)
 	if (tid == 0) {
 		for (uint32_t s = 0; s < nst; s++) {
 			mbar_init(smem_addr(smem + kOffFull + 8 * s), 1);
-			/* a stage is free once the projection warps and the look-back
-			 * warp are done with it */
-			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), P + 1);
+			/* a stage is free once its projection team and look-back warp
+			 * are done with it */
+			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), TeamWarps<THREADS>::value + 1);
 			mbar_init(smem_addr(smem + kOffCdone + 8 * s), NW);
 			mbar_init(smem_addr(smem + kOffFready + 8 * s), 1);
 			mbar_init(smem_addr(smem + kOffSready + 8 * s), 1);
 		}
 		for (uint32_t q = 0; q < kSlots; q++) {
-			mbar_init(smem_addr(smem + kOffLfree + 8 * q), S);
-			mbar_init(smem_addr(smem + kOffCready + 8 * q), P);
+			mbar_init(smem_addr(smem + kOffLfree + 8 * q), 1);
+			mbar_init(smem_addr(smem + kOffCready + 8 * q), TeamWarps<THREADS>::value);
 			mbar_init(smem_addr(smem + kOffOready + 8 * q), 1);
-			mbar_init(smem_addr(smem + kOffLbuilt + 8 * q), P);
+			mbar_init(smem_addr(smem + kOffLbuilt + 8 * q), TeamWarps<THREADS>::value);
 		}
 		for (int x = 0; x < 8; x++)
 			flags[x] = 0;
@@ -1575,16 +1602,18 @@ vm_kernel(const KParams kp)
 		producer<THREADS * R>(kp, smem, lane);
 		return;
 	}
-	if (warp == NW + 1) {
-		lookback_warp<THREADS, R>(kp, smem, lane);
+	constexpr int LB = NW + 1, PW = LB + (int)kLookbackWarps, SW = PW + P;
+	if (warp >= SW) {
+		store_warps<THREADS, R, S>(kp, smem, warp - SW, lane);
 		return;
 	}
-	if (warp >= NW + 2 + P) {
-		store_warps<THREADS, R, S>(kp, smem, warp - (NW + 2 + P), lane);
+	if (warp >= PW) {
+		constexpr int T = TeamWarps<THREADS>::value;
+		proj_warps<THREADS, R, T>(kp, smem, (warp - PW) / T, (warp - PW) % T, lane);
 		return;
 	}
-	if (warp >= NW + 2) {
-		proj_warps<THREADS, R, P>(kp, smem, warp - (NW + 2), lane);
+	if (warp >= LB) {
+		lookback_warp<THREADS, R>(kp, smem, warp - LB, lane);
 		return;
 	}
 
@@ -1714,7 +1743,7 @@ static int launch_t(const KParams &kp, unsigned grid, size_t smem, cudaStream_t 
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
 	/* THREADS filter threads, the producer and look-back warps, the projection and store warps */
-	fn<<<grid, THREADS + 32 * (2 + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem, stream>>>(kp);
+	fn<<<grid, THREADS + 32 * (1 + kLookbackWarps + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem, stream>>>(kp);
 	return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1724,7 +1753,7 @@ static int occ_t(size_t smem, int *ctas)
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (2 + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem) == cudaSuccess;
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (1 + kLookbackWarps + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem) == cudaSuccess;
 }
 
 #define VGPU_SHAPES(X) X(128, 4) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
@@ -1739,6 +1768,9 @@ int shape_supported(const Shape &s)
 
 int launch_vm(const Shape &s, const KParams &kp, unsigned grid, size_t smem, void *stream)
 {
+	/* a look-back warp per stage and slot */
+	if (kp.nstages != kLookbackWarps)
+		return 0;
 #define X(T, R) \
 	if (s.threads == T && s.rows_per_thread == R) return launch_t<T, R>(kp, grid, smem, (cudaStream_t)stream);
 	VGPU_SHAPES(X)
