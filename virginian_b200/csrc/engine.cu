@@ -117,7 +117,7 @@ int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, 
 	 * tile's fixed costs - claim, look-back, barriers - spread over many
 	 * rows, and loads in flight while two tiles are processed); then
 	 * smaller tiles for programs whose staging does not fit */
-	static const unsigned cand[][2] = {{512, 4}, {256, 8}, {256, 4}, {128, 8}};
+	static const unsigned cand[][2] = {{512, 4}, {256, 8}, {256, 4}, {128, 8}, {128, 4}};
 	const size_t limit = (size_t)e->smem_optin;
 	for (int pass = 1; pass < 2; pass++)
 	for (auto &c : cand) {

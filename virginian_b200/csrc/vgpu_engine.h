@@ -51,7 +51,7 @@ struct StageInfo {
 
 /* tiles in flight between the projection and the stores of a CTA: slots of
  * the selection lists, projection vectors, result copies and offsets */
-constexpr unsigned kSlots = 3;
+constexpr unsigned kSlots = 4;
 
 /* every stage starts with a copy of its tile's query descriptor and the
  * tile's StageInfo, then the filter's result for the tile (four bit-plane

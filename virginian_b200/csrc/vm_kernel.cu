@@ -59,7 +59,7 @@ constexpr uint32_t kSuspendHintNs = 20000;
 /* flag words of a CTA: ok per slot, then abort, end tile, -, wait limit */
 constexpr unsigned kFAbortSlot = 4;
 /* look-back warps per CTA: one per stage and slot */
-constexpr unsigned kLookbackWarps = 3;
+constexpr unsigned kLookbackWarps = kSlots;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
 /* shared memory header (kSmemHeader bytes) */
@@ -75,9 +75,9 @@ constexpr unsigned kOffOff = kOffOready + 8 * kSlots;         /* uint64[kSlots]:
 constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;          /* uint32[8]: ok[kSlots], abort, end tile */
 constexpr unsigned kOffTot = kOffFlags + 32;                  /* uint32[kSlots]: tile totals */
 constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;           /* uint32[kMaxStages]: query per stage */
-constexpr unsigned kOffSlotInfo = 512;                        /* uint32[kSlots][4]: query, segment, first row */
+constexpr unsigned kOffSlotInfo = 544;                        /* uint32[kSlots][4]: query, segment, first row */
 constexpr unsigned kOffPCount = kOffSlotInfo + 16 * kSlots;   /* uint32[kSlots]: store warps done (serving) */
-constexpr unsigned kOffLbuilt = 576;                          /* mbarrier[kSlots]: list written */
+constexpr unsigned kOffLbuilt = 640;                          /* mbarrier[kSlots]: list written */
 constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
 static_assert(kSlots <= kFAbort, "ok flags per slot");
 static_assert(kLookbackWarps == kSlots, "a look-back warp per slot");
@@ -1538,11 +1538,12 @@ __device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int 
 	}
 }
 
-/* projection warps per team: two from 256 filter threads on, else one;
- * kSlots teams.  Store warps: one per slot. */
+/* projection warps per team: two with 256 filter threads, else one (a
+ * block of 512 filter threads and kSlots two-warp teams would pass 1024
+ * threads); kSlots teams.  Store warps: one per slot. */
 template <int THREADS>
 struct TeamWarps {
-	static constexpr int value = THREADS >= 256 ? 2 : 1;
+	static constexpr int value = THREADS == 256 ? 2 : 1;
 };
 template <int THREADS>
 struct ProjWarps {
@@ -1566,6 +1567,7 @@ vm_kernel(const KParams kp)
 	static_assert(R % 4 == 0 && R <= 32, "rows per thread: whole 4-row chunks, 32-bit row masks");
 	static_assert(G <= (int)kMaxGroups, "64-row groups per tile");
 	static_assert(THREADS * R <= 65536, "tile rows are 16-bit in the selection lists");
+	static_assert(THREADS + 32 * (1 + kLookbackWarps + P + S) <= 1024, "threads per block");
 	extern __shared__ __align__(128) unsigned char smem[];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
