@@ -41,6 +41,11 @@ import numpy as np  # noqa: E402
 
 ROWS = 50_000_000
 HEADLINE_SEL = 0.10
+# DRAM bytes of the headline kernel per scanned row and per result row,
+# from ncu (dram__bytes_read.sum, dram__bytes_write.sum) on an 8M-row launch
+# of the same query: 224.27 MB read, 11.84 MB written for 800,581 result rows
+TRAFFIC_READ_PER_ROW = 224.266496e6 / 8_000_000
+TRAFFIC_WRITE_PER_RESULT_ROW = 11.84128e6 / 800_581
 SWEEP = [0.001, 0.01, 0.10, 0.50, 0.99]
 QUERY = ("SELECT id, uniformf + normalf5 * 2.5 AS fsum, normali20 / 3 AS idiv, "
          "uniformi - normali5 AS isub FROM test WHERE uniformf < {c:.6f} OR normalf20 > {d:.6f}")
@@ -562,7 +567,10 @@ def run_b200(args):
 
     def timed(p, steps, warmup):
         # pick the launch shape for this program and table (untimed; cached)
-        tuned = vb.tune(eng, p, table)
+        if args.shape:
+            eng.set_shape(*args.shape)
+        else:
+            vb.tune(eng, p, table)
         for _ in range(warmup):
             r = table.query(p)
             n = r.rows
@@ -676,7 +684,10 @@ def run_b200(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
                          "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4) if achieved else None,
-                         "traffic": None, "peak_kind": peak_kind,
+                         "traffic": int(rows * TRAFFIC_READ_PER_ROW + out_rows * TRAFFIC_WRITE_PER_RESULT_ROW),
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture "
+                                           "of this kernel on 8M rows of the same query, scaled by rows",
+                         "peak_kind": peak_kind,
                          "kernel_ms": round(kernel_ms, 4) if kernel_ms else None,
                          "algorithmic_bytes": alg},
             "sweep": sweep,
@@ -719,9 +730,12 @@ def main():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--cpu-rows", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--shape", default="", help="threads,rows_per_thread,stages: force the launch "
+                    "shape of the scan instead of tuning it (for profiling one launch)")
     ap.add_argument("--sections", default="batched,serving,streamed",
                     help="workloads besides the headline scan (comma list; empty for none)")
     args = ap.parse_args()
+    args.shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else ()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -266,8 +266,7 @@ typedef struct {
 	unsigned out_bytes_per_row;
 	unsigned nuops;                 /* interpreted device ops */
 	unsigned row_vector_bytes;      /* per row: register vectors the filter writes */
-	unsigned sel_vector_bytes;      /* per row: register vectors only the projection writes, and
-	                                   copies of the other result columns */
+	unsigned sel_vector_bytes;      /* per row: register vectors only the projection writes */
 } virg_gpu_program_info;
 
 /* thread-local description of the last failure on this thread */
@@ -430,7 +429,7 @@ typedef struct {
 	unsigned idle_us;                /* end an idle session after this long (0: 2000) */
 	unsigned max_load_bytes_per_row; /* staged column bytes a program may read (0: 32) */
 	unsigned max_row_vector_bytes;   /* filter register-vector bytes per row (0: 16) */
-	unsigned max_sel_vector_bytes;   /* projection register-vector and result-copy bytes per row (0: 48) */
+	unsigned max_sel_vector_bytes;   /* projection register-vector bytes per row (0: 48) */
 	unsigned wait_limit_ms;          /* bound of the kernel's waits (0: 60000) */
 } virg_serve_config;
 

@@ -87,7 +87,7 @@ def test_query_host_end_to_end(data_a, engine):
                                    (512, 8)])
 def test_every_launch_shape(data_a, engine, shape):
     db, _, t = data_a
-    engine.set_shape(shape[0], shape[1], 0)
+    engine.set_shape(shape[0], shape[1], 2)
     try:
         for sql in (CONFIG1, config2(30.0, 20.0), SUITE[8]):
             try:

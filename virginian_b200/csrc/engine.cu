@@ -49,59 +49,71 @@ static int type_bytes(int t)
 			VGPU_FAIL("%s: %s", what, cudaGetErrorString(e_));                      \
 	} while (0)
 
-/* smem layout of a program for a tile size.  A stage holds the query
- * descriptor, the tile's info and filter result, its staged columns and
- * the register vectors by tile row (the filter writes them; load_off and
- * those vec_off are stage offsets).  A slot (one of kSlots, one per tile
- * between projection and stores) holds the register vectors by selection
- * position (only the projection writes them) and the copies of the other
- * result columns (out_off), at slot offsets.  Any output may be null. */
-void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *vec_off, uint32_t *out_off,
-	uint32_t *stage_bytes, uint32_t *slot_bytes)
+/* smem bytes a program needs per stage and for its register vectors.
+ * Vectors indexed by tile row (written by the filter) get kSlots slots, one
+ * per tile in flight between filter and stores; vectors indexed by
+ * selection position (written and read only by the projection warps) get
+ * one.  The vector region of a launch is [row slots | selection vectors],
+ * sized for the largest of its programs, so that one query's row slot never
+ * overlaps another's selection vectors. */
+void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
+	uint32_t *row_bytes, uint32_t *sel_bytes)
 {
+	/* a stage: query descriptor + tile info header, then the columns */
 	uint32_t off = kStageHdr;
 	for (unsigned i = 0; i < P.nload; i++) {
 		if (load_off)
 			load_off[i] = off;
 		off += (uint32_t)align_up((size_t)tile * P.load_stride[i], 128);
 	}
-	uint32_t slot = 0;
+	*stage_bytes = off;
+	uint32_t row = 0, sel = 0;
 	for (unsigned i = 0; i < P.nvec; i++) {
-		uint32_t &at = P.vec_compact[i] ? slot : off;
-		if (vec_off)
-			vec_off[i] = at;
-		at += (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
+		const uint32_t sz = (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
+		if (P.vec_compact[i])
+			sel += sz;
+		else
+			row += sz;
 	}
-	for (unsigned j = 0; j < P.nout; j++) {
-		if (out_off)
-			out_off[j] = slot;
-		if (out_copied(P, j))
-			slot += (uint32_t)align_up((size_t)tile * P.out_stride[j], 128);
-	}
-	if (stage_bytes)
-		*stage_bytes = off;
-	if (slot_bytes)
-		*slot_bytes = slot;
+	*row_bytes = row;
+	*sel_bytes = sel;
 }
 
-/* stage bytes, slot bytes and vector-region bytes (kSlots slots) of a
- * launch: the largest of its programs' */
-void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uint32_t *stage_bytes,
-	uint32_t *slot_bytes, uint32_t *vec_bytes)
+/* offsets of a program's vectors in a launch's vector region whose row slots
+ * are row_slot bytes apart */
+void vec_offsets(const Program &P, unsigned tile, uint32_t row_slot, uint32_t *vec_off)
 {
-	uint32_t stage = 0, slot = 0;
+	uint32_t r = 0, s = kSlots * row_slot;
+	for (unsigned i = 0; i < P.nvec; i++) {
+		const uint32_t sz = (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
+		if (P.vec_compact[i]) {
+			vec_off[i] = s;
+			s += sz;
+		} else {
+			vec_off[i] = r;
+			r += sz;
+		}
+	}
+}
+
+/* stage bytes, row-slot bytes and vector-region bytes of a launch */
+void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uint32_t *stage_bytes,
+	uint32_t *row_slot, uint32_t *vec_bytes)
+{
+	uint32_t stage = 0, row = 0, sel = 0;
 	for (const Program *P : progs) {
-		uint32_t sb, lb;
-		program_layout(*P, tile, nullptr, nullptr, nullptr, &sb, &lb);
+		uint32_t sb, rb, vb;
+		program_layout(*P, tile, nullptr, &sb, &rb, &vb);
 		stage = std::max(stage, sb);
-		slot = std::max(slot, lb);
+		row = std::max(row, rb);
+		sel = std::max(sel, vb);
 	}
 	*stage_bytes = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
-	*slot_bytes = (uint32_t)align_up(slot, 128);
-	*vec_bytes = kSlots * *slot_bytes;
+	*row_slot = row;
+	*vec_bytes = kSlots * row + sel;
 }
 
-/* header | stages x stage bytes | slots | selection lists */
+/* header | stages x stage bytes | register vectors | selection lists */
 size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes)
 {
 	/* a selection list (a tile row per selected row) per slot: a tile's list
@@ -117,7 +129,7 @@ int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, 
 	 * tile's fixed costs - claim, look-back, barriers - spread over many
 	 * rows, and loads in flight while two tiles are processed); then
 	 * smaller tiles for programs whose staging does not fit */
-	static const unsigned cand[][2] = {{512, 4}, {256, 8}, {256, 4}, {128, 8}, {128, 4}};
+	static const unsigned cand[][2] = {{512, 4}, {256, 8}, {256, 4}, {128, 8}};
 	const size_t limit = (size_t)e->smem_optin;
 	for (int pass = 1; pass < 2; pass++)
 	for (auto &c : cand) {
@@ -126,11 +138,10 @@ int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, 
 		s.rows_per_thread = e->pref.rows_per_thread ? e->pref.rows_per_thread : c[1];
 		if (!shape_supported(s))
 			VGPU_FAIL("unsupported launch shape %u threads x %u rows", s.threads, s.rows_per_thread);
-		uint32_t stage, slot, vec;
-		launch_layout(progs, s.tile(), &stage, &slot, &vec);
+		uint32_t stage, row_slot, vec;
+		launch_layout(progs, s.tile(), &stage, &row_slot, &vec);
 		/* a requested stage count is kept, at one CTA per SM if need be */
-		/* as many stages as slots: the kernel has a look-back warp per stage */
-		const unsigned st_list[] = {kSlots};
+		const unsigned st_list[] = {e->pref.stages ? e->pref.stages : 3u, e->pref.stages ? 0u : 2u};
 		for (unsigned st : st_list) {
 			if (st == 0)
 				continue;
@@ -197,20 +208,16 @@ static uint32_t op_head(const UOp &u)
 }
 
 /* operand descriptors of a query descriptor whose program, load_off and
- * vec_off are set, for slots starting at vec_area, with the result copies
- * at out_off in a slot */
-void fill_operands(QDesc &d, uint32_t vec_area, const uint32_t *out_off)
+ * vec_off are set, for register vectors starting at vec_area */
+void fill_operands(QDesc &d, uint32_t vec_area)
 {
 	const Program &P = d.prog;
-	/* staged columns, register vectors by tile row and the stage's copy of
-	 * the descriptor's constants, by offset in stage 0; register vectors by
-	 * selection position by offset in slot 0 */
 	auto od = [&](uint8_t cls, uint8_t idx) -> uint32_t {
 		if (cls == OC_COL)
 			return OD_STAGE | (uint32_t)(kSmemHeader + d.load_off[idx]);
 		if (cls == OC_VEC)
-			return P.vec_compact[idx] ? OD_SELVEC | (vec_area + d.vec_off[idx])
-				: OD_ROWVEC | (uint32_t)(kSmemHeader + d.vec_off[idx]);
+			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | (vec_area + d.vec_off[idx]);
+		/* scalars are read from the stage's copy of the descriptor */
 		return OD_SCALAR |
 			(uint32_t)(kSmemHeader + offsetof(QDesc, prog) + offsetof(Program, consts) + idx * 8u);
 	};
@@ -222,23 +229,8 @@ void fill_operands(QDesc &d, uint32_t vec_area, const uint32_t *out_off)
 		r.b = od(u.b_cls, u.b_idx);
 		r.d = od(OC_VEC, u.dst);
 	}
-	/* the result columns, by selection position in the slot: projection
-	 * vectors as they are, everything else copied there by an op that
-	 * takes the Result's place */
-	uint32_t k = P.nuops > 0 ? P.nuops - 1 : 0;
-	for (uint32_t j = 0; j < P.nout; j++) {
-		if (!out_copied(P, j)) {
-			d.od_out[j] = od(P.out_cls[j], P.out_idx[j]);
-			continue;
-		}
-		d.od_out[j] = OD_SELVEC | (vec_area + out_off[j]);
-		OpRec &r = d.ops[k++];
-		r.head = OK_COPY | (1u << (OT_SHIFT + P.out_type[j]));
-		r.a = od(P.out_cls[j], P.out_idx[j]);
-		r.b = 0;
-		r.d = d.od_out[j];
-	}
-	d.op_end = k;
+	for (uint32_t j = 0; j < P.nout; j++)
+		d.od_out[j] = od(P.out_cls[j], P.out_idx[j]);
 }
 
 size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles)
@@ -272,8 +264,8 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 	}
 	const unsigned tile = plan.shape.tile();
 	const size_t nq = qs.size();
-	uint32_t stage_all, slot, vec_all;
-	launch_layout(progs, tile, &stage_all, &slot, &vec_all);
+	uint32_t stage_all, row_slot, vec_all;
+	launch_layout(progs, tile, &stage_all, &row_slot, &vec_all);
 	size_t off_prefix, off_tiles;
 	const size_t blob_bytes = plan_blob_bytes(qs, &off_prefix, &off_tiles);
 	plan.blob.assign(blob_bytes, 0);
@@ -288,9 +280,10 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		const QueryLaunch &q = qs[i];
 		QDesc &d = hq[i];
 		d.prog = *q.prog;
-		uint32_t sb, out_off[kMaxRegs];
-		program_layout(*q.prog, tile, d.load_off, d.vec_off, out_off, &sb, nullptr);
-		d.vec_slot = slot;
+		uint32_t sb, rb, vb;
+		program_layout(*q.prog, tile, d.load_off, &sb, &rb, &vb);
+		vec_offsets(*q.prog, tile, row_slot, d.vec_off);
+		d.vec_slot = row_slot;
 		d.stage_bytes = sb;
 		d.segs = q.d_segs;
 		d.nsegs = q.nsegs;
@@ -313,7 +306,7 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		d.total_out = q.d_total;
 		d.block_counts = q.block_counts;
 		d.base_in = q.base_in;
-		fill_operands(d, (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes), out_off);
+		fill_operands(d, (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes));
 	}
 	hprefix[nq] = work;
 	VGPU_CHECK(work < 0xFFFFFFF0ull, "too many tiles in one launch (%llu)", (unsigned long long)work);
@@ -576,7 +569,7 @@ extern "C" int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p
 	Shape best_shape = {0, 0, 0, 0};
 	std::string key;
 	for (auto &c : cand)
-		for (unsigned st : {kSlots}) {
+		for (unsigned st = 2; st <= 4; st++) {
 			e->force = Shape{c[0], c[1], st, 0};
 			float t_best = 1e30f;
 			bool ran = true;
@@ -641,7 +634,7 @@ extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 		s.rows_per_thread = rows_per_thread ? rows_per_thread : 4;
 		VGPU_CHECK(shape_supported(s), "unsupported shape %u x %u", s.threads, s.rows_per_thread);
 	}
-	VGPU_CHECK(stages == 0 || stages == kSlots, "the kernel runs %u stages", kSlots);
+	VGPU_CHECK(stages <= kMaxStages, "at most %u stages", kMaxStages);
 	e->pref.threads = threads;
 	e->pref.rows_per_thread = rows_per_thread;
 	e->pref.stages = stages;

@@ -114,12 +114,13 @@ struct Plan {
 	unsigned grid = 0;
 };
 
-void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *vec_off, uint32_t *out_off,
-	uint32_t *stage_bytes, uint32_t *slot_bytes);
+void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
+	uint32_t *row_bytes, uint32_t *sel_bytes);
+void vec_offsets(const Program &P, unsigned tile, uint32_t row_slot, uint32_t *vec_off);
 void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uint32_t *stage_bytes,
-	uint32_t *slot_bytes, uint32_t *vec_bytes);
+	uint32_t *row_slot, uint32_t *vec_bytes);
 size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes);
-void fill_operands(QDesc &d, uint32_t vec_area, const uint32_t *out_off);
+void fill_operands(QDesc &d, uint32_t vec_area);
 size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles);
 int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Shape *forced,
 	unsigned char *db, Plan &plan);

@@ -110,11 +110,11 @@ int pick_shape(const Program &P, int smem_optin, Shape *shape, size_t *smem, uin
 	const size_t limit = (size_t)smem_optin;
 	for (int pass = 0; pass < 2; pass++)
 		for (auto &c : cand)
-			for (unsigned st : {kSlots}) {
+			for (unsigned st : {3u, 2u}) {
 				Shape s = {c[0], c[1], st, 0};
-				uint32_t sb, lb;
-				program_layout(P, s.tile(), nullptr, nullptr, nullptr, &sb, &lb);
-				const uint32_t vb = kSlots * ((lb + 127) / 128 * 128);
+				uint32_t sb, rb, selb;
+				program_layout(P, s.tile(), nullptr, &sb, &rb, &selb);
+				const uint32_t vb = kSlots * rb + selb;
 				sb = ((sb < 128 ? 128 : sb) + 127) / 128 * 128;
 				const size_t need = smem_for(s, sb, vb);
 				if (need <= (pass == 0 ? limit / 2 - 1024 : limit)) {
@@ -186,9 +186,10 @@ extern "C" int virg_gpu_query_prealloc(const virg_gpu_program *p, const virg_gpu
 	unsigned char *const db = ds.scratch;
 	QDesc &d = *reinterpret_cast<QDesc *>(hb);
 	d.prog = P;
-	uint32_t sb, out_off[kMaxRegs];
-	program_layout(P, tile, d.load_off, d.vec_off, out_off, &sb, nullptr);
-	d.vec_slot = vec_bytes / kSlots;
+	uint32_t sb, rb, selb;
+	program_layout(P, tile, d.load_off, &sb, &rb, &selb);
+	vec_offsets(P, tile, rb, d.vec_off);
+	d.vec_slot = rb;
 	d.stage_bytes = sb;
 	d.segs = reinterpret_cast<const SegDesc *>(db + kOffSeg);
 	d.nsegs = 1;
@@ -202,7 +203,7 @@ extern "C" int virg_gpu_query_prealloc(const virg_gpu_program *p, const virg_gpu
 	d.block_counts = nullptr;
 	d.base_in = nullptr;
 	const uint32_t vec_area = (uint32_t)(kSmemHeader + (size_t)shape.stages * stage_bytes);
-	fill_operands(d, vec_area, out_off);
+	fill_operands(d, vec_area);
 	uint64_t *prefix = reinterpret_cast<uint64_t *>(hb + kOffPrefix);
 	prefix[0] = 0;
 	prefix[1] = ntiles;

@@ -581,10 +581,8 @@ int virg_gpu_program_info_get(const virg_gpu_program *p, virg_gpu_program_info *
 		info->out_bytes_per_row += P.out_stride[j];
 	}
 	info->nuops = P.nuops;
-	uint32_t row, sel;
-	vector_bytes_per_row(P, &row, &sel);
-	info->row_vector_bytes = row;
-	info->sel_vector_bytes = sel;
+	for (unsigned i = 0; i < P.nvec; i++)
+		(P.vec_compact[i] ? info->sel_vector_bytes : info->row_vector_bytes) += P.vec_stride[i];
 	return 1;
 }
 

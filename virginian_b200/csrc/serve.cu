@@ -127,7 +127,7 @@ struct virg_serve {
 	/* the session's launch layout (one shape for every query it takes) */
 	Shape shape{};
 	size_t smem = 0;
-	uint32_t stage_bytes = 0, slot_bytes = 0, vec_bytes = 0;
+	uint32_t stage_bytes = 0, row_slot = 0, vec_bytes = 0, sel_bytes = 0;
 	unsigned grid = 0;
 	cudaStream_t kstream = nullptr, ustream = nullptr;
 	/* device memory */
@@ -191,23 +191,24 @@ int serve_layout(virg_serve *s)
 {
 	virg_gpu_engine *e = s->e;
 	const size_t limit = (size_t)e->smem_optin;
-	static const unsigned cand[][2] = {{256, 4}, {128, 8}, {256, 8}, {512, 4}, {128, 4}};
+	static const unsigned cand[][2] = {{256, 4}, {128, 8}, {256, 8}, {512, 4}};
 	for (auto &c : cand) {
 		Shape sh = {c[0], c[1], 0, 0};
 		const unsigned tile = sh.tile();
-		const uint32_t stage = (uint32_t)align_up(
-			kStageHdr + (size_t)tile * (s->cfg.max_load_bytes_per_row + s->cfg.max_row_vector_bytes), 128);
-		const uint32_t slot = (uint32_t)align_up((size_t)tile * s->cfg.max_sel_vector_bytes, 128);
-		const uint32_t vec = kSlots * slot;
-		for (unsigned st : {kSlots}) {
+		const uint32_t stage = (uint32_t)align_up(kStageHdr + (size_t)tile * s->cfg.max_load_bytes_per_row, 128);
+		const uint32_t row = (uint32_t)align_up((size_t)tile * s->cfg.max_row_vector_bytes, 128);
+		const uint32_t sel = (uint32_t)align_up((size_t)tile * s->cfg.max_sel_vector_bytes, 128);
+		const uint32_t vec = kSlots * row + sel;
+		for (unsigned st : {3u, 2u}) {
 			sh.stages = st;
 			const size_t need = smem_for(sh, stage, vec);
 			if (need <= limit) {
 				s->shape = sh;
 				s->smem = need;
 				s->stage_bytes = stage;
-				s->slot_bytes = slot;
+				s->row_slot = row;
 				s->vec_bytes = vec;
+				s->sel_bytes = sel;
 				int per_sm = 0;
 				if (!occupancy(sh, need, &per_sm))
 					VGPU_FAIL("occupancy query failed");
@@ -222,10 +223,11 @@ int serve_layout(virg_serve *s)
 /* does a program fit the session's layout */
 int program_fits(const virg_serve *s, const Program &P, const char **why)
 {
-	uint32_t load = 0, row, sel;
+	uint32_t load = 0, row = 0, sel = 0;
 	for (unsigned i = 0; i < P.nload; i++)
 		load += P.load_stride[i];
-	vector_bytes_per_row(P, &row, &sel);
+	for (unsigned i = 0; i < P.nvec; i++)
+		(P.vec_compact[i] ? sel : row) += P.vec_stride[i];
 	if (load > s->cfg.max_load_bytes_per_row) {
 		*why = "the program stages more bytes per row than the serving layout holds";
 		return 0;
@@ -348,9 +350,10 @@ unsigned admit(virg_serve *s)
 		QDesc &d = s->h_qstage[batch.size()];
 		memset(&d, 0, sizeof(d));
 		d.prog = P;
-		uint32_t sb, out_off[kMaxRegs];
-		program_layout(P, tile, d.load_off, d.vec_off, out_off, &sb, nullptr);
-		d.vec_slot = s->slot_bytes;
+		uint32_t sb, rb, vb;
+		program_layout(P, tile, d.load_off, &sb, &rb, &vb);
+		vec_offsets(P, tile, s->row_slot, d.vec_off);
+		d.vec_slot = s->row_slot;
 		d.stage_bytes = sb;
 		d.segs = q.t->d_segs;
 		d.nsegs = (uint32_t)q.t->segs.size();
@@ -371,7 +374,7 @@ unsigned admit(virg_serve *s)
 		d.total_out = s->d_totals + qi;
 		d.block_counts = nullptr;
 		d.base_in = nullptr;
-		fill_operands(d, vec_area, out_off);
+		fill_operands(d, vec_area);
 		s->h_pstage[batch.size()] = work;
 		work += tt;
 		q.qi = qi;
@@ -531,7 +534,7 @@ extern "C" int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cf
 	if (!c.max_row_vector_bytes)
 		c.max_row_vector_bytes = 16;
 	if (!c.max_sel_vector_bytes)
-		c.max_sel_vector_bytes = 48;  /* projection vectors and result copies */
+		c.max_sel_vector_bytes = 48;
 	if (!c.wait_limit_ms)
 		c.wait_limit_ms = 60000;
 	auto fail = [&](const char *what, cudaError_t ce) {

@@ -37,30 +37,23 @@ struct Shape {
 constexpr unsigned kMaxStages = 8;
 constexpr unsigned kSmemHeader = 4096;
 
-/* per-stage work item, decoded by the issuing thread; the filter adds the
- * tile's count of selected rows */
+/* per-stage work item, decoded by the issuing thread */
 struct StageInfo {
 	uint32_t work;      /* global work index, >= total when empty */
 	uint32_t query;
 	uint32_t seg;
 	uint32_t row0;
 	uint32_t nrows;
-	uint32_t total;     /* selected rows, once the filter has run */
-	uint32_t pad[2];
+	uint32_t pad[3];
 };
 
-/* tiles in flight between the projection and the stores of a CTA: slots of
- * the selection lists, projection vectors, result copies and offsets */
-constexpr unsigned kSlots = 4;
+/* every stage starts with a copy of its tile's query descriptor and the tile's
+ * StageInfo, then the staged columns */
+/* tiles in flight between the filter and the stores of a CTA: slots of the
+ * selection lists, row vectors, counts and offsets */
+constexpr unsigned kSlots = 3;
 
-/* every stage starts with a copy of its tile's query descriptor and the
- * tile's StageInfo, then the filter's result for the tile (four bit-plane
- * ballot words per 128-row chunk, valid rows per 64-row group), then the
- * staged columns and the register vectors the filter writes */
-constexpr unsigned kMaxGroups = 128;  /* 64-row groups per tile */
-constexpr unsigned kStageMasks = (unsigned)((sizeof(QDesc) + sizeof(StageInfo) + 127) / 128 * 128);
-constexpr unsigned kStageCnt = kStageMasks + 8 * kMaxGroups;
-constexpr unsigned kStageHdr = kStageCnt + 4 * kMaxGroups;
+constexpr unsigned kStageHdr = (unsigned)((sizeof(QDesc) + sizeof(StageInfo) + 127) / 128 * 128);
 
 /* serving-session control, in host-mapped memory written by the host:
  * published queries and work items (a query's descriptor is complete before

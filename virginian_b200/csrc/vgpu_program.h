@@ -98,26 +98,6 @@ struct Program {
 	uint8_t vec_compact[kMaxRegs];
 };
 
-/* a result column the projection copies into the tile's slot: every one
- * that is not a register vector indexed by selection position */
-inline bool out_copied(const Program &P, unsigned j)
-{
-	return !(P.out_cls[j] == OC_VEC && P.vec_compact[P.out_idx[j]]);
-}
-
-/* register-vector bytes per row: vectors by tile row (the filter writes
- * them), and vectors by selection position with the result copies */
-inline void vector_bytes_per_row(const Program &P, uint32_t *row, uint32_t *sel)
-{
-	*row = 0;
-	*sel = 0;
-	for (unsigned i = 0; i < P.nvec; i++)
-		(P.vec_compact[i] ? *sel : *row) += P.vec_stride[i];
-	for (unsigned j = 0; j < P.nout; j++)
-		if (out_copied(P, j))
-			*sel += P.out_stride[j];
-}
-
 /* operand descriptor resolved for a launch shape: bits [0,30) are a shared
  * memory byte offset, bits [30,32) the kind */
 constexpr uint32_t OD_STAGE = 0u << 30;    /* staged column, + stage offset */
@@ -166,18 +146,15 @@ struct alignas(16) QDesc {
 	uint32_t load_off[kMaxLoads];
 	uint32_t stage_bytes;
 	uint32_t vec_off[kMaxRegs];
-	/* the uops as records (handler, operands): filter uops [0, nfilter),
-	 * then projection uops, then (in place of the Result) one copy per
-	 * result column that is not a projection vector, up to op_end; the
-	 * result columns' slot vectors (by selection position) */
-	OpRec ops[kMaxOps + kMaxRegs];
+	/* the uops as records (handler, operands) and the result columns'
+	 * operand descriptors */
+	OpRec ops[kMaxOps];
 	uint32_t od_out[kMaxRegs];
-	uint32_t op_end;
 	/* inputs */
 	const SegDesc *segs;
 	const uint32_t *seg_tile_prefix;  /* nsegs + 1 entries */
 	uint32_t nsegs;
-	uint32_t vec_slot;                /* distance between two tiles' slots */
+	uint32_t vec_slot;                /* distance between the two row-vector slots */
 	uint64_t work_first;              /* global work index of tile 0 */
 	uint64_t ntiles;
 	/* outputs */

@@ -5,32 +5,26 @@
  * runs one thread per row with a 16-entry register file in local memory, a
  * switch dispatch per op per thread and atomics for (unordered) result
  * placement.  Here a CTA is a pipeline over tiles of TILE = THREADS x R
- * rows, tied together by mbarriers, with five roles:
+ * rows, tied together by mbarriers, with four roles:
  *
  *  - producer warp: claims work items (one tile of one segment of one query)
  *    from a global counter, in order, decodes them warp-wide and copies the
- *    tile's columns (plus the query's descriptor when the stage does not
- *    hold it) into a ring of shared-memory stages with TMA bulk copies
+ *    tile's columns (plus the query's descriptor when the stage does not hold
+ *    it) into a ring of shared-memory stages with TMA bulk copies
  *    (cp.async.bulk completing on the stage's full barrier);
  *  - filter warps (THREADS threads): run the filter ops over every row of the
  *    tile (row state as bit masks: valid, active, and rows parked at pending
  *    jump targets; each lane holds R rows in chunks of 4 consecutive rows),
  *    count valid rows per 64 rows with bit-plane ballots, scan the counts and
- *    write the tile's selected rows, in row order, to the list of one of
- *    kSlots slots, then publish the tile's count to the query's look-back
- *    words;
+ *    write the tile's selected rows, in row order, to a shared list, then
+ *    publish the tile's count to the query's look-back words;
  *  - look-back warp: resolves the tile's position in the query's result with
  *    a warp-wide decoupled look-back over earlier tiles (32 status words per
  *    round); a tile that directly follows the CTA's previous tile of the same
  *    query starts where that one ended, with no look-back;
  *  - projection warps: run the projection ops over the tile's list in
- *    32-entry batches, with results (and a copy of every other result
- *    column) in the slot by list position, then release the stage: no stage
- *    waits for a look-back, so copies and filters of the next tiles run
- *    while up to kSlots tiles wait for their offsets;
- *  - store warps: once the offset is known, write each result row from the
- *    slot to the tile's offset plus its list position (coalesced stores),
- *    then release the slot.
+ *    32-entry batches and write each result row to the tile's offset plus
+ *    its list position (coalesced stores), then release the stage.
  *
  * Each op is one 16-byte record fetched with a single shared-memory load and
  * dispatched on one handler code; operands are read and written by 32-bit
@@ -58,33 +52,29 @@ constexpr uint32_t kSuspendHintNs = 20000;
 
 /* flag words of a CTA: ok per slot, then abort, end tile, -, wait limit */
 constexpr unsigned kFAbortSlot = 4;
-/* look-back warps per CTA: one per stage and slot */
-constexpr unsigned kLookbackWarps = kSlots;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
+/* work items claimed per atomic by the producer: one, so tiles that follow
+ * each other in a query are taken, and finished, at about the same time */
+constexpr unsigned kClaim = 1;
+
 /* shared memory header (kSmemHeader bytes) */
-constexpr unsigned kOffFull = 0;                              /* mbarrier[kMaxStages]: data landed */
-constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;     /* mbarrier[kMaxStages]: stage free */
-constexpr unsigned kOffCdone = kOffEmpty + 8 * kMaxStages;    /* mbarrier[kMaxStages]: counts written */
-constexpr unsigned kOffFready = kOffCdone + 8 * kMaxStages;   /* mbarrier[kMaxStages]: filter done */
-constexpr unsigned kOffSready = kOffFready + 8 * kMaxStages;  /* mbarrier[kMaxStages]: tile total known */
-constexpr unsigned kOffLfree = kOffSready + 8 * kMaxStages;   /* mbarrier[kSlots]: stores done */
-constexpr unsigned kOffCready = kOffLfree + 8 * kSlots;       /* mbarrier[kSlots]: projection done */
-constexpr unsigned kOffOready = kOffCready + 8 * kSlots;      /* mbarrier[kSlots]: offset ready */
-constexpr unsigned kOffOff = kOffOready + 8 * kSlots;         /* uint64[kSlots]: tile offsets */
-constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;          /* uint32[8]: ok[kSlots], abort, end tile */
-constexpr unsigned kOffTot = kOffFlags + 32;                  /* uint32[kSlots]: tile totals */
-constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;           /* uint32[kMaxStages]: query per stage */
-constexpr unsigned kOffSlotInfo = 544;                        /* uint32[kSlots][4]: query, segment, first row */
-constexpr unsigned kOffPCount = kOffSlotInfo + 16 * kSlots;   /* uint32[kSlots]: store warps done (serving) */
-constexpr unsigned kOffLbuilt = 640;                          /* mbarrier[kSlots]: list written */
+constexpr unsigned kMaxGroups = 128;  /* R x warps */
+constexpr unsigned kOffFull = 0;                            /* mbarrier[kMaxStages] */
+constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;   /* mbarrier[kMaxStages] */
+constexpr unsigned kOffLready = kOffEmpty + 8 * kMaxStages; /* mbarrier[kSlots]: list and count ready */
+constexpr unsigned kOffOready = kOffLready + 8 * kSlots;     /* mbarrier[kSlots]: offset ready */
+constexpr unsigned kOffLfree = kOffOready + 8 * kSlots;      /* mbarrier[kSlots]: projection done */
+constexpr unsigned kOffCdone = kOffLfree + 8 * kSlots;       /* mbarrier[kSlots]: all counts written */
+constexpr unsigned kOffOff = kOffCdone + 8 * kSlots;         /* uint64[kSlots]: tile offsets */
+constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;         /* uint32[8]: ok[kSlots], abort, end tile */
+constexpr unsigned kOffTot = kOffFlags + 32;                 /* uint32[kSlots]: tile totals */
+constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;          /* uint32[kMaxStages]: query per stage */
+constexpr unsigned kOffCnt = 512;                            /* uint32[kSlots][kMaxGroups]: per 64 rows */
 constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
 static_assert(kSlots <= kFAbort, "ok flags per slot");
-static_assert(kLookbackWarps == kSlots, "a look-back warp per slot");
-static_assert(kFEnd == 5 && kFWaitMs == 7, "flag words read by the waits");
-static_assert(kOffHeld + 4 * kMaxStages <= kOffSlotInfo, "smem header layout");
-static_assert(kOffPCount + 4 * kSlots <= kOffLbuilt, "smem header layout");
-static_assert(kOffLbuilt + 8 * kSlots <= kSmemHeader, "smem header overflow");
+static_assert(kOffHeld + 4 * kMaxStages <= kOffCnt, "smem header layout");
+static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
 static_assert(sizeof(QDesc) % 16 == 0, "QDesc copies in 16-byte chunks");
 static_assert(kStageHdr >= sizeof(QDesc) + sizeof(StageInfo), "stage header too small");
 static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a time");
@@ -92,8 +82,13 @@ static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a
 /* where the fields the compute warps read sit in a stage's descriptor copy */
 constexpr uint32_t kQOps = (uint32_t)offsetof(QDesc, ops);
 constexpr uint32_t kQNFilter = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nfilter));
+constexpr uint32_t kQNUops = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nuops));
+constexpr uint32_t kQNOut = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nout));
+constexpr uint32_t kQOutStride = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, out_stride));
+constexpr uint32_t kQOdOut = (uint32_t)offsetof(QDesc, od_out);
+constexpr uint32_t kQOutPtr = (uint32_t)offsetof(QDesc, out_ptr);
+constexpr uint32_t kQCapacity = (uint32_t)offsetof(QDesc, capacity);
 constexpr uint32_t kQVecSlot = (uint32_t)offsetof(QDesc, vec_slot);
-constexpr uint32_t kQOpEnd = (uint32_t)offsetof(QDesc, op_end);
 
 /* ---- PTX wrappers ---------------------------------------------------- */
 
@@ -235,36 +230,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const vo
 	}
 }
 
-/* a bounded wait for tile i's phase that also ends (2) once the tiles are
- * known to end before tile i; 1 when the phase completed, 0 on abort or
- * time-out */
-__device__ __forceinline__ int mbar_wait_or_end(uint32_t bar, uint32_t phase, const volatile uint32_t *flags,
-	uint32_t i)
-{
-	const uint64_t limit_ns = (uint64_t)flags[7] * 1000000ull;
-	const uint64_t t0 = globaltimer_ns();
-	for (;;) {
-		if (mbar_try_wait_hint(bar, phase, 1000u))
-			return 1;
-		if (flags[kFAbortSlot])
-			return 0;
-		if (flags[5] <= i)
-			return 2;
-		if (globaltimer_ns() - t0 > limit_ns)
-			return 0;
-	}
-}
-
-/* a wait that gave up: the first role to give up records the error and
- * stops the CTA's other roles (an abort already set is not reported again) */
-__device__ __forceinline__ void give_up(const KParams &kp, volatile uint32_t *flags, int lane)
-{
-	if (lane == 0 && !flags[kFAbortSlot]) {
-		report(kp.error, DE_STAGE_TIMEOUT);
-		flags[kFAbortSlot] = 1u;
-	}
-}
-
 /* ---- shared-memory access by 32-bit shared address ---------------------
  * Every tile, register-vector and descriptor access of the compute warps
  * goes through these, so each is one ld/st.shared.  They are volatile asm:
@@ -385,15 +350,17 @@ struct Opnd {
 	bool sel;
 };
 
-/* staged columns, scalars (the descriptor's constant table) and register
- * vectors by tile row live in the tile's stage, register vectors by
- * selection position in the tile's slot */
+/* staged columns and scalars (the descriptor's constant table) live in the
+ * tile's stage, row vectors in the tile's row-vector slot, selection
+ * vectors in their single area */
 template <int SIZE>
 __device__ __forceinline__ Opnd opnd(uint32_t od, uint32_t sbase, uint32_t sdelta, uint32_t vdelta)
 {
 	const uint32_t kind = od >> 30;
 	Opnd o;
-	o.addr = sbase + (od & OD_OFFSET) + (kind == (OD_SELVEC >> 30) ? vdelta : sdelta);
+	o.addr = sbase + (od & OD_OFFSET) +
+		((kind == (OD_STAGE >> 30) || kind == (OD_SCALAR >> 30)) ? sdelta
+			: kind == (OD_ROWVEC >> 30) ? vdelta : 0u);
 	o.step = kind == (OD_SCALAR >> 30) ? 0u : (uint32_t)SIZE;
 	o.sel = kind == (OD_SELVEC >> 30);
 	return o;
@@ -778,13 +745,9 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowS
 }
 
 /* ---- projection: the tile's selected rows, in row order ------------------
- * The projection warps run the projection ops over the tile's list while
- * the tile is still staged, writing results into the tile's slot indexed by
- * selection position (register vectors the projection writes, and a copy of
- * every other result column), and then release the stage: the stores wait
- * for the tile's offset on the slot alone.  The warps share the list: warp p
- * takes the 32-entry batches p, p + P, p + 2 P, ...; entry e is selection
- * index e and its result row lands at the tile's offset + e. */
+ * The projection warps share the tile's list: warp p takes the 32-entry
+ * batches p, p + P, p + 2 P, ...; entry e is selection index e and its
+ * result row lands at the tile's offset + e. */
 
 struct PArgs {
 	uint32_t sbase, sd, vd;
@@ -836,8 +799,7 @@ __device__ __forceinline__ void p_math_any(const uint4 &rec, const PArgs &c)
 }
 
 /* one projection op: arithmetic, or a copy (every listed row is active
- * here, so constants and columns are copies; result columns that are not
- * projection vectors are copied into the slot the same way) */
+ * here, so constants and columns are copies) */
 __device__ __forceinline__ void project_op(const uint4 &rec, const PArgs &c)
 {
 	const uint32_t h = rec.x;
@@ -854,21 +816,6 @@ __device__ __forceinline__ void project_op(const uint4 &rec, const PArgs &c)
 		else if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, c);
 		else p_copy<uint32_t>(rec, c);
 	}
-}
-
-/* one result column of the tile's entries, from the slot to the tile's
- * offset; false if a row lies beyond the buffers' capacity */
-template <typename T>
-__device__ __forceinline__ bool store_column(uint32_t src, uint32_t e0, uint32_t n, uint32_t step, T *out,
-	uint64_t off, uint64_t cap)
-{
-	for (uint32_t e = e0; e < n; e += step) {
-		const uint64_t pos = off + e;
-		if (pos >= cap)
-			return false;
-		out[pos] = SM<T>::ld(src + e * (uint32_t)sizeof(T));
-	}
-	return true;
 }
 
 /* ---- ordered placement ------------------------------------------------- */
@@ -924,13 +871,13 @@ __device__ __forceinline__ void publish_count(const KParams &kp, const QDesc &Q,
  * filtered.  Returns false if a predecessor never published (bounded wait). */
 constexpr int kLookbackPerLane = 4;
 
-__device__ bool lookback_excl(const KParams &kp, uint64_t work_first, uint64_t base, uint64_t g,
-	int64_t known, uint64_t known_end, int lane, uint64_t *excl_out)
+__device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int64_t known, uint64_t known_end,
+	int lane, uint64_t *excl_out)
 {
 	constexpr int W = 32 * kLookbackPerLane;
-	const int64_t first = (int64_t)work_first;
+	const int64_t first = (int64_t)Q.work_first;
 	if ((int64_t)g == first) {
-		*excl_out = base;
+		*excl_out = query_base(Q);
 		return true;
 	}
 	/* indices below `floor` are not read: the query's start, or the known
@@ -1037,10 +984,6 @@ struct ProdQuery {
 	const uint32_t *tile_prefix;
 	uint32_t nsegs, nload, qi, seg_hint;
 	uint32_t src, stride, off;   /* this lane's column */
-	/* the current segment: its tiles [seg_t0, seg_t1) of the query, rows,
-	 * and this lane's column in it; seg ~0 when none */
-	uint32_t seg, seg_t0, seg_t1, seg_rows;
-	const unsigned char *colp;
 };
 
 /* one decoded work item; src and bytes are this lane's column copy */
@@ -1052,8 +995,7 @@ struct ProdItem {
 
 /* decode work item w with the whole producer warp.  A CTA claims work items
  * in increasing order, so the query and segment searches start at the
- * previous item's, and an item in the previous item's segment needs no
- * load at all. */
+ * previous item's. */
 template <int TILE>
 __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint64_t total, uint32_t nq,
 	ProdQuery &pq, ProdItem &it, int lane)
@@ -1075,46 +1017,39 @@ __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint6
 		pq.nsegs = Q->nsegs;
 		pq.nload = Q->prog.nload;
 		pq.seg_hint = 0;
-		pq.seg = ~0u;
 		if (lane < kMaxLoads) {
 			pq.src = Q->prog.load_src[lane];
 			pq.stride = Q->prog.load_stride[lane];
 			pq.off = Q->load_off[lane];
 		}
 	}
-	const uint32_t t = (uint32_t)(w - pq.first);
-	if (pq.seg == ~0u || t >= pq.seg_t1) {
-		const uint32_t s = warp_search(pq.tile_prefix, pq.seg_hint, pq.nsegs, t, lane);
-		const SegDesc *sd = pq.segs + s;
-		pq.seg_hint = s;
-		pq.seg = s;
-		pq.seg_t0 = pq.tile_prefix[s];
-		pq.seg_t1 = pq.tile_prefix[s + 1];
-		pq.seg_rows = sd->rows;
-		if ((uint32_t)lane < pq.nload)
-			pq.colp = static_cast<const unsigned char *>(sd->col[pq.src]);
-	}
-	const uint32_t row0 = (t - pq.seg_t0) * TILE;
-	it.seg = pq.seg;
+	const uint64_t t = w - pq.first;
+	const uint32_t s = warp_search(pq.tile_prefix, pq.seg_hint, pq.nsegs, t, lane);
+	pq.seg_hint = s;
+	const SegDesc *sd = pq.segs + s;
+	const uint32_t row0 = (uint32_t)(t - pq.tile_prefix[s]) * TILE;
+	it.seg = s;
 	it.row0 = row0;
-	it.nrows = min((uint32_t)TILE, pq.seg_rows - row0);
+	it.nrows = min((uint32_t)TILE, sd->rows - row0);
 	if ((uint32_t)lane < pq.nload) {
-		it.src = pq.colp + (size_t)row0 * pq.stride;
+		it.src = static_cast<const unsigned char *>(sd->col[pq.src]) + (size_t)row0 * pq.stride;
 		it.bytes = (it.nrows * pq.stride + 15u) & ~15u;
 	}
 }
 
-/* The producer warp fills the ring of stages.  Once the projection warps
- * and the look-back warp released a stage it announces the decoded work
- * item and issues its copies (lane i copies column i; the query descriptor
- * only when the stage does not hold it already), then takes the next claim
- * (in order, with the one after it already in flight) and decodes it while
- * those copies run.  Claiming a couple of items ahead, not a whole ring
- * ahead, keeps claimed tiles from idling while other CTAs' look-backs wait
- * for their counts.  An invalid claim (past the end of the work list) is
- * announced without data and ends the CTA's pipeline.  In a serving session
- * the work list grows: a claim past the published work waits (bounded) for
- * the host's doorbell or its stop request. */
+/* The producer warp fills the ring of stages.  Once the compute warps
+ * released a stage it announces the decoded work item and issues its copies
+ * (lane i copies column i; the query descriptor only when the stage does
+ * not hold it already), then claims (kClaim per atomic, in order) and
+ * decodes the next item while those copies run.  Claiming one item ahead,
+ * not a whole ring ahead, keeps claimed tiles from idling while other CTAs'
+ * look-backs wait for their counts.  An invalid claim (past the end of the
+ * work list) is announced without data and ends the CTA's pipeline.
+ *
+ * In a serving session the work list grows: a claim past the published
+ * work waits for the host's doorbell (or its stop request), and each
+ * released stage counts its tile as stored; the tile that completes a
+ * query writes the query's completion record. */
 template <int TILE>
 __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 {
@@ -1126,46 +1061,77 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	 * in a serving session, whose kp.total_work only marks the end item */
 	uint64_t total = serving ? 0ull : kp.total_work;
 	uint32_t nq = serving ? 0u : kp.nq;
+	uint32_t pend = 0;  /* serving: stages whose tile is issued but not yet counted */
 	ProdQuery pq;
 	pq.Q = nullptr;
 	pq.qi = 0;
-	/* claims: one atomic in flight (lane 0) while the previous claim's item
-	 * is decoded and issued, so its round trip is off the per-tile path */
-	uint32_t inflight = 0;
-	bool have = false;
+	uint32_t next = 0, left = 0;
 	auto claim = [&]() -> uint32_t {
-		uint32_t v = 0;
-		if (lane == 0) {
-			if (!have) {
-				inflight = atomicAdd(kp.counter, 1u);
-				have = true;
-			}
-			v = inflight;
-			inflight = atomicAdd(kp.counter, 1u);
+		if (left == 0) {
+			uint32_t v = 0;
+			if (lane == 0)
+				v = atomicAdd(kp.counter, kClaim);
+			next = __shfl_sync(0xffffffffu, v, 0);
+			left = kClaim;
 		}
-		return __shfl_sync(0xffffffffu, v, 0);
+		left--;
+		return next++;
 	};
-	/* the next work item; ~0 ends the pipeline */
-	auto next_item = [&]() -> uint32_t {
+	/* serving: the tile of stage s is stored; the query's last one reports */
+	auto count_stored = [&](uint32_t s) {
+		const uint32_t qi = held[s];
+		__threadfence();
+		const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
+		const QDesc *Q = kp.queries + qi;
+		if (done == (unsigned)Q->ntiles) {
+			__threadfence();
+			const unsigned long long rows = *reinterpret_cast<volatile unsigned long long *>(Q->total_out);
+			volatile ServeRec *r = kp.recs + qi;
+			r->rows = rows;
+			__threadfence_system();
+			r->seq = (unsigned long long)qi + 1ull;
+		}
+	};
+	/* serving: wait for the tiles issued in iterations lo..hi to be stored
+	 * and count them (lane 0) */
+	auto drain = [&](uint32_t lo, uint32_t hi) {
+		for (uint32_t kk = lo; kk <= hi; kk++) {
+			const uint32_t s = kk % nst;
+			if ((pend >> s) & 1u) {
+				if (!mbar_wait(smem_addr(smem + kOffEmpty + 8 * s), (kk / nst) & 1u, abort))
+					return false;
+				count_stored(s);
+				pend &= ~(1u << s);
+			}
+		}
+		return true;
+	};
+	/* the next work item: in a serving session a claim past the published
+	 * work waits (bounded) for the doorbell; ~0 ends the pipeline */
+	auto next_item = [&](uint32_t issued_k) -> uint32_t {
 		const uint32_t w = claim();
 		if (!serving || w < total)
 			return w;
 		uint64_t t0 = 0;
+		int ok = 1;
 		unsigned nap = 1000;  /* ns between doorbell polls, growing while idle */
 		for (;;) {
 			unsigned long long a = 0;
 			unsigned stop = 0;
 			if (lane == 0) {
+				if (issued_k != ~0u && pend)
+					ok = drain(issued_k + 1 > nst ? issued_k + 1 - nst : 0u, issued_k) ? 1 : 0;
 				a = ld_acquire_sys(&kp.serve->avail);
 				stop = *reinterpret_cast<const volatile unsigned *>(&kp.serve->stop);
 			}
+			ok = __shfl_sync(0xffffffffu, ok, 0);
 			a = __shfl_sync(0xffffffffu, a, 0);
 			stop = __shfl_sync(0xffffffffu, stop, 0);
 			total = a & kAvailWorkMask;
 			nq = (uint32_t)(a >> 40);
 			if (w < total)
 				return w;
-			if (stop)
+			if (stop || !ok)
 				return ~0u;
 			if (t0 == 0)
 				t0 = globaltimer_ns();
@@ -1181,7 +1147,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	ProdItem it;
 	{
 		/* claim first: next_item updates total and nq */
-		const uint32_t w = next_item();
+		const uint32_t w = next_item(~0u);
 		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
 	}
 	uint32_t k = 0;
@@ -1195,6 +1161,10 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 				ok = mbar_wait(empty, (j - 1) & 1u, abort);
 				if (!ok && !*abort)
 					report(kp.error, DE_STAGE_TIMEOUT);
+				if (ok && serving && ((pend >> s) & 1u)) {
+					count_stored(s);
+					pend &= ~(1u << s);
+				}
 			}
 			if (!__shfl_sync(0xffffffffu, ok, 0))
 				break;
@@ -1217,6 +1187,9 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 			*reinterpret_cast<StageInfo *>(hdr + sizeof(QDesc)) = si;
 		}
 		if (end) {
+			/* serving: every issued tile is counted before the CTA ends */
+			if (serving && lane == 0 && k > 0)
+				drain(k > nst ? k - nst : 0u, k - 1);
 			__syncwarp();
 			if (lane == 0)
 				mbar_arrive(full);
@@ -1228,16 +1201,18 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		__syncwarp();
 		if (lane == 0) {
 			held[s] = pq.qi;
+			pend |= 1u << s;
 			fence_proxy_async_smem();
 			mbar_arrive_expect_tx(full, bytes);
 		}
+		pend = __shfl_sync(0xffffffffu, pend, 0);
 		__syncwarp();
 		const uint32_t base = smem_addr(hdr);
 		if (it.bytes)
 			bulk_load(base + pq.off, it.src, it.bytes, full);
 		if (copy_desc && lane == 31)
 			bulk_load(base, pq.Q, (uint32_t)sizeof(QDesc), full);
-		const uint32_t w = next_item();
+		const uint32_t w = next_item(k);
 		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
 	}
 	/* abandoned: wait (bounded) for the copies already issued so none lands
@@ -1251,83 +1226,55 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 
 /* ---- look-back warp: tile totals -> result offsets ----------------------- */
 
-/* Look-back warps: kLookbackWarps of them, warp k taking the tiles
- * k, k + kLookbackWarps, ... of the CTA.  A launch has as many stages as
- * slots and look-back warps, so warp k owns stage k and slot k and meets
- * their barriers' phases in order; the walks over earlier tiles of several
- * tiles run at the same time. */
 template <int THREADS, int R>
-__device__ void lookback_warp(const KParams &kp, unsigned char *smem, int k, int lane)
+__device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 {
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
+	const volatile uint32_t *tot = reinterpret_cast<const volatile uint32_t *>(smem + kOffTot);
 	uint64_t *offs = reinterpret_cast<uint64_t *>(smem + kOffOff);
 	const uint32_t nst = kp.nstages;
-	/* this warp's previous tile: a later tile of the same query can stop its
-	 * walk there, and a tile that directly follows it starts where it
-	 * ended, with no look-back */
+	/* the previous tile of this CTA: a tile that directly follows it in the
+	 * same query starts where it ended, with no look-back */
 	uint64_t prev_work = ~0ull, prev_end = 0;
-	for (uint32_t i = (uint32_t)k;; i += kLookbackWarps) {
+	for (uint32_t i = 0;; i++) {
 		const uint32_t s = i % nst, q = i % kSlots;
-		/* the tile's data has landed (its work item is known), or the tiles
-		 * ended before it */
-		const int got = mbar_wait_or_end(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags, i);
-		if (got == 2)
+		/* the tile's data has landed: its work item is known, so the walk
+		 * over earlier tiles starts while the filter warps run */
+		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort))
 			return;
-		if (got == 0) {
-			give_up(kp, flags, lane);
-			return;
-		}
+		/* the stage holds tile i until the tile's stores, which wait for
+		 * this warp */
 		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
 		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-		const volatile StageInfo &si = *reinterpret_cast<const volatile StageInfo *>(hdr + sizeof(QDesc));
-		const uint32_t work = si.work;
-		if (work >= kp.total_work)
+		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+		if (si.work >= kp.total_work)
 			return;
-		const uint64_t first = Q.work_first, last = Q.work_first + Q.ntiles - 1;
-		unsigned long long *const total_out = Q.total_out;
-		const uint64_t base = query_base(Q);
-		/* the tile's own count, left in the stage by the filter; then the
-		 * stage is released as far as this warp goes, before the walk over
-		 * other CTAs' tiles */
-		if (!mbar_wait(smem_addr(smem + kOffSready + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
-			give_up(kp, flags, lane);
-			return;
-		}
-		const uint32_t count = si.total;
-		__syncwarp();
-		if (lane == 0)
-			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
 		uint64_t excl = 0;
 		bool ok = true;
-		const bool follows = work == prev_work + 1 && work != first;
+		const bool follows = si.work == prev_work + 1 && si.work != Q.work_first;
 		if (follows)
 			excl = prev_end;
 		else
-			ok = lookback_excl(kp, first, base, work, prev_work == ~0ull ? -1 : (int64_t)prev_work, prev_end,
-				lane, &excl);
-		const uint32_t tile_total = ok ? count : 0u;
-		prev_work = work;
+			ok = lookback_excl(kp, Q, si.work, prev_work == ~0ull ? -1 : (int64_t)prev_work, prev_end, lane, &excl);
+		/* the tile's own count */
+		if (ok && !mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
+			return;
+		const uint32_t tile_total = ok ? tot[q] : 0u;
+		prev_work = si.work;
 		prev_end = excl + tile_total;
+		__syncwarp();
 		if (lane == 0) {
 			if (!ok) {
 				report(kp.error, DE_LOOKBACK_TIMEOUT);
 			} else {
 				/* the inclusive prefix (a query's first tile published its own) */
-				if (work != first)
-					st_status(status_at(kp, work),
-						(status_tag(kp, work) << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
+				if (si.work != Q.work_first)
+					st_status(status_at(kp, si.work),
+						(status_tag(kp, si.work) << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
 						((excl + tile_total) & kStatusValueMask));
-				if (work == last)
-					*total_out = excl + tile_total;
+				if (si.work == Q.work_first + Q.ntiles - 1)
+					*Q.total_out = excl + tile_total;
 			}
-		}
-		/* the slot's offset: free once the tile's projection is done, which
-		 * waited for the stores of the slot's previous tile */
-		if (!mbar_wait(smem_addr(smem + kOffCready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
-			give_up(kp, flags, lane);
-			return;
-		}
-		if (lane == 0) {
 			offs[q] = excl;
 			flags[q] = ok ? 1u : 0u;
 			if (!ok)
@@ -1339,235 +1286,105 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int k, int
 	}
 }
 
-/* projection warps: kSlots teams of PT warps, team t taking the tiles t,
- * t + kSlots, ... (it owns stage t and slot t and meets their barriers'
- * phases in order), so the projections of different tiles run at the same
- * time.  A team builds the tile's list of selected rows from the filter's
- * ballots, runs the projection ops over it into the tile's slot, then gives
- * the stage back to the producer. */
+/* ---- projection warps: projection and ordered stores of each tile -------- */
+
 template <int THREADS, int R, int P>
-__device__ void proj_warps(const KParams &kp, unsigned char *smem, int team, int pw, int lane)
+__device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int lane)
 {
 	constexpr int TILE = THREADS * R;
-	constexpr int NW = THREADS / 32;
-	constexpr int C = R / 4;
-	constexpr int G = 2 * C * NW;          /* 64-row groups per tile */
-	constexpr int PER = (G + 31) / 32;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
 	const uint32_t sbase = smem_addr(smem);
 	const uint32_t nst = kp.nstages;
-	for (uint32_t i = (uint32_t)team;; i += kSlots) {
+	for (uint32_t i = 0;; i++) {
 		const uint32_t s = i % nst, q = i % kSlots;
-		/* the filter is done with the tile, or the tiles ended before it */
-		const int got = mbar_wait_or_end(smem_addr(smem + kOffFready + 8 * s), (i / nst) & 1u, flags, i);
-		/* the end of the tiles (no arrival: the slot's store warp and
-		 * look-back warp see the end themselves) */
-		if (got == 2 || (got == 1 && flags[kFEnd] == i))
-			return;
-		/* the slot is free once the stores of its previous tile are done */
-		const bool ok = got == 1 && (i < kSlots ||
-			mbar_wait(smem_addr(smem + kOffLfree + 8 * q), ((i - kSlots) / kSlots) & 1u, flags + kFAbort));
-		if (!ok) {
-			give_up(kp, flags, lane);
+		if (!mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
+			if (lane == 0 && !flags[kFAbort]) {
+				report(kp.error, DE_STAGE_TIMEOUT);
+				flags[kFAbort] = 1u;
+			}
 			return;
 		}
+		if (flags[kFEnd] == i)
+			return;
 		const uint32_t sd = s * kp.stage_bytes;
 		const uint32_t qd = sbase + kp.stage_area + sd;
-		const uint32_t sinfo = qd + (uint32_t)sizeof(QDesc);
-		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
-
-		/* ---- the list: every warp scans the group counts ((chunk, warp,
-		 * half) is row order); warp p of the team writes the rows of chunks
-		 * p, p + P, ... */
-		const uint32_t cnt = qd + kStageCnt;
-		uint32_t lane_pre[PER];
-		uint32_t sum = 0;
-#pragma unroll
-		for (int x = 0; x < PER; x++) {
-			const int g = lane * PER + x;
-			lane_pre[x] = sum;
-			sum += g < G ? lds_u32(cnt + 4 * g) : 0u;
-		}
-		uint32_t incl = sum;
-#pragma unroll
-		for (int d = 1; d < 32; d <<= 1) {
-			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
-			if (lane >= d)
-				incl += v;
-		}
-		const uint32_t ex = incl - sum;
-		const uint32_t lt = (1u << lane) - 1u;
-		for (int ch = pw; ch < C * NW; ch += P) {
-			const uint32_t g = 2u * (uint32_t)ch;
-			uint32_t v = 0;
-#pragma unroll
-			for (int x = 0; x < PER; x++)
-				if ((uint32_t)x == g % PER)
-					v = ex + lane_pre[x];
-			const uint32_t base = __shfl_sync(0xffffffffu, v, (int)(g / PER));
-			const uint4 b = lds_v4(qd + kStageMasks + 16u * (uint32_t)ch);
-			const uint32_t m = ((b.x >> lane) & 1u) | (((b.y >> lane) & 1u) << 1) | (((b.z >> lane) & 1u) << 2) |
-				(((b.w >> lane) & 1u) << 3);
-			if (m) {
-				uint32_t at = base + __popc(b.x & lt) + __popc(b.y & lt) + __popc(b.z & lt) + __popc(b.w & lt);
-				/* chunk c of filter warp w: tile rows c * 4 * THREADS + 128 w + 4 lane + k */
-				const uint32_t row0 = (uint32_t)(ch / NW) * 4u * THREADS + 128u * (uint32_t)(ch % NW) + 4u * lane;
-#pragma unroll
-				for (int k = 0; k < 4; k++)
-					if ((m >> k) & 1u)
-						sts_u16(list + 2 * at++, row0 + k);
-			}
-		}
-		/* every warp of the team reads entries the others wrote (a bounded
-		 * rendezvous of the team) */
-		if (P > 1) {
-			__syncwarp();
-			if (lane == 0)
-				mbar_arrive(smem_addr(smem + kOffLbuilt + 8 * q));
-			if (!mbar_wait(smem_addr(smem + kOffLbuilt + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
-				give_up(kp, flags, lane);
-				return;
-			}
-		}
-		__syncwarp();
-
 		PArgs c;
 		c.sbase = sbase;
 		c.sd = sd;
 		c.vd = q * lds_u32(qd + kQVecSlot);
-		c.list = list;
-		c.n = lds_u32(sinfo + offsetof(StageInfo, total));
+		c.list = sbase + kp.sel_area + q * TILE * 2;
+		c.n = lds_u32(sbase + kOffTot + 4 * q);
 		c.e0 = 32u * (uint32_t)pw + (uint32_t)lane;
 		c.step = 32u * P;
 		const uint32_t ops = qd + kQOps;
 		if (c.e0 - (uint32_t)lane < c.n) {
-			const uint32_t end = lds_u32(qd + kQOpEnd);
-			for (uint32_t k = lds_u32(qd + kQNFilter); k < end; k++)
+			const uint32_t nu = lds_u32(qd + kQNUops) - 1u;
+			for (uint32_t k = lds_u32(qd + kQNFilter); k < nu; k++)
 				project_op(lds_v4(ops + 16u * k), c);
 		}
-		if (pw == 0 && lane == 0) {
-			/* what the store warps need, after the stage is released */
-			sts_u32(sbase + kOffTot + 4 * q, c.n);
-			sts_u32(sbase + kOffSlotInfo + 16 * q, lds_u32(sinfo + offsetof(StageInfo, query)));
-			sts_u32(sbase + kOffSlotInfo + 16 * q + 4, lds_u32(sinfo + offsetof(StageInfo, seg)));
-			sts_u32(sbase + kOffSlotInfo + 16 * q + 8, lds_u32(sinfo + offsetof(StageInfo, row0)));
-		}
-		__syncwarp();
-		if (lane == 0) {
-			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
-			mbar_arrive(smem_addr(smem + kOffCready + 8 * q));
-		}
-	}
-}
 
-/* store warps: one per slot.  Once the tile's projection is done and the
- * look-back resolved its offset, its result columns go from the slot to
- * device memory at offset + entry (coalesced), and the slot is released */
-template <int THREADS, int R, int S>
-__device__ void store_warps(const KParams &kp, unsigned char *smem, int sw, int lane)
-{
-	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	const uint32_t sbase = smem_addr(smem);
-	/* store warp q owns slot q: the tiles q, q + kSlots, ... */
-	for (uint32_t i = (uint32_t)sw;; i += kSlots) {
-		const uint32_t q = i % kSlots;
-		const int got = mbar_wait_or_end(smem_addr(smem + kOffCready + 8 * q), (i / kSlots) & 1u, flags, i);
-		if (got == 2)
+		/* ---- stores at the tile's offset, once the look-back resolved it */
+		if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
 			return;
-		if (got == 0) {
-			give_up(kp, flags, lane);
-			return;
-		}
-		if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
-			give_up(kp, flags, lane);
-			return;
-		}
 		if (!flags[q])
 			return;
 		const uint64_t off = lds_u64(sbase + kOffOff + 8 * q);
-		const uint32_t n = lds_u32(sbase + kOffTot + 4 * q);
-		const uint32_t qi = lds_u32(sbase + kOffSlotInfo + 16 * q);
-		/* the stage is gone: the result columns' fields come from the
-		 * descriptor in device memory (plain loads, not the read-only path:
-		 * a serving session's host writes descriptors while the kernel
-		 * runs) */
-		const QDesc *gq = kp.queries + qi;
-		const uint32_t e0 = (uint32_t)lane;
-		if (n) {
-			const uint32_t vd = q * gq->vec_slot;
-			const uint64_t cap = gq->capacity;
-			const uint32_t nout = gq->prog.nout;
-			bool ok = true;
+		if (c.e0 - (uint32_t)lane < c.n) {
+			const uint64_t cap = lds_u64(qd + kQCapacity);
+			bool overflow = false;
+			const uint32_t nout = lds_u32(qd + kQNOut);
 			for (uint32_t j = 0; j < nout; j++) {
-				const uint32_t src = sbase + (gq->od_out[j] & OD_OFFSET) + vd;
-				void *out = gq->out_ptr[j];
-				const uint32_t stride = gq->prog.out_stride[j];
-				if (stride == 4)
-					ok &= store_column<uint32_t>(src, e0, n, 32u, static_cast<uint32_t *>(out), off, cap);
-				else if (stride == 8)
-					ok &= store_column<unsigned long long>(src, e0, n, 32u,
-						static_cast<unsigned long long *>(out), off, cap);
-				else
-					ok &= store_column<unsigned char>(src, e0, n, 32u, static_cast<unsigned char *>(out),
-						off, cap);
+				const uint32_t od = lds_u32(qd + kQOdOut + 4 * j);
+				unsigned char *out = reinterpret_cast<unsigned char *>(lds_u64(qd + kQOutPtr + 8 * j));
+				const uint32_t stride = lds_u8(qd + kQOutStride + j);
+				const Opnd a = stride == 8 ? opnd<8>(od, sbase, sd, c.vd)
+					: stride == 4 ? opnd<4>(od, sbase, sd, c.vd) : opnd<1>(od, sbase, sd, c.vd);
+				for (uint32_t e = c.e0; e < c.n; e += c.step) {
+					const uint64_t pos = off + e;
+					if (pos >= cap) {
+						overflow = true;
+						break;
+					}
+					const uint32_t at = p_addr(a, lds_u16(c.list + 2 * e), e);
+					if (stride == 4)
+						reinterpret_cast<uint32_t *>(out)[pos] = lds_u32(at);
+					else if (stride == 8)
+						reinterpret_cast<unsigned long long *>(out)[pos] = lds_u64(at);
+					else
+						out[pos] = (unsigned char)lds_u8(at);
+				}
 			}
 			/* a serving session reports rows beyond capacity in the
 			 * query's completion record instead */
-			if (!ok && kp.serve == nullptr)
+			if (overflow && kp.serve == nullptr)
 				report(kp.error, DE_OUTPUT_OVERFLOW);
 		}
 		__syncwarp();
 		if (lane == 0) {
-			if (kp.serve != nullptr) {
-				/* serving: the tile is stored; the query's last tile writes
-				 * its completion record */
-				__threadfence();
-				const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
-				if (done == (unsigned)gq->ntiles) {
-					__threadfence();
-					const unsigned long long rows =
-						*reinterpret_cast<volatile unsigned long long *>(gq->total_out);
-					volatile ServeRec *r = kp.recs + qi;
-					r->rows = rows;
-					__threadfence_system();
-					r->seq = (unsigned long long)qi + 1ull;
-				}
-			}
+			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
 			mbar_arrive(smem_addr(smem + kOffLfree + 8 * q));
 		}
 	}
 }
 
-/* projection warps per team: two with 256 filter threads, else one (a
- * block of 512 filter threads and kSlots two-warp teams would pass 1024
- * threads); kSlots teams.  Store warps: one per slot. */
-template <int THREADS>
-struct TeamWarps {
-	static constexpr int value = THREADS == 256 ? 2 : 1;
-};
+/* projection warps per CTA: half the filter warps, 1 to 4 */
 template <int THREADS>
 struct ProjWarps {
-	static constexpr int value = (int)kSlots * TeamWarps<THREADS>::value;
-};
-template <int THREADS>
-struct StoreWarps {
-	static constexpr int value = (int)kSlots;
+	static constexpr int value = THREADS / 64 < 1 ? 1 : THREADS / 64 > 4 ? 4 : THREADS / 64;
 };
 
 template <int THREADS, int R>
-__global__ void __launch_bounds__(THREADS + 32 * (1 + kLookbackWarps + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), 1)
-vm_kernel(const KParams kp)
+__global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)) vm_kernel(const KParams kp)
 {
+	constexpr int TILE = THREADS * R;
 	constexpr int NW = THREADS / 32;
 	constexpr int C = R / 4;
 	constexpr int P = ProjWarps<THREADS>::value;
-	constexpr int S = StoreWarps<THREADS>::value;
 	constexpr int G = 2 * C * NW;          /* 64-row groups per tile */
 	constexpr int PER = (G + 31) / 32;
 	static_assert(R % 4 == 0 && R <= 32, "rows per thread: whole 4-row chunks, 32-bit row masks");
 	static_assert(G <= (int)kMaxGroups, "64-row groups per tile");
-	static_assert(THREADS * R <= 65536, "tile rows are 16-bit in the selection lists");
-	static_assert(THREADS + 32 * (1 + kLookbackWarps + P + S) <= 1024, "threads per block");
+	static_assert(TILE <= 65536, "tile rows are 16-bit in the selection lists");
 	extern __shared__ __align__(128) unsigned char smem[];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
@@ -1576,23 +1393,16 @@ vm_kernel(const KParams kp)
 	if (tid == 0) {
 		for (uint32_t s = 0; s < nst; s++) {
 			mbar_init(smem_addr(smem + kOffFull + 8 * s), 1);
-			/* a stage is free once its projection team and look-back warp
-			 * are done with it */
-			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), TeamWarps<THREADS>::value + 1);
-			mbar_init(smem_addr(smem + kOffCdone + 8 * s), NW);
-			mbar_init(smem_addr(smem + kOffFready + 8 * s), 1);
-			mbar_init(smem_addr(smem + kOffSready + 8 * s), 1);
+			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), P);
 		}
 		for (uint32_t q = 0; q < kSlots; q++) {
-			mbar_init(smem_addr(smem + kOffLfree + 8 * q), 1);
-			mbar_init(smem_addr(smem + kOffCready + 8 * q), TeamWarps<THREADS>::value);
+			mbar_init(smem_addr(smem + kOffLready + 8 * q), NW);
 			mbar_init(smem_addr(smem + kOffOready + 8 * q), 1);
-			mbar_init(smem_addr(smem + kOffLbuilt + 8 * q), TeamWarps<THREADS>::value);
+			mbar_init(smem_addr(smem + kOffLfree + 8 * q), P);
+			mbar_init(smem_addr(smem + kOffCdone + 8 * q), NW);
 		}
 		for (int x = 0; x < 8; x++)
 			flags[x] = 0;
-		for (uint32_t q = 0; q < kSlots; q++)
-			reinterpret_cast<uint32_t *>(smem + kOffPCount)[q] = 0;
 		flags[kFEnd] = ~0u;
 		flags[kFWaitMs] = kp.wait_limit_ms;
 		for (uint32_t s = 0; s < kMaxStages; s++)
@@ -1601,30 +1411,28 @@ vm_kernel(const KParams kp)
 	}
 	__syncthreads();
 	if (warp == NW) {
-		producer<THREADS * R>(kp, smem, lane);
+		producer<TILE>(kp, smem, lane);
 		return;
 	}
-	constexpr int LB = NW + 1, PW = LB + (int)kLookbackWarps, SW = PW + P;
-	if (warp >= SW) {
-		store_warps<THREADS, R, S>(kp, smem, warp - SW, lane);
+	if (warp == NW + 1) {
+		lookback_warp<THREADS, R>(kp, smem, lane);
 		return;
 	}
-	if (warp >= PW) {
-		constexpr int T = TeamWarps<THREADS>::value;
-		proj_warps<THREADS, R, T>(kp, smem, (warp - PW) / T, (warp - PW) % T, lane);
-		return;
-	}
-	if (warp >= LB) {
-		lookback_warp<THREADS, R>(kp, smem, warp - LB, lane);
+	if (warp >= NW + 2) {
+		proj_warps<THREADS, R, P>(kp, smem, warp - (NW + 2), lane);
 		return;
 	}
 
-	/* filter warps: they wait for data only, so a tile's count is
-	 * published as soon as its columns have landed */
+	/* filter warps */
 	const uint32_t sbase = smem_addr(smem);
 	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst;
-		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
+		const uint32_t s = i % nst, q = i % kSlots;
+		/* the list and row-vector slot q are free once the projection of
+		 * tile i - kSlots is done */
+		bool ok = i < kSlots ||
+			mbar_wait(smem_addr(smem + kOffLfree + 8 * q), ((i - kSlots) / kSlots) & 1u, flags + kFAbort);
+		ok = ok && mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort);
+		if (!ok) {
 			if (lane == 0 && !flags[kFAbort]) {
 				report(kp.error, DE_STAGE_TIMEOUT);
 				flags[kFAbort] = 1u;
@@ -1635,15 +1443,16 @@ vm_kernel(const KParams kp)
 		const uint32_t qd = sbase + kp.stage_area + sd;
 		const uint32_t sinfo = qd + (uint32_t)sizeof(QDesc);
 		if (lds_u32(sinfo + offsetof(StageInfo, work)) >= kp.total_work) {
-			/* no more tiles: tell the projection warps (and through them the
-			 * store warps) */
-			if (warp == 0 && lane == 0) {
+			/* no more tiles: tell the look-back and projection warps */
+			__syncwarp();
+			if (lane == 0) {
 				flags[kFEnd] = i;
-				mbar_arrive(smem_addr(smem + kOffFready + 8 * s));
+				mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
 			}
 			return;
 		}
 		const uint32_t nrows = lds_u32(sinfo + offsetof(StageInfo, nrows));
+		const uint32_t vd = q * lds_u32(qd + kQVecSlot);
 
 		/* ---- filter over every row */
 		RowState st;
@@ -1661,7 +1470,7 @@ vm_kernel(const KParams kp)
 		{
 			const uint32_t ops = qd + kQOps;
 			const uint32_t nf = lds_u32(qd + kQNFilter);
-			const FArgs f{sbase, sd, 0u, tid};
+			const FArgs f{sbase, sd, vd, tid};
 			uint4 rec = lds_v4(ops);
 			for (uint32_t k = 0; k < nf; k++) {
 				const uint4 cur = rec;
@@ -1671,9 +1480,11 @@ vm_kernel(const KParams kp)
 			}
 		}
 
-		/* ---- four bit-plane ballots per 128-row chunk of the warp (row k of
-		 * each lane's 4) and the valid rows per 64 rows, into the stage */
-		const uint32_t cnt = qd + kStageCnt;
+		/* ---- counts per 64 rows, from four bit-plane ballots per 128-row
+		 * chunk of the warp (row k of each lane's 4) */
+		const uint32_t cnt = sbase + kOffCnt + q * kMaxGroups * 4;
+		const uint32_t lt = (1u << lane) - 1u;
+		uint32_t rank[C], total[C];
 #pragma unroll
 		for (int c = 0; c < C; c++) {
 			const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
@@ -1681,58 +1492,91 @@ vm_kernel(const KParams kp)
 			const uint32_t b1 = __ballot_sync(0xffffffffu, m & 2u);
 			const uint32_t b2 = __ballot_sync(0xffffffffu, m & 4u);
 			const uint32_t b3 = __ballot_sync(0xffffffffu, m & 8u);
+			total[c] = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+			rank[c] = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
 			if (lane == 0) {
 				/* lanes 0-15 hold the chunk's first 64 rows */
-				const uint32_t total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
 				const uint32_t h0 = __popc(b0 & 0xffffu) + __popc(b1 & 0xffffu) + __popc(b2 & 0xffffu) +
 					__popc(b3 & 0xffffu);
-				sts_v4(qd + kStageMasks + 16u * (uint32_t)(c * NW + warp), make_uint4(b0, b1, b2, b3));
 				sts_u32(cnt + 8 * (c * NW + warp), h0);
-				sts_u32(cnt + 8 * (c * NW + warp) + 4, total - h0);
+				sts_u32(cnt + 8 * (c * NW + warp) + 4, total[c] - h0);
 			}
 		}
 		__syncwarp();
 		if (lane == 0)
-			mbar_arrive(smem_addr(smem + kOffCdone + 8 * s));
-		if (warp != 0)
-			continue;
-
-		/* ---- warp 0: the tile's count, to the look-back words and the
-		 * other roles */
-		if (!mbar_wait(smem_addr(smem + kOffCdone + 8 * s), (i / nst) & 1u, flags + kFAbort)) {
+			mbar_arrive(smem_addr(smem + kOffCdone + 8 * q));
+		if (!mbar_wait(smem_addr(smem + kOffCdone + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
 			if (lane == 0 && !flags[kFAbort]) {
 				report(kp.error, DE_STAGE_TIMEOUT);
 				flags[kFAbort] = 1u;
 			}
 			return;
 		}
+
+		/* ---- every warp scans the tile's counts: (chunk, warp, half) is row
+		 * order, so a chunk's rows start at the sum of the counts before it */
+		uint32_t loc[PER], lane_pre[PER];
 		uint32_t sum = 0;
 #pragma unroll
 		for (int x = 0; x < PER; x++) {
 			const int g = lane * PER + x;
-			sum += g < G ? lds_u32(cnt + 4 * g) : 0u;
+			loc[x] = g < G ? lds_u32(cnt + 4 * g) : 0u;
+			lane_pre[x] = sum;
+			sum += loc[x];
 		}
-		const uint32_t tile_total = __reduce_add_sync(0xffffffffu, sum);
-		const unsigned char *hdr = smem + kp.stage_area + sd;
-		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-		if (lane == 0) {
-			publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
-			sts_u32(sinfo + offsetof(StageInfo, total), tile_total);
+		uint32_t incl = sum;
+#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+			if (lane >= d)
+				incl += v;
 		}
-		/* valid rows per 64-row block, for result-tablet splitting on the
-		 * host: group g covers tile rows 64 g .. 64 g + 63 */
-		if (Q.block_counts != nullptr) {
-			const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-			for (int g = lane; g < G; g += 32)
-				if (64u * (uint32_t)g < si.nrows)
-					Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
-						(uint8_t)lds_u32(cnt + 4 * g);
+		const uint32_t ex = incl - sum;
+		const uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
+
+		/* ---- the tile-ordered list of selected rows */
+		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
+#pragma unroll
+		for (int c = 0; c < C; c++) {
+			const uint32_t g = 2u * (uint32_t)(c * NW + warp);
+			uint32_t v = 0;
+#pragma unroll
+			for (int x = 0; x < PER; x++)
+				if ((uint32_t)x == g % PER)
+					v = ex + lane_pre[x];
+			const uint32_t base = __shfl_sync(0xffffffffu, v, (int)(g / PER));
+			if (total[c]) {
+				const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
+				uint32_t at = base + rank[c];
+				const uint32_t row0 = chunk_row<THREADS>(c, tid);
+#pragma unroll
+				for (int k = 0; k < 4; k++)
+					if ((m >> k) & 1u)
+						sts_u16(list + 2 * at++, row0 + k);
+			}
+		}
+
+		/* ---- the tile's count: to the look-back words and the other roles */
+		if (warp == 0) {
+			const unsigned char *hdr = smem + kp.stage_area + sd;
+			const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
+			if (lane == 0) {
+				publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
+				sts_u32(sbase + kOffTot + 4 * q, tile_total);
+			}
+			/* valid rows per 64-row block, for result-tablet splitting on the
+			 * host: group g covers tile rows 64 g .. 64 g + 63 */
+			if (Q.block_counts != nullptr) {
+				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+				for (int g = lane; g < G; g += 32)
+					if (64u * (uint32_t)g < si.nrows)
+						Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
+							(uint8_t)lds_u32(cnt + 4 * g);
+			}
 		}
 		__syncwarp();
-		if (lane == 0) {
-			mbar_arrive(smem_addr(smem + kOffSready + 8 * s));
-			mbar_arrive(smem_addr(smem + kOffFready + 8 * s));
-		}
+		if (lane == 0)
+			mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
 	}
 }
 
@@ -1744,8 +1588,8 @@ static int launch_t(const KParams &kp, unsigned grid, size_t smem, cudaStream_t 
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	/* THREADS filter threads, the producer and look-back warps, the projection and store warps */
-	fn<<<grid, THREADS + 32 * (1 + kLookbackWarps + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem, stream>>>(kp);
+	/* THREADS filter threads, the producer and look-back warps and the projection warps */
+	fn<<<grid, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem, stream>>>(kp);
 	return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1755,10 +1599,10 @@ static int occ_t(size_t smem, int *ctas)
 	auto fn = vm_kernel<THREADS, R>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (1 + kLookbackWarps + ProjWarps<THREADS>::value + StoreWarps<THREADS>::value), smem) == cudaSuccess;
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem) == cudaSuccess;
 }
 
-#define VGPU_SHAPES(X) X(128, 4) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
+#define VGPU_SHAPES(X) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
 
 int shape_supported(const Shape &s)
 {
@@ -1770,9 +1614,6 @@ int shape_supported(const Shape &s)
 
 int launch_vm(const Shape &s, const KParams &kp, unsigned grid, size_t smem, void *stream)
 {
-	/* a look-back warp per stage and slot */
-	if (kp.nstages != kLookbackWarps)
-		return 0;
 #define X(T, R) \
 	if (s.threads == T && s.rows_per_thread == R) return launch_t<T, R>(kp, grid, smem, (cudaStream_t)stream);
 	VGPU_SHAPES(X)
