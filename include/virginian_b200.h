@@ -456,7 +456,9 @@ int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_gpu_table *
 	uint64_t estimated_rows, uint64_t *ticket);
 /* a query's state; wait_ms < 0 waits for completion, > 0 up to that long */
 int virg_serve_poll(virg_serve *s, uint64_t ticket, int wait_ms, virg_serve_status *st);
-/* copy a completed query's rows to host buffers, one per result column */
+/* copy a completed query's rows to host buffers, one per result column;
+ * submissions go on meanwhile (the copy runs outside the loop's lock), so a
+ * ticket must not be released while it is being downloaded */
 int virg_serve_download(virg_serve *s, uint64_t ticket, void *const *host_cols);
 /* device pointer of result column c of a completed query */
 const void *virg_serve_column(virg_serve *s, uint64_t ticket, unsigned c);

@@ -642,15 +642,27 @@ extern "C" int virg_serve_poll(virg_serve *s, uint64_t ticket, int wait_ms, virg
 extern "C" int virg_serve_download(virg_serve *s, uint64_t ticket, void *const *host_cols)
 {
 	VGPU_CHECK(s != nullptr && host_cols != nullptr, "null argument");
-	std::unique_lock<std::mutex> lk(s->mu);
-	auto it = s->queries.find(ticket);
-	VGPU_CHECK(it != s->queries.end(), "unknown ticket %llu", (unsigned long long)ticket);
-	const auto &q = it->second;
-	VGPU_CHECK(q.state == 2, "query %llu has not completed", (unsigned long long)ticket);
-	const Program &P = q.p->prog;
-	for (unsigned j = 0; j < P.nout && q.rows; j++)
-		CUDA_OK(cudaMemcpy(host_cols[j], q.out[j], q.rows * P.out_stride[j], cudaMemcpyDeviceToHost),
-			"result download");
+	/* the columns' places under the lock; the copies without it, so that
+	 * submissions and the scheduler go on during a long download (a
+	 * completed result stays where it is until its ticket is released) */
+	const void *src[kMaxRegs];
+	size_t bytes[kMaxRegs];
+	unsigned nout = 0;
+	{
+		std::lock_guard<std::mutex> lk(s->mu);
+		auto it = s->queries.find(ticket);
+		VGPU_CHECK(it != s->queries.end(), "unknown ticket %llu", (unsigned long long)ticket);
+		const auto &q = it->second;
+		VGPU_CHECK(q.state == 2, "query %llu has not completed", (unsigned long long)ticket);
+		const Program &P = q.p->prog;
+		nout = q.rows ? P.nout : 0u;
+		for (unsigned j = 0; j < nout; j++) {
+			src[j] = q.out[j];
+			bytes[j] = q.rows * P.out_stride[j];
+		}
+	}
+	for (unsigned j = 0; j < nout; j++)
+		CUDA_OK(cudaMemcpy(host_cols[j], src[j], bytes[j], cudaMemcpyDeviceToHost), "result download");
 	return 1;
 }
 
