@@ -83,7 +83,7 @@ def test_query_host_end_to_end(data_a, engine):
     assert_same_stream(got, db.query(CONFIG1).columns, "query_host")
 
 
-@pytest.mark.parametrize("shape", [(128, 8), (128, 16), (256, 4), (256, 8), (256, 16), (512, 4),
+@pytest.mark.parametrize("shape", [(128, 4), (128, 8), (128, 16), (256, 4), (256, 8), (256, 16), (512, 4),
                                    (512, 8)])
 def test_every_launch_shape(data_a, engine, shape):
     db, _, t = data_a

@@ -193,7 +193,7 @@ int autotune(virg_gpu_batch *b)
 	auto hit = e->tuned.find(key);
 	if (hit != e->tuned.end())
 		return build_with(b, &hit->second);
-	static const unsigned cand[][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
+	static const unsigned cand[][2] = {{128, 4}, {128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
 		{512, 8}};
 	float best = 1e30f;
 	Shape best_shape = {0, 0, 0, 0};

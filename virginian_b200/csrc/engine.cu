@@ -560,7 +560,7 @@ extern "C" int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p
 	const virg_gpu_table *t, unsigned *shape4)
 {
 	VGPU_CHECK(e != nullptr && p != nullptr && t != nullptr, "null argument");
-	static const unsigned cand[][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
+	static const unsigned cand[][2] = {{128, 4}, {128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
 		{512, 8}};
 	cudaEvent_t a, z;
 	CUDA_OK(cudaEventCreate(&a), "event");

@@ -1602,7 +1602,7 @@ static int occ_t(size_t smem, int *ctas)
 	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem) == cudaSuccess;
 }
 
-#define VGPU_SHAPES(X) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
+#define VGPU_SHAPES(X) X(128, 4) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
 
 int shape_supported(const Shape &s)
 {
