@@ -70,10 +70,12 @@ constexpr unsigned kOffOff = kOffCdone + 8 * kSlots;         /* uint64[kSlots]: 
 constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;         /* uint32[8]: ok[kSlots], abort, end tile */
 constexpr unsigned kOffTot = kOffFlags + 32;                 /* uint32[kSlots]: tile totals */
 constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;          /* uint32[kMaxStages]: query per stage */
+constexpr unsigned kOffTready = 328;                          /* mbarrier[kSlots]: tile count ready */
 constexpr unsigned kOffCnt = 512;                            /* uint32[kSlots][kMaxGroups]: per 64 rows */
 constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
 static_assert(kSlots <= kFAbort, "ok flags per slot");
-static_assert(kOffHeld + 4 * kMaxStages <= kOffCnt, "smem header layout");
+static_assert(kOffHeld + 4 * kMaxStages <= kOffTready, "smem header layout");
+static_assert(kOffTready + 8 * kSlots <= kOffCnt, "smem header layout");
 static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
 static_assert(sizeof(QDesc) % 16 == 0, "QDesc copies in 16-byte chunks");
 static_assert(kStageHdr >= sizeof(QDesc) + sizeof(StageInfo), "stage header too small");
@@ -1257,7 +1259,7 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 		else
 			ok = lookback_excl(kp, Q, si.work, prev_work == ~0ull ? -1 : (int64_t)prev_work, prev_end, lane, &excl);
 		/* the tile's own count */
-		if (ok && !mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
+		if (ok && !mbar_wait(smem_addr(smem + kOffTready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
 			return;
 		const uint32_t tile_total = ok ? tot[q] : 0u;
 		prev_work = si.work;
@@ -1397,6 +1399,7 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		}
 		for (uint32_t q = 0; q < kSlots; q++) {
 			mbar_init(smem_addr(smem + kOffLready + 8 * q), NW);
+			mbar_init(smem_addr(smem + kOffTready + 8 * q), 1);
 			mbar_init(smem_addr(smem + kOffOready + 8 * q), 1);
 			mbar_init(smem_addr(smem + kOffLfree + 8 * q), P);
 			mbar_init(smem_addr(smem + kOffCdone + 8 * q), NW);
@@ -1534,6 +1537,27 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		const uint32_t ex = incl - sum;
 		const uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
 
+		/* ---- the tile's count: to the look-back words (before the list, so
+		 * that other CTAs' look-backs see it as early as possible) and the
+		 * other roles */
+		if (warp == 0) {
+			const unsigned char *hdr = smem + kp.stage_area + sd;
+			const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
+			if (lane == 0) {
+				publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
+				sts_u32(sbase + kOffTot + 4 * q, tile_total);
+				mbar_arrive(smem_addr(smem + kOffTready + 8 * q));
+			}
+			/* valid rows per 64-row block, for result-tablet splitting on the
+			 * host: group g covers tile rows 64 g .. 64 g + 63 */
+			if (Q.block_counts != nullptr) {
+				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+				for (int g = lane; g < G; g += 32)
+					if (64u * (uint32_t)g < si.nrows)
+						Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
+							(uint8_t)lds_u32(cnt + 4 * g);
+			}
+		}
 		/* ---- the tile-ordered list of selected rows */
 		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
 #pragma unroll
@@ -1556,24 +1580,6 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 			}
 		}
 
-		/* ---- the tile's count: to the look-back words and the other roles */
-		if (warp == 0) {
-			const unsigned char *hdr = smem + kp.stage_area + sd;
-			const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-			if (lane == 0) {
-				publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
-				sts_u32(sbase + kOffTot + 4 * q, tile_total);
-			}
-			/* valid rows per 64-row block, for result-tablet splitting on the
-			 * host: group g covers tile rows 64 g .. 64 g + 63 */
-			if (Q.block_counts != nullptr) {
-				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
-				for (int g = lane; g < G; g += 32)
-					if (64u * (uint32_t)g < si.nrows)
-						Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
-							(uint8_t)lds_u32(cnt + 4 * g);
-			}
-		}
 		__syncwarp();
 		if (lane == 0)
 			mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
