@@ -41,6 +41,9 @@ import numpy as np  # noqa: E402
 
 ROWS = 50_000_000
 HEADLINE_SEL = 0.10
+METRIC = "filter scan GB/s (% HBM peak)"
+WORKLOAD = ("device-resident filter scan + arithmetic (7-column table, 50M rows per GPU, "
+            "10% selectivity)")
 # DRAM bytes of the headline kernel per scanned row and per result row,
 # from ncu (dram__bytes_read.sum, dram__bytes_write.sum) on an 8M-row launch
 # of the same query: 224.27 MB read, 11.84 MB written for 800,581 result rows
@@ -525,12 +528,12 @@ def run_reference(args):
     total = sum(times)
     value = alg * len(times) / total / 1e9
     line = {
-        "impl": "reference", "metric": "filter scan GB/s", "value": round(value, 3), "unit": "GB/s",
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total / len(times) * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/float32", "data": "synthetic",
-        "config": {"workload": "device-resident filter scan + arithmetic, 10% selectivity",
-                   "rows": rows, "query": sql, "l2": "inputs larger than L2"},
+        "config": {"workload": WORKLOAD, "rows_per_step": rows, "query": sql,
+                   "sample": "each step scans a 1M-row sample of the workload's table on the host"},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
                          "kind": "reference",
                          "sample": f"{rows} rows of the same table and query per step, "
@@ -677,12 +680,11 @@ def run_b200(args):
                          "kind": "reference", "vm": "virginia_multi"}
         shape = eng.last_launch()
         line = {
-            "metric": "filter scan GB/s (% HBM peak)", "value": round(value, 2), "unit": "GB/s",
+            "metric": METRIC, "value": round(value, 2), "unit": "GB/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32/float32", "data": "synthetic",
-            "config": {"workload": "device-resident filter scan + arithmetic (7-column table, "
-                                   "50M rows per GPU, 10% selectivity)",
+            "config": {"workload": WORKLOAD,
                        "rows_per_gpu": rows, "query": QUERY.format(c=constants(cols, 0.1)[0],
                                                                    d=constants(cols, 0.1)[1]),
                        "result_rows": out_rows, "l2": "inputs larger than L2 (1.4 GB per step)",
