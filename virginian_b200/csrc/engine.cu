@@ -212,6 +212,14 @@ static uint32_t op_head(const UOp &u)
 void fill_operands(QDesc &d, uint32_t vec_area)
 {
 	const Program &P = d.prog;
+	/* the kernel's view of the program, in the staged prefix */
+	for (unsigned i = 0; i < kMaxRegs; i++) {
+		d.consts[i] = P.consts[i];
+		d.out_stride[i] = P.out_stride[i];
+	}
+	d.nfilter = P.nfilter;
+	d.nuops = P.nuops;
+	d.nout = P.nout;
 	auto od = [&](uint8_t cls, uint8_t idx) -> uint32_t {
 		if (cls == OC_COL)
 			return OD_STAGE | (uint32_t)(kSmemHeader + d.load_off[idx]);
@@ -219,7 +227,7 @@ void fill_operands(QDesc &d, uint32_t vec_area)
 			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | (vec_area + d.vec_off[idx]);
 		/* scalars are read from the stage's copy of the descriptor */
 		return OD_SCALAR |
-			(uint32_t)(kSmemHeader + offsetof(QDesc, prog) + offsetof(Program, consts) + idx * 8u);
+			(uint32_t)(kSmemHeader + offsetof(QDesc, consts) + idx * 8u);
 	};
 	for (uint32_t k = 0; k < P.nuops; k++) {
 		const UOp &u = P.uops[k];

@@ -35,7 +35,7 @@ struct Shape {
  * info and the result-scan scratch */
 /* (the kernel's fixed header: barriers, tile offsets, scan scratch) */
 constexpr unsigned kMaxStages = 8;
-constexpr unsigned kSmemHeader = 4096;
+constexpr unsigned kSmemHeader = 2048;
 
 /* per-stage work item, decoded by the issuing thread */
 struct StageInfo {
@@ -53,7 +53,7 @@ struct StageInfo {
  * selection lists, row vectors, counts and offsets */
 constexpr unsigned kSlots = 3;
 
-constexpr unsigned kStageHdr = (unsigned)((sizeof(QDesc) + sizeof(StageInfo) + 127) / 128 * 128);
+constexpr unsigned kStageHdr = (unsigned)((kQDescStaged + sizeof(StageInfo) + 127) / 128 * 128);
 
 /* serving-session control, in host-mapped memory written by the host:
  * published queries and work items (a query's descriptor is complete before

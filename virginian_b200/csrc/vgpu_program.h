@@ -141,7 +141,16 @@ struct SegDesc {
 
 /* per-query launch descriptor, in device memory */
 struct alignas(16) QDesc {
-	Program prog;
+	/* Everything before `prog` is what the kernel reads from a stage's copy
+	 * of the descriptor (the stage holds only that prefix); the decoded
+	 * program itself is read from device memory by the producer (its loads)
+	 * and is host-side otherwise. */
+	/* the program's constants, split point, op count and result columns */
+	uint64_t consts[kMaxRegs];
+	uint32_t nfilter;
+	uint32_t nuops;
+	uint32_t nout;
+	uint8_t out_stride[kMaxRegs];
 	/* smem layout for this launch shape */
 	uint32_t load_off[kMaxLoads];
 	uint32_t stage_bytes;
@@ -166,7 +175,11 @@ struct alignas(16) QDesc {
 	 * query; its first tile starts there */
 	const unsigned long long *base_in;
 	uint64_t pad1;
+	Program prog;
 };
+
+/* bytes of a descriptor that a stage holds (the kernel's view) */
+constexpr unsigned kQDescStaged = (unsigned)((offsetof(QDesc, prog) + 15) / 16 * 16);
 
 /* device error codes (written once per launch to the error word) */
 enum DevError : unsigned {

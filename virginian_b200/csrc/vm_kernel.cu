@@ -77,16 +77,16 @@ static_assert(kSlots <= kFAbort, "ok flags per slot");
 static_assert(kOffHeld + 4 * kMaxStages <= kOffTready, "smem header layout");
 static_assert(kOffTready + 8 * kSlots <= kOffCnt, "smem header layout");
 static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
-static_assert(sizeof(QDesc) % 16 == 0, "QDesc copies in 16-byte chunks");
-static_assert(kStageHdr >= sizeof(QDesc) + sizeof(StageInfo), "stage header too small");
+static_assert(kQDescStaged % 16 == 0 && kQDescStaged <= sizeof(QDesc), "descriptor copies in 16-byte chunks");
+static_assert(kStageHdr >= kQDescStaged + sizeof(StageInfo), "stage header too small");
 static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a time");
 
 /* where the fields the compute warps read sit in a stage's descriptor copy */
 constexpr uint32_t kQOps = (uint32_t)offsetof(QDesc, ops);
-constexpr uint32_t kQNFilter = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nfilter));
-constexpr uint32_t kQNUops = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nuops));
-constexpr uint32_t kQNOut = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, nout));
-constexpr uint32_t kQOutStride = (uint32_t)(offsetof(QDesc, prog) + offsetof(Program, out_stride));
+constexpr uint32_t kQNFilter = (uint32_t)offsetof(QDesc, nfilter);
+constexpr uint32_t kQNUops = (uint32_t)offsetof(QDesc, nuops);
+constexpr uint32_t kQNOut = (uint32_t)offsetof(QDesc, nout);
+constexpr uint32_t kQOutStride = (uint32_t)offsetof(QDesc, out_stride);
 constexpr uint32_t kQOdOut = (uint32_t)offsetof(QDesc, od_out);
 constexpr uint32_t kQOutPtr = (uint32_t)offsetof(QDesc, out_ptr);
 constexpr uint32_t kQCapacity = (uint32_t)offsetof(QDesc, capacity);
@@ -1186,7 +1186,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 			si.seg = it.seg;
 			si.row0 = it.row0;
 			si.nrows = it.nrows;
-			*reinterpret_cast<StageInfo *>(hdr + sizeof(QDesc)) = si;
+			*reinterpret_cast<StageInfo *>(hdr + kQDescStaged) = si;
 		}
 		if (end) {
 			/* serving: every issued tile is counted before the CTA ends */
@@ -1199,7 +1199,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		}
 		const bool copy_desc = held[s] != pq.qi;
 		const uint32_t bytes = __reduce_add_sync(0xffffffffu, it.bytes) +
-			(copy_desc ? (uint32_t)sizeof(QDesc) : 0u);
+			(copy_desc ? (uint32_t)kQDescStaged : 0u);
 		__syncwarp();
 		if (lane == 0) {
 			held[s] = pq.qi;
@@ -1213,7 +1213,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		if (it.bytes)
 			bulk_load(base + pq.off, it.src, it.bytes, full);
 		if (copy_desc && lane == 31)
-			bulk_load(base, pq.Q, (uint32_t)sizeof(QDesc), full);
+			bulk_load(base, pq.Q, (uint32_t)kQDescStaged, full);
 		const uint32_t w = next_item(k);
 		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
 	}
@@ -1248,7 +1248,7 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 		 * this warp */
 		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
 		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + kQDescStaged);
 		if (si.work >= kp.total_work)
 			return;
 		uint64_t excl = 0;
@@ -1444,7 +1444,7 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 		}
 		const uint32_t sd = s * kp.stage_bytes;
 		const uint32_t qd = sbase + kp.stage_area + sd;
-		const uint32_t sinfo = qd + (uint32_t)sizeof(QDesc);
+		const uint32_t sinfo = qd + (uint32_t)kQDescStaged;
 		if (lds_u32(sinfo + offsetof(StageInfo, work)) >= kp.total_work) {
 			/* no more tiles: tell the look-back and projection warps */
 			__syncwarp();
@@ -1551,7 +1551,7 @@ __global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)
 			/* valid rows per 64-row block, for result-tablet splitting on the
 			 * host: group g covers tile rows 64 g .. 64 g + 63 */
 			if (Q.block_counts != nullptr) {
-				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + sizeof(QDesc));
+				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + kQDescStaged);
 				for (int g = lane; g < G; g += 32)
 					if (64u * (uint32_t)g < si.nrows)
 						Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
