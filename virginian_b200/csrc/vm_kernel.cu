@@ -54,10 +54,6 @@ constexpr uint32_t kSuspendHintNs = 20000;
 constexpr unsigned kFAbortSlot = 4;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
-/* work items claimed per atomic by the producer: one, so tiles that follow
- * each other in a query are taken, and finished, at about the same time */
-constexpr unsigned kClaim = 1;
-
 /* shared memory header (kSmemHeader bytes) */
 constexpr unsigned kMaxGroups = 128;  /* R x warps */
 constexpr unsigned kOffFull = 0;                            /* mbarrier[kMaxStages] */
@@ -986,6 +982,10 @@ struct ProdQuery {
 	const uint32_t *tile_prefix;
 	uint32_t nsegs, nload, qi, seg_hint;
 	uint32_t src, stride, off;   /* this lane's column */
+	/* the current segment: its tiles [seg_t0, seg_t1) of the query, rows,
+	 * and this lane's column in it; seg ~0 when none */
+	uint32_t seg, seg_t0, seg_t1, seg_rows;
+	const unsigned char *colp;
 };
 
 /* one decoded work item; src and bytes are this lane's column copy */
@@ -1019,22 +1019,32 @@ __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint6
 		pq.nsegs = Q->nsegs;
 		pq.nload = Q->prog.nload;
 		pq.seg_hint = 0;
+		pq.seg = ~0u;
 		if (lane < kMaxLoads) {
 			pq.src = Q->prog.load_src[lane];
 			pq.stride = Q->prog.load_stride[lane];
 			pq.off = Q->load_off[lane];
 		}
 	}
-	const uint64_t t = w - pq.first;
-	const uint32_t s = warp_search(pq.tile_prefix, pq.seg_hint, pq.nsegs, t, lane);
-	pq.seg_hint = s;
-	const SegDesc *sd = pq.segs + s;
-	const uint32_t row0 = (uint32_t)(t - pq.tile_prefix[s]) * TILE;
-	it.seg = s;
+	/* an item in the previous item's segment needs no load at all */
+	const uint32_t t = (uint32_t)(w - pq.first);
+	if (pq.seg == ~0u || t >= pq.seg_t1) {
+		const uint32_t s = warp_search(pq.tile_prefix, pq.seg_hint, pq.nsegs, t, lane);
+		const SegDesc *sd = pq.segs + s;
+		pq.seg_hint = s;
+		pq.seg = s;
+		pq.seg_t0 = pq.tile_prefix[s];
+		pq.seg_t1 = pq.tile_prefix[s + 1];
+		pq.seg_rows = sd->rows;
+		if ((uint32_t)lane < pq.nload)
+			pq.colp = static_cast<const unsigned char *>(sd->col[pq.src]);
+	}
+	const uint32_t row0 = (t - pq.seg_t0) * TILE;
+	it.seg = pq.seg;
 	it.row0 = row0;
-	it.nrows = min((uint32_t)TILE, sd->rows - row0);
+	it.nrows = min((uint32_t)TILE, pq.seg_rows - row0);
 	if ((uint32_t)lane < pq.nload) {
-		it.src = static_cast<const unsigned char *>(sd->col[pq.src]) + (size_t)row0 * pq.stride;
+		it.src = pq.colp + (size_t)row0 * pq.stride;
 		it.bytes = (it.nrows * pq.stride + 15u) & ~15u;
 	}
 }
@@ -1042,10 +1052,13 @@ __device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint6
 /* The producer warp fills the ring of stages.  Once the compute warps
  * released a stage it announces the decoded work item and issues its copies
  * (lane i copies column i; the query descriptor only when the stage does
- * not hold it already), then claims (kClaim per atomic, in order) and
- * decodes the next item while those copies run.  Claiming one item ahead,
- * not a whole ring ahead, keeps claimed tiles from idling while other CTAs'
- * look-backs wait for their counts.  An invalid claim (past the end of the
+ * not hold it already), then takes the next claim (in order, with the one
+ * after it already in flight) and decodes it while those copies run.
+ * Claiming a couple of items ahead, not a whole ring ahead, keeps claimed
+ * tiles from idling while other CTAs' look-backs wait for their counts.
+ * The claim and decode are the producer's serial path per tile, so the
+ * claim's atomic round trip is overlapped and an item in the previous
+ * item's segment is decoded without loads.  An invalid claim (past the end of the
  * work list) is announced without data and ends the CTA's pipeline.
  *
  * In a serving session the work list grows: a claim past the published
@@ -1067,17 +1080,21 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	ProdQuery pq;
 	pq.Q = nullptr;
 	pq.qi = 0;
-	uint32_t next = 0, left = 0;
+	/* claims: one atomic in flight (lane 0) while the previous claim's item
+	 * is decoded and issued, so its round trip is off the per-tile path */
+	uint32_t inflight = 0;
+	bool have = false;
 	auto claim = [&]() -> uint32_t {
-		if (left == 0) {
-			uint32_t v = 0;
-			if (lane == 0)
-				v = atomicAdd(kp.counter, kClaim);
-			next = __shfl_sync(0xffffffffu, v, 0);
-			left = kClaim;
+		uint32_t v = 0;
+		if (lane == 0) {
+			if (!have) {
+				inflight = atomicAdd(kp.counter, 1u);
+				have = true;
+			}
+			v = inflight;
+			inflight = atomicAdd(kp.counter, 1u);
 		}
-		left--;
-		return next++;
+		return __shfl_sync(0xffffffffu, v, 0);
 	};
 	/* serving: the tile of stage s is stored; the query's last one reports */
 	auto count_stored = [&](uint32_t s) {
