@@ -207,6 +207,14 @@ unsigned long long orc_result_rows(orc_result *r) { return r->rows; }
 unsigned orc_result_ncols(orc_result *r) { return r->ncols; }
 unsigned orc_result_ntablets(orc_result *r) { return r->ntablets; }
 double orc_result_seconds(orc_result *r) { return r->seconds; }
+/* the GPU VM's own timing of the last run, seconds (src/vm/vm_gpu.cu:207-240):
+ * k = 1 host-to-device copies, 2 kernels, 3 device-to-host copies */
+double orc_result_timing(orc_result *r, int k)
+{
+	if(!r->vm)
+		return 0;
+	return k == 1 ? r->vm->timing1 : k == 2 ? r->vm->timing2 : r->vm->timing3;
+}
 int orc_result_type(orc_result *r, unsigned c) { return r->types[c]; }
 unsigned orc_result_stride(orc_result *r, unsigned c) { return r->strides[c]; }
 const virg_vm *orc_result_vm(orc_result *r) { return r->vm; }

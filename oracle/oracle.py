@@ -21,6 +21,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libvirg_ref.so")
+REFGPU_LIB = os.path.join(HERE, "_ref", "libvirg_refgpu.so")
 HOST_LIB = os.path.join(HERE, "_ref", "libvirg_host.so")
 
 # virg_t (src/virginian.h:196-204)
@@ -79,6 +80,8 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.orc_result_ntablets.argtypes = [vp]
     lib.orc_result_seconds.restype = ctypes.c_double
     lib.orc_result_seconds.argtypes = [vp]
+    lib.orc_result_timing.restype = ctypes.c_double
+    lib.orc_result_timing.argtypes = [vp, ctypes.c_int]
     lib.orc_result_type.restype = i
     lib.orc_result_type.argtypes = [vp, u]
     lib.orc_result_stride.restype = u
@@ -195,7 +198,9 @@ class OracleDB:
             nt = self.lib.orc_result_ntablets(r)
             trows = (ctypes.c_uint * max(1, nt))()
             self.lib.orc_result_tablet_rows(self.h, r, trows)
-            return Result(cols, types, list(trows)[:nt], self.lib.orc_result_seconds(r))
+            res = Result(cols, types, list(trows)[:nt], self.lib.orc_result_seconds(r))
+            res.gpu_timing = tuple(self.lib.orc_result_timing(r, k) for k in (1, 2, 3))
+            return res
         finally:
             self.lib.orc_result_free(self.h, r)
 
