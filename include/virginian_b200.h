@@ -228,6 +228,19 @@ int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
  */
 const size_t *virg_gpu_getsizes(void);
 
+/*
+ * Residency cache of the drop-in (no reference counterpart; the reference
+ * copies every tablet for every query, src/vm/vm_gpu.cu:147-160): with a
+ * capacity in bytes, virg_vm_gpu keeps the data tablets it copies to HBM
+ * (every column and the key, keyed by tablet id, checked against the
+ * tablet's row count and host slot), evicting the least recently used.  0
+ * (the default) turns it off and frees it; clear it after rebuilding a table
+ * under the same tablet ids.  Stats: cache hits and misses of virg_vm_gpu
+ * and bytes held.
+ */
+int virg_gpu_dropin_cache(uint64_t bytes);
+int virg_gpu_dropin_cache_stats(uint64_t *hits, uint64_t *misses, uint64_t *bytes);
+
 /* ======================================================================
  * 2. Engine API (no reference counterpart)
  * ====================================================================== */

@@ -79,6 +79,8 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_last_error": (ctypes.c_char_p, []),
         "virg_gpu_getsizes": (P(ctypes.c_size_t), []),
         "virg_vm_gpu": (i, [vp, vp, vp, vp, u]),
+        "virg_gpu_dropin_cache": (i, [u64]),
+        "virg_gpu_dropin_cache_stats": (i, [P(u64), P(u64), P(u64)]),
         "virg_gpu_engine_create": (i, [i, P(vp)]),
         "virg_gpu_engine_destroy": (None, [vp]),
         "virg_gpu_engine_stream": (vp, [vp]),

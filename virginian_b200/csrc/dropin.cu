@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -71,6 +72,89 @@ bool resolve(HostApi &h)
 std::mutex g_mu;
 virg_gpu_engine *g_engine = nullptr;
 
+/* Residency cache of data tablets in HBM (off unless a capacity is set):
+ * every column and the key of a tablet, in the engine's device layout,
+ * keyed by tablet id and checked against the tablet's row count and host
+ * slot, least recently used evicted first.  The reference's tables only
+ * grow by appends (a changed row count is a miss); a caller that rebuilds a
+ * table under the same tablet ids clears the cache (capacity 0). */
+struct CachedTablet {
+	uint64_t rows = 0;
+	const void *slot = nullptr;
+	void *mem = nullptr;
+	size_t bytes = 0;
+	const void *col[kMaxLoads] = {};
+	uint64_t last_use = 0;
+};
+std::map<unsigned, CachedTablet> g_cache;
+size_t g_cache_cap = 0, g_cache_bytes = 0;
+uint64_t g_cache_clock = 0, g_cache_hits = 0, g_cache_misses = 0;
+
+void cache_drop(std::map<unsigned, CachedTablet>::iterator it)
+{
+	cudaFree(it->second.mem);
+	g_cache_bytes -= it->second.bytes;
+	g_cache.erase(it);
+}
+
+/* the tablet's device copy from the cache, or a new one (all columns and the
+ * key); nullptr if it cannot be cached (too big, or a copy failed) */
+const CachedTablet *cache_get(const virg_tablet_meta *t, const virg_gpu_schema &schema, cudaStream_t st)
+{
+	auto it = g_cache.find(t->id);
+	if (it != g_cache.end()) {
+		if (it->second.rows == t->rows && it->second.slot == (const void *)t) {
+			it->second.last_use = ++g_cache_clock;
+			g_cache_hits++;
+			return &it->second;
+		}
+		cache_drop(it);
+	}
+	g_cache_misses++;
+	const uint32_t pr = (uint32_t)((t->rows + 63) / 64 * 64 + 16);
+	size_t bytes = 0;
+	for (unsigned c = 0; c < schema.ncols; c++)
+		bytes += (pr * (size_t)t->fixed_stride[c] + 255) / 256 * 256;
+	bytes += (pr * (size_t)t->key_stride + 255) / 256 * 256;
+	if (bytes > g_cache_cap)
+		return nullptr;
+	while (g_cache_bytes + bytes > g_cache_cap && !g_cache.empty()) {
+		auto lru = g_cache.begin();
+		for (auto i = g_cache.begin(); i != g_cache.end(); ++i)
+			if (i->second.last_use < lru->second.last_use)
+				lru = i;
+		cache_drop(lru);
+	}
+	CachedTablet ct;
+	if (cudaMalloc(&ct.mem, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		return nullptr;
+	}
+	ct.rows = t->rows;
+	ct.slot = t;
+	ct.bytes = bytes;
+	ct.last_use = ++g_cache_clock;
+	unsigned char *p = static_cast<unsigned char *>(ct.mem);
+	bool ok = true;
+	for (unsigned c = 0; c < schema.ncols; c++) {
+		const size_t sz = t->fixed_stride[c];
+		ok = ok && cudaMemcpyAsync(p, (const char *)t + t->fixed_block + t->fixed_offset[c], t->rows * sz,
+			cudaMemcpyHostToDevice, st) == cudaSuccess;
+		ct.col[c] = p;
+		p += (pr * sz + 255) / 256 * 256;
+	}
+	ok = ok && cudaMemcpyAsync(p, (const char *)t + t->key_block, t->rows * (size_t)t->key_stride,
+		cudaMemcpyHostToDevice, st) == cudaSuccess;
+	ct.col[kKeySlot] = p;
+	if (!ok) {
+		cudaStreamSynchronize(st);
+		cudaFree(ct.mem);
+		return nullptr;
+	}
+	g_cache_bytes += bytes;
+	return &(g_cache[t->id] = ct);
+}
+
 /* VIRG_CUDADEVICE (src/virginian.h:103) */
 constexpr int kDevice = 0;
 
@@ -86,6 +170,32 @@ struct Timers {
 };
 
 }  // namespace
+
+extern "C" int virg_gpu_dropin_cache(uint64_t bytes)
+{
+	std::lock_guard<std::mutex> glk(g_mu);
+	g_cache_cap = (size_t)bytes;
+	while (g_cache_bytes > g_cache_cap && !g_cache.empty()) {
+		auto lru = g_cache.begin();
+		for (auto i = g_cache.begin(); i != g_cache.end(); ++i)
+			if (i->second.last_use < lru->second.last_use)
+				lru = i;
+		cache_drop(lru);
+	}
+	return 1;
+}
+
+extern "C" int virg_gpu_dropin_cache_stats(uint64_t *hits, uint64_t *misses, uint64_t *bytes)
+{
+	std::lock_guard<std::mutex> glk(g_mu);
+	if (hits)
+		*hits = g_cache_hits;
+	if (misses)
+		*misses = g_cache_misses;
+	if (bytes)
+		*bytes = g_cache_bytes;
+	return 1;
+}
 
 extern "C" const size_t *virg_gpu_getsizes(void)
 {
@@ -167,8 +277,26 @@ extern "C" int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
 		cudaEventRecord(tm.a, e->stream);
 		virg_gpu_result *r = nullptr;
 		const uint64_t nblocks = (t->rows + 63) / 64;
-		ok = table_add_segments(&stage, &seg, 1, want, want_key, e->stream) && table_sync_desc(&stage) &&
-			result_alloc(e, P, t->rows, true, nblocks, &r);
+		/* the tablet's columns in HBM: from the residency cache when it is
+		 * on, else copied for this query only */
+		const CachedTablet *ct = g_cache_cap && t->rows ? cache_get(t, schema, e->stream) : nullptr;
+		if (ct) {
+			SegDesc d;
+			memset(&d, 0, sizeof(d));
+			d.rows = t->rows;
+			d.block_base = 0;
+			for (unsigned c = 0; c < kMaxLoads; c++)
+				d.col[c] = ct->col[c];
+			stage.segs.push_back(d);
+			stage.seg_rows.push_back((uint32_t)t->rows);
+			stage.rows = t->rows;
+			stage.blocks = nblocks;
+			stage.dirty = true;
+			ok = table_sync_desc(&stage);
+		} else {
+			ok = table_add_segments(&stage, &seg, 1, want, want_key, e->stream) && table_sync_desc(&stage);
+		}
+		ok = ok && result_alloc(e, P, t->rows, true, nblocks, &r);
 		cudaEventRecord(tm.b, e->stream);
 		if (ok && t->rows) {
 			QueryLaunch q;
