@@ -464,7 +464,9 @@ typedef struct {
 } virg_serve_counters;
 
 int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cfg, virg_serve **out);
-/* queue a query; estimated_rows 0 reserves the bound (the table's rows) */
+/* queue a query; estimated_rows 0 reserves the rows the same program last
+ * returned on the same table, plus a quarter, or else the bound (the
+ * table's rows); a short reservation is admitted again with the exact rows */
 int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_gpu_table *t,
 	uint64_t estimated_rows, uint64_t *ticket);
 /* a query's state; wait_ms < 0 waits for completion, > 0 up to that long */

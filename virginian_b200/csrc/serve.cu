@@ -183,6 +183,9 @@ struct virg_serve {
 	std::thread sched;
 	std::atomic<bool> quit{false};
 	std::string fail;
+	/* result rows each (program, table) pair last had, with the table's rows
+	 * then: the default estimate of its next submission */
+	std::map<std::pair<const virg_gpu_program *, const virg_gpu_table *>, std::pair<uint64_t, uint64_t>> history;
 };
 
 namespace {
@@ -452,6 +455,7 @@ unsigned harvest(virg_serve *s)
 		q.rows = rows;
 		q.state = 2;
 		q.completed = Clock::now();
+		s->history[{q.p, q.t}] = {rows, q.t->rows};
 	}
 	s->inflight.swap(keep);
 	return n;
@@ -599,7 +603,15 @@ extern "C" int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_
 			return 0;
 	}
 	const uint64_t bound = t->rows;
-	const uint64_t est = estimated_rows ? std::min(estimated_rows, bound) : bound;
+	uint64_t est = estimated_rows ? std::min(estimated_rows, bound) : bound;
+	if (!estimated_rows) {
+		/* the selectivity this program last had on this table, with a
+		 * margin; a short estimate is admitted again with its exact rows */
+		std::lock_guard<std::mutex> lk(s->mu);
+		auto h = s->history.find({p, t});
+		if (h != s->history.end() && h->second.second == bound)
+			est = std::min<uint64_t>(bound, h->second.first + h->second.first / 4 + 1024);
+	}
 	VGPU_CHECK(arena_need(P, est) <= s->cfg.result_budget_bytes,
 		"the query's result reservation (%zu bytes) exceeds the result budget", arena_need(P, est));
 	std::lock_guard<std::mutex> lk(s->mu);
