@@ -63,6 +63,8 @@ namespace {
 constexpr unsigned kStatusRingBits = 22;  /* 4M look-back words, 32 MB */
 constexpr uint64_t kStatusRing = 1ull << kStatusRingBits;
 constexpr uint64_t kSessionWorkLimit = 1ull << 31;
+/* (program, table) pairs whose last result size is remembered */
+constexpr size_t kHistoryLimit = 1 << 16;
 constexpr size_t kTilePoolWords = 4u << 20;  /* segment tile prefixes per session */
 
 using Clock = std::chrono::steady_clock;
@@ -455,6 +457,8 @@ unsigned harvest(virg_serve *s)
 		q.rows = rows;
 		q.state = 2;
 		q.completed = Clock::now();
+		if (s->history.size() >= kHistoryLimit)
+			s->history.clear();
 		s->history[{q.p, q.t}] = {rows, q.t->rows};
 	}
 	s->inflight.swap(keep);
