@@ -1358,7 +1358,24 @@ __device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int l
 				const uint32_t stride = lds_u8(qd + kQOutStride + j);
 				const Opnd a = stride == 8 ? opnd<8>(od, sbase, sd, c.vd)
 					: stride == 4 ? opnd<4>(od, sbase, sd, c.vd) : opnd<1>(od, sbase, sd, c.vd);
-				for (uint32_t e = c.e0; e < c.n; e += c.step) {
+				uint32_t e0 = c.e0;
+				if (stride == 4) {
+					/* four entries per lane in flight: their list and value
+					 * loads overlap */
+					uint32_t *o32 = reinterpret_cast<uint32_t *>(out);
+					for (; e0 + 3 * c.step < c.n && off + e0 + 3 * c.step < cap; e0 += 4 * c.step) {
+						const uint32_t e1 = e0 + c.step, e2 = e1 + c.step, e3 = e2 + c.step;
+						const uint32_t r0 = lds_u16(c.list + 2 * e0), r1 = lds_u16(c.list + 2 * e1);
+						const uint32_t r2 = lds_u16(c.list + 2 * e2), r3 = lds_u16(c.list + 2 * e3);
+						const uint32_t v0 = lds_u32(p_addr(a, r0, e0)), v1 = lds_u32(p_addr(a, r1, e1));
+						const uint32_t v2 = lds_u32(p_addr(a, r2, e2)), v3 = lds_u32(p_addr(a, r3, e3));
+						o32[off + e0] = v0;
+						o32[off + e1] = v1;
+						o32[off + e2] = v2;
+						o32[off + e3] = v3;
+					}
+				}
+				for (uint32_t e = e0; e < c.n; e += c.step) {
 					const uint64_t pos = off + e;
 					if (pos >= cap) {
 						overflow = true;
