@@ -57,9 +57,11 @@ QUERY = ("SELECT id, uniformf + normalf5 * 2.5 AS fsum, normali20 / 3 AS idiv, "
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
-        with open(p) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        try:
+            with open(p) as f:
+                return float(json.load(f)["hbm_gbs"]), "measured"
+        except (OSError, ValueError, KeyError, TypeError):
+            pass
     return 6650.0, "fallback"
 
 
