@@ -740,7 +740,7 @@ def main():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--cpu-rows", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--shape", default="", help="threads,rows_per_thread,stages: force the launch "
+    ap.add_argument("--shape", default="", help="threads,stage_kb,stages,ctas_per_sm,chunk_rows: force the launch "
                     "shape of the scan instead of tuning it (for profiling one launch)")
     ap.add_argument("--sections", default="batched,serving,streamed",
                     help="workloads besides the headline scan (comma list; empty for none)")

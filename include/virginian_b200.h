@@ -293,10 +293,18 @@ void *virg_gpu_engine_stream(virg_gpu_engine *e);
 /* device error word set by bounded waits inside kernels (0 = none); reading
  * it synchronises the engine stream and clears it */
 int virg_gpu_engine_check(virg_gpu_engine *e, unsigned *device_error);
-/* launch shape: threads per CTA, rows per thread, staging depth, CTAs per
- * SM; 0 in a field keeps the automatic choice */
+/* launch shape: compute threads per CTA (128, 256 or 512; the CTA adds a
+ * producer and a look-back warp), bytes per staging buffer in KB, number of
+ * staging buffers, CTAs per SM; 0 in a field keeps the automatic choice */
 int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
-	unsigned rows_per_thread, unsigned stages, unsigned ctas_per_sm);
+	unsigned stage_kb, unsigned stages, unsigned ctas_per_sm);
+/* upper bound on the rows of a chunk (the unit a CTA claims and places in
+ * the ordered result): a multiple of 256 in [256, 8192], 0 for automatic */
+int virg_gpu_engine_set_chunk_rows(virg_gpu_engine *e, unsigned rows);
+/* how the full phase reads the columns the results need: 0 (default)
+ * loads only the selected rows' values from device memory where a program
+ * allows it, 1 always stages whole tiles of them in shared memory */
+int virg_gpu_engine_set_staging(virg_gpu_engine *e, int staged_full);
 /* record CUDA events around each of the next kernel launches in a ring of
  * `slots` entries (0 turns it off) */
 int virg_gpu_engine_timing(virg_gpu_engine *e, unsigned slots);
@@ -305,8 +313,8 @@ int virg_gpu_engine_timing(virg_gpu_engine *e, unsigned slots);
 int virg_gpu_engine_kernel_times(virg_gpu_engine *e, float *ms, unsigned n, unsigned *got);
 /* how many kernels the engine has launched since creation */
 unsigned long long virg_gpu_engine_launches(virg_gpu_engine *e);
-/* launch shape chosen for the engine's last launch: shape4 = {threads,
- * rows per thread, stages, CTAs per SM requested}, grid size, shared memory */
+/* launch shape chosen for the engine's last launch: shape4 = {compute
+ * threads, stage KB, stages, CTAs per SM requested}, grid size, shared memory */
 int virg_gpu_engine_last_launch(virg_gpu_engine *e, unsigned *shape4, unsigned *grid,
 	unsigned *smem);
 
@@ -351,7 +359,7 @@ int virg_gpu_query(virg_gpu_engine *e, const virg_gpu_program *p,
 /* time the candidate launch shapes for this program over this table and
  * cache the fastest in the engine (keyed by program shape and table size
  * class); later queries with the same key use it.  shape4 (may be NULL)
- * receives {threads, rows per thread, stages, 0}. */
+ * receives {compute threads, stage KB, stages, CTAs per SM}. */
 int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p,
 	const virg_gpu_table *t, unsigned *shape4);
 int virg_gpu_result_rows(virg_gpu_result *r, uint64_t *rows);
@@ -361,6 +369,14 @@ const void *virg_gpu_result_column(const virg_gpu_result *r, unsigned c);
 int virg_gpu_result_download(virg_gpu_result *r, void *const *host_cols,
 	uint64_t first, uint64_t count);
 void virg_gpu_result_destroy(virg_gpu_result *r);
+
+/* read-bandwidth ceiling of a resident table (a measurement aid, no
+ * reference counterpart): reads every listed column (-1 for the key) of
+ * every segment, mode 0 with 16-byte loads, modes 1-3 with bulk copies into
+ * a shared-memory ring of 4, 6 or 2 stages of 32 KB, and returns the best
+ * device time of `reps` launches (ms) and the bytes one launch reads */
+int virg_gpu_table_read_ceiling(virg_gpu_table *t, const int *cols, unsigned ncols, unsigned mode,
+	unsigned reps, double *ms, unsigned long long *bytes);
 
 /* end to end: host segments in, host result columns out.  Copies the
  * referenced columns to the device, runs the program and copies the result
@@ -404,7 +420,7 @@ int virg_gpu_query_streamed(virg_gpu_engine *e, const virg_gpu_program *p,
 	virg_gpu_result **out, virg_gpu_stream_stats *stats);
 
 /* Batched persistent execution: every query added to a batch runs in one
- * launch of the VM kernel (tiles of all queries in one ordered work list).
+ * launch of the VM kernel (chunks of all queries in one ordered work list).
  * A batch owns its descriptors and counters, so virg_gpu_batch_run with
  * use_graph captures the launch in a CUDA graph once and replays it after.
  * With autotune on, the first run times the candidate launch shapes on the
@@ -421,7 +437,7 @@ int virg_gpu_batch_rows(virg_gpu_batch *b, unsigned slot, uint64_t *rows);
 const void *virg_gpu_batch_column(const virg_gpu_batch *b, unsigned slot, unsigned c);
 int virg_gpu_batch_download(virg_gpu_batch *b, unsigned slot, void *const *host_cols,
 	uint64_t first, uint64_t count);
-/* shape4 = {threads, rows per thread, stages, grid}; work = tiles */
+/* shape4 = {compute threads, stage KB, stages, grid}; work = chunks */
 int virg_gpu_batch_shape(const virg_gpu_batch *b, unsigned *shape4, uint64_t *work);
 void virg_gpu_batch_destroy(virg_gpu_batch *b);
 
@@ -460,7 +476,7 @@ typedef struct {
 	unsigned long long pending, inflight;
 	unsigned long long arena_used;   /* result bytes reserved */
 	unsigned device_error;           /* first device error of any session */
-	unsigned shape[4];               /* threads, rows per thread, stages, grid */
+	unsigned shape[4];               /* compute threads, stage KB, stages, grid */
 } virg_serve_counters;
 
 int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cfg, virg_serve **out);

@@ -83,23 +83,46 @@ def test_query_host_end_to_end(data_a, engine):
     assert_same_stream(got, db.query(CONFIG1).columns, "query_host")
 
 
-@pytest.mark.parametrize("shape", [(128, 4), (128, 8), (128, 16), (256, 4), (256, 8), (256, 16), (512, 4),
-                                   (512, 8)])
+# (compute threads, stage KB, buffers (0: as many as fit), CTAs per SM, chunk rows, staged full tiles)
+@pytest.mark.parametrize("shape", [(128, 16, 0, 1, 1024, 0), (128, 32, 3, 2, 2048, 0), (256, 16, 0, 1, 8192, 0),
+                                   (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 0), (512, 24, 0, 1, 2048, 0),
+                                   (512, 32, 4, 1, 8192, 0), (256, 8, 0, 1, 256, 0), (256, 24, 0, 1, 4096, 1),
+                                   (128, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1)])
 def test_every_launch_shape(data_a, engine, shape):
     db, _, t = data_a
-    engine.set_shape(shape[0], shape[1], 2)
+    engine.set_shape(*shape)
     try:
-        for sql in (CONFIG1, config2(30.0, 20.0), SUITE[8]):
+        for sql in (CONFIG1, config2(30.0, 20.0), SUITE[8], REFILTER[0]):
             try:
                 got, want, _ = run_both(db, t, sql, TYPES_A)
             except vb.VirgError as e:
-                if "shared memory" in str(e):
-                    continue  # this tile size cannot stage the program's columns
+                if "shared memory" in str(e) or "cannot hold" in str(e):
+                    continue  # this stage size cannot stage the program's columns
                 raise
             assert_same_stream(got, want, f"{shape} {sql}")
         assert engine.last_launch()["threads"] == shape[0]
     finally:
-        engine.set_shape(0, 0, 0, 0)
+        engine.set_shape(0, 0, 0, 0, 0, 0)
+
+
+# result columns that reuse a register the filter computed (the code
+# generator's expression reuse): the full phase runs the filter again
+REFILTER = ["select uniformf + normalf5 as s, id from test where uniformf + normalf5 > 50.0",
+            "select normali5 * normali20 as p from test where normali5 * normali20 > 10 and uniformi < 50",
+            "select id, uniformi - normali5 as d, normalf20 from test where uniformi - normali5 < 20 or normalf20 > 30.0"]
+
+
+@pytest.mark.parametrize("staged", [0, 1])
+def test_filter_vectors_in_results(data_a, engine, staged):
+    db, _, t = data_a
+    engine.set_shape(staged_full=staged)
+    try:
+        for sql in REFILTER + ["select id, uniformi, normali5, normali20, uniformf, normalf5, normalf20 "
+                               "from test where uniformi > 90"]:
+            got, want, _ = run_both(db, t, sql, TYPES_A)
+            assert_same_stream(got, want, sql)
+    finally:
+        engine.set_shape(0, 0, 0, 0, 0, 0)
 
 
 @pytest.mark.parametrize("n", [0, 1, 63, 64, 65, 1023, 1024, 1025, 4097, 70_001])

@@ -79,10 +79,16 @@ class Engine:
     def stream(self) -> int:
         return lib().virg_gpu_engine_stream(self.h)
 
-    def set_shape(self, threads: int = 0, rows_per_thread: int = 0, stages: int = 0,
-                  ctas_per_sm: int = 0) -> None:
-        check(lib().virg_gpu_engine_set_shape(self.h, threads, rows_per_thread, stages,
+    def set_shape(self, threads: int = 0, stage_kb: int = 0, stages: int = 0,
+                  ctas_per_sm: int = 0, chunk_rows: int = 0, staged_full: int = 0) -> None:
+        """Launch shape of later queries: compute threads per CTA, KB per
+        staging buffer, buffers, CTAs per SM, the chunk bound and whether
+        the full phase stages whole tiles; 0 in a field keeps the automatic
+        choice."""
+        check(lib().virg_gpu_engine_set_shape(self.h, threads, stage_kb, stages,
                                               ctas_per_sm), "set shape")
+        check(lib().virg_gpu_engine_set_chunk_rows(self.h, chunk_rows), "set chunk rows")
+        check(lib().virg_gpu_engine_set_staging(self.h, staged_full), "set staging")
 
     def device_error(self) -> int:
         e = ctypes.c_uint()
@@ -109,7 +115,7 @@ class Engine:
         g, m = ctypes.c_uint(), ctypes.c_uint()
         check(lib().virg_gpu_engine_last_launch(self.h, s, ctypes.byref(g), ctypes.byref(m)),
               "last launch")
-        return {"threads": s[0], "rows_per_thread": s[1], "stages": s[2], "ctas_per_sm": s[3],
+        return {"threads": s[0], "stage_kb": s[1], "stages": s[2], "ctas_per_sm": s[3],
                 "grid": g.value, "smem": m.value}
 
     def query_host(self, program: "Program", segments: Sequence[dict], capacity: Optional[int] = None):
@@ -289,8 +295,8 @@ class Batch:
         s = (ctypes.c_uint * 4)()
         w = ctypes.c_uint64()
         check(lib().virg_gpu_batch_shape(self.h, s, ctypes.byref(w)), "batch shape")
-        return {"threads": s[0], "rows_per_thread": s[1], "stages": s[2], "grid": s[3],
-                "tiles": w.value}
+        return {"threads": s[0], "stage_kb": s[1], "stages": s[2], "grid": s[3],
+                "chunks": w.value}
 
     def close(self) -> None:
         if self.h:
@@ -357,7 +363,7 @@ class Serve:
         return {"sessions": c.sessions, "admitted": c.admitted, "readmitted": c.readmitted,
                 "pending": c.pending, "inflight": c.inflight, "arena_used": c.arena_used,
                 "device_error": c.device_error,
-                "shape": {"threads": c.shape[0], "rows_per_thread": c.shape[1], "stages": c.shape[2],
+                "shape": {"threads": c.shape[0], "stage_kb": c.shape[1], "stages": c.shape[2],
                           "grid": c.shape[3]}}
 
     def close(self) -> None:
@@ -385,4 +391,4 @@ def tune(engine: Engine, program: Program, table: Table) -> Dict[str, int]:
     """Times the launch shapes for this query and caches the fastest."""
     s = (ctypes.c_uint * 4)()
     check(lib().virg_gpu_query_tune(engine.h, program.h, table.h, s), "query tune")
-    return {"threads": s[0], "rows_per_thread": s[1], "stages": s[2]}
+    return {"threads": s[0], "stage_kb": s[1], "stages": s[2], "ctas_per_sm": s[3]}

@@ -4,15 +4,16 @@
  *
  * The reference runs one query at a time: one launch sequence per data
  * tablet with a blocking copy of its result count after each
- * (src/vm/vm_gpu.cu:474-565).  A batch numbers the tiles of all its queries
- * into one work list; persistent CTAs claim tiles in order, so small and
+ * (src/vm/vm_gpu.cu:474-565).  A batch numbers the chunks of all its queries
+ * into one work list; persistent CTAs claim chunks in order, so small and
  * large tables share the machine and a query's ordered look-back chain only
- * waits on that query's earlier tiles.  A batch owns its descriptors,
+ * waits on that query's earlier chunks.  A batch owns its descriptors,
  * look-back words, work counter and result counters, so its launch (counter
  * and status reset, kernel, count read-back) can be captured once in a CUDA
- * graph and replayed.  The launch shape (CTA width, rows per thread, staging
- * depth) can be tuned by timing the candidates on the batch itself; the
- * winner is cached in the engine per program-shape key.
+ * graph and replayed.  The launch shape (compute warps, stage size and
+ * count, CTAs per SM, chunk size) can be tuned by timing the candidates on
+ * the batch itself; the winner is cached in the engine per program-shape
+ * key.
  */
 #include <algorithm>
 #include <cstdio>
@@ -130,7 +131,7 @@ int issue(virg_gpu_batch *b)
 		CUDA_OK(cudaMemsetAsync(b->d_status, 0, plan.work * sizeof(uint64_t), s), "batch status reset");
 		const KParams kp = plan_params(plan, b->d_blob, b->d_ctrl, b->d_status, b->d_ctrl + 1,
 			kBatchEpoch);
-		if (!launch_vm(plan.shape, kp, plan.grid, plan.smem, s))
+		if (!launch_vm(plan.geom.shape, kp, plan.grid, plan.geom.smem, s))
 			VGPU_FAIL("batch kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
 	}
 	CUDA_OK(cudaMemcpyAsync(b->h_totals, b->d_totals, b->items.size() * sizeof(unsigned long long),
@@ -144,8 +145,8 @@ int build_with(virg_gpu_batch *b, const Shape *forced)
 {
 	virg_gpu_engine *e = b->e;
 	std::vector<QueryLaunch> qs = launches_of(b);
-	size_t off_prefix, off_tiles;
-	const size_t bytes = plan_blob_bytes(qs, &off_prefix, &off_tiles);
+	size_t off_prefix, off_chunks;
+	const size_t bytes = plan_blob_bytes(qs, &off_prefix, &off_chunks);
 	if (!b->d_blob)
 		CUDA_OK(cudaMalloc((void **)&b->d_blob, bytes), "batch descriptor alloc");
 	Plan plan;
@@ -193,28 +194,24 @@ int autotune(virg_gpu_batch *b)
 	auto hit = e->tuned.find(key);
 	if (hit != e->tuned.end())
 		return build_with(b, &hit->second);
-	static const unsigned cand[][2] = {{128, 4}, {128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
-		{512, 8}};
 	float best = 1e30f;
-	Shape best_shape = {0, 0, 0, 0};
-	for (auto &c : cand)
-		for (unsigned st = 2; st <= 4; st++) {
-			Shape s = {c[0], c[1], st, 0};
-			set_error("%s", "");
-			if (!build_with(b, &s))
-				continue;  /* does not fit shared memory */
-			float t = 1e30f;
-			for (int rep = 0; rep < 3; rep++) {
-				float ms = time_once(b);
-				if (ms < 0)
-					VGPU_FAIL("autotune run failed");
-				t = std::min(t, ms);
-			}
-			if (t < best) {
-				best = t;
-				best_shape = s;
-			}
+	Shape best_shape = {0, 0, 0, 0, 0, 0};
+	for (const Shape &c : tune_candidates()) {
+		set_error("%s", "");
+		if (!build_with(b, &c))
+			continue;  /* does not fit shared memory */
+		float t = 1e30f;
+		for (int rep = 0; rep < 3; rep++) {
+			float ms = time_once(b);
+			if (ms < 0)
+				VGPU_FAIL("autotune run failed");
+			t = std::min(t, ms);
 		}
+		if (t < best) {
+			best = t;
+			best_shape = b->plan.geom.shape;
+		}
+	}
 	VGPU_CHECK(best_shape.threads != 0, "no launch shape fits this batch");
 	e->tuned[key] = best_shape;
 	return build_with(b, &best_shape);
@@ -321,9 +318,9 @@ extern "C" int virg_gpu_batch_run(virg_gpu_batch *b, int use_graph)
 	}
 	CUDA_OK(cudaEventRecord(b->done, s), "batch event record");
 	e->launches += b->plan.work ? 1 : 0;
-	e->last_shape = b->plan.shape;
+	e->last_shape = b->plan.geom.shape;
 	e->last_grid = b->plan.grid;
-	e->last_smem = b->plan.smem;
+	e->last_smem = b->plan.geom.smem;
 	b->ran = true;
 	return 1;
 }
@@ -371,9 +368,9 @@ extern "C" int virg_gpu_batch_shape(const virg_gpu_batch *b, unsigned *shape4, u
 {
 	VGPU_CHECK(b != nullptr && b->built, "batch not built");
 	if (shape4) {
-		shape4[0] = b->plan.shape.threads;
-		shape4[1] = b->plan.shape.rows_per_thread;
-		shape4[2] = b->plan.shape.stages;
+		shape4[0] = b->plan.geom.shape.threads;
+		shape4[1] = b->plan.geom.shape.stage_kb;
+		shape4[2] = b->plan.geom.shape.stages;
 		shape4[3] = b->plan.grid;
 	}
 	if (work)

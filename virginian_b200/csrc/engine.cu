@@ -49,120 +49,6 @@ static int type_bytes(int t)
 			VGPU_FAIL("%s: %s", what, cudaGetErrorString(e_));                      \
 	} while (0)
 
-/* smem bytes a program needs per stage and for its register vectors.
- * Vectors indexed by tile row (written by the filter) get kSlots slots, one
- * per tile in flight between filter and stores; vectors indexed by
- * selection position (written and read only by the projection warps) get
- * one.  The vector region of a launch is [row slots | selection vectors],
- * sized for the largest of its programs, so that one query's row slot never
- * overlaps another's selection vectors. */
-void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
-	uint32_t *row_bytes, uint32_t *sel_bytes)
-{
-	/* a stage: query descriptor + tile info header, then the columns */
-	uint32_t off = kStageHdr;
-	for (unsigned i = 0; i < P.nload; i++) {
-		if (load_off)
-			load_off[i] = off;
-		off += (uint32_t)align_up((size_t)tile * P.load_stride[i], 128);
-	}
-	*stage_bytes = off;
-	uint32_t row = 0, sel = 0;
-	for (unsigned i = 0; i < P.nvec; i++) {
-		const uint32_t sz = (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
-		if (P.vec_compact[i])
-			sel += sz;
-		else
-			row += sz;
-	}
-	*row_bytes = row;
-	*sel_bytes = sel;
-}
-
-/* offsets of a program's vectors in a launch's vector region whose row slots
- * are row_slot bytes apart */
-void vec_offsets(const Program &P, unsigned tile, uint32_t row_slot, uint32_t *vec_off)
-{
-	uint32_t r = 0, s = kSlots * row_slot;
-	for (unsigned i = 0; i < P.nvec; i++) {
-		const uint32_t sz = (uint32_t)align_up((size_t)tile * P.vec_stride[i], 128);
-		if (P.vec_compact[i]) {
-			vec_off[i] = s;
-			s += sz;
-		} else {
-			vec_off[i] = r;
-			r += sz;
-		}
-	}
-}
-
-/* stage bytes, row-slot bytes and vector-region bytes of a launch */
-void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uint32_t *stage_bytes,
-	uint32_t *row_slot, uint32_t *vec_bytes)
-{
-	uint32_t stage = 0, row = 0, sel = 0;
-	for (const Program *P : progs) {
-		uint32_t sb, rb, vb;
-		program_layout(*P, tile, nullptr, &sb, &rb, &vb);
-		stage = std::max(stage, sb);
-		row = std::max(row, rb);
-		sel = std::max(sel, vb);
-	}
-	*stage_bytes = (uint32_t)align_up(std::max<uint32_t>(stage, 128), 128);
-	*row_slot = row;
-	*vec_bytes = kSlots * row + sel;
-}
-
-/* header | stages x stage bytes | register vectors | selection lists */
-size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes)
-{
-	/* a selection list (a tile row per selected row) per slot: a tile's list
-	 * is built while earlier tiles' are projected */
-	return kSmemHeader + (size_t)s.stages * stage_bytes + (size_t)vec_bytes +
-		kSlots * align_up((size_t)s.tile() * sizeof(uint16_t), 128);
-}
-
-int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, Shape *out,
-	size_t *smem_out, uint32_t *stage_out, uint32_t *vec_out)
-{
-	/* first choice: one CTA per SM with 2048-row tiles and three stages (a
-	 * tile's fixed costs - claim, look-back, barriers - spread over many
-	 * rows, and loads in flight while two tiles are processed); then
-	 * smaller tiles for programs whose staging does not fit */
-	static const unsigned cand[][2] = {{512, 4}, {256, 8}, {256, 4}, {128, 8}};
-	const size_t limit = (size_t)e->smem_optin;
-	for (int pass = 1; pass < 2; pass++)
-	for (auto &c : cand) {
-		Shape s;
-		s.threads = e->pref.threads ? e->pref.threads : c[0];
-		s.rows_per_thread = e->pref.rows_per_thread ? e->pref.rows_per_thread : c[1];
-		if (!shape_supported(s))
-			VGPU_FAIL("unsupported launch shape %u threads x %u rows", s.threads, s.rows_per_thread);
-		uint32_t stage, row_slot, vec;
-		launch_layout(progs, s.tile(), &stage, &row_slot, &vec);
-		/* a requested stage count is kept, at one CTA per SM if need be */
-		const unsigned st_list[] = {e->pref.stages ? e->pref.stages : 3u, e->pref.stages ? 0u : 2u};
-		for (unsigned st : st_list) {
-			if (st == 0)
-				continue;
-			s.stages = std::min(st, kMaxStages);
-			size_t smem = smem_for(s, stage, vec);
-			/* 1 KB of the SM's shared memory is reserved per resident CTA */
-			if (smem <= (pass == 0 ? limit / 2 - 1024 : limit)) {
-				s.ctas_per_sm = e->pref.ctas_per_sm;
-				*out = s;
-				*smem_out = smem;
-				*stage_out = stage;
-				*vec_out = vec;
-				return 1;
-			}
-		}
-		if (e->pref.threads || e->pref.rows_per_thread)
-			break;
-	}
-	VGPU_FAIL("program needs more shared memory than the device offers");
-}
-
 static int ensure_status(virg_gpu_engine *e, size_t n)
 {
 	if (n <= e->status_cap)
@@ -188,6 +74,140 @@ static int ensure_blob(virg_gpu_engine *e, size_t n)
 	return 1;
 }
 
+/* ---- launch planning --------------------------------------------------- */
+
+/* The staging plan of a program, independent of the launch geometry.  The
+ * count phase stages the columns the filter uops read; the full phase the
+ * columns the projection uops and result columns read.  If the projection
+ * or a result column touches a register vector the filter wrote (a
+ * register indexed by block row), the full phase runs the filter again and
+ * stages every column the program reads. */
+/* which operand fields a uop reads, and whether it writes its destination */
+static bool uses_a(const UOp &u)
+{
+	return u.kind == UK_CMP || u.kind == UK_NOT || u.kind == UK_MATH || u.kind == UK_SETCONST ||
+		u.kind == UK_COPYCOL;
+}
+static bool uses_b(const UOp &u) { return u.kind == UK_CMP || u.kind == UK_MATH; }
+static bool writes_d(const UOp &u) { return u.kind == UK_MATH || u.kind == UK_SETCONST || u.kind == UK_COPYCOL; }
+
+void plan_program(const Program &P, ProgPlan &pp, bool allow_gather)
+{
+	memset(&pp, 0, sizeof(pp));
+	bool in_count[kMaxLoads] = {false}, in_proj[kMaxLoads] = {false};
+	bool refilter = false;
+	const uint32_t nproj_end = P.nuops ? P.nuops - 1 : 0;
+	auto col_of = [&](uint8_t cls, uint8_t idx, bool *set) {
+		if (cls == OC_COL)
+			set[idx] = true;
+	};
+	auto rowvec = [&](uint8_t cls, uint8_t idx) { return cls == OC_VEC && !P.vec_compact[idx]; };
+	for (uint32_t k = 0; k < P.nfilter; k++) {
+		const UOp &u = P.uops[k];
+		if (uses_a(u))
+			col_of(u.a_cls, u.a_idx, in_count);
+		if (uses_b(u))
+			col_of(u.b_cls, u.b_idx, in_count);
+	}
+	for (uint32_t k = P.nfilter; k < nproj_end; k++) {
+		const UOp &u = P.uops[k];
+		if (uses_a(u))
+			col_of(u.a_cls, u.a_idx, in_proj);
+		if (uses_b(u))
+			col_of(u.b_cls, u.b_idx, in_proj);
+		if ((uses_a(u) && rowvec(u.a_cls, u.a_idx)) || (uses_b(u) && rowvec(u.b_cls, u.b_idx)) ||
+			(writes_d(u) && !P.vec_compact[u.dst]))
+			refilter = true;
+	}
+	for (uint32_t j = 0; j < P.nout; j++) {
+		col_of(P.out_cls[j], P.out_idx[j], in_proj);
+		if (rowvec(P.out_cls[j], P.out_idx[j]))
+			refilter = true;
+	}
+	pp.mode = refilter ? FM_REFILTER : FM_BITMAP;
+	for (uint32_t i = 0; i < P.nload; i++) {
+		if (in_count[i]) {
+			pp.count_cols[pp.ncount++] = (uint8_t)i;
+			pp.count_bpr += P.load_stride[i];
+		}
+		if (in_proj[i] || (refilter && in_count[i])) {
+			pp.full_cols[pp.nfull++] = (uint8_t)i;
+			pp.full_bpr += P.load_stride[i];
+		}
+	}
+	/* the full phase gathers the selected rows' values unless they are
+	 * many bytes per row */
+	if (allow_gather && pp.mode == FM_BITMAP && pp.full_bpr <= kGatherMaxBpr) {
+		pp.mode = FM_GATHER;
+		pp.gather_bpr = pp.full_bpr;
+	}
+	/* selection vectors hold a projection batch's entries, row vectors a
+	 * count group's rows */
+	uint32_t sel = 0, row = 0;
+	for (uint32_t i = 0; i < P.nvec; i++) {
+		if (P.vec_compact[i]) {
+			pp.vec_off[i] = sel;
+			sel += 32u * kBatchE * P.vec_stride[i];
+		} else {
+			pp.vec_off[i] = row;
+			row += kCountGroup * kBlockRows * P.vec_stride[i];
+		}
+		(P.vec_compact[i] ? pp.sel_bpr : pp.row_bpr) += P.vec_stride[i];
+	}
+}
+
+/* the launch geometry of a shape whose compute warps hold sel_bpr and
+ * row_bpr bytes of vectors per row; stages == 0 takes as many stages as fit
+ * the shared memory left per CTA */
+int geom_make(const Shape &s0, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gather_bpr, int smem_block, int smem_sm,
+	Geom *g)
+{
+	Shape s = s0;
+	VGPU_CHECK(shape_supported(s), "unsupported launch shape: %u compute threads", s.threads);
+	VGPU_CHECK(s.stage_kb >= 1 && s.stage_kb <= 192, "stage size %u KB out of range", s.stage_kb);
+	g->wl = warp_layout(sel_bpr, row_bpr, gather_bpr);
+	g->stage_area = (uint32_t)align_up(kWarpArea + (size_t)s.warps() * g->wl.bytes, 128);
+	const unsigned ctas = s.ctas_per_sm ? s.ctas_per_sm : 1;
+	/* 1 KB of an SM's shared memory is reserved per resident CTA */
+	const size_t budget = std::min<size_t>((size_t)smem_block, (size_t)smem_sm / ctas - 1024);
+	if (budget <= g->stage_area)
+		return 0;
+	const size_t fit = (budget - g->stage_area) / s.stage_bytes();
+	if (s.stages == 0)
+		s.stages = (unsigned)std::min<size_t>(fit, kMaxStages);
+	if (s.stages < 2 || s.stages > kMaxStages || s.stages > fit)
+		return 0;
+	g->shape = s;
+	g->smem = g->stage_area + (size_t)s.stages * s.stage_bytes();
+	return 1;
+}
+
+/* a phase's staged columns for tiles of `rows` rows */
+static void load_set(LoadSet &ls, const Program &P, const uint8_t *cols, uint32_t n, uint32_t rows)
+{
+	memset(&ls, 0, sizeof(ls));
+	ls.n = n;
+	ls.rows = rows;
+	uint32_t off = 0;
+	for (uint32_t i = 0; i < n; i++) {
+		const uint32_t slot = cols[i];
+		ls.src[i] = P.load_src[slot];
+		ls.stride[i] = P.load_stride[slot];
+		ls.off[i] = off;
+		ls.bytes_per_row += P.load_stride[slot];
+		off += (uint32_t)align_up((size_t)rows * P.load_stride[slot], 128);
+	}
+}
+
+/* tile rows of a phase staging bpr bytes per row in a stage of `stage`
+ * bytes (whole blocks, at most `cap` rows); 0 if not one block fits */
+static uint32_t tile_rows(uint32_t bpr, uint32_t stage, uint32_t cap)
+{
+	if (bpr == 0)
+		return cap;
+	return std::min<uint32_t>(cap, stage / bpr / kBlockRows * kBlockRows);
+}
+
 /* the head word of a uop's record (one-hot kind, type and operator) */
 static uint32_t op_head(const UOp &u)
 {
@@ -207,12 +227,39 @@ static uint32_t op_head(const UOp &u)
 		((u.flags & UF_SINGLE_DEF) ? OPH_SINGLE_DEF : 0u) | ((uint32_t)u.join << OPH_JOIN_SHIFT);
 }
 
-/* operand descriptors of a query descriptor whose program, load_off and
- * vec_off are set, for register vectors starting at vec_area */
-void fill_operands(QDesc &d, uint32_t vec_area)
+int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uint32_t chunk_cap)
 {
-	const Program &P = d.prog;
-	/* the kernel's view of the program, in the staged prefix */
+	const uint32_t stage = g.shape.stage_bytes();
+	chunk_cap = std::max<uint32_t>(kBlockRows, std::min<uint32_t>(chunk_cap, kMaxChunkRows) / kBlockRows * kBlockRows);
+	const uint32_t tf = tile_rows(pp.full_bpr, stage, chunk_cap);
+	VGPU_CHECK(tf >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the results read",
+		g.shape.stage_kb, kBlockRows, pp.full_bpr);
+	const uint32_t chunk = std::max(tf, chunk_cap / tf * tf);
+	const uint32_t tc = tile_rows(pp.count_bpr, stage, chunk);
+	VGPU_CHECK(tc >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the filter reads",
+		g.shape.stage_kb, kBlockRows, pp.count_bpr);
+	d.prog = P;
+	load_set(d.count_set, P, pp.count_cols, pp.ncount, tc);
+	if (pp.mode == FM_GATHER) {
+		/* one full entry per chunk; the staged columns of a batch are its
+		 * 32 kBatchE gathered entries, in the warp's gather area */
+		const uint32_t gchunk = chunk_cap;
+		load_set(d.full_set, P, pp.full_cols, pp.nfull, 32u * kBatchE);
+		d.full_set.rows = gchunk;
+		d.chunk_rows = gchunk;
+		load_set(d.count_set, P, pp.count_cols, pp.ncount, tile_rows(pp.count_bpr, stage, gchunk));
+		VGPU_CHECK(d.count_set.rows >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the filter reads",
+			g.shape.stage_kb, kBlockRows, pp.count_bpr);
+		d.gather_n = d.full_set.n;
+		for (uint32_t i = 0; i < d.full_set.n; i++) {
+			d.gather_stride[i] = d.full_set.stride[i];
+			d.gather_off[i] = d.full_set.off[i];
+		}
+	} else {
+		load_set(d.full_set, P, pp.full_cols, pp.nfull, tf);
+		d.chunk_rows = chunk;
+	}
+	d.full_mode = pp.mode;
 	for (unsigned i = 0; i < kMaxRegs; i++) {
 		d.consts[i] = P.consts[i];
 		d.out_stride[i] = P.out_stride[i];
@@ -220,119 +267,212 @@ void fill_operands(QDesc &d, uint32_t vec_area)
 	d.nfilter = P.nfilter;
 	d.nuops = P.nuops;
 	d.nout = P.nout;
-	auto od = [&](uint8_t cls, uint8_t idx) -> uint32_t {
-		if (cls == OC_COL)
-			return OD_STAGE | (uint32_t)(kSmemHeader + d.load_off[idx]);
+	/* operand descriptors over one phase's layout (bad: a column the phase
+	 * does not stage, never read in that phase) */
+	auto od = [&](uint8_t cls, uint8_t idx, const LoadSet &ls, const uint8_t *cols, uint32_t n, bool *bad) -> uint32_t {
+		if (cls == OC_COL) {
+			for (uint32_t i = 0; i < n; i++)
+				if (cols[i] == idx)
+					return OD_STAGE | ls.off[i];
+			*bad = true;
+			return OD_STAGE;
+		}
 		if (cls == OC_VEC)
-			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | (vec_area + d.vec_off[idx]);
-		/* scalars are read from the stage's copy of the descriptor */
-		return OD_SCALAR |
-			(uint32_t)(kSmemHeader + offsetof(QDesc, consts) + idx * 8u);
+			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | pp.vec_off[idx];
+		return OD_SCALAR | (uint32_t)(offsetof(QDesc, consts) + idx * 8u);
 	};
-	for (uint32_t k = 0; k < P.nuops; k++) {
-		const UOp &u = P.uops[k];
-		OpRec &r = d.ops[k];
+	/* a record over one phase's layout; operand fields the uop does not use
+	 * stay 0 */
+	auto rec = [&](const UOp &u, const LoadSet &ls, const uint8_t *cols, uint32_t n, bool *bad) {
+		OpRec r;
 		r.head = op_head(u);
-		r.a = od(u.a_cls, u.a_idx);
-		r.b = od(u.b_cls, u.b_idx);
-		r.d = od(OC_VEC, u.dst);
+		r.a = uses_a(u) ? od(u.a_cls, u.a_idx, ls, cols, n, bad) : 0u;
+		r.b = uses_b(u) ? od(u.b_cls, u.b_idx, ls, cols, n, bad) : 0u;
+		r.d = writes_d(u) ? od(OC_VEC, u.dst, ls, cols, n, bad) : 0u;
+		return r;
+	};
+	bool bad = false;
+	for (uint32_t k = 0; k < P.nfilter; k++)
+		d.ops_count[k] = rec(P.uops[k], d.count_set, pp.count_cols, pp.ncount, &bad);
+	VGPU_CHECK(!bad, "internal: a filter operand is not staged in the count phase");
+	for (uint32_t k = 0; k < P.nuops; k++) {
+		/* the full phase runs filter uops only when it runs the filter again */
+		if (k < P.nfilter && pp.mode != FM_REFILTER) {
+			d.ops_full[k] = OpRec{op_head(P.uops[k]), 0u, 0u, 0u};
+			continue;
+		}
+		d.ops_full[k] = rec(P.uops[k], d.full_set, pp.full_cols, pp.nfull, &bad);
 	}
 	for (uint32_t j = 0; j < P.nout; j++)
-		d.od_out[j] = od(P.out_cls[j], P.out_idx[j]);
+		d.od_out[j] = od(P.out_cls[j], P.out_idx[j], d.full_set, pp.full_cols, pp.nfull, &bad);
+	VGPU_CHECK(!bad, "internal: a result operand is not staged in the full phase");
+	return 1;
 }
 
-size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles)
+uint64_t chunk_prefix(const uint32_t *seg_rows, uint32_t nsegs, uint32_t chunk_rows, uint32_t *pre)
+{
+	uint64_t t = 0;
+	for (uint32_t s = 0; s < nsegs; s++) {
+		if (pre)
+			pre[s] = (uint32_t)t;
+		t += (seg_rows[s] + chunk_rows - 1) / chunk_rows;
+	}
+	if (pre)
+		pre[nsegs] = (uint32_t)t;
+	return t;
+}
+
+KParams geom_params(const Geom &g)
+{
+	KParams kp;
+	kp.queries = nullptr;
+	kp.q_work_prefix = nullptr;
+	kp.nq = 0;
+	kp.total_work = 0;
+	kp.counter = nullptr;
+	kp.status = nullptr;
+	kp.error = nullptr;
+	kp.epoch = 1;
+	kp.nstages = g.shape.stages;
+	kp.stage_bytes = g.shape.stage_bytes();
+	kp.stage_area = g.stage_area;
+	kp.warp_bytes = g.wl.bytes;
+	kp.sel_off = g.wl.sel_off;
+	kp.gat_off = g.wl.gat_off;
+	kp.row_off = g.wl.row_off;
+	return kp;
+}
+
+/* the widest vector areas and staging of a launch's programs */
+static void launch_needs(const std::vector<QueryLaunch> &qs, bool allow_gather, uint32_t *sel, uint32_t *row,
+	uint32_t *gat, uint32_t *bpr)
+{
+	*sel = *row = *gat = *bpr = 0;
+	for (const QueryLaunch &q : qs) {
+		ProgPlan pp;
+		plan_program(*q.prog, pp, allow_gather);
+		*sel = std::max(*sel, pp.sel_bpr);
+		*row = std::max(*row, pp.row_bpr);
+		*gat = std::max(*gat, pp.gather_bpr);
+		*bpr = std::max({*bpr, pp.count_bpr, pp.mode == FM_GATHER ? 0u : pp.full_bpr});
+	}
+}
+
+int choose_shape(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, Geom *g)
+{
+	uint32_t sel, row, gat, bpr;
+	launch_needs(qs, !e->pref.staged_full, &sel, &row, &gat, &bpr);
+	Shape s;
+	s.staged_full = e->pref.staged_full;
+	s.threads = e->pref.threads ? e->pref.threads : 256;
+	s.stage_kb = e->pref.stage_kb ? e->pref.stage_kb : 32;
+	s.stages = e->pref.stages;
+	s.ctas_per_sm = e->pref.ctas_per_sm;
+	s.chunk_rows = e->pref.chunk_rows;
+	/* a stage holds at least one block of the widest phase */
+	if (!e->pref.stage_kb)
+		s.stage_kb = std::max<unsigned>(s.stage_kb, (kBlockRows * bpr + 1023) / 1024);
+	if (geom_make(s, sel, row, gat, e->smem_optin, e->smem_sm, g))
+		return 1;
+	VGPU_FAIL("launch shape (%u threads, %u KB x %u stages, %u CTAs per SM) does not fit shared memory",
+		s.threads, s.stage_kb, s.stages, s.ctas_per_sm);
+}
+
+size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_chunks)
 {
 	const size_t nq = qs.size();
 	*off_prefix = align_up(nq * sizeof(QDesc), 16);
-	*off_tiles = align_up(*off_prefix + (nq + 1) * sizeof(uint64_t), 16);
+	*off_chunks = align_up(*off_prefix + (nq + 1) * sizeof(uint64_t), 16);
 	size_t words = 0;
 	for (const QueryLaunch &q : qs)
 		words += q.nsegs + 1;
-	return *off_tiles + words * sizeof(uint32_t);
+	return *off_chunks + words * sizeof(uint32_t);
 }
 
-/* descriptor blob: QDesc[nq] | q_work_prefix[nq+1] | seg_tile_prefix...,
+/* the automatic chunk bound: 4096 rows, smaller (down to 1024) when the
+ * launch has too few rows to give every CTA a few chunks */
+static uint32_t auto_chunk(uint64_t rows, unsigned ctas)
+{
+	const uint64_t want = rows / (4ull * std::max(ctas, 1u));
+	return (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(4096, want / kBlockRows * kBlockRows));
+}
+
+/* descriptor blob: QDesc[nq] | q_work_prefix[nq+1] | seg_chunk_prefix...,
  * built in host memory with pointers into the device copy at `db` */
 int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Shape *forced,
 	unsigned char *db, Plan &plan)
 {
 	VGPU_CHECK(!qs.empty(), "no queries");
-	std::vector<const Program *> progs;
-	for (const QueryLaunch &q : qs)
-		progs.push_back(q.prog);
 	if (forced) {
-		plan.shape = *forced;
-		uint32_t forced_slot;
-		launch_layout(progs, forced->tile(), &plan.stage_bytes, &forced_slot, &plan.vec_bytes);
-		plan.smem = smem_for(plan.shape, plan.stage_bytes, plan.vec_bytes);
-		VGPU_CHECK(plan.smem <= (size_t)e->smem_optin, "shape does not fit shared memory");
-	} else if (!choose_shape(e, progs, &plan.shape, &plan.smem, &plan.stage_bytes, &plan.vec_bytes)) {
+		uint32_t sel, row, gat, bpr;
+		launch_needs(qs, !forced->staged_full, &sel, &row, &gat, &bpr);
+		VGPU_CHECK(geom_make(*forced, sel, row, gat, e->smem_optin, e->smem_sm, &plan.geom),
+			"shape does not fit shared memory");
+	} else if (!choose_shape(e, qs, &plan.geom)) {
 		return 0;
 	}
-	const unsigned tile = plan.shape.tile();
+	const Geom &g = plan.geom;
+	/* resident CTAs per SM: the shape's request, capped by what its shared
+	 * memory and registers allow */
+	int per_sm = 0;
+	if (!occupancy(g.shape, g.smem, &per_sm))
+		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+	if (g.shape.ctas_per_sm)
+		per_sm = std::min(per_sm, (int)g.shape.ctas_per_sm);
+	per_sm = std::max(per_sm, 1);
+	const unsigned slots = (unsigned)per_sm * (unsigned)e->nsm;
+	uint64_t all_rows = 0;
+	for (const QueryLaunch &q : qs)
+		for (uint32_t s = 0; s < q.nsegs; s++)
+			all_rows += q.seg_rows[s];
+	const uint32_t cap = g.shape.chunk_rows ? g.shape.chunk_rows : auto_chunk(all_rows, slots);
+
 	const size_t nq = qs.size();
-	uint32_t stage_all, row_slot, vec_all;
-	launch_layout(progs, tile, &stage_all, &row_slot, &vec_all);
-	size_t off_prefix, off_tiles;
-	const size_t blob_bytes = plan_blob_bytes(qs, &off_prefix, &off_tiles);
+	size_t off_prefix, off_chunks;
+	const size_t blob_bytes = plan_blob_bytes(qs, &off_prefix, &off_chunks);
 	plan.blob.assign(blob_bytes, 0);
 	plan.off_prefix = off_prefix;
 	unsigned char *hb = plan.blob.data();
 	QDesc *hq = reinterpret_cast<QDesc *>(hb);
 	uint64_t *hprefix = reinterpret_cast<uint64_t *>(hb + off_prefix);
-	uint32_t *htiles = reinterpret_cast<uint32_t *>(hb + off_tiles);
+	uint32_t *hchunks = reinterpret_cast<uint32_t *>(hb + off_chunks);
 	uint64_t work = 0;
-	size_t tw = 0;
+	size_t cw = 0;
 	for (size_t i = 0; i < nq; i++) {
 		const QueryLaunch &q = qs[i];
 		QDesc &d = hq[i];
-		d.prog = *q.prog;
-		uint32_t sb, rb, vb;
-		program_layout(*q.prog, tile, d.load_off, &sb, &rb, &vb);
-		vec_offsets(*q.prog, tile, row_slot, d.vec_off);
-		d.vec_slot = row_slot;
-		d.stage_bytes = sb;
+		ProgPlan pp;
+		plan_program(*q.prog, pp, !g.shape.staged_full);
+		if (!desc_fill(d, *q.prog, pp, g, cap))
+			return 0;
 		d.segs = q.d_segs;
 		d.nsegs = q.nsegs;
-		d.seg_tile_prefix = reinterpret_cast<const uint32_t *>(db + off_tiles + tw * sizeof(uint32_t));
-		uint32_t *pre = htiles + tw;
-		uint64_t t = 0;
-		for (uint32_t s = 0; s < q.nsegs; s++) {
-			pre[s] = (uint32_t)t;
-			t += (q.seg_rows[s] + tile - 1) / tile;
-		}
-		pre[q.nsegs] = (uint32_t)t;
-		tw += q.nsegs + 1;
+		d.seg_chunk_prefix = reinterpret_cast<const uint32_t *>(db + off_chunks + cw * sizeof(uint32_t));
+		const uint64_t nch = chunk_prefix(q.seg_rows, q.nsegs, d.chunk_rows, hchunks + cw);
+		cw += q.nsegs + 1;
 		d.work_first = work;
-		d.ntiles = t;
+		d.nchunks = nch;
 		hprefix[i] = work;
-		work += t;
+		work += nch;
 		for (unsigned j = 0; j < q.prog->nout; j++)
 			d.out_ptr[j] = q.out[j];
 		d.capacity = q.capacity;
 		d.total_out = q.d_total;
 		d.block_counts = q.block_counts;
 		d.base_in = q.base_in;
-		fill_operands(d, (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes));
 	}
 	hprefix[nq] = work;
-	VGPU_CHECK(work < 0xFFFFFFF0ull, "too many tiles in one launch (%llu)", (unsigned long long)work);
+	VGPU_CHECK(work < 0xFFFFFFF0ull, "too many chunks in one launch (%llu)", (unsigned long long)work);
 	plan.work = work;
 	plan.nq = (uint32_t)nq;
-
-	int per_sm = (int)plan.shape.ctas_per_sm;
-	if (per_sm == 0 && !occupancy(plan.shape, plan.smem, &per_sm))
-		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
-	per_sm = std::max(per_sm, 1);
-	plan.grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(work, 1), (uint64_t)per_sm * e->nsm);
+	plan.grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(work, 1), slots);
 	return 1;
 }
 
 KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter, uint64_t *status,
 	unsigned *error, uint32_t epoch)
 {
-	KParams kp;
+	KParams kp = geom_params(plan.geom);
 	kp.queries = reinterpret_cast<const QDesc *>(db);
 	kp.q_work_prefix = reinterpret_cast<const uint64_t *>(db + plan.off_prefix);
 	kp.nq = plan.nq;
@@ -341,33 +481,25 @@ KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter
 	kp.status = status;
 	kp.error = error;
 	kp.epoch = epoch;
-	kp.nstages = plan.shape.stages;
-	kp.stage_bytes = plan.stage_bytes;
-	kp.stage_area = kSmemHeader;
-	kp.vec_area = (uint32_t)(kSmemHeader + (size_t)plan.shape.stages * plan.stage_bytes);
-	kp.vec_bytes = plan.vec_bytes;
-	kp.sel_area = kp.vec_area + plan.vec_bytes;
 	return kp;
 }
 
 /* the key a tuned launch shape is cached under: the largest per-row staging
- * and register-vector bytes and program length of the launch's queries, the
- * number of queries and the size class of the rows they scan */
+ * of a phase and register-vector bytes, program length and result columns
+ * of the launch's queries, the number of queries and the size class of the
+ * rows they scan */
 std::string shape_key(const std::vector<QueryLaunch> &qs)
 {
-	unsigned ld = 0, vec = 0, nuops = 0, nout = 0;
+	unsigned cb = 0, fb = 0, vec = 0, nuops = 0, nout = 0;
 	uint64_t rows = 0;
 	for (const QueryLaunch &q : qs) {
-		const Program &P = *q.prog;
-		unsigned l = 0, v = 0;
-		for (unsigned i = 0; i < P.nload; i++)
-			l += P.load_stride[i];
-		for (unsigned i = 0; i < P.nvec; i++)
-			v += P.vec_stride[i];
-		ld = std::max(ld, l);
-		vec = std::max(vec, v);
-		nuops = std::max(nuops, P.nuops);
-		nout = std::max(nout, P.nout);
+		ProgPlan pp;
+		plan_program(*q.prog, pp);
+		cb = std::max(cb, pp.count_bpr);
+		fb = std::max(fb, pp.full_bpr);
+		vec = std::max(vec, pp.sel_bpr + pp.row_bpr);
+		nuops = std::max(nuops, q.prog->nuops);
+		nout = std::max(nout, q.prog->nout);
 		for (uint32_t s = 0; s < q.nsegs; s++)
 			rows += q.seg_rows[s];
 	}
@@ -375,14 +507,14 @@ std::string shape_key(const std::vector<QueryLaunch> &qs)
 	while ((1ull << size_class) < rows && size_class < 63)
 		size_class++;
 	char buf[96];
-	snprintf(buf, sizeof(buf), "l%u-v%u-u%u-o%u-q%zu-r%u", ld, vec, nuops, nout, qs.size(), size_class);
+	snprintf(buf, sizeof(buf), "c%u-f%u-v%u-u%u-o%u-q%zu-r%u", cb, fb, vec, nuops, nout, qs.size(), size_class);
 	return buf;
 }
 
 int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing)
 {
-	size_t off_prefix, off_tiles;
-	if (!ensure_blob(e, plan_blob_bytes(qs, &off_prefix, &off_tiles)))
+	size_t off_prefix, off_chunks;
+	if (!ensure_blob(e, plan_blob_bytes(qs, &off_prefix, &off_chunks)))
 		return 0;
 	unsigned char *db = static_cast<unsigned char *>(e->blob);
 	Plan plan;
@@ -410,8 +542,8 @@ int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTi
 		"descriptor copy");
 	CUDA_OK(cudaMemsetAsync(e->ctrl, 0, sizeof(unsigned), e->stream), "counter reset");
 	const KParams kp = plan_params(plan, db, e->ctrl, e->status, e->ctrl + 1, e->epoch);
-	const Shape shape = plan.shape;
-	const size_t smem = plan.smem;
+	const Shape shape = plan.geom.shape;
+	const size_t smem = plan.geom.smem;
 	const unsigned grid = plan.grid;
 
 	if (timing && timing->start)
@@ -478,6 +610,7 @@ extern "C" int virg_gpu_engine_create(int device, virg_gpu_engine **out)
 	e->device = device;
 	e->nsm = prop.multiProcessorCount;
 	e->smem_optin = (int)prop.sharedMemPerBlockOptin;
+	e->smem_sm = (int)prop.sharedMemPerMultiprocessor;
 	if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
 		cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
 		cudaMalloc((void **)&e->ctrl, 64) != cudaSuccess || cudaMemset(e->ctrl, 0, 64) != cudaSuccess) {
@@ -564,44 +697,56 @@ extern "C" void virg_gpu_engine_destroy(virg_gpu_engine *e)
 
 extern "C" void *virg_gpu_engine_stream(virg_gpu_engine *e) { return e ? (void *)e->stream : nullptr; }
 
+/* the launch shapes the tuners try: compute warps, stage size, CTAs per SM
+ * and chunk bound (each with as many stages as fit) */
+namespace vgpu {
+std::vector<Shape> tune_candidates()
+{
+	std::vector<Shape> c;
+	for (unsigned threads : {256u, 512u})
+		for (unsigned kb : {16u, 24u, 32u, 48u})
+			for (unsigned chunk : {2048u, 4096u, 8192u})
+				c.push_back(Shape{threads, kb, 0, 1, chunk, 0});
+	for (unsigned kb : {24u, 48u})
+		c.push_back(Shape{256, kb, 0, 1, 8192, 1});
+	return c;
+}
+}  // namespace vgpu
+
 extern "C" int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p,
 	const virg_gpu_table *t, unsigned *shape4)
 {
 	VGPU_CHECK(e != nullptr && p != nullptr && t != nullptr, "null argument");
-	static const unsigned cand[][2] = {{128, 4}, {128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 16}, {512, 4},
-		{512, 8}};
 	cudaEvent_t a, z;
 	CUDA_OK(cudaEventCreate(&a), "event");
 	CUDA_OK(cudaEventCreate(&z), "event");
 	float best = 1e30f;
-	Shape best_shape = {0, 0, 0, 0};
-	std::string key;
-	for (auto &c : cand)
-		for (unsigned st = 2; st <= 4; st++) {
-			e->force = Shape{c[0], c[1], st, 0};
-			float t_best = 1e30f;
-			bool ran = true;
-			for (int rep = 0; rep < 3 && ran; rep++) {
-				virg_gpu_result *r = nullptr;
-				cudaEventRecord(a, e->stream);
-				if (!virg_gpu_query(e, p, t, &r)) {
-					ran = false;  /* shape does not fit this program */
-					break;
-				}
-				cudaEventRecord(z, e->stream);
-				uint64_t rows;
-				ran = virg_gpu_result_rows(r, &rows);
-				float ms = 0;
-				cudaEventElapsedTime(&ms, a, z);
-				virg_gpu_result_destroy(r);
-				t_best = std::min(t_best, ms);
+	Shape best_shape = {0, 0, 0, 0, 0, 0};
+	for (const Shape &c : tune_candidates()) {
+		e->force = c;
+		float t_best = 1e30f;
+		bool ran = true;
+		for (int rep = 0; rep < 3 && ran; rep++) {
+			virg_gpu_result *r = nullptr;
+			cudaEventRecord(a, e->stream);
+			if (!virg_gpu_query(e, p, t, &r)) {
+				ran = false;  /* shape does not fit this program */
+				break;
 			}
-			if (ran && t_best < best) {
-				best = t_best;
-				best_shape = e->force;
-			}
+			cudaEventRecord(z, e->stream);
+			uint64_t rows;
+			ran = virg_gpu_result_rows(r, &rows);
+			float ms = 0;
+			cudaEventElapsedTime(&ms, a, z);
+			virg_gpu_result_destroy(r);
+			t_best = std::min(t_best, ms);
 		}
-	e->force = Shape{0, 0, 0, 0};
+		if (ran && t_best < best) {
+			best = t_best;
+			best_shape = e->last_shape;
+		}
+	}
+	e->force = Shape{0, 0, 0, 0, 0, 0};
 	cudaEventDestroy(a);
 	cudaEventDestroy(z);
 	VGPU_CHECK(best_shape.threads != 0, "no launch shape fits this program");
@@ -613,9 +758,9 @@ extern "C" int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p
 	e->tuned[shape_key(std::vector<QueryLaunch>(1, q))] = best_shape;
 	if (shape4) {
 		shape4[0] = best_shape.threads;
-		shape4[1] = best_shape.rows_per_thread;
+		shape4[1] = best_shape.stage_kb;
 		shape4[2] = best_shape.stages;
-		shape4[3] = 0;
+		shape4[3] = best_shape.ctas_per_sm;
 	}
 	set_error("%s", "");
 	return 1;
@@ -633,20 +778,35 @@ extern "C" int virg_gpu_engine_check(virg_gpu_engine *e, unsigned *device_error)
 }
 
 extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
-	unsigned rows_per_thread, unsigned stages, unsigned ctas_per_sm)
+	unsigned stage_kb, unsigned stages, unsigned ctas_per_sm)
 {
 	VGPU_CHECK(e != nullptr, "null engine");
-	if (threads || rows_per_thread) {
-		Shape s;
-		s.threads = threads ? threads : 256;
-		s.rows_per_thread = rows_per_thread ? rows_per_thread : 4;
-		VGPU_CHECK(shape_supported(s), "unsupported shape %u x %u", s.threads, s.rows_per_thread);
+	if (threads) {
+		Shape s = {threads, 32, 2, 1, 0, 0};
+		VGPU_CHECK(shape_supported(s), "unsupported shape: %u compute threads (128, 256 or 512)", threads);
 	}
+	VGPU_CHECK(stage_kb <= 192, "stage size %u KB out of range", stage_kb);
 	VGPU_CHECK(stages <= kMaxStages, "at most %u stages", kMaxStages);
 	e->pref.threads = threads;
-	e->pref.rows_per_thread = rows_per_thread;
+	e->pref.stage_kb = stage_kb;
 	e->pref.stages = stages;
 	e->pref.ctas_per_sm = ctas_per_sm;
+	return 1;
+}
+
+extern "C" int virg_gpu_engine_set_staging(virg_gpu_engine *e, int staged_full)
+{
+	VGPU_CHECK(e != nullptr, "null engine");
+	e->pref.staged_full = staged_full ? 1u : 0u;
+	return 1;
+}
+
+extern "C" int virg_gpu_engine_set_chunk_rows(virg_gpu_engine *e, unsigned rows)
+{
+	VGPU_CHECK(e != nullptr, "null engine");
+	VGPU_CHECK(rows == 0 || (rows >= kBlockRows && rows <= kMaxChunkRows && rows % kBlockRows == 0),
+		"chunk rows must be 0 or a multiple of %u in [%u, %u]", kBlockRows, kBlockRows, kMaxChunkRows);
+	e->pref.chunk_rows = rows;
 	return 1;
 }
 
@@ -661,7 +821,7 @@ extern "C" int virg_gpu_engine_last_launch(virg_gpu_engine *e, unsigned *shape4,
 	VGPU_CHECK(e != nullptr, "null engine");
 	if (shape4) {
 		shape4[0] = e->last_shape.threads;
-		shape4[1] = e->last_shape.rows_per_thread;
+		shape4[1] = e->last_shape.stage_kb;
 		shape4[2] = e->last_shape.stages;
 		shape4[3] = e->last_shape.ctas_per_sm;
 	}

@@ -24,7 +24,8 @@ struct ScratchBuf {
 struct virg_gpu_engine {
 	int device = 0;
 	int nsm = 0;
-	int smem_optin = 0;
+	int smem_optin = 0;                  /* shared memory per CTA (opt-in limit) */
+	int smem_sm = 0;                     /* shared memory per SM */
 	cudaStream_t stream = nullptr;       /* launches, descriptor and result copies */
 	cudaStream_t copy_stream = nullptr;  /* streamed tablet uploads */
 	unsigned *ctrl = nullptr;            /* [0] work counter, [1] error word */
@@ -35,8 +36,8 @@ struct virg_gpu_engine {
 	size_t blob_cap = 0;
 	std::vector<unsigned char> host_blob;
 	std::map<int, vgpu::ScratchBuf> scratch;
-	vgpu::Shape pref = {0, 0, 0, 0};
-	vgpu::Shape last_shape = {0, 0, 0, 0};
+	vgpu::Shape pref = {0, 0, 0, 0, 0, 0};
+	vgpu::Shape last_shape = {0, 0, 0, 0, 0, 0};
 	unsigned last_grid = 0;
 	size_t last_smem = 0;
 	unsigned long long launches = 0;
@@ -48,7 +49,7 @@ struct virg_gpu_engine {
 	unsigned long long ring_count = 0;
 	/* launch shapes found by autotuning, per program-shape key */
 	std::map<std::string, vgpu::Shape> tuned;
-	vgpu::Shape force = {0, 0, 0, 0};  /* shape under trial while tuning */
+	vgpu::Shape force = {0, 0, 0, 0, 0, 0};  /* shape under trial while tuning */
 	std::mutex mu;
 };
 
@@ -102,26 +103,45 @@ struct LaunchTiming {
 	cudaEvent_t stop;
 };
 
+/* the staging plan of a program, independent of the launch geometry:
+ * which load slots each phase stages, how the full phase gets validity and
+ * where the program's register vectors sit in a compute warp's areas */
+struct ProgPlan {
+	uint8_t count_cols[kMaxLoads], full_cols[kMaxLoads];
+	uint32_t ncount, nfull;
+	uint32_t count_bpr, full_bpr;  /* staged bytes per row of each phase */
+	uint32_t mode;                 /* FM_GATHER, FM_BITMAP or FM_REFILTER */
+	uint32_t sel_bpr, row_bpr;     /* register-vector bytes per row */
+	uint32_t gather_bpr;           /* gathered bytes per row (FM_GATHER) */
+	uint32_t vec_off[kMaxRegs];    /* offset in the selection or row-vector area */
+};
+
+/* a launch geometry: its shape and the shared-memory layout that every
+ * query of the launch fits */
+struct Geom {
+	Shape shape;
+	WarpLayout wl;
+	uint32_t stage_area;
+	size_t smem;
+};
+
 /* a launch of one or more queries, ready to issue */
 struct Plan {
-	Shape shape;
-	size_t smem = 0;
-	uint32_t stage_bytes = 0, vec_bytes = 0;
+	Geom geom;
 	std::vector<unsigned char> blob;  /* host copy of the device descriptors */
 	size_t off_prefix = 0;
-	uint64_t work = 0;
+	uint64_t work = 0;                /* chunks */
 	uint32_t nq = 0;
 	unsigned grid = 0;
 };
 
-void program_layout(const Program &P, unsigned tile, uint32_t *load_off, uint32_t *stage_bytes,
-	uint32_t *row_bytes, uint32_t *sel_bytes);
-void vec_offsets(const Program &P, unsigned tile, uint32_t row_slot, uint32_t *vec_off);
-void launch_layout(const std::vector<const Program *> &progs, unsigned tile, uint32_t *stage_bytes,
-	uint32_t *row_slot, uint32_t *vec_bytes);
-size_t smem_for(const Shape &s, uint32_t stage_bytes, uint32_t vec_bytes);
-void fill_operands(QDesc &d, uint32_t vec_area);
-size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_tiles);
+void plan_program(const Program &P, ProgPlan &pp, bool allow_gather = true);
+int geom_make(const Shape &s, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gather_bpr, int smem_block, int smem_sm,
+	Geom *g);
+int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uint32_t chunk_cap);
+uint64_t chunk_prefix(const uint32_t *seg_rows, uint32_t nsegs, uint32_t chunk_rows, uint32_t *pre);
+KParams geom_params(const Geom &g);
+size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, size_t *off_chunks);
 int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Shape *forced,
 	unsigned char *db, Plan &plan);
 KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter, uint64_t *status,
@@ -136,8 +156,9 @@ int table_add_segments(virg_gpu_table *t, const virg_gpu_segment *segs, unsigned
 int table_sync_desc(virg_gpu_table *t);
 int result_alloc(virg_gpu_engine *e, const Program &P, uint64_t capacity, bool block_counts,
 	uint64_t nblocks, virg_gpu_result **out);
-int choose_shape(virg_gpu_engine *e, const std::vector<const Program *> &progs, Shape *out,
-	size_t *smem_out, uint32_t *stage_out, uint32_t *vec_out);
+int choose_shape(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, Geom *g);
+/* the launch shapes the autotuners time */
+std::vector<Shape> tune_candidates();
 
 }  // namespace vgpu
 

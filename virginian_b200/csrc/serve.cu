@@ -16,12 +16,12 @@
  *    device memory on an upload stream, waits for that copy, then publishes
  *    the new query and work counts through a doorbell word in host-mapped
  *    memory.  The kernel's producer warps poll the doorbell when they run
- *    out of published work, so new tiles are claimed as soon as CTAs free
- *    up, interleaved with the tiles of queries already running;
- *  - completion: after a tile's rows are stored, the producer warp of its
- *    CTA counts it; the tile that completes a query writes the query's row
- *    count and sequence number to a completion record in host-mapped memory,
- *    which the scheduler polls;
+ *    out of published work, so new chunks are claimed as soon as CTAs free
+ *    up, interleaved with the chunks of queries already running;
+ *  - completion: after a chunk's rows are stored, the last compute warp of
+ *    its CTA to finish counts it; the chunk that completes a query writes
+ *    the query's row count and sequence number to a completion record in
+ *    host-mapped memory, which the scheduler polls;
  *  - sessions end when the loop is idle, when the session's descriptor
  *    slots are used up or when its work numbering nears 2^31; the next
  *    admission starts a new one.
@@ -65,7 +65,8 @@ constexpr uint64_t kStatusRing = 1ull << kStatusRingBits;
 constexpr uint64_t kSessionWorkLimit = 1ull << 31;
 /* (program, table) pairs whose last result size is remembered */
 constexpr size_t kHistoryLimit = 1 << 16;
-constexpr size_t kTilePoolWords = 4u << 20;  /* segment tile prefixes per session */
+constexpr size_t kChunkPoolWords = 4u << 20;  /* segment chunk prefixes per session */
+constexpr uint32_t kServeChunkRows = 4096;
 
 using Clock = std::chrono::steady_clock;
 
@@ -126,16 +127,14 @@ struct Arena {
 struct virg_serve {
 	virg_gpu_engine *e = nullptr;
 	virg_serve_config cfg{};
-	/* the session's launch layout (one shape for every query it takes) */
-	Shape shape{};
-	size_t smem = 0;
-	uint32_t stage_bytes = 0, row_slot = 0, vec_bytes = 0, sel_bytes = 0;
+	/* the session's launch geometry (one for every query it takes) */
+	Geom geom{};
 	unsigned grid = 0;
 	cudaStream_t kstream = nullptr, ustream = nullptr;
 	/* device memory */
 	QDesc *d_queries = nullptr;
 	uint64_t *d_prefix = nullptr;
-	uint32_t *d_tiles = nullptr;
+	uint32_t *d_chunks = nullptr;
 	uint64_t *d_status = nullptr;
 	unsigned *d_done = nullptr;
 	unsigned long long *d_totals = nullptr;
@@ -147,7 +146,7 @@ struct virg_serve {
 	/* pinned staging for descriptor uploads */
 	QDesc *h_qstage = nullptr;
 	uint64_t *h_pstage = nullptr;
-	uint32_t *h_tstage = nullptr;
+	uint32_t *h_cstage = nullptr;
 
 	struct Query {
 		uint64_t ticket;
@@ -157,6 +156,7 @@ struct virg_serve {
 		Clock::time_point submitted, admitted, completed;
 		/* while in flight */
 		uint32_t qi = 0;
+		uint64_t nchunks = 0;
 		size_t arena_off = 0, arena_bytes = 0;
 		uint64_t capacity = 0;
 		void *out[kMaxRegs] = {nullptr};
@@ -174,7 +174,7 @@ struct virg_serve {
 	bool running = false;
 	uint32_t nq = 0;
 	uint64_t work = 0;
-	size_t tiles_used = 0;
+	size_t chunk_words = 0;  /* segment chunk prefixes written this session */
 	Clock::time_point idle_since;
 	unsigned sessions = 0;
 	unsigned long long launches = 0, admitted_total = 0, readmitted = 0;
@@ -195,49 +195,31 @@ namespace {
 int serve_layout(virg_serve *s)
 {
 	virg_gpu_engine *e = s->e;
-	const size_t limit = (size_t)e->smem_optin;
-	static const unsigned cand[][2] = {{256, 4}, {128, 8}, {256, 8}, {512, 4}};
-	for (auto &c : cand) {
-		Shape sh = {c[0], c[1], 0, 0};
-		const unsigned tile = sh.tile();
-		const uint32_t stage = (uint32_t)align_up(kStageHdr + (size_t)tile * s->cfg.max_load_bytes_per_row, 128);
-		const uint32_t row = (uint32_t)align_up((size_t)tile * s->cfg.max_row_vector_bytes, 128);
-		const uint32_t sel = (uint32_t)align_up((size_t)tile * s->cfg.max_sel_vector_bytes, 128);
-		const uint32_t vec = kSlots * row + sel;
-		for (unsigned st : {3u, 2u}) {
-			sh.stages = st;
-			const size_t need = smem_for(sh, stage, vec);
-			if (need <= limit) {
-				s->shape = sh;
-				s->smem = need;
-				s->stage_bytes = stage;
-				s->row_slot = row;
-				s->vec_bytes = vec;
-				s->sel_bytes = sel;
-				int per_sm = 0;
-				if (!occupancy(sh, need, &per_sm))
-					VGPU_FAIL("occupancy query failed");
-				s->grid = (unsigned)std::max(per_sm, 1) * (unsigned)e->nsm;
-				return 1;
-			}
-		}
-	}
-	VGPU_FAIL("serving layout does not fit shared memory");
+	/* eight compute warps, stages of at least 32 KB that hold a block of the
+	 * widest staging the session admits, one CTA per SM */
+	Shape sh = {256, std::max<unsigned>(32, (kBlockRows * s->cfg.max_load_bytes_per_row + 1023) / 1024), 0, 1,
+		kServeChunkRows, 0};
+	if (!geom_make(sh, s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes,
+			std::min<unsigned>(s->cfg.max_load_bytes_per_row, kGatherMaxBpr), e->smem_optin, e->smem_sm, &s->geom))
+		VGPU_FAIL("serving layout does not fit shared memory");
+	int per_sm = 0;
+	if (!occupancy(s->geom.shape, s->geom.smem, &per_sm))
+		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+	VGPU_CHECK(per_sm >= 1, "the serving kernel cannot be resident");
+	s->grid = (unsigned)e->nsm;
+	return 1;
 }
 
 /* does a program fit the session's layout */
 int program_fits(const virg_serve *s, const Program &P, const char **why)
 {
-	uint32_t load = 0, row = 0, sel = 0;
-	for (unsigned i = 0; i < P.nload; i++)
-		load += P.load_stride[i];
-	for (unsigned i = 0; i < P.nvec; i++)
-		(P.vec_compact[i] ? sel : row) += P.vec_stride[i];
-	if (load > s->cfg.max_load_bytes_per_row) {
+	ProgPlan pp;
+	plan_program(P, pp);
+	if (pp.count_bpr > s->cfg.max_load_bytes_per_row || pp.full_bpr > s->cfg.max_load_bytes_per_row) {
 		*why = "the program stages more bytes per row than the serving layout holds";
 		return 0;
 	}
-	if (row > s->cfg.max_row_vector_bytes || sel > s->cfg.max_sel_vector_bytes) {
+	if (pp.row_bpr > s->cfg.max_row_vector_bytes || pp.sel_bpr > s->cfg.max_sel_vector_bytes) {
 		*why = "the program needs more register-vector bytes than the serving layout holds";
 		return 0;
 	}
@@ -252,12 +234,9 @@ size_t arena_need(const Program &P, uint64_t cap)
 	return std::max<size_t>(b, 256);
 }
 
-uint64_t query_tiles(const virg_gpu_table *t, unsigned tile)
+uint64_t query_chunks(const virg_gpu_table *t, uint32_t chunk_rows)
 {
-	uint64_t n = 0;
-	for (uint32_t r : t->seg_rows)
-		n += (r + tile - 1) / tile;
-	return n;
+	return chunk_prefix(t->seg_rows.data(), (uint32_t)t->seg_rows.size(), chunk_rows, nullptr);
 }
 
 /* start a session: clear its counters and look-back ring, launch the kernel */
@@ -270,7 +249,7 @@ int session_start(virg_serve *s)
 	s->h_ctl->stop = 0;
 	memset(s->h_recs, 0, s->cfg.max_queries * sizeof(ServeRec));
 	std::atomic_thread_fence(std::memory_order_seq_cst);
-	KParams kp;
+	KParams kp = geom_params(s->geom);
 	kp.queries = s->d_queries;
 	kp.q_work_prefix = s->d_prefix;
 	kp.nq = 0;
@@ -279,24 +258,18 @@ int session_start(virg_serve *s)
 	kp.status = s->d_status;
 	kp.error = s->d_ctrl + 1;
 	kp.epoch = 1;
-	kp.nstages = s->shape.stages;
-	kp.stage_bytes = s->stage_bytes;
-	kp.stage_area = kSmemHeader;
-	kp.vec_area = (uint32_t)(kSmemHeader + (size_t)s->shape.stages * s->stage_bytes);
-	kp.vec_bytes = s->vec_bytes;
-	kp.sel_area = kp.vec_area + s->vec_bytes;
 	kp.status_mask = kStatusRing - 1;
 	kp.status_shift = kStatusRingBits;
 	kp.wait_limit_ms = s->cfg.wait_limit_ms;
 	kp.serve = s->d_ctl;
 	kp.recs = s->d_recs;
-	kp.done_tiles = s->d_done;
-	if (!launch_vm(s->shape, kp, s->grid, s->smem, s->kstream))
+	kp.done_chunks = s->d_done;
+	if (!launch_vm(s->geom.shape, kp, s->grid, s->geom.smem, s->kstream))
 		VGPU_FAIL("serving kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
 	s->running = true;
 	s->nq = 0;
 	s->work = 0;
-	s->tiles_used = 0;
+	s->chunk_words = 0;
 	s->sessions++;
 	s->launches++;
 	s->idle_since = Clock::now();
@@ -325,17 +298,26 @@ int session_stop(virg_serve *s)
  * doorbell.  Returns the number admitted. */
 unsigned admit(virg_serve *s)
 {
-	const unsigned tile = s->shape.tile();
-	const uint32_t vec_area = (uint32_t)(kSmemHeader + (size_t)s->shape.stages * s->stage_bytes);
 	std::vector<uint64_t> batch;
 	const uint32_t nq0 = s->nq;
 	uint64_t work = s->work;
-	size_t tiles_used = s->tiles_used;
+	size_t chunk_words = s->chunk_words;
 	while (!s->pending.empty() && nq0 + batch.size() < s->cfg.max_queries) {
 		auto &q = s->queries[s->pending.front()];
 		const Program &P = q.p->prog;
-		const uint64_t ntiles = query_tiles(q.t, tile);
-		if (work + ntiles >= kSessionWorkLimit || tiles_used + q.t->segs.size() + 1 > kTilePoolWords)
+		/* descriptor (its chunking depends on the program's staging) */
+		const uint32_t qi = nq0 + (uint32_t)batch.size();
+		QDesc &d = s->h_qstage[batch.size()];
+		memset(&d, 0, sizeof(d));
+		ProgPlan pp;
+		plan_program(P, pp);
+		if (!desc_fill(d, P, pp, s->geom, kServeChunkRows)) {
+			s->fail = last_error();
+			return 0;
+		}
+		const uint32_t nsegs = (uint32_t)q.t->segs.size();
+		const uint64_t nchunks = query_chunks(q.t, d.chunk_rows);
+		if (work + nchunks >= kSessionWorkLimit || chunk_words + nsegs + 1 > kChunkPoolWords)
 			break;
 		const uint64_t cap = std::min<uint64_t>(q.estimate_rows, q.t->rows);
 		const size_t need = arena_need(P, cap);
@@ -350,39 +332,23 @@ unsigned admit(virg_serve *s)
 			q.out[j] = p;
 			p += align_up(std::max<uint64_t>(cap, 1) * P.out_stride[j], 256);
 		}
-		/* descriptor */
-		const uint32_t qi = nq0 + (uint32_t)batch.size();
-		QDesc &d = s->h_qstage[batch.size()];
-		memset(&d, 0, sizeof(d));
-		d.prog = P;
-		uint32_t sb, rb, vb;
-		program_layout(P, tile, d.load_off, &sb, &rb, &vb);
-		vec_offsets(P, tile, s->row_slot, d.vec_off);
-		d.vec_slot = s->row_slot;
-		d.stage_bytes = sb;
 		d.segs = q.t->d_segs;
-		d.nsegs = (uint32_t)q.t->segs.size();
-		d.seg_tile_prefix = s->d_tiles + tiles_used;
-		uint32_t *pre = s->h_tstage + tiles_used;
-		uint64_t tt = 0;
-		for (uint32_t g = 0; g < d.nsegs; g++) {
-			pre[g] = (uint32_t)tt;
-			tt += (q.t->seg_rows[g] + tile - 1) / tile;
-		}
-		pre[d.nsegs] = (uint32_t)tt;
-		tiles_used += d.nsegs + 1;
+		d.nsegs = nsegs;
+		d.seg_chunk_prefix = s->d_chunks + chunk_words;
+		chunk_prefix(q.t->seg_rows.data(), nsegs, d.chunk_rows, s->h_cstage + chunk_words);
+		chunk_words += nsegs + 1;
 		d.work_first = work;
-		d.ntiles = tt;
+		d.nchunks = nchunks;
 		for (unsigned j = 0; j < P.nout; j++)
 			d.out_ptr[j] = q.out[j];
 		d.capacity = cap;
 		d.total_out = s->d_totals + qi;
 		d.block_counts = nullptr;
 		d.base_in = nullptr;
-		fill_operands(d, vec_area);
 		s->h_pstage[batch.size()] = work;
-		work += tt;
+		work += nchunks;
 		q.qi = qi;
+		q.nchunks = nchunks;
 		q.state = 1;
 		q.admitted = Clock::now();
 		batch.push_back(q.ticket);
@@ -391,14 +357,14 @@ unsigned admit(virg_serve *s)
 	if (batch.empty())
 		return 0;
 	const size_t b = batch.size();
-	const size_t t0 = s->tiles_used;
+	const size_t c0 = s->chunk_words;
 	cudaError_t ce = cudaMemcpyAsync(s->d_queries + nq0, s->h_qstage, b * sizeof(QDesc), cudaMemcpyHostToDevice,
 		s->ustream);
 	if (ce == cudaSuccess)
 		ce = cudaMemcpyAsync(s->d_prefix + nq0, s->h_pstage, b * sizeof(uint64_t), cudaMemcpyHostToDevice,
 			s->ustream);
 	if (ce == cudaSuccess)
-		ce = cudaMemcpyAsync(s->d_tiles + t0, s->h_tstage + t0, (tiles_used - t0) * sizeof(uint32_t),
+		ce = cudaMemcpyAsync(s->d_chunks + c0, s->h_cstage + c0, (chunk_words - c0) * sizeof(uint32_t),
 			cudaMemcpyHostToDevice, s->ustream);
 	if (ce == cudaSuccess)
 		ce = cudaStreamSynchronize(s->ustream);
@@ -408,7 +374,7 @@ unsigned admit(virg_serve *s)
 	}
 	s->nq = nq0 + (uint32_t)b;
 	s->work = work;
-	s->tiles_used = tiles_used;
+	s->chunk_words = chunk_words;
 	/* the doorbell: descriptors are in device memory before they are counted */
 	std::atomic_thread_fence(std::memory_order_seq_cst);
 	s->h_ctl->avail = ((unsigned long long)s->nq << 40) | (s->work & kAvailWorkMask);
@@ -417,7 +383,7 @@ unsigned admit(virg_serve *s)
 	for (uint64_t tk : batch) {
 		auto &q = s->queries[tk];
 		s->admitted_total++;
-		if (q.t->rows == 0 || query_tiles(q.t, tile) == 0) {
+		if (q.nchunks == 0) {
 			q.rows = 0;
 			q.state = 2;
 			q.completed = Clock::now();
@@ -492,7 +458,7 @@ void scheduler(virg_serve *s)
 			/* a session that cannot take the next query ends once drained */
 			if (s->running && !s->pending.empty() && s->inflight.empty() &&
 				(s->nq >= s->cfg.max_queries || s->work >= kSessionWorkLimit / 2 ||
-				 s->tiles_used > kTilePoolWords / 2)) {
+				 s->chunk_words > kChunkPoolWords / 2)) {
 				if (!session_stop(s))
 					s->fail = last_error();
 			}
@@ -562,7 +528,7 @@ extern "C" int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cf
 	const size_t nqc = c.max_queries;
 	if ((ce = cudaMalloc((void **)&s->d_queries, nqc * sizeof(QDesc))) != cudaSuccess ||
 		(ce = cudaMalloc((void **)&s->d_prefix, (nqc + 1) * sizeof(uint64_t))) != cudaSuccess ||
-		(ce = cudaMalloc((void **)&s->d_tiles, kTilePoolWords * sizeof(uint32_t))) != cudaSuccess ||
+		(ce = cudaMalloc((void **)&s->d_chunks, kChunkPoolWords * sizeof(uint32_t))) != cudaSuccess ||
 		(ce = cudaMalloc((void **)&s->d_status, kStatusRing * sizeof(uint64_t))) != cudaSuccess ||
 		(ce = cudaMalloc((void **)&s->d_done, nqc * sizeof(unsigned))) != cudaSuccess ||
 		(ce = cudaMalloc((void **)&s->d_totals, nqc * sizeof(unsigned long long))) != cudaSuccess ||
@@ -576,7 +542,7 @@ extern "C" int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cf
 		return fail("serving mapped memory", ce);
 	if ((ce = cudaMallocHost((void **)&s->h_qstage, nqc * sizeof(QDesc))) != cudaSuccess ||
 		(ce = cudaMallocHost((void **)&s->h_pstage, (nqc + 1) * sizeof(uint64_t))) != cudaSuccess ||
-		(ce = cudaMallocHost((void **)&s->h_tstage, kTilePoolWords * sizeof(uint32_t))) != cudaSuccess)
+		(ce = cudaMallocHost((void **)&s->h_cstage, kChunkPoolWords * sizeof(uint32_t))) != cudaSuccess)
 		return fail("serving staging memory", ce);
 	memset(s->h_ctl, 0, sizeof(ServeCtl));
 	s->arena.reset(c.result_budget_bytes);
@@ -717,9 +683,9 @@ extern "C" int virg_serve_stats(virg_serve *s, virg_serve_counters *c)
 	c->inflight = s->inflight.size();
 	c->arena_used = s->arena.used;
 	c->device_error = s->device_error;
-	c->shape[0] = s->shape.threads;
-	c->shape[1] = s->shape.rows_per_thread;
-	c->shape[2] = s->shape.stages;
+	c->shape[0] = s->geom.shape.threads;
+	c->shape[1] = s->geom.shape.stage_kb;
+	c->shape[2] = s->geom.shape.stages;
 	c->shape[3] = s->grid;
 	return 1;
 }
@@ -737,7 +703,7 @@ extern "C" void virg_serve_destroy(virg_serve *s)
 		cudaStreamSynchronize(s->kstream);
 	cudaFree(s->d_queries);
 	cudaFree(s->d_prefix);
-	cudaFree(s->d_tiles);
+	cudaFree(s->d_chunks);
 	cudaFree(s->d_status);
 	cudaFree(s->d_done);
 	cudaFree(s->d_totals);
@@ -751,8 +717,8 @@ extern "C" void virg_serve_destroy(virg_serve *s)
 		cudaFreeHost(s->h_qstage);
 	if (s->h_pstage)
 		cudaFreeHost(s->h_pstage);
-	if (s->h_tstage)
-		cudaFreeHost(s->h_tstage);
+	if (s->h_cstage)
+		cudaFreeHost(s->h_cstage);
 	if (s->kstream)
 		cudaStreamDestroy(s->kstream);
 	if (s->ustream)

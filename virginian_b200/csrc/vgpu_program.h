@@ -21,6 +21,7 @@
 #ifndef VGPU_PROGRAM_H
 #define VGPU_PROGRAM_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 namespace vgpu {
@@ -98,11 +99,13 @@ struct Program {
 	uint8_t vec_compact[kMaxRegs];
 };
 
-/* operand descriptor resolved for a launch shape: bits [0,30) are a shared
- * memory byte offset, bits [30,32) the kind */
-constexpr uint32_t OD_STAGE = 0u << 30;    /* staged column, + stage offset */
-constexpr uint32_t OD_ROWVEC = 1u << 30;   /* register vector by tile row */
-constexpr uint32_t OD_SELVEC = 2u << 30;   /* register vector by selection index */
+/* operand descriptor resolved for a launch layout: bits [0,30) are a byte
+ * offset, bits [30,32) the kind.  The kernel adds the base the kind names:
+ * the stage holding the tile (staged columns), the warp's row-vector or
+ * selection-vector area, or the chunk slot's descriptor copy (scalars). */
+constexpr uint32_t OD_STAGE = 0u << 30;    /* staged column, indexed by tile row */
+constexpr uint32_t OD_ROWVEC = 1u << 30;   /* register vector, indexed by block row */
+constexpr uint32_t OD_SELVEC = 2u << 30;   /* register vector, indexed by selection entry */
 constexpr uint32_t OD_SCALAR = 3u << 30;   /* scalar register */
 constexpr uint32_t OD_OFFSET = (1u << 30) - 1;
 
@@ -139,47 +142,93 @@ struct SegDesc {
 	uint32_t block_base;         /* first 64-row block of this segment */
 };
 
+/* Rows are processed in blocks of kBlockRows (8 words of 32 rows; lane l of
+ * a warp holds rows l, l + 32, ..., l + 224 of its block) and scanned in
+ * chunks of at most kMaxChunkRows rows that lie inside one segment.  A chunk
+ * is the unit of claiming and of ordered placement: its count phase stages
+ * the columns the filter reads and leaves one validity bit per row, its full
+ * phase stages the columns the results need and stores the selected rows at
+ * the chunk's offset. */
+constexpr unsigned kBlockRows = 256;
+constexpr unsigned kMaxChunkRows = 8192;
+constexpr unsigned kMaxChunkBlocks = kMaxChunkRows / kBlockRows;  /* 32: one lane each */
+constexpr unsigned kChunkWords = kMaxChunkRows / 32;
+
+/* how the full phase gets its rows: FM_GATHER and FM_BITMAP take the
+ * rows' validity from the count phase's bitmap (the results read only
+ * columns, constants and vectors computed after the filter); FM_GATHER
+ * then loads only the selected rows' values of the columns the results
+ * read, straight from device memory, while FM_BITMAP stages full tiles of
+ * them (programs whose results read many bytes per row).  FM_REFILTER
+ * stages full tiles of every column and runs the filter again (the results
+ * read register vectors the filter computed). */
+constexpr uint32_t FM_BITMAP = 0;
+constexpr uint32_t FM_REFILTER = 1;
+constexpr uint32_t FM_GATHER = 2;
+/* the largest bytes per row a gathering full phase loads */
+constexpr uint32_t kGatherMaxBpr = 32;
+
+/* the staged columns of one phase: which segment columns, where in a stage */
+struct LoadSet {
+	uint32_t n;
+	uint32_t rows;                /* rows per tile of this phase (multiple of kBlockRows) */
+	uint32_t bytes_per_row;
+	uint32_t pad;
+	uint8_t src[kMaxLoads];       /* segment column index, kKeySlot for the key */
+	uint8_t stride[kMaxLoads];
+	uint8_t pad2[14];
+	uint32_t off[kMaxLoads];      /* byte offset of the column in the stage */
+	uint32_t pad3[3];
+};
+
 /* per-query launch descriptor, in device memory */
 struct alignas(16) QDesc {
-	/* Everything before `prog` is what the kernel reads from a stage's copy
-	 * of the descriptor (the stage holds only that prefix); the decoded
-	 * program itself is read from device memory by the producer (its loads)
-	 * and is host-side otherwise. */
-	/* the program's constants, split point, op count and result columns */
-	uint64_t consts[kMaxRegs];
-	uint32_t nfilter;
-	uint32_t nuops;
+	/* ---- the kernel's view: the producer copies everything up to `segs`
+	 * into the chunk slot of each chunk it claims (unless the slot holds the
+	 * same query already); compute and look-back warps read only that copy */
+	uint64_t consts[kMaxRegs];     /* scalar registers (OD_SCALAR offsets point here) */
+	uint32_t nfilter;              /* uops [0, nfilter) are the filter */
+	uint32_t nuops;                /* uops [nfilter, nuops - 1) the projection, then Result */
 	uint32_t nout;
+	uint32_t full_mode;            /* FM_BITMAP or FM_REFILTER */
+	uint32_t chunk_rows;           /* rows per chunk (a multiple of both tile sizes) */
+	uint32_t pad0[3];
 	uint8_t out_stride[kMaxRegs];
-	/* smem layout for this launch shape */
-	uint32_t load_off[kMaxLoads];
-	uint32_t stage_bytes;
-	uint32_t vec_off[kMaxRegs];
-	/* the uops as records (handler, operands) and the result columns'
-	 * operand descriptors */
-	OpRec ops[kMaxOps];
-	uint32_t od_out[kMaxRegs];
-	/* inputs */
-	const SegDesc *segs;
-	const uint32_t *seg_tile_prefix;  /* nsegs + 1 entries */
-	uint32_t nsegs;
-	uint32_t vec_slot;                /* distance between the two row-vector slots */
-	uint64_t work_first;              /* global work index of tile 0 */
-	uint64_t ntiles;
-	/* outputs */
+	/* the filter over the count phase's staged columns, and every uop over
+	 * the full phase's (the filter part only used by FM_REFILTER) */
+	OpRec ops_count[kMaxOps];
+	OpRec ops_full[kMaxOps];
+	uint32_t od_out[kMaxRegs];     /* result columns, over the full phase's layout */
+	/* FM_GATHER: the gathered columns (the full set) and where a batch of
+	 * them sits in a compute warp's gather area */
+	uint32_t gather_n;
+	uint8_t gather_stride[kMaxLoads];
+	uint8_t pad3[3];
+	uint32_t gather_off[kMaxLoads];
+	uint32_t pad4[5];
 	void *out_ptr[kMaxRegs];
-	uint64_t capacity;                /* rows each out column can hold */
-	unsigned long long *total_out;    /* written by the last tile */
-	uint8_t *block_counts;            /* optional: valid rows per 64-row block */
+	uint64_t capacity;             /* rows each out column can hold */
+	unsigned long long *total_out; /* the query's row count, written with its last chunk's offset */
+	uint8_t *block_counts;         /* optional: valid rows per 64-row block */
 	/* optional: result rows already written by earlier launches of the same
-	 * query; its first tile starts there */
+	 * query; its first chunk starts there */
 	const unsigned long long *base_in;
-	uint64_t pad1;
+	uint64_t work_first;           /* global work index of the query's chunk 0 */
+	uint64_t nchunks;
+	/* ---- the producer's view, read from device memory */
+	const SegDesc *segs;
+	const uint32_t *seg_chunk_prefix;  /* nsegs + 1 entries */
+	uint32_t nsegs;
+	uint32_t pad1[3];
+	LoadSet count_set, full_set;
 	Program prog;
 };
 
-/* bytes of a descriptor that a stage holds (the kernel's view) */
-constexpr unsigned kQDescStaged = (unsigned)((offsetof(QDesc, prog) + 15) / 16 * 16);
+/* bytes of a descriptor that a chunk slot holds (the kernel's view), and the
+ * slot area that holds them */
+constexpr unsigned kQDescCopy = (unsigned)offsetof(QDesc, segs);
+constexpr unsigned kQDescView = (kQDescCopy + 127) / 128 * 128;
+static_assert(kQDescCopy % 16 == 0, "the view is copied in 16-byte units");
 
 /* device error codes (written once per launch to the error word) */
 enum DevError : unsigned {

@@ -4,34 +4,35 @@
  * Replaces the reference's virginia_gpu (src/vm/vm_gpu.cu:1152-1225), which
  * runs one thread per row with a 16-entry register file in local memory, a
  * switch dispatch per op per thread and atomics for (unordered) result
- * placement.  Here a CTA is a pipeline over tiles of TILE = THREADS x R
- * rows, tied together by mbarriers, with four roles:
+ * placement.  Here persistent CTAs claim chunks of rows (at most
+ * kMaxChunkRows rows of one segment of one query) in order and run each
+ * chunk in two phases through a ring of shared-memory stages:
  *
- *  - producer warp: claims work items (one tile of one segment of one query)
- *    from a global counter, in order, decodes them warp-wide and copies the
- *    tile's columns (plus the query's descriptor when the stage does not hold
- *    it) into a ring of shared-memory stages with TMA bulk copies
- *    (cp.async.bulk completing on the stage's full barrier);
- *  - filter warps (THREADS threads): run the filter ops over every row of the
- *    tile (row state as bit masks: valid, active, and rows parked at pending
- *    jump targets; each lane holds R rows in chunks of 4 consecutive rows),
- *    count valid rows per 64 rows with bit-plane ballots, scan the counts and
- *    write the tile's selected rows, in row order, to a shared list, then
- *    publish the tile's count to the query's look-back words;
- *  - look-back warp: resolves the tile's position in the query's result with
- *    a warp-wide decoupled look-back over earlier tiles (32 status words per
- *    round); a tile that directly follows the CTA's previous tile of the same
- *    query starts where that one ended, with no look-back;
- *  - projection warps: run the projection ops over the tile's list in
- *    32-entry batches and write each result row to the tile's offset plus
- *    its list position (coalesced stores), then release the stage.
+ *  - count phase: the producer warp bulk-copies (cp.async.bulk, completing
+ *    on the stage's mbarrier) only the columns the filter reads; compute
+ *    warps run the filter ops over 256-row blocks (a lane holds rows l,
+ *    l + 32, ..., l + 224 as bits of its row masks) and leave one validity
+ *    bit per row in the chunk slot's bitmap and a count per block;
+ *  - the look-back warp sums the chunk's block counts, publishes them to the
+ *    query's look-back words and resolves the chunk's place in the query's
+ *    result with a decoupled look-back over earlier chunks, then writes
+ *    each block's result offset;
+ *  - full phase: the producer stages the columns the result columns need;
+ *    compute warps build each block's selection list from the bitmap, run
+ *    the projection ops on the selected rows 32 at a time and store them
+ *    at the block's offset (coalesced, original row order).
  *
- * Each op is one 16-byte record fetched with a single shared-memory load and
- * dispatched on one handler code; operands are read and written by 32-bit
- * shared-memory address.  Rows land in original row order (the single-core
- * CPU VM's order, src/vm/virginia.c:476-578) with plain stores; no output
- * atomics.  Arithmetic matches the CPU VM bit for bit: float/double use the
- * _rn intrinsics (no FMA contraction, IEEE division) and x86 NaN results,
+ * The producer issues a chunk's count phase kCountAhead chunks before its
+ * full phase, so a chunk's offset is resolved while the CTA counts the next
+ * chunks: no stage waits for another CTA, and a column both phases read is
+ * read from HBM once and found in L2 the second time.
+ *
+ * Each op is one 16-byte record read with one shared-memory load and
+ * dispatched by bit tests on its head; operands are read and written by
+ * 32-bit shared-memory address.  Rows land in the single-core CPU VM's
+ * order (src/vm/virginia.c:476-578) with plain stores; no output atomics.
+ * Arithmetic matches the CPU VM bit for bit: float/double use the _rn
+ * intrinsics (no FMA contraction, IEEE division) and x86 NaN results,
  * integers wrap as on x86.  Every wait is bounded; on expiry the kernel
  * records an error code and stops instead of hanging.
  */
@@ -45,48 +46,34 @@
 
 namespace vgpu {
 
-/* bounded waits: a stage or offset wait gives up after the launch's limit
- * (a second by default), far beyond any real wait; look-back polls after
- * 2^24 rounds of 32-256 ns */
+/* bounded waits: a stage, slot or offset wait gives up after the launch's
+ * limit (a second by default), far beyond any real wait; look-back polls
+ * after 2^24 rounds of 32-256 ns */
 constexpr uint32_t kSuspendHintNs = 20000;
-
-/* flag words of a CTA: ok per slot, then abort, end tile, -, wait limit */
-constexpr unsigned kFAbortSlot = 4;
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
-/* shared memory header (kSmemHeader bytes) */
-constexpr unsigned kMaxGroups = 128;  /* R x warps */
-constexpr unsigned kOffFull = 0;                            /* mbarrier[kMaxStages] */
-constexpr unsigned kOffEmpty = kOffFull + 8 * kMaxStages;   /* mbarrier[kMaxStages] */
-constexpr unsigned kOffLready = kOffEmpty + 8 * kMaxStages; /* mbarrier[kSlots]: list and count ready */
-constexpr unsigned kOffOready = kOffLready + 8 * kSlots;     /* mbarrier[kSlots]: offset ready */
-constexpr unsigned kOffLfree = kOffOready + 8 * kSlots;      /* mbarrier[kSlots]: projection done */
-constexpr unsigned kOffCdone = kOffLfree + 8 * kSlots;       /* mbarrier[kSlots]: all counts written */
-constexpr unsigned kOffOff = kOffCdone + 8 * kSlots;         /* uint64[kSlots]: tile offsets */
-constexpr unsigned kOffFlags = kOffOff + 8 * kSlots;         /* uint32[8]: ok[kSlots], abort, end tile */
-constexpr unsigned kOffTot = kOffFlags + 32;                 /* uint32[kSlots]: tile totals */
-constexpr unsigned kOffHeld = kOffTot + 4 * kSlots;          /* uint32[kMaxStages]: query per stage */
-constexpr unsigned kOffTready = 328;                          /* mbarrier[kSlots]: tile count ready */
-constexpr unsigned kOffCnt = 512;                            /* uint32[kSlots][kMaxGroups]: per 64 rows */
-constexpr unsigned kFAbort = kFAbortSlot, kFEnd = 5, kFWaitMs = 7;  /* flag words */
-static_assert(kSlots <= kFAbort, "ok flags per slot");
-static_assert(kOffHeld + 4 * kMaxStages <= kOffTready, "smem header layout");
-static_assert(kOffTready + 8 * kSlots <= kOffCnt, "smem header layout");
-static_assert(kOffCnt + 4 * kSlots * kMaxGroups <= kSmemHeader, "smem header overflow");
-static_assert(kQDescStaged % 16 == 0 && kQDescStaged <= sizeof(QDesc), "descriptor copies in 16-byte chunks");
-static_assert(kStageHdr >= kQDescStaged + sizeof(StageInfo), "stage header too small");
-static_assert(offsetof(QDesc, ops) % 16 == 0, "op records are read 16 bytes at a time");
-
-/* where the fields the compute warps read sit in a stage's descriptor copy */
-constexpr uint32_t kQOps = (uint32_t)offsetof(QDesc, ops);
+/* where the fields the kernel's warps read sit in a slot's descriptor copy */
 constexpr uint32_t kQNFilter = (uint32_t)offsetof(QDesc, nfilter);
 constexpr uint32_t kQNUops = (uint32_t)offsetof(QDesc, nuops);
 constexpr uint32_t kQNOut = (uint32_t)offsetof(QDesc, nout);
+constexpr uint32_t kQFullMode = (uint32_t)offsetof(QDesc, full_mode);
 constexpr uint32_t kQOutStride = (uint32_t)offsetof(QDesc, out_stride);
+constexpr uint32_t kQOpsCount = (uint32_t)offsetof(QDesc, ops_count);
+constexpr uint32_t kQOpsFull = (uint32_t)offsetof(QDesc, ops_full);
 constexpr uint32_t kQOdOut = (uint32_t)offsetof(QDesc, od_out);
 constexpr uint32_t kQOutPtr = (uint32_t)offsetof(QDesc, out_ptr);
 constexpr uint32_t kQCapacity = (uint32_t)offsetof(QDesc, capacity);
-constexpr uint32_t kQVecSlot = (uint32_t)offsetof(QDesc, vec_slot);
+constexpr uint32_t kQTotalOut = (uint32_t)offsetof(QDesc, total_out);
+constexpr uint32_t kQBlockCounts = (uint32_t)offsetof(QDesc, block_counts);
+constexpr uint32_t kQBaseIn = (uint32_t)offsetof(QDesc, base_in);
+constexpr uint32_t kQWorkFirst = (uint32_t)offsetof(QDesc, work_first);
+constexpr uint32_t kQNChunks = (uint32_t)offsetof(QDesc, nchunks);
+constexpr uint32_t kQGatherN = (uint32_t)offsetof(QDesc, gather_n);
+constexpr uint32_t kQGatherStride = (uint32_t)offsetof(QDesc, gather_stride);
+constexpr uint32_t kQGatherOff = (uint32_t)offsetof(QDesc, gather_off);
+static_assert(kQOpsCount % 16 == 0 && kQOpsFull % 16 == 0, "op records are read 16 bytes at a time");
+static_assert(kSlotBitmap % 16 == 0 && kSlotBlockOff % 8 == 0, "slot layout");
+static_assert(kOffStageInfo % 16 == 0 && sizeof(StageInfo) == 32, "stage info is read as two 16-byte words");
 
 /* ---- PTX wrappers ---------------------------------------------------- */
 
@@ -129,6 +116,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase)
 	return ok != 0;
 }
 
+/* try_wait that suspends the thread until the phase completes or about
+ * hint_ns pass, so a waiting warp takes no issue slots meanwhile */
+__device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t phase, uint32_t hint_ns)
+{
+	uint32_t ok;
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+		"selp.u32 %0, 1, 0, p;\n\t}"
+		: "=r"(ok)
+		: "r"(bar), "r"(phase), "r"(hint_ns)
+		: "memory");
+	return ok != 0;
+}
+
 /* global -> shared bulk copy completing on an mbarrier; dst, src and bytes
  * are multiples of 16 */
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
@@ -146,8 +148,7 @@ __device__ __forceinline__ void fence_proxy_async_smem()
 
 /* Look-back status words carry epoch, flag and count in one aligned 64-bit
  * word, and no other data is published with them, so relaxed (single-copy
- * atomic) accesses suffice: an acquire or release here would fence the
- * warp's outstanding result stores on every tile. */
+ * atomic) accesses suffice. */
 __device__ __forceinline__ uint64_t ld_status(const uint64_t *p)
 {
 	uint64_t v;
@@ -160,10 +161,10 @@ __device__ __forceinline__ void st_status(uint64_t *p, uint64_t v)
 	asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-/* the serving doorbell, with acquire semantics: descriptors, work prefixes
- * and tile prefixes the host wrote before ringing it are seen by every
- * later load of this CTA (ordered through its mbarriers), even where a load
- * of a neighbouring entry had cached their lines before the host wrote them */
+/* the serving doorbell, with acquire semantics: descriptors and prefixes the
+ * host wrote before ringing it are seen by every later load of this CTA
+ * (ordered through its mbarriers), even where a load of a neighbouring entry
+ * had cached their lines before the host wrote them */
 __device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long *p)
 {
 	unsigned long long v;
@@ -183,68 +184,12 @@ __device__ __forceinline__ uint64_t globaltimer_ns()
 	return t;
 }
 
-/* try_wait that suspends the thread until the phase completes or about
- * hint_ns pass, so a waiting warp takes no issue slots meanwhile */
-__device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t phase, uint32_t hint_ns)
-{
-	uint32_t ok;
-	asm volatile(
-		"{\n\t.reg .pred p;\n\t"
-		"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-		"selp.u32 %0, 1, 0, p;\n\t}"
-		: "=r"(ok)
-		: "r"(bar), "r"(phase), "r"(hint_ns)
-		: "memory");
-	return ok != 0;
-}
-
-/* bounded wait for an mbarrier phase; false on timeout or when the CTA's
- * abort flag (a shared-memory word, if given) is set.  The bound is the
- * launch's wait limit, which the CTA keeps in the last of its flag words
- * (the abort flag's neighbours); a second without an abort flag. */
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const volatile uint32_t *abort)
-{
-	if (mbar_try_wait(bar, phase))
-		return true;
-	const uint32_t abort_addr = abort ? smem_addr(const_cast<const uint32_t *>(abort)) : 0u;
-	uint64_t limit_ns = 1000000000ull;
-	if (abort_addr) {
-		uint32_t ms;
-		asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(ms) : "r"(abort_addr + 4 * (7 - kFAbortSlot)));
-		limit_ns = (uint64_t)ms * 1000000ull;
-	}
-	const uint64_t t0 = globaltimer_ns();
-	for (;;) {
-		if (mbar_try_wait_hint(bar, phase, kSuspendHintNs))
-			return true;
-		if (abort_addr) {
-			uint32_t v;
-			asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(abort_addr));
-			if (v)
-				return false;
-		}
-		if (globaltimer_ns() - t0 > limit_ns)
-			return false;
-	}
-}
-
-/* ---- shared-memory access by 32-bit shared address ---------------------
- * Every tile, register-vector and descriptor access of the compute warps
- * goes through these, so each is one ld/st.shared.  They are volatile asm:
- * the compiler keeps them in program order, and the hardware still
- * pipelines consecutive independent loads. */
+/* ---- shared-memory access by 32-bit shared address --------------------- */
 
 __device__ __forceinline__ uint32_t lds_u8(uint32_t a)
 {
 	uint32_t v;
 	asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a));
-	return v;
-}
-
-__device__ __forceinline__ uint32_t lds_u16(uint32_t a)
-{
-	uint16_t v;
-	asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
 	return v;
 }
 
@@ -275,11 +220,6 @@ __device__ __forceinline__ void sts_u8(uint32_t a, uint32_t v)
 	asm volatile("st.shared.u8 [%0], %1;" ::"r"(a), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ void sts_u16(uint32_t a, uint32_t v)
-{
-	asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"((uint16_t)v) : "memory");
-}
-
 __device__ __forceinline__ void sts_u32(uint32_t a, uint32_t v)
 {
 	asm volatile("st.shared.b32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
@@ -294,6 +234,56 @@ __device__ __forceinline__ void sts_v4(uint32_t a, uint4 v)
 {
 	asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(a), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
 		: "memory");
+}
+
+/* bounded wait for an mbarrier phase; false on timeout or when the CTA's
+ * abort flag is set.  The bound is the launch's wait limit, which the CTA
+ * keeps in its flag words. */
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t phase)
+{
+	uint32_t ok;
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		"selp.u32 %0, 1, 0, p;\n\t}"
+		: "=r"(ok)
+		: "r"(bar), "r"(phase)
+		: "memory");
+	return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, uint32_t flags)
+{
+	if (mbar_try_wait(bar, phase))
+		return true;
+	const uint64_t limit_ns = (uint64_t)lds_u32(flags + 4 * kFWaitMs) * 1000000ull;
+	const uint64_t t0 = globaltimer_ns();
+	for (;;) {
+#ifdef VGPU_SPIN_WAIT
+		if (mbar_test(bar, phase))
+			return true;
+#else
+		if (mbar_try_wait_hint(bar, phase, kSuspendHintNs))
+			return true;
+#endif
+		uint32_t v;
+		asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(flags + 4 * kFAbort));
+		if (v)
+			return false;
+		if (globaltimer_ns() - t0 > limit_ns)
+			return false;
+	}
+}
+
+/* a failed wait: record the error (unless another warp already aborted the
+ * CTA for its own reason) and make every other wait of the CTA give up */
+__device__ __forceinline__ void abort_cta(const KParams &kp, uint32_t flags, unsigned code)
+{
+	uint32_t v;
+	asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(flags + 4 * kFAbort));
+	if (!v)
+		report(kp.error, code);
+	asm volatile("st.volatile.shared.u32 [%0], %1;" ::"r"(flags + 4 * kFAbort), "r"(1u) : "memory");
 }
 
 /* typed element access */
@@ -340,39 +330,38 @@ struct SM<unsigned char> {
 	static __device__ __forceinline__ void st(uint32_t a, unsigned char v) { sts_u8(a, v); }
 };
 
-/* an operand resolved for one tile: element i at addr + i * step (step 0 for
- * a scalar), indexed by selection position instead of tile row when sel */
+/* ---- operands ----------------------------------------------------------- */
+
+/* the bases of one block's operands: the stage holding its tile (and the
+ * block's first tile row), the warp's vector areas and the chunk slot */
+struct Bases {
+	uint32_t stage;
+	uint32_t blk_row0;
+	uint32_t rowv;
+	uint32_t selv;
+	uint32_t slot;
+};
+
+/* an operand resolved for one block: element i at addr + i * step (step 0
+ * for a scalar), indexed by selection entry instead of block row when sel */
 struct Opnd {
 	uint32_t addr;
 	uint32_t step;
 	bool sel;
 };
 
-/* staged columns and scalars (the descriptor's constant table) live in the
- * tile's stage, row vectors in the tile's row-vector slot, selection
- * vectors in their single area */
 template <int SIZE>
-__device__ __forceinline__ Opnd opnd(uint32_t od, uint32_t sbase, uint32_t sdelta, uint32_t vdelta)
+__device__ __forceinline__ Opnd opnd(uint32_t od, const Bases &b)
 {
 	const uint32_t kind = od >> 30;
+	const uint32_t off = od & OD_OFFSET;
 	Opnd o;
-	o.addr = sbase + (od & OD_OFFSET) +
-		((kind == (OD_STAGE >> 30) || kind == (OD_SCALAR >> 30)) ? sdelta
-			: kind == (OD_ROWVEC >> 30) ? vdelta : 0u);
+	o.addr = off + (kind == (OD_STAGE >> 30) ? b.stage + b.blk_row0 * (uint32_t)SIZE
+		: kind == (OD_ROWVEC >> 30) ? b.rowv
+		: kind == (OD_SELVEC >> 30) ? b.selv : b.slot);
 	o.step = kind == (OD_SCALAR >> 30) ? 0u : (uint32_t)SIZE;
 	o.sel = kind == (OD_SELVEC >> 30);
 	return o;
-}
-
-/* Rows of a tile: thread tid holds R = 4 C rows, in C chunks of 4
- * consecutive rows; chunk c of thread tid starts at tile row
- * c * 4 * THREADS + 4 * tid, and row k of the chunk is bit 4 c + k of the
- * thread's row masks.  One 16-byte shared load fetches a chunk of a 4-byte
- * column. */
-template <int THREADS>
-__device__ __forceinline__ uint32_t chunk_row(int c, int tid)
-{
-	return (uint32_t)(c * 4 * THREADS + 4 * tid);
 }
 
 /* ---- op semantics (src/vm/virginia.c:48-194, :598-680) ------------------ */
@@ -487,7 +476,14 @@ struct Math<signed char, OP> {
 	}
 };
 
-/* ---- filter: every row of the tile, row state in bit masks --------------- */
+/* operand type and operator tests on a record head */
+__device__ __forceinline__ bool h_type(uint32_t h, int t) { return (h >> (OT_SHIFT + t)) & 1u; }
+__device__ __forceinline__ bool h_op(uint32_t h, int o) { return (h >> (OO_SHIFT + o)) & 1u; }
+
+/* ---- filter: every row of a group, row state in bit masks ---------------
+ * A count group is kCountGroup blocks; lane l holds its rows l, l + 32, ...,
+ * as bits 0, 1, ... of its row masks, so a ballot of bit u is the group's
+ * validity word u. */
 
 struct RowState {
 	uint32_t valid;
@@ -496,212 +492,174 @@ struct RowState {
 };
 
 /* rows in `jumped` leave the active set, park in the op's target slot and,
- * for a jump with p4 == 0, stop being valid (src/vm/virginia.c:59-63) */
+ * for a jump with p4 == 0, stop being valid (src/vm/virginia.c:59-63).  The
+ * code generator's programs park rows in the first two slots. */
 __device__ __forceinline__ void take_jump(RowState &st, uint32_t head, uint32_t jumped)
 {
 	st.active &= ~jumped;
 	if (!(head & OPH_VJUMP))
 		st.valid &= ~jumped;
 	const uint32_t slot = (head >> OPH_SLOT_SHIFT) & 7u;
+	if (slot == 0) {
+		st.pend[0] |= jumped;
+	} else if (slot == 1) {
+		st.pend[1] |= jumped;
+	} else {
 #pragma unroll
-	for (int s = 0; s < kMaxSlots; s++)
-		if (slot == (uint32_t)s)
-			st.pend[s] |= jumped;
-}
-
-/* element bits <-> values */
-template <typename T>
-__device__ __forceinline__ T from_bits(uint64_t b)
-{
-	if constexpr (sizeof(T) == 8) {
-		const long long v = (long long)b;
-		return *reinterpret_cast<const T *>(&v);
-	} else if constexpr (sizeof(T) == 4) {
-		const uint32_t v = (uint32_t)b;
-		return *reinterpret_cast<const T *>(&v);
-	} else {
-		const unsigned char v = (unsigned char)b;
-		return *reinterpret_cast<const T *>(&v);
+		for (int s = 2; s < kMaxSlots; s++)
+			if (slot == (uint32_t)s)
+				st.pend[s] |= jumped;
 	}
 }
 
-template <typename T>
-__device__ __forceinline__ uint64_t to_bits(T x)
-{
-	if constexpr (sizeof(T) == 8)
-		return *reinterpret_cast<const unsigned long long *>(&x);
-	else if constexpr (sizeof(T) == 4)
-		return *reinterpret_cast<const uint32_t *>(&x);
-	else
-		return *reinterpret_cast<const unsigned char *>(&x);
-}
-
-/* one chunk (4 consecutive rows) of a column or row vector */
-template <typename T>
-__device__ __forceinline__ void ld_chunk(uint32_t a, T *v)
-{
-	if constexpr (sizeof(T) == 4) {
-		const uint4 q = lds_v4(a);
-		v[0] = from_bits<T>(q.x); v[1] = from_bits<T>(q.y); v[2] = from_bits<T>(q.z); v[3] = from_bits<T>(q.w);
-	} else if constexpr (sizeof(T) == 8) {
-		const uint4 q0 = lds_v4(a), q1 = lds_v4(a + 16);
-		v[0] = from_bits<T>((uint64_t)q0.y << 32 | q0.x);
-		v[1] = from_bits<T>((uint64_t)q0.w << 32 | q0.z);
-		v[2] = from_bits<T>((uint64_t)q1.y << 32 | q1.x);
-		v[3] = from_bits<T>((uint64_t)q1.w << 32 | q1.z);
-	} else {
-		const uint32_t w = lds_u32(a);
-		v[0] = from_bits<T>(w & 0xffu); v[1] = from_bits<T>((w >> 8) & 0xffu);
-		v[2] = from_bits<T>((w >> 16) & 0xffu); v[3] = from_bits<T>(w >> 24);
-	}
-}
-
-template <typename T>
-__device__ __forceinline__ void st_chunk(uint32_t a, const T *v)
-{
-	if constexpr (sizeof(T) == 4) {
-		sts_v4(a, make_uint4((uint32_t)to_bits(v[0]), (uint32_t)to_bits(v[1]), (uint32_t)to_bits(v[2]),
-			(uint32_t)to_bits(v[3])));
-	} else if constexpr (sizeof(T) == 8) {
-		const uint64_t b0 = to_bits(v[0]), b1 = to_bits(v[1]), b2 = to_bits(v[2]), b3 = to_bits(v[3]);
-		sts_v4(a, make_uint4((uint32_t)b0, (uint32_t)(b0 >> 32), (uint32_t)b1, (uint32_t)(b1 >> 32)));
-		sts_v4(a + 16, make_uint4((uint32_t)b2, (uint32_t)(b2 >> 32), (uint32_t)b3, (uint32_t)(b3 >> 32)));
-	} else {
-		sts_u32(a, (uint32_t)(to_bits(v[0]) | to_bits(v[1]) << 8 | to_bits(v[2]) << 16 | to_bits(v[3]) << 24));
-	}
-}
-
-/* the operand's elements for this thread's R rows */
-template <typename T, int THREADS, int R>
-__device__ __forceinline__ void load_rows(const Opnd &o, int tid, T (&v)[R])
+/* the operand's elements for this lane's U rows of the group */
+template <typename T, int U>
+__device__ __forceinline__ void load_rows(const Opnd &o, int lane, T (&v)[U])
 {
 	if (o.step == 0) {
 		const T x = SM<T>::ld(o.addr);
 #pragma unroll
-		for (int r = 0; r < R; r++)
-			v[r] = x;
+		for (int u = 0; u < U; u++)
+			v[u] = x;
 	} else {
 #pragma unroll
-		for (int c = 0; c < R / 4; c++)
-			ld_chunk<T>(o.addr + chunk_row<THREADS>(c, tid) * (uint32_t)sizeof(T), v + 4 * c);
+		for (int u = 0; u < U; u++)
+			v[u] = SM<T>::ld(o.addr + (uint32_t)(32 * u + lane) * (uint32_t)sizeof(T));
 	}
 }
 
-/* store the rows whose bit is set in `mask` (whole chunks at once) */
-template <typename T, int THREADS, int R>
-__device__ __forceinline__ void store_rows(uint32_t addr, int tid, const T (&v)[R], uint32_t mask)
+/* store the rows whose bit is set in `mask` */
+template <typename T, int U>
+__device__ __forceinline__ void store_rows(uint32_t addr, int lane, const T (&v)[U], uint32_t mask)
 {
 #pragma unroll
-	for (int c = 0; c < R / 4; c++) {
-		const uint32_t a = addr + chunk_row<THREADS>(c, tid) * (uint32_t)sizeof(T);
-		const uint32_t m = (mask >> (4 * c)) & 0xfu;
-		if (m == 0xfu) {
-			st_chunk<T>(a, v + 4 * c);
-		} else if (m) {
-#pragma unroll
-			for (int k = 0; k < 4; k++)
-				if ((m >> k) & 1u)
-					SM<T>::st(a + k * (uint32_t)sizeof(T), v[4 * c + k]);
-		}
-	}
+	for (int u = 0; u < U; u++)
+		if ((mask >> u) & 1u)
+			SM<T>::st(addr + (uint32_t)(32 * u + lane) * (uint32_t)sizeof(T), v[u]);
 }
 
-/* per-op arguments of the filter */
-struct FArgs {
-	uint32_t sbase, sd, vd;
-	int tid;
+/* Ops over 8-byte values run over a group's rows in halves (rows 32 u +
+ * lane for u in [h0, h0 + H)), so no op holds more than 16 values of a
+ * lane in registers. */
+template <typename T, int U>
+struct Halves {
+	static constexpr int H = sizeof(T) == 8 && U > 8 ? U / 2 : U;
+	static constexpr int N = U / H;
 };
 
-template <typename T, int OP, int THREADS, int R>
-__device__ __forceinline__ void f_cmp(const uint4 &rec, const FArgs &f, RowState &st)
+/* an operand seen from row 32 h0 + lane onward */
+__device__ __forceinline__ Opnd shifted(Opnd o, int h0)
 {
-	T x[R], y[R];
-	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
-	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.z, f.sbase, f.sd, f.vd), f.tid, y);
-	uint32_t bits = 0;
-#pragma unroll
-	for (int r = 0; r < R; r++)
-		bits |= (uint32_t)cmp_eval<T, OP>(x[r], y[r]) << r;
-	take_jump(st, rec.x, st.active & bits);
+	o.addr += (uint32_t)(32 * h0) * o.step;
+	return o;
 }
 
-template <typename T, int THREADS, int R>
-__device__ __forceinline__ void f_not(const uint4 &rec, const FArgs &f, RowState &st)
+template <typename T, int OP, int U>
+__device__ __forceinline__ void f_cmp(const uint4 &rec, const Bases &b, int lane, RowState &st)
 {
-	T x[R];
-	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
-	uint32_t bits = 0;
+	constexpr int H = Halves<T, U>::H;
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b);
+	uint32_t acc[4] = {0u, 0u, 0u, 0u};  /* four independent chains */
 #pragma unroll
-	for (int r = 0; r < R; r++)
-		bits |= (uint32_t)(x[r] == T(0)) << r;
-	take_jump(st, rec.x, st.active & bits);
+	for (int h = 0; h < Halves<T, U>::N; h++) {
+		T x[H], y[H];
+		load_rows<T, H>(shifted(oa, h * H), lane, x);
+		load_rows<T, H>(shifted(ob, h * H), lane, y);
+#pragma unroll
+		for (int u = 0; u < H; u++)
+			acc[u & 3] |= (uint32_t)cmp_eval<T, OP>(x[u], y[u]) << (h * H + u);
+	}
+	take_jump(st, rec.x, st.active & ((acc[0] | acc[1]) | (acc[2] | acc[3])));
+}
+
+template <typename T, int U>
+__device__ __forceinline__ void f_not(const uint4 &rec, const Bases &b, int lane, RowState &st)
+{
+	constexpr int H = Halves<T, U>::H;
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b);
+	uint32_t acc[4] = {0u, 0u, 0u, 0u};  /* four independent chains */
+#pragma unroll
+	for (int h = 0; h < Halves<T, U>::N; h++) {
+		T x[H];
+		load_rows<T, H>(shifted(oa, h * H), lane, x);
+#pragma unroll
+		for (int u = 0; u < H; u++)
+			acc[u & 3] |= (uint32_t)(x[u] == T(0)) << (h * H + u);
+	}
+	take_jump(st, rec.x, st.active & ((acc[0] | acc[1]) | (acc[2] | acc[3])));
 }
 
 /* arithmetic into a register vector: active rows only, unless the register
  * has this single definition (then no row that skips it reads it) */
-template <typename T, int OP, int THREADS, int R>
-__device__ __forceinline__ void f_math(const uint4 &rec, const FArgs &f, const RowState &st)
+template <typename T, int OP, int U>
+__device__ __forceinline__ void f_math(const uint4 &rec, const Bases &b, int lane, const RowState &st)
 {
-	T x[R], y[R];
-	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
-	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.z, f.sbase, f.sd, f.vd), f.tid, y);
+	constexpr int H = Halves<T, U>::H;
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b), od = opnd<sizeof(T)>(rec.w, b);
+	const uint32_t mask = (rec.x & OPH_SINGLE_DEF) ? 0xffffffffu : st.active;
 #pragma unroll
-	for (int r = 0; r < R; r++)
-		x[r] = Math<T, OP>::eval(x[r], y[r]);
-	store_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.w, f.sbase, f.sd, f.vd).addr, f.tid, x,
-		(rec.x & OPH_SINGLE_DEF) ? 0xffffffffu : st.active);
+	for (int h = 0; h < Halves<T, U>::N; h++) {
+		T x[H], y[H];
+		load_rows<T, H>(shifted(oa, h * H), lane, x);
+		load_rows<T, H>(shifted(ob, h * H), lane, y);
+#pragma unroll
+		for (int u = 0; u < H; u++)
+			x[u] = Math<T, OP>::eval(x[u], y[u]);
+		store_rows<T, H>(shifted(od, h * H).addr, lane, x, mask >> (h * H));
+	}
 }
 
 /* Integer/Float into a register vector: active rows only */
-template <int THREADS, int R>
-__device__ __forceinline__ void f_setconst(const uint4 &rec, const FArgs &f, const RowState &st)
+template <int U>
+__device__ __forceinline__ void f_setconst(const uint4 &rec, const Bases &b, int lane, const RowState &st)
 {
-	uint32_t v[R];
-	load_rows<uint32_t, THREADS, R>(opnd<4>(rec.y, f.sbase, f.sd, f.vd), f.tid, v);
-	store_rows<uint32_t, THREADS, R>(opnd<4>(rec.w, f.sbase, f.sd, f.vd).addr, f.tid, v, st.active);
+	uint32_t v[U];
+	load_rows<uint32_t, U>(opnd<4>(rec.y, b), lane, v);
+	store_rows<uint32_t, U>(opnd<4>(rec.w, b).addr, lane, v, st.active);
 }
 
 /* Column/Rowid into a register vector: every row (the CPU copies the whole
  * block, src/vm/virginia.c:448) */
-template <typename T, int THREADS, int R>
-__device__ __forceinline__ void f_copy(const uint4 &rec, const FArgs &f)
+template <typename T, int U>
+__device__ __forceinline__ void f_copy(const uint4 &rec, const Bases &b, int lane)
 {
-	T x[R];
-	load_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.y, f.sbase, f.sd, f.vd), f.tid, x);
-	store_rows<T, THREADS, R>(opnd<sizeof(T)>(rec.w, f.sbase, f.sd, f.vd).addr, f.tid, x, 0xffffffffu);
+	constexpr int H = Halves<T, U>::H;
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), od = opnd<sizeof(T)>(rec.w, b);
+#pragma unroll
+	for (int h = 0; h < Halves<T, U>::N; h++) {
+		T x[H];
+		load_rows<T, H>(shifted(oa, h * H), lane, x);
+		store_rows<T, H>(shifted(od, h * H).addr, lane, x, 0xffffffffu);
+	}
 }
 
-/* operand type and operator tests on a record head */
-__device__ __forceinline__ bool h_type(uint32_t h, int t) { return (h >> (OT_SHIFT + t)) & 1u; }
-__device__ __forceinline__ bool h_op(uint32_t h, int o) { return (h >> (OO_SHIFT + o)) & 1u; }
-
-template <typename T, int THREADS, int R>
-__device__ __forceinline__ void f_cmp_any(const uint4 &rec, const FArgs &f, RowState &st)
+template <typename T, int U>
+__device__ __forceinline__ void f_cmp_any(const uint4 &rec, const Bases &b, int lane, RowState &st)
 {
 	const uint32_t h = rec.x;
-	if (h_op(h, CO_LT)) f_cmp<T, CO_LT, THREADS, R>(rec, f, st);
-	else if (h_op(h, CO_GT)) f_cmp<T, CO_GT, THREADS, R>(rec, f, st);
-	else if (h_op(h, CO_LE)) f_cmp<T, CO_LE, THREADS, R>(rec, f, st);
-	else if (h_op(h, CO_GE)) f_cmp<T, CO_GE, THREADS, R>(rec, f, st);
-	else if (h_op(h, CO_EQ)) f_cmp<T, CO_EQ, THREADS, R>(rec, f, st);
-	else if (h_op(h, CO_NEQ)) f_cmp<T, CO_NEQ, THREADS, R>(rec, f, st);
-	else if (h_op(h, CO_AND)) f_cmp<T, CO_AND, THREADS, R>(rec, f, st);
-	else f_cmp<T, CO_OR, THREADS, R>(rec, f, st);
+	if (h_op(h, CO_LT)) f_cmp<T, CO_LT, U>(rec, b, lane, st);
+	else if (h_op(h, CO_GT)) f_cmp<T, CO_GT, U>(rec, b, lane, st);
+	else if (h_op(h, CO_LE)) f_cmp<T, CO_LE, U>(rec, b, lane, st);
+	else if (h_op(h, CO_GE)) f_cmp<T, CO_GE, U>(rec, b, lane, st);
+	else if (h_op(h, CO_EQ)) f_cmp<T, CO_EQ, U>(rec, b, lane, st);
+	else if (h_op(h, CO_NEQ)) f_cmp<T, CO_NEQ, U>(rec, b, lane, st);
+	else if (h_op(h, CO_AND)) f_cmp<T, CO_AND, U>(rec, b, lane, st);
+	else f_cmp<T, CO_OR, U>(rec, b, lane, st);
 }
 
-template <typename T, int THREADS, int R>
-__device__ __forceinline__ void f_math_any(const uint4 &rec, const FArgs &f, const RowState &st)
+template <typename T, int U>
+__device__ __forceinline__ void f_math_any(const uint4 &rec, const Bases &b, int lane, const RowState &st)
 {
 	const uint32_t h = rec.x;
-	if (h_op(h, MO_ADD)) f_math<T, MO_ADD, THREADS, R>(rec, f, st);
-	else if (h_op(h, MO_SUB)) f_math<T, MO_SUB, THREADS, R>(rec, f, st);
-	else if (h_op(h, MO_MUL)) f_math<T, MO_MUL, THREADS, R>(rec, f, st);
-	else f_math<T, MO_DIV, THREADS, R>(rec, f, st);
+	if (h_op(h, MO_ADD)) f_math<T, MO_ADD, U>(rec, b, lane, st);
+	else if (h_op(h, MO_SUB)) f_math<T, MO_SUB, U>(rec, b, lane, st);
+	else if (h_op(h, MO_MUL)) f_math<T, MO_MUL, U>(rec, b, lane, st);
+	else f_math<T, MO_DIV, U>(rec, b, lane, st);
 }
 
 /* one filter op: kind, then type, then operator, each by bit tests */
-template <int THREADS, int R>
-__device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowState &st)
+template <int U>
+__device__ __forceinline__ void filter_op(const uint4 &rec, const Bases &b, int lane, RowState &st)
 {
 	const uint32_t h = rec.x;
 	const uint32_t join = h >> OPH_JOIN_SHIFT;
@@ -714,106 +672,322 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const FArgs &f, RowS
 			}
 	}
 	if (h & OK_CMP) {
-		if (h_type(h, VT_FLOAT)) f_cmp_any<float, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_INT)) f_cmp_any<int32_t, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_DOUBLE)) f_cmp_any<double, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_INT64)) f_cmp_any<long long, THREADS, R>(rec, f, st);
-		else f_cmp_any<signed char, THREADS, R>(rec, f, st);
+		if (h_type(h, VT_FLOAT)) f_cmp_any<float, U>(rec, b, lane, st);
+		else if (h_type(h, VT_INT)) f_cmp_any<int32_t, U>(rec, b, lane, st);
+		else if (h_type(h, VT_DOUBLE)) f_cmp_any<double, U>(rec, b, lane, st);
+		else if (h_type(h, VT_INT64)) f_cmp_any<long long, U>(rec, b, lane, st);
+		else f_cmp_any<signed char, U>(rec, b, lane, st);
 	} else if (h & OK_INVALID) {
 		st.valid &= ~st.active;
 	} else if (h & OK_MATH) {
-		if (h_type(h, VT_FLOAT)) f_math_any<float, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_INT)) f_math_any<int32_t, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_DOUBLE)) f_math_any<double, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_INT64)) f_math_any<long long, THREADS, R>(rec, f, st);
-		else f_math_any<signed char, THREADS, R>(rec, f, st);
+		if (h_type(h, VT_FLOAT)) f_math_any<float, U>(rec, b, lane, st);
+		else if (h_type(h, VT_INT)) f_math_any<int32_t, U>(rec, b, lane, st);
+		else if (h_type(h, VT_DOUBLE)) f_math_any<double, U>(rec, b, lane, st);
+		else if (h_type(h, VT_INT64)) f_math_any<long long, U>(rec, b, lane, st);
+		else f_math_any<signed char, U>(rec, b, lane, st);
 	} else if (h & OK_NOT) {
-		if (h_type(h, VT_FLOAT)) f_not<float, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_INT)) f_not<int32_t, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_DOUBLE)) f_not<double, THREADS, R>(rec, f, st);
-		else if (h_type(h, VT_INT64)) f_not<long long, THREADS, R>(rec, f, st);
-		else f_not<signed char, THREADS, R>(rec, f, st);
+		if (h_type(h, VT_FLOAT)) f_not<float, U>(rec, b, lane, st);
+		else if (h_type(h, VT_INT)) f_not<int32_t, U>(rec, b, lane, st);
+		else if (h_type(h, VT_DOUBLE)) f_not<double, U>(rec, b, lane, st);
+		else if (h_type(h, VT_INT64)) f_not<long long, U>(rec, b, lane, st);
+		else f_not<signed char, U>(rec, b, lane, st);
 	} else if (h & OK_SETCONST) {
-		f_setconst<THREADS, R>(rec, f, st);
+		f_setconst<U>(rec, b, lane, st);
 	} else if (h & OK_COPY) {
-		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) f_copy<unsigned long long, THREADS, R>(rec, f);
-		else if (h_type(h, VT_CHAR)) f_copy<unsigned char, THREADS, R>(rec, f);
-		else f_copy<uint32_t, THREADS, R>(rec, f);
+		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) f_copy<unsigned long long, U>(rec, b, lane);
+		else if (h_type(h, VT_CHAR)) f_copy<unsigned char, U>(rec, b, lane);
+		else f_copy<uint32_t, U>(rec, b, lane);
 	}
 }
 
-/* ---- projection: the tile's selected rows, in row order ------------------
- * The projection warps share the tile's list: warp p takes the 32-entry
- * batches p, p + P, p + 2 P, ...; entry e is selection index e and its
- * result row lands at the tile's offset + e. */
-
-struct PArgs {
-	uint32_t sbase, sd, vd;
-	uint32_t list;   /* smem address of the tile's list of tile rows (u16) */
-	uint32_t n;      /* entries */
-	uint32_t e0;     /* this lane's first entry */
-	uint32_t step;   /* entries between this lane's entries: 32 P */
-};
-
-/* element address of a list entry */
-__device__ __forceinline__ uint32_t p_addr(const Opnd &o, uint32_t row, uint32_t e)
+/* the filter ops [0, nf) of a record array over one group; returns the
+ * lane's validity bits (rows at or past nrows start invalid) */
+template <int U>
+__device__ __forceinline__ uint32_t run_filter(uint32_t ops, uint32_t nf, const Bases &b, uint32_t nrows, int lane)
 {
-	return o.addr + (o.sel ? e : row) * o.step;
+	RowState st;
+	st.valid = 0;
+#pragma unroll
+	for (int u = 0; u < U; u++)
+		if ((uint32_t)(32 * u + lane) < nrows)
+			st.valid |= 1u << u;
+	st.active = st.valid;
+#pragma unroll
+	for (int s = 0; s < kMaxSlots; s++)
+		st.pend[s] = 0;
+	uint4 rec = lds_v4(ops);
+	for (uint32_t k = 0; k < nf; k++) {
+		const uint4 cur = rec;
+		/* the next record's load overlaps this op */
+		rec = lds_v4(ops + 16u * min(k + 1u, (uint32_t)kMaxOps - 1u));
+		filter_op<U>(cur, b, lane, st);
+	}
+	return st.valid;
 }
+
+/* ---- projection: kBatchE selection entries per lane ----------------------
+ * A batch is 32 kBatchE entries of a group's selection list; entry i of a
+ * lane is batch entry 32 i + lane, at group row row[i].  Register vectors
+ * indexed by selection entry use the batch entry. */
 
 template <typename T, int OP>
-__device__ __forceinline__ void p_math(const uint4 &rec, const PArgs &c)
+__device__ __forceinline__ void p_math(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
+	uint32_t act, int lane)
 {
-	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
-	const Opnd b = opnd<sizeof(T)>(rec.z, c.sbase, c.sd, c.vd);
-	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
-	for (uint32_t e = c.e0; e < c.n; e += c.step) {
-		const uint32_t row = lds_u16(c.list + 2 * e);
-		const T x = SM<T>::ld(p_addr(a, row, e));
-		const T y = SM<T>::ld(p_addr(b, row, e));
-		SM<T>::st(p_addr(d, row, e), Math<T, OP>::eval(x, y));
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b), od = opnd<sizeof(T)>(rec.w, b);
+	T x[kBatchE], y[kBatchE];
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++) {
+		x[i] = SM<T>::ld(oa.addr + (oa.sel ? (uint32_t)(32 * i + lane) : row[i]) * oa.step);
+		y[i] = SM<T>::ld(ob.addr + (ob.sel ? (uint32_t)(32 * i + lane) : row[i]) * ob.step);
 	}
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++)
+		if ((act >> i) & 1u)
+			SM<T>::st(od.addr + (od.sel ? (uint32_t)(32 * i + lane) : row[i]) * od.step, Math<T, OP>::eval(x[i], y[i]));
 }
 
 template <typename T>
-__device__ __forceinline__ void p_copy(const uint4 &rec, const PArgs &c)
+__device__ __forceinline__ void p_copy(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
+	uint32_t act, int lane)
 {
-	const Opnd a = opnd<sizeof(T)>(rec.y, c.sbase, c.sd, c.vd);
-	const Opnd d = opnd<sizeof(T)>(rec.w, c.sbase, c.sd, c.vd);
-	for (uint32_t e = c.e0; e < c.n; e += c.step) {
-		const uint32_t row = lds_u16(c.list + 2 * e);
-		SM<T>::st(p_addr(d, row, e), SM<T>::ld(p_addr(a, row, e)));
-	}
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), od = opnd<sizeof(T)>(rec.w, b);
+	T x[kBatchE];
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++)
+		x[i] = SM<T>::ld(oa.addr + (oa.sel ? (uint32_t)(32 * i + lane) : row[i]) * oa.step);
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++)
+		if ((act >> i) & 1u)
+			SM<T>::st(od.addr + (od.sel ? (uint32_t)(32 * i + lane) : row[i]) * od.step, x[i]);
 }
 
 template <typename T>
-__device__ __forceinline__ void p_math_any(const uint4 &rec, const PArgs &c)
+__device__ __forceinline__ void p_math_any(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
+	uint32_t act, int lane)
 {
 	const uint32_t h = rec.x;
-	if (h_op(h, MO_ADD)) p_math<T, MO_ADD>(rec, c);
-	else if (h_op(h, MO_SUB)) p_math<T, MO_SUB>(rec, c);
-	else if (h_op(h, MO_MUL)) p_math<T, MO_MUL>(rec, c);
-	else p_math<T, MO_DIV>(rec, c);
+	if (h_op(h, MO_ADD)) p_math<T, MO_ADD>(rec, b, row, act, lane);
+	else if (h_op(h, MO_SUB)) p_math<T, MO_SUB>(rec, b, row, act, lane);
+	else if (h_op(h, MO_MUL)) p_math<T, MO_MUL>(rec, b, row, act, lane);
+	else p_math<T, MO_DIV>(rec, b, row, act, lane);
 }
 
 /* one projection op: arithmetic, or a copy (every listed row is active
  * here, so constants and columns are copies) */
-__device__ __forceinline__ void project_op(const uint4 &rec, const PArgs &c)
+__device__ __forceinline__ void project_op(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
+	uint32_t act, int lane)
 {
 	const uint32_t h = rec.x;
 	if (h & OK_MATH) {
-		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, c);
-		else if (h_type(h, VT_INT)) p_math_any<int32_t>(rec, c);
-		else if (h_type(h, VT_DOUBLE)) p_math_any<double>(rec, c);
-		else if (h_type(h, VT_INT64)) p_math_any<long long>(rec, c);
-		else p_math_any<signed char>(rec, c);
+		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, b, row, act, lane);
+		else if (h_type(h, VT_INT)) p_math_any<int32_t>(rec, b, row, act, lane);
+		else if (h_type(h, VT_DOUBLE)) p_math_any<double>(rec, b, row, act, lane);
+		else if (h_type(h, VT_INT64)) p_math_any<long long>(rec, b, row, act, lane);
+		else p_math_any<signed char>(rec, b, row, act, lane);
 	} else if (h & OK_SETCONST) {
-		p_copy<uint32_t>(rec, c);
+		p_copy<uint32_t>(rec, b, row, act, lane);
 	} else if (h & OK_COPY) {
-		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) p_copy<unsigned long long>(rec, c);
-		else if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, c);
-		else p_copy<uint32_t>(rec, c);
+		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) p_copy<unsigned long long>(rec, b, row, act, lane);
+		else if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, b, row, act, lane);
+		else p_copy<uint32_t>(rec, b, row, act, lane);
 	}
+}
+
+/* one result column of a batch: entries whose bit is set in `in` are stored
+ * at pos0 + their batch entry */
+template <typename T>
+__device__ __forceinline__ void p_store(uint32_t od, const Bases &b, const uint32_t (&row)[kBatchE], uint32_t in,
+	T *out, uint64_t pos0, int lane)
+{
+	const Opnd o = opnd<sizeof(T)>(od, b);
+	T v[kBatchE];
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++)
+		v[i] = SM<T>::ld(o.addr + (o.sel ? (uint32_t)(32 * i + lane) : row[i]) * o.step);
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++)
+		if ((in >> i) & 1u)
+			out[pos0 + (uint64_t)(32 * i + lane)] = v[i];
+}
+
+/* ---- groups ------------------------------------------------------------- */
+
+/* count phase: the filter over one group of up to kCountGroup blocks (its
+ * first block is chunk block blk, nblk of them exist); its validity words
+ * go to the chunk's bitmap and a count per block to the block counts */
+__device__ __forceinline__ void count_group(const Bases &b, uint32_t blk, uint32_t nblk, uint32_t nrows, int lane)
+{
+	constexpr int U = kCountGroup * kBlockRows / 32;
+	const uint32_t valid = run_filter<U>(b.slot + kQOpsCount, lds_u32(b.slot + kQNFilter), b, nrows, lane);
+	uint32_t w[U];
+#pragma unroll
+	for (int u = 0; u < U; u++)
+		w[u] = __ballot_sync(0xffffffffu, (valid >> u) & 1u);
+	if (lane == 0) {
+		const uint32_t bm = b.slot + kSlotBitmap + 32u * blk;
+#pragma unroll
+		for (int k = 0; k < kCountGroup; k++)
+			if ((uint32_t)k < nblk) {
+				sts_v4(bm + 32 * k, make_uint4(w[8 * k], w[8 * k + 1], w[8 * k + 2], w[8 * k + 3]));
+				sts_v4(bm + 32 * k + 16, make_uint4(w[8 * k + 4], w[8 * k + 5], w[8 * k + 6], w[8 * k + 7]));
+				uint32_t n = 0;
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+					n += __popc(w[8 * k + u]);
+				sts_u32(b.slot + kSlotBlockCnt + 4u * (blk + k), n);
+			}
+	}
+}
+
+/* one value of a gathered column, read through the non-coherent path (the
+ * tables do not change while a launch runs) */
+__device__ __forceinline__ uint64_t ldg_val(const unsigned char *p, uint32_t stride)
+{
+	if (stride == 4) {
+		uint32_t v;
+		asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
+		return v;
+	}
+	if (stride == 8) {
+		uint64_t v;
+		asm volatile("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(p));
+		return v;
+	}
+	uint32_t v;
+	asm volatile("ld.global.nc.u8 %0, [%1];" : "=r"(v) : "l"(p));
+	return v;
+}
+
+/* FM_GATHER: the batch's selected rows of every gathered column, from
+ * device memory into the warp's gather area (batch entry 32 i + lane at
+ * row grow[i] of the chunk); four columns' loads in flight at a time */
+__device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&grow)[kBatchE], int lane)
+{
+	const uint32_t n = lds_u32(b.slot + kQGatherN);
+	for (uint32_t c0 = 0; c0 < n; c0 += 4) {
+		uint64_t v[4][kBatchE];
+		uint32_t st[4];
+#pragma unroll
+		for (int cc = 0; cc < 4; cc++) {
+			st[cc] = c0 + cc < n ? lds_u8(b.slot + kQGatherStride + c0 + cc) : 0u;
+			if (st[cc]) {
+				const unsigned char *col =
+					reinterpret_cast<const unsigned char *>(lds_u64(b.slot + kSlotColPtr + 8 * (c0 + cc)));
+#pragma unroll
+				for (int i = 0; i < kBatchE; i++)
+					v[cc][i] = ldg_val(col + (size_t)grow[i] * st[cc], st[cc]);
+			}
+		}
+#pragma unroll
+		for (int cc = 0; cc < 4; cc++)
+			if (st[cc]) {
+				const uint32_t dst = b.stage + lds_u32(b.slot + kQGatherOff + 4 * (c0 + cc));
+#pragma unroll
+				for (int i = 0; i < kBatchE; i++) {
+					const uint32_t a = dst + (uint32_t)(32 * i + lane) * st[cc];
+					if (st[cc] == 4)
+						sts_u32(a, (uint32_t)v[cc][i]);
+					else if (st[cc] == 8)
+						sts_u64(a, v[cc][i]);
+					else
+						sts_u8(a, (uint32_t)v[cc][i]);
+				}
+			}
+	}
+}
+
+/* full phase: one group's selected rows (up to kFullGroup blocks from chunk
+ * block blk, nrows rows), in row order, projected and stored at the group's
+ * offset; returns false on an output overflow.  With FM_GATHER the staged
+ * columns are the batch's gathered values (b.stage is the warp's gather
+ * area), indexed by batch entry. */
+__device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32_t blk, uint32_t nrows,
+	uint32_t mode, int lane)
+{
+	/* lane l holds validity word l of the group (32 rows) */
+	const uint32_t nw = (nrows + 31) / 32;
+	const uint32_t word = (uint32_t)lane < nw ? lds_u32(b.slot + kSlotBitmap + 32u * blk + 4u * lane) : 0u;
+	const uint32_t cnt = __popc(word);
+	uint32_t incl = cnt;
+#pragma unroll
+	for (int d = 1; d < 32; d <<= 1) {
+		const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+		if (lane >= d)
+			incl += v;
+	}
+	const uint32_t n = __shfl_sync(0xffffffffu, incl, 31);
+	if (n == 0)
+		return true;
+	const uint32_t nf = lds_u32(b.slot + kQNFilter);
+	const uint32_t ops = b.slot + kQOpsFull;
+	if (mode == FM_REFILTER)
+		(void)run_filter<kCountGroup * kBlockRows / 32>(ops, nf, b, nrows, lane);  /* the filter's register vectors */
+	/* the selection list: entry i is the group row of the group's i-th
+	 * selected row; each lane lists its own word's rows */
+	{
+		uint32_t pos = incl - cnt, w = word;
+		while (w) {
+			const uint32_t bit = __ffs(w) - 1;
+			asm volatile("st.shared.u16 [%0], %1;" ::"r"(list + 2 * pos), "h"((uint16_t)(32 * lane + bit)) : "memory");
+			pos++;
+			w &= w - 1;
+		}
+	}
+	__syncwarp();
+	const uint64_t off = lds_u64(b.slot + kSlotBlockOff + 8u * blk);
+	const uint64_t cap = lds_u64(b.slot + kQCapacity);
+	const uint32_t nu = lds_u32(b.slot + kQNUops) - 1u;
+	const uint32_t nout = lds_u32(b.slot + kQNOut);
+	bool ok = true;
+	for (uint32_t base = 0; base < n; base += 32 * kBatchE) {
+		uint32_t row[kBatchE];
+		uint32_t act = 0, in = 0;
+#pragma unroll
+		for (int i = 0; i < kBatchE; i++) {
+			const uint32_t e = base + 32 * i + (uint32_t)lane;
+			const bool a = e < n;
+			row[i] = 0;
+			if (a) {
+				uint16_t r;
+				asm volatile("ld.shared.u16 %0, [%1];" : "=h"(r) : "r"(list + 2 * e));
+				row[i] = r;
+			}
+			act |= (a ? 1u : 0u) << i;
+			if (a && off + e < cap)
+				in |= 1u << i;
+		}
+		ok = ok && act == in;
+		if (mode == FM_GATHER) {
+			/* gathered values are indexed by batch entry; the chunk row
+			 * of entry i is the group's first row plus its group row */
+			uint32_t grow[kBatchE];
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++) {
+				grow[i] = blk * kBlockRows + row[i];
+				row[i] = 32u * i + (uint32_t)lane;
+			}
+			gather_batch(b, grow, lane);
+			__syncwarp();
+		}
+		for (uint32_t k = nf; k < nu; k++)
+			project_op(lds_v4(ops + 16u * k), b, row, act, lane);
+		for (uint32_t j = 0; j < nout; j++) {
+			const uint32_t od = lds_u32(b.slot + kQOdOut + 4 * j);
+			void *out = reinterpret_cast<void *>(lds_u64(b.slot + kQOutPtr + 8 * j));
+			const uint32_t stride = lds_u8(b.slot + kQOutStride + j);
+			if (stride == 4)
+				p_store<uint32_t>(od, b, row, in, static_cast<uint32_t *>(out), off + base, lane);
+			else if (stride == 8)
+				p_store<unsigned long long>(od, b, row, in, static_cast<unsigned long long *>(out), off + base, lane);
+			else
+				p_store<unsigned char>(od, b, row, in, static_cast<unsigned char *>(out), off + base, lane);
+		}
+		if (mode == FM_GATHER)
+			__syncwarp();  /* the next batch's gather overwrites this one's values */
+	}
+	__syncwarp();
+	return ok;
 }
 
 /* ---- ordered placement ------------------------------------------------- */
@@ -837,47 +1011,25 @@ __device__ __forceinline__ uint64_t status_tag(const KParams &kp, uint64_t idx)
 	return (uint64_t)((kp.epoch + (uint32_t)(idx >> kp.status_shift)) & kEpochMask);
 }
 
-/* rows the query wrote before its first tile: nonzero only for a query
- * continued from an earlier launch */
-__device__ __forceinline__ uint64_t query_base(const QDesc &Q)
+__device__ __forceinline__ void publish(const KParams &kp, uint64_t g, uint64_t flag, uint64_t value)
 {
-	return Q.base_in != nullptr ? *Q.base_in : 0ull;
+	st_status(status_at(kp, g), (status_tag(kp, g) << kStatusEpochShift) | (flag << kStatusFlagShift) |
+		(value & kStatusValueMask));
 }
 
-/* the tile's own count, published by the last compute warp to finish its
- * ballots: an aggregate, or at once an inclusive prefix for a query's first
- * tile.  Publishing here, not in the sequencer, keeps one CTA's look-back
- * from delaying the counts that other CTAs' look-backs wait for. */
-__device__ __forceinline__ void publish_count(const KParams &kp, const QDesc &Q, uint64_t g,
-	uint32_t tile_total)
-{
-	const uint64_t ep = status_tag(kp, g) << kStatusEpochShift;
-	if (g == Q.work_first)
-		st_status(status_at(kp, g), ep | (kFlagPrefix << kStatusFlagShift) |
-			((query_base(Q) + tile_total) & kStatusValueMask));
-	else
-		st_status(status_at(kp, g), ep | (kFlagAggregate << kStatusFlagShift) | tile_total);
-}
-
-/* Rows written by the query's tiles before tile g (its exclusive prefix):
- * walks back over earlier tiles' status words, kLookbackPerLane per lane
+/* Rows written by the query's chunks before chunk g (its exclusive prefix):
+ * walks back over earlier chunks' status words, kLookbackPerLane per lane
  * per round, summing aggregates up to the nearest inclusive prefix.  The
- * caller's own latest tile of the query (known, the index `known` with
- * inclusive prefix `known_end`, or none when known < the query's first
- * tile) is a prefix that needs no load, so the walk never passes it.  It
- * needs only the predecessors, so it runs while tile g itself is still being
- * filtered.  Returns false if a predecessor never published (bounded wait). */
+ * caller's own latest chunk of the query (index `known` with inclusive
+ * prefix `known_end`, or none when known < first) is a prefix that needs no
+ * load, so the walk never passes it.  Returns false if a predecessor never
+ * published (bounded wait). */
 constexpr int kLookbackPerLane = 4;
 
-__device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int64_t known, uint64_t known_end,
+__device__ bool lookback_excl(const KParams &kp, int64_t first, uint64_t g, int64_t known, uint64_t known_end,
 	int lane, uint64_t *excl_out)
 {
 	constexpr int W = 32 * kLookbackPerLane;
-	const int64_t first = (int64_t)Q.work_first;
-	if ((int64_t)g == first) {
-		*excl_out = query_base(Q);
-		return true;
-	}
 	/* indices below `floor` are not read: the query's start, or the known
 	 * prefix (read as a stop) */
 	const int64_t floor = known >= first ? known : first;
@@ -891,14 +1043,13 @@ __device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int
 		for (int x = 0; x < kLookbackPerLane; x++) {
 			const int64_t idx = j - (lane * kLookbackPerLane + x);
 			if (idx < floor || idx == known) {
-				/* a stop: the known prefix, or nothing before the query */
 				v[x] = (idx == known) ? (known_end & kStatusValueMask) : 0ull;
 				stopbits |= 1u << x;
 			} else {
 				v[x] = ld_status(status_at(kp, (uint64_t)idx));
 			}
 		}
-		/* wait until every loaded word carries this launch's epoch and a flag */
+		/* wait until every loaded word carries this launch's tag and a flag */
 		while (true) {
 			wait = 0;
 #pragma unroll
@@ -953,7 +1104,86 @@ __device__ bool lookback_excl(const KParams &kp, const QDesc &Q, uint64_t g, int
 	return true;
 }
 
-/* ---- producer: claims work items and stages their columns ---------------- */
+/* ---- look-back warp: chunk counts -> block offsets ----------------------- */
+
+__device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
+{
+	const uint32_t sbase = smem_addr(smem);
+	const uint32_t flags = sbase + kOffFlags;
+	/* the CTA's previous chunk: one that directly follows it in the same
+	 * query starts where it ended, with no look-back */
+	uint64_t prev_work = ~0ull, prev_end = 0;
+	for (uint32_t i = 0;; i++) {
+		const uint32_t s = i % kChunkSlots;
+		if (!mbar_wait(sbase + kOffCounted + 8 * s, (i / kChunkSlots) & 1u, flags)) {
+			abort_cta(kp, flags, DE_STAGE_TIMEOUT);
+			return;
+		}
+		const uint32_t ci = sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * s;
+		if (!lds_u32(ci + offsetof(ChunkInfo, valid)))
+			return;
+		const uint32_t slot = sbase + kSlotArea + s * kSlotBytes;
+		const uint64_t g = lds_u64(ci + offsetof(ChunkInfo, work));
+		const uint32_t rows = lds_u32(ci + offsetof(ChunkInfo, rows));
+		const uint64_t first = lds_u64(slot + kQWorkFirst);
+		const uint64_t nchunks = lds_u64(slot + kQNChunks);
+		/* the chunk's count: a scan of its block counts, one per lane */
+		const uint32_t nblk = (rows + kBlockRows - 1) / kBlockRows;
+		const uint32_t cnt = (uint32_t)lane < nblk ? lds_u32(slot + kSlotBlockCnt + 4 * lane) : 0u;
+		uint32_t incl = cnt;
+#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+			if (lane >= d)
+				incl += v;
+		}
+		const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+		uint64_t excl = 0;
+		bool ok = true;
+		if (g == first) {
+			const unsigned long long *base_in =
+				reinterpret_cast<const unsigned long long *>(lds_u64(slot + kQBaseIn));
+			excl = base_in != nullptr ? *base_in : 0ull;
+		} else if (g == prev_work + 1) {
+			excl = prev_end;
+		} else {
+			/* the count first, so other CTAs' look-backs see it at once */
+			if (lane == 0)
+				publish(kp, g, kFlagAggregate, total);
+			ok = lookback_excl(kp, (int64_t)first, g,
+				prev_work != ~0ull && prev_work >= first && prev_work < g ? (int64_t)prev_work : -1, prev_end,
+				lane, &excl);
+		}
+		if (!ok) {
+			if (lane == 0)
+				abort_cta(kp, flags, DE_LOOKBACK_TIMEOUT);
+			return;
+		}
+		if (lane == 0) {
+			publish(kp, g, kFlagPrefix, excl + total);
+			if (g == first + nchunks - 1)
+				*reinterpret_cast<unsigned long long *>(lds_u64(slot + kQTotalOut)) = excl + total;
+		}
+		if ((uint32_t)lane < nblk)
+			sts_u64(slot + kSlotBlockOff + 8 * lane, excl + incl - cnt);
+		/* valid rows per 64-row block, for result-tablet splitting on the
+		 * host (the chunk starts on a 64-row block of its segment) */
+		uint8_t *bc = reinterpret_cast<uint8_t *>(lds_u64(slot + kQBlockCounts));
+		if (bc != nullptr) {
+			const uint32_t base = lds_u32(ci + offsetof(ChunkInfo, block_base));
+			for (uint32_t k = (uint32_t)lane; 64 * k < rows; k += 32)
+				bc[base + k] = (uint8_t)(__popc(lds_u32(slot + kSlotBitmap + 8 * k)) +
+					__popc(lds_u32(slot + kSlotBitmap + 8 * k + 4)));
+		}
+		__syncwarp();
+		if (lane == 0)
+			mbar_arrive(sbase + kOffBased + 8 * s);
+		prev_work = g;
+		prev_end = excl + total;
+	}
+}
+
+/* ---- producer: claims chunks and stages their columns -------------------- */
 
 /* last index i in [lo, hi) with a[i] <= t, given a[lo] <= t: a k-ary
  * search in which each of the warp's 32 lanes tests one probe per round, so
@@ -973,115 +1203,132 @@ __device__ __forceinline__ uint32_t warp_search(const T *a, uint32_t lo, uint32_
 	return lo;
 }
 
-/* the producer's copy of the current query's fields (every lane) and of one
- * staged column (lane i < nload holds column i) */
-struct ProdQuery {
-	const QDesc *Q;
-	uint64_t first, end;         /* the query's work items */
-	const SegDesc *segs;
-	const uint32_t *tile_prefix;
-	uint32_t nsegs, nload, qi, seg_hint;
-	uint32_t src, stride, off;   /* this lane's column */
-	/* the current segment: its tiles [seg_t0, seg_t1) of the query, rows,
-	 * and this lane's column in it; seg ~0 when none */
-	uint32_t seg, seg_t0, seg_t1, seg_rows;
-	const unsigned char *colp;
+/* one phase's column for this lane (lane i < n holds column i of the set) */
+struct LaneCol {
+	uint32_t src, stride, off;
+	bool has;
 };
 
-/* one decoded work item; src and bytes are this lane's column copy */
-struct ProdItem {
-	uint32_t w, seg, row0, nrows;
-	const unsigned char *src;
-	uint32_t bytes;
+__device__ __forceinline__ LaneCol lane_col(const LoadSet &ls, int lane)
+{
+	LaneCol c;
+	c.has = (uint32_t)lane < ls.n;
+	c.src = c.has ? ls.src[lane] : 0u;
+	c.stride = c.has ? ls.stride[lane] : 0u;
+	c.off = c.has ? ls.off[lane] : 0u;
+	return c;
+}
+
+/* the producer's copy of the current query's fields (every lane) */
+struct ProdQuery {
+	const QDesc *Q;
+	uint64_t first, end;          /* the query's work items */
+	const SegDesc *segs;
+	const uint32_t *chunk_prefix;
+	uint32_t nsegs, qi, seg_hint, chunk_rows;
+	uint32_t count_tile, full_tile;
+	bool gather;                  /* the full phase gathers (FM_GATHER) */
+	LaneCol cc, fc;               /* this lane's count and full column */
+	/* the current segment: its chunks [seg_c0, seg_c1) of the query, rows,
+	 * first 64-row block and this lane's columns in it; seg ~0 when none */
+	uint32_t seg, seg_c0, seg_c1, seg_rows, seg_block;
+	const unsigned char *ccol, *fcol;
+};
+
+/* a claimed chunk, as the producer issues its phases */
+struct ProdChunk {
+	uint32_t w, slot, seq, rows, row0, qi, block_base;
+	uint32_t count_tile, full_tile;
+	bool gather;
+	LaneCol cc, fc;
+	const unsigned char *ccol, *fcol;  /* this lane's columns at the chunk's first row */
 };
 
 /* decode work item w with the whole producer warp.  A CTA claims work items
  * in increasing order, so the query and segment searches start at the
  * previous item's. */
-template <int TILE>
-__device__ __forceinline__ void decode_item(const KParams &kp, uint32_t w, uint64_t total, uint32_t nq,
-	ProdQuery &pq, ProdItem &it, int lane)
+__device__ __forceinline__ void decode_chunk(const KParams &kp, uint32_t w, uint32_t nq, ProdQuery &pq,
+	ProdChunk &c, int lane)
 {
-	it.w = w;
-	it.bytes = 0;
-	it.src = nullptr;
-	if (w >= total)
-		return;
 	if (pq.Q == nullptr || w >= pq.end) {
 		const uint32_t qi = warp_search(kp.q_work_prefix, pq.Q ? pq.qi : 0u, nq, w, lane);
 		const QDesc *Q = kp.queries + qi;
 		pq.Q = Q;
 		pq.qi = qi;
 		pq.first = Q->work_first;
-		pq.end = pq.first + Q->ntiles;
+		pq.end = pq.first + Q->nchunks;
 		pq.segs = Q->segs;
-		pq.tile_prefix = Q->seg_tile_prefix;
+		pq.chunk_prefix = Q->seg_chunk_prefix;
 		pq.nsegs = Q->nsegs;
-		pq.nload = Q->prog.nload;
+		pq.chunk_rows = Q->chunk_rows;
+		pq.count_tile = Q->count_set.rows;
+		pq.full_tile = Q->full_set.rows;
+		pq.gather = Q->full_mode == FM_GATHER;
+		pq.cc = lane_col(Q->count_set, lane);
+		pq.fc = lane_col(Q->full_set, lane);
 		pq.seg_hint = 0;
 		pq.seg = ~0u;
-		if (lane < kMaxLoads) {
-			pq.src = Q->prog.load_src[lane];
-			pq.stride = Q->prog.load_stride[lane];
-			pq.off = Q->load_off[lane];
-		}
 	}
-	/* an item in the previous item's segment needs no load at all */
+	/* a chunk in the previous chunk's segment needs no load at all */
 	const uint32_t t = (uint32_t)(w - pq.first);
-	if (pq.seg == ~0u || t >= pq.seg_t1) {
-		const uint32_t s = warp_search(pq.tile_prefix, pq.seg_hint, pq.nsegs, t, lane);
+	if (pq.seg == ~0u || t >= pq.seg_c1) {
+		const uint32_t s = warp_search(pq.chunk_prefix, pq.seg_hint, pq.nsegs, t, lane);
 		const SegDesc *sd = pq.segs + s;
 		pq.seg_hint = s;
 		pq.seg = s;
-		pq.seg_t0 = pq.tile_prefix[s];
-		pq.seg_t1 = pq.tile_prefix[s + 1];
+		pq.seg_c0 = pq.chunk_prefix[s];
+		pq.seg_c1 = pq.chunk_prefix[s + 1];
 		pq.seg_rows = sd->rows;
-		if ((uint32_t)lane < pq.nload)
-			pq.colp = static_cast<const unsigned char *>(sd->col[pq.src]);
+		pq.seg_block = sd->block_base;
+		pq.ccol = pq.cc.has ? static_cast<const unsigned char *>(sd->col[pq.cc.src]) : nullptr;
+		pq.fcol = pq.fc.has ? static_cast<const unsigned char *>(sd->col[pq.fc.src]) : nullptr;
 	}
-	const uint32_t row0 = (t - pq.seg_t0) * TILE;
-	it.seg = pq.seg;
-	it.row0 = row0;
-	it.nrows = min((uint32_t)TILE, pq.seg_rows - row0);
-	if ((uint32_t)lane < pq.nload) {
-		it.src = pq.colp + (size_t)row0 * pq.stride;
-		it.bytes = (it.nrows * pq.stride + 15u) & ~15u;
-	}
+	c.w = w;
+	c.qi = pq.qi;
+	c.row0 = (t - pq.seg_c0) * pq.chunk_rows;
+	c.rows = min(pq.chunk_rows, pq.seg_rows - c.row0);
+	c.block_base = pq.seg_block + c.row0 / 64u;
+	c.count_tile = pq.count_tile;
+	c.full_tile = pq.full_tile;
+	c.gather = pq.gather;
+	c.cc = pq.cc;
+	c.fc = pq.fc;
+	c.ccol = pq.ccol ? pq.ccol + (size_t)c.row0 * pq.cc.stride : nullptr;
+	c.fcol = pq.fcol ? pq.fcol + (size_t)c.row0 * pq.fc.stride : nullptr;
 }
 
-/* The producer warp fills the ring of stages.  Once the compute warps
- * released a stage it announces the decoded work item and issues its copies
- * (lane i copies column i; the query descriptor only when the stage does
- * not hold it already), then takes the next claim (in order, with the one
- * after it already in flight) and decodes it while those copies run.
- * Claiming a couple of items ahead, not a whole ring ahead, keeps claimed
- * tiles from idling while other CTAs' look-backs wait for their counts.
- * The claim and decode are the producer's serial path per tile, so the
- * claim's atomic round trip is overlapped and an item in the previous
- * item's segment is decoded without loads.  An invalid claim (past the end of the
- * work list) is announced without data and ends the CTA's pipeline.
+/* The producer warp fills the ring of stages.  For each chunk it claims (in
+ * order, with the next claim's atomic in flight) it waits until the chunk's
+ * slot is free, writes the chunk's info, copies the query's descriptor view
+ * into the slot if the slot held another query, and issues the chunk's
+ * count tiles; then it issues the full tiles of the chunk claimed
+ * kCountAhead chunks earlier.  Lane i
+ * copies column i of a tile; the bytes of a column past its last 16-byte
+ * boundary (a segment's end) are copied with plain loads before the tile is
+ * announced, so no copy reads past a column.  After the last chunk it
+ * announces the end on the next slot and stage.
  *
  * In a serving session the work list grows: a claim past the published
- * work waits for the host's doorbell (or its stop request), and each
- * released stage counts its tile as stored; the tile that completes a
- * query writes the query's completion record. */
-template <int TILE>
+ * work first issues the pending chunks' full tiles (so queries complete),
+ * then waits (bounded) for the host's doorbell or its stop request. */
 __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 {
-	const volatile uint32_t *abort = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags) + kFAbort;
-	uint32_t *held = reinterpret_cast<uint32_t *>(smem + kOffHeld);
+	const uint32_t sbase = smem_addr(smem);
+	const uint32_t flags = sbase + kOffFlags;
 	const uint32_t nst = kp.nstages;
 	const bool serving = kp.serve != nullptr;
-	/* published work and queries: fixed for a launch, growing (from none)
-	 * in a serving session, whose kp.total_work only marks the end item */
 	uint64_t total = serving ? 0ull : kp.total_work;
 	uint32_t nq = serving ? 0u : kp.nq;
-	uint32_t pend = 0;  /* serving: stages whose tile is issued but not yet counted */
 	ProdQuery pq;
 	pq.Q = nullptr;
 	pq.qi = 0;
-	/* claims: one atomic in flight (lane 0) while the previous claim's item
-	 * is decoded and issued, so its round trip is off the per-tile path */
+	uint32_t k = 0;   /* entries issued */
+	uint32_t nb = 0;  /* data buffers taken */
+	uint32_t i = 0;   /* chunks set up (and the end) */
+	bool failed = false;
+
+	/* claims: one atomic in flight (lane 0) while the previous claim's chunk
+	 * is issued, so its round trip is off the per-chunk path */
 	uint32_t inflight = 0;
 	bool have = false;
 	auto claim = [&]() -> uint32_t {
@@ -1096,575 +1343,416 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		}
 		return __shfl_sync(0xffffffffu, v, 0);
 	};
-	/* serving: the tile of stage s is stored; the query's last one reports */
-	auto count_stored = [&](uint32_t s) {
-		const uint32_t qi = held[s];
-		__threadfence();
-		const unsigned done = atomicAdd(&kp.done_tiles[qi], 1u) + 1u;
-		const QDesc *Q = kp.queries + qi;
-		if (done == (unsigned)Q->ntiles) {
-			__threadfence();
-			const unsigned long long rows = *reinterpret_cast<volatile unsigned long long *>(Q->total_out);
-			volatile ServeRec *r = kp.recs + qi;
-			r->rows = rows;
-			__threadfence_system();
-			r->seq = (unsigned long long)qi + 1ull;
+
+	/* one entry: wait for its ring place (and, if it stages data, for a data
+	 * buffer), announce it, copy this lane's column */
+	auto issue = [&](uint32_t kind, const ProdChunk &c, uint32_t row0, uint32_t nrows, bool last,
+		const LaneCol &col, const unsigned char *src, bool desc, bool staged) -> bool {
+		const uint32_t s = k % kEntries;
+		const uint32_t full = sbase + kOffFull + 8 * s;
+		const uint32_t bf = staged ? nb % nst : kNoBuf;
+		int ok = 1;
+		if (lane == 0) {
+			if (k >= kEntries)
+				ok = mbar_wait(sbase + kOffEmpty + 8 * s, ((k / kEntries) - 1) & 1u, flags);
+			if (ok && staged && nb >= nst)
+				ok = mbar_wait(sbase + kOffBfree + 8 * bf, ((nb / nst) - 1) & 1u, flags);
 		}
-	};
-	/* serving: wait for the tiles issued in iterations lo..hi to be stored
-	 * and count them (lane 0) */
-	auto drain = [&](uint32_t lo, uint32_t hi) {
-		for (uint32_t kk = lo; kk <= hi; kk++) {
-			const uint32_t s = kk % nst;
-			if ((pend >> s) & 1u) {
-				if (!mbar_wait(smem_addr(smem + kOffEmpty + 8 * s), (kk / nst) & 1u, abort))
-					return false;
-				count_stored(s);
-				pend &= ~(1u << s);
+		if (!__shfl_sync(0xffffffffu, ok, 0))
+			return false;
+		const uint32_t data = sbase + kp.stage_area + (staged ? bf : 0u) * kp.stage_bytes;
+		uint32_t bulk = 0;
+		if (staged && col.has && nrows) {
+			const uint32_t bytes = nrows * col.stride;
+			bulk = bytes & ~15u;
+			/* the column's last bytes past a 16-byte boundary, with plain
+			 * stores; this lane's later bulk copies into the same stage
+			 * bytes are ordered after them by the proxy fence */
+			if (bulk < bytes) {
+				const unsigned char *p = src + (size_t)row0 * col.stride;
+				for (uint32_t b = bulk; b < bytes; b++)
+					sts_u8(data + col.off + b, *(p + b));
+				fence_proxy_async_smem();
 			}
 		}
+		const uint32_t tx = __reduce_add_sync(0xffffffffu, bulk) + (desc ? kQDescCopy : 0u);
+		if (lane == 0) {
+			const uint32_t si = sbase + kOffStageInfo + (uint32_t)sizeof(StageInfo) * s;
+			sts_v4(si, make_uint4(kind, c.slot, c.seq, row0));
+			sts_v4(si + 16, make_uint4(nrows, last ? 1u : 0u, bf, 0u));
+		}
+		__syncwarp();
+		if (lane == 0) {
+			mbar_arrive_expect_tx(full, tx);
+			/* the tile's info is readable now; its data lands later */
+			mbar_arrive(sbase + kOffAnn + 8 * s);
+		}
+		__syncwarp();
+		if (bulk)
+			bulk_load(data + col.off, src + (size_t)row0 * col.stride, bulk, full);
+		if (desc && lane == 31)
+			bulk_load(sbase + kSlotArea + c.slot * kSlotBytes, kp.queries + c.qi, kQDescCopy, full);
+		k++;
+		if (staged)
+			nb++;
 		return true;
 	};
-	/* the next work item: in a serving session a claim past the published
-	 * work waits (bounded) for the doorbell; ~0 ends the pipeline */
-	auto next_item = [&](uint32_t issued_k) -> uint32_t {
-		const uint32_t w = claim();
-		if (!serving || w < total)
-			return w;
-		uint64_t t0 = 0;
-		int ok = 1;
-		unsigned nap = 1000;  /* ns between doorbell polls, growing while idle */
-		for (;;) {
-			unsigned long long a = 0;
-			unsigned stop = 0;
-			if (lane == 0) {
-				if (issued_k != ~0u && pend)
-					ok = drain(issued_k + 1 > nst ? issued_k + 1 - nst : 0u, issued_k) ? 1 : 0;
-				a = ld_acquire_sys(&kp.serve->avail);
-				stop = *reinterpret_cast<const volatile unsigned *>(&kp.serve->stop);
-			}
-			ok = __shfl_sync(0xffffffffu, ok, 0);
-			a = __shfl_sync(0xffffffffu, a, 0);
-			stop = __shfl_sync(0xffffffffu, stop, 0);
-			total = a & kAvailWorkMask;
-			nq = (uint32_t)(a >> 40);
-			if (w < total)
-				return w;
-			if (stop || !ok)
-				return ~0u;
-			if (t0 == 0)
-				t0 = globaltimer_ns();
-			else if (globaltimer_ns() - t0 > (uint64_t)kp.wait_limit_ms * 1000000ull) {
-				if (lane == 0)
-					report(kp.error, DE_STAGE_TIMEOUT);
-				return ~0u;
-			}
-			__nanosleep(nap);
-			nap = nap < 16000 ? nap * 2 : nap;
-		}
+
+	/* the full phase of a chunk whose count tiles were issued: one entry
+	 * without data when it gathers, else its full tiles */
+	auto issue_full = [&](const ProdChunk &c) -> bool {
+		if (c.gather)
+			return issue(SK_FULL, c, 0, c.rows, true, c.fc, nullptr, false, false);
+		for (uint32_t r = 0; r < c.rows; r += c.full_tile)
+			if (!issue(SK_FULL, c, r, min(c.full_tile, c.rows - r), r + c.full_tile >= c.rows, c.fc, c.fcol, false,
+					true))
+				return false;
+		return true;
 	};
-	ProdItem it;
-	{
-		/* claim first: next_item updates total and nq */
-		const uint32_t w = next_item(~0u);
-		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
+
+	/* wait until slot i % kChunkSlots no longer holds chunk i - kChunkSlots */
+	auto slot_free = [&](uint32_t n) -> bool {
+		if (n < kChunkSlots)
+			return true;
+		int ok = 1;
+		if (lane == 0)
+			ok = mbar_wait(sbase + kOffDone + 8 * (n % kChunkSlots), ((n - kChunkSlots) / kChunkSlots) & 1u, flags);
+		return __shfl_sync(0xffffffffu, ok, 0) != 0;
+	};
+
+	/* chunks whose count tiles are issued and full tiles are not, oldest
+	 * first */
+	ProdChunk pend[kCountAhead];
+	uint32_t npend = 0;
+	auto flush_one = [&]() -> bool {
+		const bool ok = issue_full(pend[0]);
+#pragma unroll
+		for (uint32_t x = 0; x + 1 < kCountAhead; x++)
+			pend[x] = pend[x + 1];
+		npend--;
+		return ok;
+	};
+	for (;;) {
+		uint32_t w = claim();
+		if (serving && w >= total) {
+			/* nothing published to claim yet: finish the pending chunks, then
+			 * wait (bounded) for the doorbell */
+			while (npend && !failed)
+				failed = !flush_one();
+			if (failed)
+				break;
+			uint64_t t0 = 0;
+			unsigned nap = 1000;  /* ns between doorbell polls, growing while idle */
+			bool stop = false;
+			for (;;) {
+				unsigned long long a = 0;
+				unsigned st = 0;
+				if (lane == 0) {
+					a = ld_acquire_sys(&kp.serve->avail);
+					st = *reinterpret_cast<const volatile unsigned *>(&kp.serve->stop);
+				}
+				a = __shfl_sync(0xffffffffu, a, 0);
+				st = __shfl_sync(0xffffffffu, st, 0);
+				total = a & kAvailWorkMask;
+				nq = (uint32_t)(a >> 40);
+				if (w < total)
+					break;
+				if (st || lds_u32(flags + 4 * kFAbort)) {
+					stop = true;
+					break;
+				}
+				if (t0 == 0) {
+					t0 = globaltimer_ns();
+				} else if (globaltimer_ns() - t0 > (uint64_t)kp.wait_limit_ms * 1000000ull) {
+					if (lane == 0)
+						report(kp.error, DE_STAGE_TIMEOUT);
+					stop = true;
+					break;
+				}
+				__nanosleep(nap);
+				nap = nap < 16000 ? nap * 2 : nap;
+			}
+			if (stop)
+				w = ~0u;
+		}
+		if (w >= total) {
+			/* the end: the pending chunks' full tiles, then the end marker */
+			while (npend && !failed)
+				failed = !flush_one();
+			if (failed || !slot_free(i)) {
+				failed = true;
+				break;
+			}
+			ProdChunk e;
+			e.slot = i % kChunkSlots;
+			e.seq = i;
+			e.qi = 0;
+			e.gather = false;
+			if (lane == 0)
+				sts_u32(sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * e.slot + offsetof(ChunkInfo, valid), 0u);
+			LaneCol none;
+			none.has = false;
+			none.src = none.stride = none.off = 0;
+			if (!issue(SK_END, e, 0, 0, true, none, nullptr, false, false))
+				failed = true;
+			break;
+		}
+		ProdChunk c;
+		decode_chunk(kp, w, nq, pq, c, lane);
+		c.slot = i % kChunkSlots;
+		c.seq = i;
+		if (!slot_free(i)) {
+			failed = true;
+			break;
+		}
+		/* a gathering full phase reads the full set's columns of this chunk
+		 * from device memory: their addresses at the chunk's first row */
+		if (c.gather && c.fc.has)
+			sts_u64(sbase + kSlotArea + c.slot * kSlotBytes + kSlotColPtr + 8 * lane,
+				reinterpret_cast<uint64_t>(c.fcol));
+		bool desc = false;
+		if (lane == 0) {
+			const uint32_t ci = sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * c.slot;
+			sts_v4(ci, make_uint4(1u, c.qi, (uint32_t)c.w, 0u));
+			sts_v4(ci + 16, make_uint4(c.rows, c.block_base, 0u, 0u));
+			const uint32_t held = sbase + kOffHeld + 4 * c.slot;
+			desc = lds_u32(held) != c.qi;
+			sts_u32(held, c.qi);
+		}
+		desc = __shfl_sync(0xffffffffu, desc ? 1 : 0, 0) != 0;
+		bool ok = true;
+		for (uint32_t r = 0; ok && r < c.rows; r += c.count_tile)
+			ok = issue(SK_COUNT, c, r, min(c.count_tile, c.rows - r), r + c.count_tile >= c.rows, c.cc, c.ccol,
+				desc && r == 0, true);
+		if (ok && npend == kCountAhead)
+			ok = flush_one();
+		if (!ok) {
+			failed = true;
+			break;
+		}
+		pend[npend++] = c;
+		i++;
 	}
-	uint32_t k = 0;
-	for (;; k++) {
-		const uint32_t s = k % nst, j = k / nst;
-		const uint32_t full = smem_addr(smem + kOffFull + 8 * s);
-		const uint32_t empty = smem_addr(smem + kOffEmpty + 8 * s);
-		if (j >= 1) {
-			int ok = 1;
-			if (lane == 0) {
-				ok = mbar_wait(empty, (j - 1) & 1u, abort);
-				if (!ok && !*abort)
-					report(kp.error, DE_STAGE_TIMEOUT);
-				if (ok && serving && ((pend >> s) & 1u)) {
-					count_stored(s);
-					pend &= ~(1u << s);
+	if (failed) {
+		if (lane == 0) {
+			abort_cta(kp, flags, DE_STAGE_TIMEOUT);
+			/* wait (bounded) for the copies already issued so none lands
+			 * after the CTA exits (entries without data complete at once) */
+			const uint32_t first = k > kEntries ? k - kEntries : 0;
+			for (uint32_t kk = first; kk < k; kk++) {
+				const uint32_t bar = sbase + kOffFull + 8 * (kk % kEntries);
+				const uint64_t t0 = globaltimer_ns();
+				while (!mbar_try_wait_hint(bar, (kk / kEntries) & 1u, kSuspendHintNs) &&
+					globaltimer_ns() - t0 < 1000000000ull) {
 				}
 			}
-			if (!__shfl_sync(0xffffffffu, ok, 0))
-				break;
 		}
-		unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
-		bool end = it.w >= total;
-		if (!end && pq.Q == nullptr) {
-			/* a work item without a decoded query: never copy from it */
+	}
+}
+
+/* ---- compute warps ------------------------------------------------------- */
+
+/* Every compute warp walks the stages in order.  A stage's blocks form
+ * groups (kCountGroup blocks in the count phase; kFullGroup in the full
+ * phase, or kCountGroup when it runs the filter again), and the groups of
+ * all stages are dealt round-robin over the compute warps (warp w takes the
+ * groups whose running number is w mod W), so a stage's groups run in
+ * parallel and a warp with nothing in a stage moves on to the next.  After
+ * a stage a warp releases it; after a chunk's last count tile it arrives on
+ * the chunk's counted barrier; before its first full group of a chunk it
+ * waits for the chunk's offsets; after the chunk's last full tile it arrives
+ * on the chunk's done barrier (the slot is free once all have). */
+template <int W>
+__device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int lane)
+{
+	const uint32_t sbase = smem_addr(smem);
+	const uint32_t flags = sbase + kOffFlags;
+	const uint32_t nst = kp.nstages;
+	const uint32_t warp_base = sbase + kWarpArea + (uint32_t)w * kp.warp_bytes;
+	const uint32_t list = warp_base;
+	const uint32_t gat = warp_base + kp.gat_off;
+	Bases b;
+	b.rowv = warp_base + kp.row_off;
+	b.selv = warp_base + kp.sel_off;
+	uint32_t ng = 0;             /* groups of the stages seen so far */
+	uint32_t based_seq = ~0u;    /* the chunk whose offsets this warp waited for */
+	for (uint32_t k = 0;; k++) {
+		const uint32_t s = k % kEntries;
+		/* the entry's info first: a warp with no group in it releases the
+		 * entry without waiting for its data */
+		if (!mbar_wait(sbase + kOffAnn + 8 * s, (k / kEntries) & 1u, flags)) {
 			if (lane == 0)
-				report(kp.error, DE_BAD_WORK);
-			end = true;
+				abort_cta(kp, flags, DE_STAGE_TIMEOUT);
+			return;
 		}
-		if (lane == 0) {
-			StageInfo si;
-			si.work = end ? ~0u : it.w;
-			si.query = pq.qi;
-			si.seg = it.seg;
-			si.row0 = it.row0;
-			si.nrows = it.nrows;
-			*reinterpret_cast<StageInfo *>(hdr + kQDescStaged) = si;
-		}
-		if (end) {
-			/* serving: every issued tile is counted before the CTA ends */
-			if (serving && lane == 0 && k > 0)
-				drain(k > nst ? k - nst : 0u, k - 1);
+		const uint32_t sia = sbase + kOffStageInfo + (uint32_t)sizeof(StageInfo) * s;
+		const uint4 s0 = lds_v4(sia), s1 = lds_v4(sia + 16);
+		const uint32_t kind = s0.x, slot = s0.y, seq = s0.z, row0 = s0.w, nrows = s1.x, last = s1.y, buf = s1.z;
+		if (kind == SK_END) {
 			__syncwarp();
 			if (lane == 0)
-				mbar_arrive(full);
+				mbar_arrive(sbase + kOffCounted + 8 * slot);
 			return;
 		}
-		const bool copy_desc = held[s] != pq.qi;
-		const uint32_t bytes = __reduce_add_sync(0xffffffffu, it.bytes) +
-			(copy_desc ? (uint32_t)kQDescStaged : 0u);
-		__syncwarp();
-		if (lane == 0) {
-			held[s] = pq.qi;
-			pend |= 1u << s;
-			fence_proxy_async_smem();
-			mbar_arrive_expect_tx(full, bytes);
+		b.slot = sbase + kSlotArea + slot * kSlotBytes;
+		b.stage = buf != kNoBuf ? sbase + kp.stage_area + buf * kp.stage_bytes : gat;
+		const uint32_t nblk = (nrows + kBlockRows - 1) / kBlockRows;
+		const uint32_t blk0 = row0 / kBlockRows;
+		const uint32_t mode = kind == SK_FULL ? lds_u32(b.slot + kQFullMode) : FM_BITMAP;
+		const uint32_t G = kind == SK_COUNT || mode == FM_REFILTER ? (uint32_t)kCountGroup : (uint32_t)kFullGroup;
+		const uint32_t ngs = (nblk + G - 1) / G;
+		const uint32_t j0 = ((uint32_t)w + W - ng % W) % W;
+		ng += ngs;
+		if (j0 < ngs && !mbar_wait(sbase + kOffFull + 8 * s, (k / kEntries) & 1u, flags)) {
+			if (lane == 0)
+				abort_cta(kp, flags, DE_STAGE_TIMEOUT);
+			return;
 		}
-		pend = __shfl_sync(0xffffffffu, pend, 0);
-		__syncwarp();
-		const uint32_t base = smem_addr(hdr);
-		if (it.bytes)
-			bulk_load(base + pq.off, it.src, it.bytes, full);
-		if (copy_desc && lane == 31)
-			bulk_load(base, pq.Q, (uint32_t)kQDescStaged, full);
-		const uint32_t w = next_item(k);
-		decode_item<TILE>(kp, w, total, nq, pq, it, lane);
-	}
-	/* abandoned: wait (bounded) for the copies already issued so none lands
-	 * after the CTA exits */
-	if (lane == 0) {
-		const uint32_t first = k > nst ? k - nst : 0;
-		for (uint32_t kk = first; kk < k; kk++)
-			mbar_wait(smem_addr(smem + kOffFull + 8 * (kk % nst)), (kk / nst) & 1u, nullptr);
-	}
-}
-
-/* ---- look-back warp: tile totals -> result offsets ----------------------- */
-
-template <int THREADS, int R>
-__device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
-{
-	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	const volatile uint32_t *tot = reinterpret_cast<const volatile uint32_t *>(smem + kOffTot);
-	uint64_t *offs = reinterpret_cast<uint64_t *>(smem + kOffOff);
-	const uint32_t nst = kp.nstages;
-	/* the previous tile of this CTA: a tile that directly follows it in the
-	 * same query starts where it ended, with no look-back */
-	uint64_t prev_work = ~0ull, prev_end = 0;
-	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst, q = i % kSlots;
-		/* the tile's data has landed: its work item is known, so the walk
-		 * over earlier tiles starts while the filter warps run */
-		if (!mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort))
-			return;
-		/* the stage holds tile i until the tile's stores, which wait for
-		 * this warp */
-		const unsigned char *hdr = smem + kp.stage_area + s * kp.stage_bytes;
-		const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-		const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + kQDescStaged);
-		if (si.work >= kp.total_work)
-			return;
-		uint64_t excl = 0;
 		bool ok = true;
-		const bool follows = si.work == prev_work + 1 && si.work != Q.work_first;
-		if (follows)
-			excl = prev_end;
-		else
-			ok = lookback_excl(kp, Q, si.work, prev_work == ~0ull ? -1 : (int64_t)prev_work, prev_end, lane, &excl);
-		/* the tile's own count */
-		if (ok && !mbar_wait(smem_addr(smem + kOffTready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
-			return;
-		const uint32_t tile_total = ok ? tot[q] : 0u;
-		prev_work = si.work;
-		prev_end = excl + tile_total;
+		if (kind == SK_COUNT) {
+			for (uint32_t j = j0; j < ngs; j += W) {
+				const uint32_t r = j * kCountGroup * kBlockRows;
+				b.blk_row0 = r;
+				count_group(b, blk0 + j * kCountGroup, min((uint32_t)kCountGroup, nblk - j * kCountGroup),
+					min((uint32_t)(kCountGroup * kBlockRows), nrows - r), lane);
+			}
+		} else {
+			uint32_t j = j0;
+			if (j < ngs && based_seq != seq) {
+				if (!mbar_wait(sbase + kOffBased + 8 * slot, (seq / kChunkSlots) & 1u, flags)) {
+					if (lane == 0)
+						abort_cta(kp, flags, DE_STAGE_TIMEOUT);
+					return;
+				}
+				based_seq = seq;
+			}
+			for (; j < ngs; j += W) {
+				const uint32_t r = j * G * kBlockRows;
+				/* staged columns: the group's rows of the tile; gathered
+				 * columns: the batch's entries of the warp's gather area */
+				b.blk_row0 = mode == FM_GATHER ? 0u : r;
+				ok = full_group(b, list, blk0 + j * G, min(G * kBlockRows, nrows - r), mode, lane) && ok;
+			}
+		}
+		/* a serving session reports rows beyond capacity in the query's
+		 * completion record instead */
+		if (!__all_sync(0xffffffffu, ok) && lane == 0 && kp.serve == nullptr)
+			report(kp.error, DE_OUTPUT_OVERFLOW);
+		const bool account = kind == SK_FULL && last && kp.serve != nullptr;
+		if (account)
+			__threadfence();  /* this warp's result rows before the chunk counts as stored */
 		__syncwarp();
 		if (lane == 0) {
-			if (!ok) {
-				report(kp.error, DE_LOOKBACK_TIMEOUT);
-			} else {
-				/* the inclusive prefix (a query's first tile published its own) */
-				if (si.work != Q.work_first)
-					st_status(status_at(kp, si.work),
-						(status_tag(kp, si.work) << kStatusEpochShift) | (kFlagPrefix << kStatusFlagShift) |
-						((excl + tile_total) & kStatusValueMask));
-				if (si.work == Q.work_first + Q.ntiles - 1)
-					*Q.total_out = excl + tile_total;
-			}
-			offs[q] = excl;
-			flags[q] = ok ? 1u : 0u;
-			if (!ok)
-				flags[kFAbort] = 1u;
-			mbar_arrive(smem_addr(smem + kOffOready + 8 * q));
-		}
-		if (!ok)
-			return;
-	}
-}
-
-/* ---- projection warps: projection and ordered stores of each tile -------- */
-
-template <int THREADS, int R, int P>
-__device__ void proj_warps(const KParams &kp, unsigned char *smem, int pw, int lane)
-{
-	constexpr int TILE = THREADS * R;
-	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	const uint32_t sbase = smem_addr(smem);
-	const uint32_t nst = kp.nstages;
-	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst, q = i % kSlots;
-		if (!mbar_wait(smem_addr(smem + kOffLready + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
-			if (lane == 0 && !flags[kFAbort]) {
-				report(kp.error, DE_STAGE_TIMEOUT);
-				flags[kFAbort] = 1u;
-			}
-			return;
-		}
-		if (flags[kFEnd] == i)
-			return;
-		const uint32_t sd = s * kp.stage_bytes;
-		const uint32_t qd = sbase + kp.stage_area + sd;
-		PArgs c;
-		c.sbase = sbase;
-		c.sd = sd;
-		c.vd = q * lds_u32(qd + kQVecSlot);
-		c.list = sbase + kp.sel_area + q * TILE * 2;
-		c.n = lds_u32(sbase + kOffTot + 4 * q);
-		c.e0 = 32u * (uint32_t)pw + (uint32_t)lane;
-		c.step = 32u * P;
-		const uint32_t ops = qd + kQOps;
-		if (c.e0 - (uint32_t)lane < c.n) {
-			const uint32_t nu = lds_u32(qd + kQNUops) - 1u;
-			for (uint32_t k = lds_u32(qd + kQNFilter); k < nu; k++)
-				project_op(lds_v4(ops + 16u * k), c);
-		}
-
-		/* ---- stores at the tile's offset, once the look-back resolved it */
-		if (!mbar_wait(smem_addr(smem + kOffOready + 8 * q), (i / kSlots) & 1u, flags + kFAbort))
-			return;
-		if (!flags[q])
-			return;
-		const uint64_t off = lds_u64(sbase + kOffOff + 8 * q);
-		if (c.e0 - (uint32_t)lane < c.n) {
-			const uint64_t cap = lds_u64(qd + kQCapacity);
-			bool overflow = false;
-			const uint32_t nout = lds_u32(qd + kQNOut);
-			for (uint32_t j = 0; j < nout; j++) {
-				const uint32_t od = lds_u32(qd + kQOdOut + 4 * j);
-				unsigned char *out = reinterpret_cast<unsigned char *>(lds_u64(qd + kQOutPtr + 8 * j));
-				const uint32_t stride = lds_u8(qd + kQOutStride + j);
-				const Opnd a = stride == 8 ? opnd<8>(od, sbase, sd, c.vd)
-					: stride == 4 ? opnd<4>(od, sbase, sd, c.vd) : opnd<1>(od, sbase, sd, c.vd);
-				uint32_t e0 = c.e0;
-				if (stride == 4) {
-					/* four entries per lane in flight: their list and value
-					 * loads overlap */
-					uint32_t *o32 = reinterpret_cast<uint32_t *>(out);
-					for (; e0 + 3 * c.step < c.n && off + e0 + 3 * c.step < cap; e0 += 4 * c.step) {
-						const uint32_t e1 = e0 + c.step, e2 = e1 + c.step, e3 = e2 + c.step;
-						const uint32_t r0 = lds_u16(c.list + 2 * e0), r1 = lds_u16(c.list + 2 * e1);
-						const uint32_t r2 = lds_u16(c.list + 2 * e2), r3 = lds_u16(c.list + 2 * e3);
-						const uint32_t v0 = lds_u32(p_addr(a, r0, e0)), v1 = lds_u32(p_addr(a, r1, e1));
-						const uint32_t v2 = lds_u32(p_addr(a, r2, e2)), v3 = lds_u32(p_addr(a, r3, e3));
-						o32[off + e0] = v0;
-						o32[off + e1] = v1;
-						o32[off + e2] = v2;
-						o32[off + e3] = v3;
+			if (account) {
+				/* the last warp done with the chunk counts it for its query;
+				 * the chunk that completes the query writes its record */
+				unsigned *fd = reinterpret_cast<unsigned *>(smem + kOffFdone) + slot;
+				if (atomicAdd(fd, 1u) == (unsigned)W - 1u) {
+					*fd = 0u;
+					const uint32_t qi = lds_u32(sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * slot +
+						offsetof(ChunkInfo, query));
+					const uint64_t nch = lds_u64(b.slot + kQNChunks);
+					unsigned long long *tot = reinterpret_cast<unsigned long long *>(lds_u64(b.slot + kQTotalOut));
+					__threadfence();
+					const unsigned done = atomicAdd(&kp.done_chunks[qi], 1u) + 1u;
+					if (done == (unsigned)nch) {
+						__threadfence();
+						const unsigned long long nrow = *reinterpret_cast<volatile unsigned long long *>(tot);
+						volatile ServeRec *r = kp.recs + qi;
+						r->rows = nrow;
+						__threadfence_system();
+						r->seq = (unsigned long long)qi + 1ull;
 					}
 				}
-				for (uint32_t e = e0; e < c.n; e += c.step) {
-					const uint64_t pos = off + e;
-					if (pos >= cap) {
-						overflow = true;
-						break;
-					}
-					const uint32_t at = p_addr(a, lds_u16(c.list + 2 * e), e);
-					if (stride == 4)
-						reinterpret_cast<uint32_t *>(out)[pos] = lds_u32(at);
-					else if (stride == 8)
-						reinterpret_cast<unsigned long long *>(out)[pos] = lds_u64(at);
-					else
-						out[pos] = (unsigned char)lds_u8(at);
-				}
 			}
-			/* a serving session reports rows beyond capacity in the
-			 * query's completion record instead */
-			if (overflow && kp.serve == nullptr)
-				report(kp.error, DE_OUTPUT_OVERFLOW);
-		}
-		__syncwarp();
-		if (lane == 0) {
-			mbar_arrive(smem_addr(smem + kOffEmpty + 8 * s));
-			mbar_arrive(smem_addr(smem + kOffLfree + 8 * q));
+			mbar_arrive(sbase + kOffEmpty + 8 * s);
+			if (buf != kNoBuf)
+				mbar_arrive(sbase + kOffBfree + 8 * buf);
+			if (last)
+				mbar_arrive(sbase + (kind == SK_COUNT ? kOffCounted : kOffDone) + 8 * slot);
 		}
 	}
 }
 
-/* projection warps per CTA: half the filter warps, 1 to 4 */
-template <int THREADS>
-struct ProjWarps {
-	static constexpr int value = THREADS / 64 < 1 ? 1 : THREADS / 64 > 4 ? 4 : THREADS / 64;
-};
-
-template <int THREADS, int R>
-__global__ void __launch_bounds__(THREADS + 32 * (2 + ProjWarps<THREADS>::value)) vm_kernel(const KParams kp)
+template <int W>
+__global__ void __launch_bounds__(32 * (W + 2), 1) vm_kernel(const KParams kp)
 {
-	constexpr int TILE = THREADS * R;
-	constexpr int NW = THREADS / 32;
-	constexpr int C = R / 4;
-	constexpr int P = ProjWarps<THREADS>::value;
-	constexpr int G = 2 * C * NW;          /* 64-row groups per tile */
-	constexpr int PER = (G + 31) / 32;
-	static_assert(R % 4 == 0 && R <= 32, "rows per thread: whole 4-row chunks, 32-bit row masks");
-	static_assert(G <= (int)kMaxGroups, "64-row groups per tile");
-	static_assert(TILE <= 65536, "tile rows are 16-bit in the selection lists");
 	extern __shared__ __align__(128) unsigned char smem[];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	volatile uint32_t *flags = reinterpret_cast<volatile uint32_t *>(smem + kOffFlags);
-	const uint32_t nst = kp.nstages;
-
 	if (tid == 0) {
-		for (uint32_t s = 0; s < nst; s++) {
-			mbar_init(smem_addr(smem + kOffFull + 8 * s), 1);
-			mbar_init(smem_addr(smem + kOffEmpty + 8 * s), P);
+		const uint32_t sbase = smem_addr(smem);
+		for (uint32_t s = 0; s < kEntries; s++) {
+			mbar_init(sbase + kOffFull + 8 * s, 1);
+			mbar_init(sbase + kOffEmpty + 8 * s, W);
+			mbar_init(sbase + kOffAnn + 8 * s, 1);
 		}
-		for (uint32_t q = 0; q < kSlots; q++) {
-			mbar_init(smem_addr(smem + kOffLready + 8 * q), NW);
-			mbar_init(smem_addr(smem + kOffTready + 8 * q), 1);
-			mbar_init(smem_addr(smem + kOffOready + 8 * q), 1);
-			mbar_init(smem_addr(smem + kOffLfree + 8 * q), P);
-			mbar_init(smem_addr(smem + kOffCdone + 8 * q), NW);
+		for (uint32_t s = 0; s < kp.nstages; s++)
+			mbar_init(sbase + kOffBfree + 8 * s, W);
+		for (uint32_t q = 0; q < kChunkSlots; q++) {
+			mbar_init(sbase + kOffCounted + 8 * q, W);
+			mbar_init(sbase + kOffBased + 8 * q, 1);
+			mbar_init(sbase + kOffDone + 8 * q, W);
+			sts_u32(sbase + kOffFdone + 4 * q, 0u);
+			sts_u32(sbase + kOffHeld + 4 * q, ~0u);
 		}
 		for (int x = 0; x < 8; x++)
-			flags[x] = 0;
-		flags[kFEnd] = ~0u;
-		flags[kFWaitMs] = kp.wait_limit_ms;
-		for (uint32_t s = 0; s < kMaxStages; s++)
-			reinterpret_cast<uint32_t *>(smem + kOffHeld)[s] = ~0u;
+			sts_u32(sbase + kOffFlags + 4 * x, 0u);
+		sts_u32(sbase + kOffFlags + 4 * kFWaitMs, kp.wait_limit_ms);
 		fence_mbar_init();
 	}
 	__syncthreads();
-	if (warp == NW) {
-		producer<TILE>(kp, smem, lane);
-		return;
-	}
-	if (warp == NW + 1) {
-		lookback_warp<THREADS, R>(kp, smem, lane);
-		return;
-	}
-	if (warp >= NW + 2) {
-		proj_warps<THREADS, R, P>(kp, smem, warp - (NW + 2), lane);
-		return;
-	}
-
-	/* filter warps */
-	const uint32_t sbase = smem_addr(smem);
-	for (uint32_t i = 0;; i++) {
-		const uint32_t s = i % nst, q = i % kSlots;
-		/* the list and row-vector slot q are free once the projection of
-		 * tile i - kSlots is done */
-		bool ok = i < kSlots ||
-			mbar_wait(smem_addr(smem + kOffLfree + 8 * q), ((i - kSlots) / kSlots) & 1u, flags + kFAbort);
-		ok = ok && mbar_wait(smem_addr(smem + kOffFull + 8 * s), (i / nst) & 1u, flags + kFAbort);
-		if (!ok) {
-			if (lane == 0 && !flags[kFAbort]) {
-				report(kp.error, DE_STAGE_TIMEOUT);
-				flags[kFAbort] = 1u;
-			}
-			return;
-		}
-		const uint32_t sd = s * kp.stage_bytes;
-		const uint32_t qd = sbase + kp.stage_area + sd;
-		const uint32_t sinfo = qd + (uint32_t)kQDescStaged;
-		if (lds_u32(sinfo + offsetof(StageInfo, work)) >= kp.total_work) {
-			/* no more tiles: tell the look-back and projection warps */
-			__syncwarp();
-			if (lane == 0) {
-				flags[kFEnd] = i;
-				mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
-			}
-			return;
-		}
-		const uint32_t nrows = lds_u32(sinfo + offsetof(StageInfo, nrows));
-		const uint32_t vd = q * lds_u32(qd + kQVecSlot);
-
-		/* ---- filter over every row */
-		RowState st;
-		st.valid = 0;
-#pragma unroll
-		for (int c = 0; c < C; c++)
-#pragma unroll
-			for (int k = 0; k < 4; k++)
-				if (chunk_row<THREADS>(c, tid) + k < nrows)
-					st.valid |= 1u << (4 * c + k);
-		st.active = st.valid;
-#pragma unroll
-		for (int sl = 0; sl < kMaxSlots; sl++)
-			st.pend[sl] = 0;
-		{
-			const uint32_t ops = qd + kQOps;
-			const uint32_t nf = lds_u32(qd + kQNFilter);
-			const FArgs f{sbase, sd, vd, tid};
-			uint4 rec = lds_v4(ops);
-			for (uint32_t k = 0; k < nf; k++) {
-				const uint4 cur = rec;
-				/* the next record's load overlaps this op */
-				rec = lds_v4(ops + 16u * min(k + 1u, (uint32_t)kMaxOps - 1u));
-				filter_op<THREADS, R>(cur, f, st);
-			}
-		}
-
-		/* ---- counts per 64 rows, from four bit-plane ballots per 128-row
-		 * chunk of the warp (row k of each lane's 4) */
-		const uint32_t cnt = sbase + kOffCnt + q * kMaxGroups * 4;
-		const uint32_t lt = (1u << lane) - 1u;
-		uint32_t rank[C], total[C];
-#pragma unroll
-		for (int c = 0; c < C; c++) {
-			const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
-			const uint32_t b0 = __ballot_sync(0xffffffffu, m & 1u);
-			const uint32_t b1 = __ballot_sync(0xffffffffu, m & 2u);
-			const uint32_t b2 = __ballot_sync(0xffffffffu, m & 4u);
-			const uint32_t b3 = __ballot_sync(0xffffffffu, m & 8u);
-			total[c] = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
-			rank[c] = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
-			if (lane == 0) {
-				/* lanes 0-15 hold the chunk's first 64 rows */
-				const uint32_t h0 = __popc(b0 & 0xffffu) + __popc(b1 & 0xffffu) + __popc(b2 & 0xffffu) +
-					__popc(b3 & 0xffffu);
-				sts_u32(cnt + 8 * (c * NW + warp), h0);
-				sts_u32(cnt + 8 * (c * NW + warp) + 4, total[c] - h0);
-			}
-		}
-		__syncwarp();
-		if (lane == 0)
-			mbar_arrive(smem_addr(smem + kOffCdone + 8 * q));
-		if (!mbar_wait(smem_addr(smem + kOffCdone + 8 * q), (i / kSlots) & 1u, flags + kFAbort)) {
-			if (lane == 0 && !flags[kFAbort]) {
-				report(kp.error, DE_STAGE_TIMEOUT);
-				flags[kFAbort] = 1u;
-			}
-			return;
-		}
-
-		/* ---- every warp scans the tile's counts: (chunk, warp, half) is row
-		 * order, so a chunk's rows start at the sum of the counts before it */
-		uint32_t loc[PER], lane_pre[PER];
-		uint32_t sum = 0;
-#pragma unroll
-		for (int x = 0; x < PER; x++) {
-			const int g = lane * PER + x;
-			loc[x] = g < G ? lds_u32(cnt + 4 * g) : 0u;
-			lane_pre[x] = sum;
-			sum += loc[x];
-		}
-		uint32_t incl = sum;
-#pragma unroll
-		for (int d = 1; d < 32; d <<= 1) {
-			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
-			if (lane >= d)
-				incl += v;
-		}
-		const uint32_t ex = incl - sum;
-		const uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
-
-		/* ---- the tile's count: to the look-back words (before the list, so
-		 * that other CTAs' look-backs see it as early as possible) and the
-		 * other roles */
-		if (warp == 0) {
-			const unsigned char *hdr = smem + kp.stage_area + sd;
-			const QDesc &Q = *reinterpret_cast<const QDesc *>(hdr);
-			if (lane == 0) {
-				publish_count(kp, Q, lds_u32(sinfo + offsetof(StageInfo, work)), tile_total);
-				sts_u32(sbase + kOffTot + 4 * q, tile_total);
-				mbar_arrive(smem_addr(smem + kOffTready + 8 * q));
-			}
-			/* valid rows per 64-row block, for result-tablet splitting on the
-			 * host: group g covers tile rows 64 g .. 64 g + 63 */
-			if (Q.block_counts != nullptr) {
-				const StageInfo si = *reinterpret_cast<const StageInfo *>(hdr + kQDescStaged);
-				for (int g = lane; g < G; g += 32)
-					if (64u * (uint32_t)g < si.nrows)
-						Q.block_counts[(uint64_t)Q.segs[si.seg].block_base + (si.row0 + 64u * g) / 64] =
-							(uint8_t)lds_u32(cnt + 4 * g);
-			}
-		}
-		/* ---- the tile-ordered list of selected rows */
-		const uint32_t list = sbase + kp.sel_area + q * TILE * 2;
-#pragma unroll
-		for (int c = 0; c < C; c++) {
-			const uint32_t g = 2u * (uint32_t)(c * NW + warp);
-			uint32_t v = 0;
-#pragma unroll
-			for (int x = 0; x < PER; x++)
-				if ((uint32_t)x == g % PER)
-					v = ex + lane_pre[x];
-			const uint32_t base = __shfl_sync(0xffffffffu, v, (int)(g / PER));
-			if (total[c]) {
-				const uint32_t m = (st.valid >> (4 * c)) & 0xfu;
-				uint32_t at = base + rank[c];
-				const uint32_t row0 = chunk_row<THREADS>(c, tid);
-#pragma unroll
-				for (int k = 0; k < 4; k++)
-					if ((m >> k) & 1u)
-						sts_u16(list + 2 * at++, row0 + k);
-			}
-		}
-
-		__syncwarp();
-		if (lane == 0)
-			mbar_arrive(smem_addr(smem + kOffLready + 8 * q));
-	}
+	if (warp == W)
+		producer(kp, smem, lane);
+	else if (warp == W + 1)
+		lookback_warp(kp, smem, lane);
+	else
+		compute_warp<W>(kp, smem, warp, lane);
 }
 
 /* ---- host-side launcher ------------------------------------------------ */
 
-template <int THREADS, int R>
+template <int W>
 static int launch_t(const KParams &kp, unsigned grid, size_t smem, cudaStream_t stream)
 {
-	auto fn = vm_kernel<THREADS, R>;
+	auto fn = vm_kernel<W>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	/* THREADS filter threads, the producer and look-back warps and the projection warps */
-	fn<<<grid, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem, stream>>>(kp);
+	/* W compute warps, the producer and the look-back warp */
+	fn<<<grid, 32 * (W + 2), smem, stream>>>(kp);
 	return cudaGetLastError() == cudaSuccess;
 }
 
-template <int THREADS, int R>
+template <int W>
 static int occ_t(size_t smem, int *ctas)
 {
-	auto fn = vm_kernel<THREADS, R>;
+	auto fn = vm_kernel<W>;
 	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return 0;
-	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, THREADS + 32 * (2 + ProjWarps<THREADS>::value), smem) == cudaSuccess;
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, 32 * (W + 2), smem) == cudaSuccess;
 }
 
-#define VGPU_SHAPES(X) X(128, 4) X(128, 8) X(128, 16) X(256, 4) X(256, 8) X(256, 16) X(512, 4) X(512, 8)
+#define VGPU_WARPS(X) X(4) X(8) X(16)
 
 int shape_supported(const Shape &s)
 {
-#define X(T, R) if (s.threads == T && s.rows_per_thread == R) return 1;
-	VGPU_SHAPES(X)
+#define X(W) if (s.threads == 32 * W) return 1;
+	VGPU_WARPS(X)
 #undef X
 	return 0;
 }
 
 int launch_vm(const Shape &s, const KParams &kp, unsigned grid, size_t smem, void *stream)
 {
-#define X(T, R) \
-	if (s.threads == T && s.rows_per_thread == R) return launch_t<T, R>(kp, grid, smem, (cudaStream_t)stream);
-	VGPU_SHAPES(X)
+#define X(W) if (s.threads == 32 * W) return launch_t<W>(kp, grid, smem, (cudaStream_t)stream);
+	VGPU_WARPS(X)
 #undef X
 	return 0;
 }
 
 int occupancy(const Shape &s, size_t smem, int *ctas)
 {
-#define X(T, R) if (s.threads == T && s.rows_per_thread == R) return occ_t<T, R>(smem, ctas);
-	VGPU_SHAPES(X)
+#define X(W) if (s.threads == 32 * W) return occ_t<W>(smem, ctas);
+	VGPU_WARPS(X)
 #undef X
 	return 0;
 }
