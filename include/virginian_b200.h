@@ -477,6 +477,9 @@ typedef struct {
 	unsigned long long arena_used;   /* result bytes reserved */
 	unsigned device_error;           /* first device error of any session */
 	unsigned shape[4];               /* compute threads, stage KB, stages, grid */
+	unsigned long long restarts;     /* sessions that ended by themselves (a
+	                                  * bounded wait ran out); their unfinished
+	                                  * queries ran again in the next session */
 } virg_serve_counters;
 
 int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cfg, virg_serve **out);
@@ -485,7 +488,9 @@ int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cfg, virg_ser
  * table's rows); a short reservation is admitted again with the exact rows */
 int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_gpu_table *t,
 	uint64_t estimated_rows, uint64_t *ticket);
-/* a query's state; wait_ms < 0 waits for completion, > 0 up to that long */
+/* a query's state; wait_ms < 0 waits for completion, > 0 up to that long.
+ * Fails for a query whose exact result rows need more memory than the
+ * whole result budget (found after it ran with a shorter estimate). */
 int virg_serve_poll(virg_serve *s, uint64_t ticket, int wait_ms, virg_serve_status *st);
 /* copy a completed query's rows to host buffers, one per result column;
  * submissions go on meanwhile (the copy runs outside the loop's lock), so a

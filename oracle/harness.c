@@ -144,7 +144,28 @@ int orc_compile(orc_db *d, const char *sql, virg_vm *out, char *names)
  * library was linked against a real GPU VM).  `repeat` executions are timed
  * and the best wall time is kept; the last run's results stay attached.
  */
+static orc_result *run_query(orc_db *d, const char *sql, int mode, unsigned threads, unsigned repeat,
+	const virg_op *ops, unsigned nops);
+
 orc_result *orc_query(orc_db *d, const char *sql, int mode, unsigned threads, unsigned repeat)
+{
+	return run_query(d, sql, mode, threads, repeat, NULL, 0);
+}
+
+/*
+ * Run a hand-assembled program: `sql` is compiled for its Table,
+ * ResultColumn and Parallel ops (the result layout), then every op of
+ * `ops` except the ResultColumn ops (whose names stay the compiled ones)
+ * replaces the compiled op at the same index and num_ops becomes `nops`.
+ * Used to run opcodes the code generator never emits (And, Or, Not).
+ */
+orc_result *orc_query_ops(orc_db *d, const char *sql, const virg_op *ops, unsigned nops)
+{
+	return run_query(d, sql, 0, 0, 1, ops, nops);
+}
+
+static orc_result *run_query(orc_db *d, const char *sql, int mode, unsigned threads, unsigned repeat,
+	const virg_op *ops, unsigned nops)
 {
 	orc_result *res = calloc(1, sizeof(orc_result));
 	virginian *v = &d->v;
@@ -164,6 +185,18 @@ orc_result *orc_query(orc_db *d, const char *sql, int mode, unsigned threads, un
 			free(vm);
 			free(res);
 			return NULL;
+		}
+		if(ops) {
+			unsigned k;
+			if(nops > VIRG_OPS) {
+				virg_vm_cleanup(v, vm);
+				free(res);
+				return NULL;
+			}
+			for(k = 0; k < nops; k++)
+				if(k >= vm->num_ops || vm->stmt[k].op != OP_ResultColumn)
+					vm->stmt[k] = ops[k];
+			vm->num_ops = nops;
 		}
 		virg_table_loadmem(v, vm->stmt[0].p1);
 		double t0 = now_s();

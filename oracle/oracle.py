@@ -72,6 +72,8 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.orc_compile.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(VirgVM), ctypes.c_char_p]
     lib.orc_query.restype = vp
     lib.orc_query.argtypes = [vp, ctypes.c_char_p, i, u, u]
+    lib.orc_query_ops.restype = vp
+    lib.orc_query_ops.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(VirgOp), u]
     lib.orc_result_rows.restype = ull
     lib.orc_result_rows.argtypes = [vp]
     lib.orc_result_ncols.restype = u
@@ -188,6 +190,19 @@ class OracleDB:
         r = self.lib.orc_query(self.h, sql.encode(), mode, threads, repeat)
         if not r:
             raise ValueError(f"oracle query failed: {sql}")
+        return self._result(r)
+
+    def query_ops(self, sql: str, ops: Sequence[VirgOp]) -> Result:
+        """A hand-assembled program on the single-core CPU VM: `sql` gives
+        the result layout (Table, ResultColumn, Parallel), `ops` the whole
+        program (see orc_query_ops in harness.c)."""
+        arr = (VirgOp * max(1, len(ops)))(*ops)
+        r = self.lib.orc_query_ops(self.h, sql.encode(), arr, len(ops))
+        if not r:
+            raise ValueError(f"oracle could not run the program for: {sql}")
+        return self._result(r)
+
+    def _result(self, r) -> Result:
         try:
             n = self.lib.orc_result_rows(r)
             ncols = self.lib.orc_result_ncols(r)

@@ -6,8 +6,8 @@ import pytest
 
 import virginian_b200 as vb
 from virginian_b200 import datagen
-from tests.helpers import (CONFIG1, EXTRA, SUITE, assert_same_stream, build_oracle_db, col_types,
-                           config2)
+from tests.helpers import (CONFIG1, EXTRA, HAND_PROGRAMS, SUITE, assemble, assert_same_stream, build_oracle_db,
+                           col_types, config2, hand_table)
 
 pytestmark = pytest.mark.gpu
 
@@ -217,3 +217,49 @@ def test_streamed_matches_oracle(oracle_mod, engine, per_chunk):
             assert_same_stream(r.download(), db.query(sql).columns, f"{per_chunk} {sql}")
             assert stats["h2d_bytes"] == n * p.info.load_bytes_per_row
             r.close()
+
+
+@pytest.mark.parametrize("k", range(len(HAND_PROGRAMS)))
+@pytest.mark.parametrize("staged", [0, 1])
+def test_hand_programs_and_or_not(oracle_mod, engine, k, staged):
+    """Hand-assembled programs with And, Or and Not (which the code
+    generator never emits) on both VMs, over a table with many zeros, NaN and
+    signed zeros in its columns."""
+    from oracle.oracle import VirgOp
+    skel, body, _, _ = HAND_PROGRAMS[k]
+    cols = hand_table(300_001, seed=6)
+    db = oracle_mod.OracleDB()
+    with db:
+        db.create_table("test", datagen.SCHEMA_A)
+        db.insert("test", cols["id"], [cols[c] for c, _ in datagen.SCHEMA_A])
+        vm, _ = db.compile(skel)
+        ops, pc = assemble([vm.stmt[j] for j in range(vm.num_ops)], body)
+        vops = []
+        for t in ops:
+            o = VirgOp()
+            o.op, o.p1, o.p2, o.p3, o.p4.i = t
+            vops.append(o)
+        want = db.query_ops(skel, vops).columns
+        t = vb.Table(engine, TYPES_A)
+        t.append(datagen.segments(cols, datagen.SCHEMA_A))
+        engine.set_shape(staged_full=staged)
+        try:
+            r = t.query(vb.Program(ops, pc, TYPES_A))
+            got = r.download()
+            r.close()
+        finally:
+            engine.set_shape(0, 0, 0, 0, 0, 0)
+            t.close()
+        assert_same_stream(got, want, f"hand program {k}")
+
+
+def test_config1_at_one_million_rows(oracle_mod, engine):
+    """The plain CPU-runnable filter at its stated size: 1,000,000 rows."""
+    db, cols = build_oracle_db(oracle_mod, 1_000_000, seed=21)
+    with db:
+        t = vb.Table(engine, TYPES_A)
+        t.append(datagen.segments(cols, datagen.SCHEMA_A))
+        got, want, _ = run_both(db, t, CONFIG1, TYPES_A)
+        assert_same_stream(got, want, "config 1, 1M rows")
+        assert len(want[0]) > 100_000
+        t.close()

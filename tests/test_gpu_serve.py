@@ -146,3 +146,55 @@ def test_rejects_program_beyond_layout(setup):
             s.submit(wide, tables[0])
     finally:
         s.close()
+
+
+def test_bounded_wait_ends_an_idle_session(setup):
+    """A session kernel whose producer waits for the doorbell longer than the
+    session's wait limit stops by itself and reports a stage-wait timeout
+    (no fault, no hang); the loop notices, keeps finished results and runs
+    later queries in a new session."""
+    eng, db, tables, work, alone = setup
+    s = vb.Serve(eng, result_budget_bytes=256 << 20, idle_us=2_000_000, wait_limit_ms=5)
+    try:
+        q, k, p = work[0]
+        t = s.submit(p, tables[k])
+        assert_same_stream(s.download(t), alone[0], "before the timeout")
+        s.release(t)
+        # no submissions for far longer than the wait limit
+        time.sleep(0.3)
+        st = s.stats()
+        assert st["device_error"] == 2, st   # DE_STAGE_TIMEOUT
+        assert st["restarts"] >= 1, st
+        for i in range(1, 4):
+            q, k, p = work[i]
+            t = s.submit(p, tables[k])
+            assert_same_stream(s.download(t), alone[i], "after the timeout")
+            s.release(t)
+        assert s.stats()["sessions"] >= 2
+    finally:
+        s.close()
+
+
+def test_result_larger_than_budget_fails_cleanly(setup):
+    """A query admitted with a short estimate whose exact result needs more
+    memory than the whole result budget fails with an error (it cannot be
+    admitted again), and the loop goes on serving other queries."""
+    eng, db, tables, work, alone = setup
+    big = max(range(len(work)), key=lambda i: len(alone[i][0]) * work[i][2].info.out_bytes_per_row)
+    need = len(alone[big][0]) * work[big][2].info.out_bytes_per_row
+    assert need > 64 << 10
+    s = vb.Serve(eng, result_budget_bytes=32 << 10)
+    try:
+        q, k, p = work[big]
+        t = s.submit(p, tables[k], estimated_rows=1)
+        with pytest.raises(vb.VirgError, match="result budget"):
+            s.wait(t, timeout_s=60)
+        s.release(t)
+        small = min(range(len(work)), key=lambda i: len(alone[i][0]) * work[i][2].info.out_bytes_per_row)
+        assert len(alone[small][0]) * work[small][2].info.out_bytes_per_row < 8 << 10
+        q, k, p = work[small]
+        t = s.submit(p, tables[k], estimated_rows=max(1, len(alone[small][0])))
+        assert_same_stream(s.download(t), alone[small], "after the rejected query")
+        s.release(t)
+    finally:
+        s.close()

@@ -109,3 +109,31 @@ def test_group_must_end_condition_list(oracle_mod):
         with pytest.raises(ValueError):
             db.compile("select col0 from test where (col0 = 1 or col0 = 2) and col0 < 5")
         assert db.query("select col0 from test where col0 < 5 and (col0 = 1 or col0 = 2)").rows == 2
+
+
+def test_hand_programs_and_or_not(oracle_mod):
+    """The CPU VM on hand-assembled And / Or / Not programs equals an
+    independent numpy evaluation (pins the oracle for opcodes the code
+    generator never emits)."""
+    from virginian_b200 import datagen
+    from tests.helpers import HAND_PROGRAMS, assemble, hand_table
+    from oracle.oracle import VirgOp
+    cols = hand_table(20_000, seed=4)
+    db = oracle_mod.OracleDB()
+    with db:
+        db.create_table("test", datagen.SCHEMA_A)
+        db.insert("test", cols["id"], [cols[c] for c, _ in datagen.SCHEMA_A])
+        for skel, body, sel, names in HAND_PROGRAMS:
+            vm, _ = db.compile(skel)
+            ops, _ = assemble([vm.stmt[k] for k in range(vm.num_ops)], body)
+            vops = []
+            for t in ops:
+                o = VirgOp()
+                o.op, o.p1, o.p2, o.p3, o.p4.i = t
+                vops.append(o)
+            got = db.query_ops(skel, vops).columns
+            m = sel(cols)
+            assert m.sum() > 0 and (~m).sum() > 0
+            for g, name in zip(got, names):
+                want = cols[name][m]
+                assert np.array_equal(g.view(np.uint8), want.view(np.uint8)), (skel, body, name)

@@ -362,7 +362,7 @@ class Serve:
         check(lib().virg_serve_stats(self.h, ctypes.byref(c)), "serve stats")
         return {"sessions": c.sessions, "admitted": c.admitted, "readmitted": c.readmitted,
                 "pending": c.pending, "inflight": c.inflight, "arena_used": c.arena_used,
-                "device_error": c.device_error,
+                "device_error": c.device_error, "restarts": c.restarts,
                 "shape": {"threads": c.shape[0], "stage_kb": c.shape[1], "stages": c.shape[2],
                           "grid": c.shape[3]}}
 

@@ -60,7 +60,8 @@ class ServeCounters(ctypes.Structure):
     _fields_ = [("sessions", ctypes.c_uint), ("admitted", ctypes.c_ulonglong),
                 ("readmitted", ctypes.c_ulonglong), ("pending", ctypes.c_ulonglong),
                 ("inflight", ctypes.c_ulonglong), ("arena_used", ctypes.c_ulonglong),
-                ("device_error", ctypes.c_uint), ("shape", ctypes.c_uint * 4)]
+                ("device_error", ctypes.c_uint), ("shape", ctypes.c_uint * 4),
+                ("restarts", ctypes.c_ulonglong)]
 
 
 class ProgramInfo(ctypes.Structure):

@@ -162,6 +162,7 @@ struct virg_serve {
 		void *out[kMaxRegs] = {nullptr};
 		uint64_t rows = 0;
 		int state = 0;  /* 0 pending, 1 in flight, 2 done, 3 failed */
+		std::string error;  /* why it failed */
 		unsigned readmits = 0;
 	};
 	std::map<uint64_t, Query> queries;
@@ -177,7 +178,7 @@ struct virg_serve {
 	size_t chunk_words = 0;  /* segment chunk prefixes written this session */
 	Clock::time_point idle_since;
 	unsigned sessions = 0;
-	unsigned long long launches = 0, admitted_total = 0, readmitted = 0;
+	unsigned long long launches = 0, admitted_total = 0, readmitted = 0, restarts = 0;
 	unsigned device_error = 0;
 
 	std::mutex mu;
@@ -195,13 +196,22 @@ namespace {
 int serve_layout(virg_serve *s)
 {
 	virg_gpu_engine *e = s->e;
-	/* eight compute warps, stages of at least 32 KB that hold a block of the
-	 * widest staging the session admits, one CTA per SM */
-	Shape sh = {256, std::max<unsigned>(32, (kBlockRows * s->cfg.max_load_bytes_per_row + 1023) / 1024), 0, 1,
-		kServeChunkRows, 0};
-	if (!geom_make(sh, s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes,
-			std::min<unsigned>(s->cfg.max_load_bytes_per_row, kGatherMaxBpr), e->smem_optin, e->smem_sm, &s->geom))
-		VGPU_FAIL("serving layout does not fit shared memory");
+	/* eight compute warps, one CTA per SM, the largest data buffers (32 KB
+	 * down to 8 KB, each holding a block of the widest staging the session
+	 * admits) of which at least two fit beside the warps' vector areas */
+	const unsigned min_kb = (kBlockRows * s->cfg.max_load_bytes_per_row + 1023) / 1024;
+	bool fit = false;
+	for (unsigned kb : {32u, 24u, 16u, 8u}) {
+		Shape sh = {256, std::max(kb, min_kb), 0, 1, kServeChunkRows, 0};
+		if (geom_make(sh, s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes,
+				std::min<unsigned>(s->cfg.max_load_bytes_per_row, kGatherMaxBpr), e->smem_optin, e->smem_sm,
+				&s->geom)) {
+			fit = true;
+			break;
+		}
+	}
+	VGPU_CHECK(fit, "serving layout does not fit shared memory (vectors of %u + %u bytes per row)",
+		s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes);
 	int per_sm = 0;
 	if (!occupancy(s->geom.shape, s->geom.smem, &per_sm))
 		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -411,8 +421,19 @@ unsigned harvest(virg_serve *s)
 		const uint64_t rows = r->rows;
 		n++;
 		if (rows > q.capacity) {
-			/* more rows than reserved: again, with exactly that many */
+			/* more rows than reserved: again, with exactly that many, unless
+			 * that many can never fit the result budget */
 			s->arena.release(q.arena_off, q.arena_bytes);
+			q.arena_bytes = 0;
+			if (arena_need(q.p->prog, rows) > s->cfg.result_budget_bytes) {
+				char buf[160];
+				snprintf(buf, sizeof(buf), "the query's %llu result rows need %zu bytes, more than the result budget",
+					(unsigned long long)rows, arena_need(q.p->prog, rows));
+				q.error = buf;
+				q.state = 3;
+				q.completed = Clock::now();
+				continue;
+			}
 			q.estimate_rows = rows;
 			q.state = 0;
 			q.readmits++;
@@ -440,20 +461,26 @@ void scheduler(virg_serve *s)
 			std::unique_lock<std::mutex> lk(s->mu);
 			if (s->running && !s->inflight.empty() && harvest(s))
 				busy = true;
-			/* a session kernel that ended with queries still in flight (a
-			 * device error ended it) fails the loop */
-			if (s->running && !s->inflight.empty() && cudaStreamQuery(s->kstream) != cudaErrorNotReady) {
+			/* a session kernel that ended by itself (a bounded wait ran out:
+			 * the device error word says which) is over: its finished
+			 * queries keep their results, the others are admitted again
+			 * into a new session */
+			if (s->running && cudaStreamQuery(s->kstream) != cudaErrorNotReady) {
 				harvest(s);
-				if (!s->inflight.empty()) {
-					unsigned err = 0;
-					cudaMemcpy(&err, s->d_ctrl + 1, sizeof(err), cudaMemcpyDeviceToHost);
-					char buf[160];
-					snprintf(buf, sizeof(buf), "the serving kernel ended with %zu queries in flight (device error %u: %s)",
-						s->inflight.size(), err, device_error_text(err));
-					s->fail = buf;
-					s->running = false;
-					busy = true;
+				if (!session_stop(s))
+					s->fail = last_error();
+				for (auto it = s->inflight.rbegin(); it != s->inflight.rend(); ++it) {
+					auto &q = s->queries[*it];
+					s->arena.release(q.arena_off, q.arena_bytes);
+					q.arena_bytes = 0;
+					q.state = 0;
+					q.readmits++;
+					s->readmitted++;
+					s->pending.push_front(*it);
 				}
+				s->inflight.clear();
+				s->restarts++;
+				busy = true;
 			}
 			/* a session that cannot take the next query ends once drained */
 			if (s->running && !s->pending.empty() && s->inflight.empty() &&
@@ -613,6 +640,7 @@ extern "C" int virg_serve_poll(virg_serve *s, uint64_t ticket, int wait_ms, virg
 	}
 	VGPU_CHECK(s->fail.empty(), "serving loop failed: %s", s->fail.c_str());
 	const auto &q = it->second;
+	VGPU_CHECK(q.state != 3, "query %llu failed: %s", (unsigned long long)ticket, q.error.c_str());
 	st->done = q.state == 2;
 	st->rows = q.rows;
 	st->readmits = q.readmits;
@@ -665,7 +693,7 @@ extern "C" int virg_serve_release(virg_serve *s, uint64_t ticket)
 	std::lock_guard<std::mutex> lk(s->mu);
 	auto it = s->queries.find(ticket);
 	VGPU_CHECK(it != s->queries.end(), "unknown ticket %llu", (unsigned long long)ticket);
-	VGPU_CHECK(it->second.state == 2, "query %llu has not completed", (unsigned long long)ticket);
+	VGPU_CHECK(it->second.state >= 2, "query %llu has not completed", (unsigned long long)ticket);
 	if (it->second.arena_bytes)
 		s->arena.release(it->second.arena_off, it->second.arena_bytes);
 	s->queries.erase(it);
@@ -683,6 +711,7 @@ extern "C" int virg_serve_stats(virg_serve *s, virg_serve_counters *c)
 	c->inflight = s->inflight.size();
 	c->arena_used = s->arena.used;
 	c->device_error = s->device_error;
+	c->restarts = s->restarts;
 	c->shape[0] = s->geom.shape.threads;
 	c->shape[1] = s->geom.shape.stage_kb;
 	c->shape[2] = s->geom.shape.stages;
