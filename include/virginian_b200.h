@@ -293,7 +293,7 @@ void *virg_gpu_engine_stream(virg_gpu_engine *e);
 /* device error word set by bounded waits inside kernels (0 = none); reading
  * it synchronises the engine stream and clears it */
 int virg_gpu_engine_check(virg_gpu_engine *e, unsigned *device_error);
-/* launch shape: compute threads per CTA (128, 256 or 512; the CTA adds a
+/* launch shape: compute threads per CTA (256, 320, 448 or 512; the CTA adds a
  * producer and a look-back warp), bytes per staging buffer in KB, number of
  * staging buffers, CTAs per SM; 0 in a field keeps the automatic choice */
 int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
@@ -301,10 +301,12 @@ int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 /* upper bound on the rows of a chunk (the unit a CTA claims and places in
  * the ordered result): a multiple of 256 in [256, 8192], 0 for automatic */
 int virg_gpu_engine_set_chunk_rows(virg_gpu_engine *e, unsigned rows);
-/* how the full phase reads the columns the results need: 0 (default)
- * loads only the selected rows' values from device memory where a program
- * allows it, 1 always stages whole tiles of them in shared memory */
-int virg_gpu_engine_set_staging(virg_gpu_engine *e, int staged_full);
+/* how the full phase reads the columns the results need, for programs
+ * whose results read at most 32 bytes per row: 0 (default) stages tiles of
+ * them and picks each batch's selected rows out of the tile, 1 loads only
+ * the selected rows' values straight from device memory, 2 reads the
+ * staged tile in place until the rows are stored */
+int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode);
 /* record CUDA events around each of the next kernel launches in a ring of
  * `slots` entries (0 turns it off) */
 int virg_gpu_engine_timing(virg_gpu_engine *e, unsigned slots);
@@ -398,7 +400,11 @@ int virg_gpu_query_host(virg_gpu_engine *e, const virg_gpu_program *p,
  * it before any stream capture.  Runs on `stream` (a cudaStream_t, NULL for
  * the default stream) and waits for it to return the row count in *out_rows.
  * All calls on a device share the array: calls that overlap in time (other
- * streams or host threads) race; run them one after another. */
+ * streams or host threads) race; run them one after another.
+ * When the result has more rows than `capacity` the call returns 0 with an
+ * error naming both counts, *out_rows still holds the full row count, and the
+ * buffers hold the result's first `capacity` rows; nothing carries over to
+ * the next call. */
 int virg_gpu_query_prealloc(const virg_gpu_program *p, const virg_gpu_segment *seg,
 	void *const *out_cols, uint64_t capacity, uint64_t *out_rows, void *stream);
 

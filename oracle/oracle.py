@@ -55,9 +55,15 @@ class VirgVM(ctypes.Structure):
                 ("timing3", ctypes.c_float)]
 
 
-def build(ref_root: str = "/root/reference") -> None:
+def ref_root() -> str:
+    """The reference checkout the oracle compiles from: $VIRGINIAN_REF, else
+    the path it is mounted at on the build machine."""
+    return os.environ.get("VIRGINIAN_REF", "/root/reference")
+
+
+def build(root: str = "") -> None:
     """Compile the oracle libraries from the reference sources (needs them)."""
-    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_root}"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={root or ref_root()}"], check=True)
 
 
 def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:

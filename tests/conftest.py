@@ -8,7 +8,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REF_SRC = "/root/reference/src"
+REF_SRC = os.path.join(os.environ.get("VIRGINIAN_REF", "/root/reference"), "src")
 
 
 def pytest_configure(config):
@@ -18,7 +18,8 @@ def pytest_configure(config):
 def _ensure_oracle():
     lib = os.path.join(ROOT, "oracle", "_ref", "libvirg_ref.so")
     if not os.path.exists(lib) and os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"),
+                        "REF=" + os.path.dirname(REF_SRC)], check=True)
     return lib
 
 

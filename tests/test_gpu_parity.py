@@ -83,11 +83,11 @@ def test_query_host_end_to_end(data_a, engine):
     assert_same_stream(got, db.query(CONFIG1).columns, "query_host")
 
 
-# (compute threads, stage KB, buffers (0: as many as fit), CTAs per SM, chunk rows, staged full tiles)
-@pytest.mark.parametrize("shape", [(128, 16, 0, 1, 1024, 0), (128, 32, 3, 2, 2048, 0), (256, 16, 0, 1, 8192, 0),
-                                   (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 0), (512, 24, 0, 1, 2048, 0),
-                                   (512, 32, 4, 1, 8192, 0), (256, 8, 0, 1, 256, 0), (256, 24, 0, 1, 4096, 1),
-                                   (128, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1)])
+# (compute threads, stage KB, buffers (0: as many as fit), CTAs per SM, chunk rows, full-phase mode)
+@pytest.mark.parametrize("shape", [(320, 16, 0, 1, 1024, 0), (448, 32, 3, 1, 2048, 2), (256, 16, 0, 1, 8192, 0),
+                                   (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 2), (512, 24, 0, 1, 2048, 0),
+                                   (512, 32, 4, 1, 8192, 2), (256, 8, 0, 1, 256, 0), (256, 24, 0, 1, 4096, 1),
+                                   (320, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1), (256, 8, 0, 1, 256, 2)])
 def test_every_launch_shape(data_a, engine, shape):
     db, _, t = data_a
     engine.set_shape(*shape)
@@ -112,10 +112,10 @@ REFILTER = ["select uniformf + normalf5 as s, id from test where uniformf + norm
             "select id, uniformi - normali5 as d, normalf20 from test where uniformi - normali5 < 20 or normalf20 > 30.0"]
 
 
-@pytest.mark.parametrize("staged", [0, 1])
-def test_filter_vectors_in_results(data_a, engine, staged):
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_filter_vectors_in_results(data_a, engine, mode):
     db, _, t = data_a
-    engine.set_shape(staged_full=staged)
+    engine.set_shape(full_mode=mode)
     try:
         for sql in REFILTER + ["select id, uniformi, normali5, normali20, uniformf, normalf5, normalf20 "
                                "from test where uniformi > 90"]:
@@ -162,9 +162,17 @@ def test_int64_and_double_columns(oracle_mod, engine):
         for sql in ["select id, uniforml, normald from test where normali20 > 15 and uniformf < 50.0",
                     "select normald * normald - normald / normald as dd, id from test where normald > normald * normald",
                     "select uniforml + uniforml as l2, uniforml * uniforml as l3 from test where uniforml < uniforml - uniforml",
-                    "select id, normald from test where normald >= normald + normald or uniformi = 3"]:
-            got, want, _ = run_both(db, t, sql, TYPES_B)
-            assert_same_stream(got, want, sql)
+                    "select id, normald from test where normald >= normald + normald or uniformi = 3",
+                    # 36 result bytes per row: read from the staged tile in place
+                    "select id, uniforml, normald, uniformi, uniformf, normalf5, normalf20 from test "
+                    "where normali20 > 10 or uniformf < 5.0"]:
+            for mode in (0, 1, 2):
+                engine.set_shape(full_mode=mode)
+                try:
+                    got, want, _ = run_both(db, t, sql, TYPES_B)
+                finally:
+                    engine.set_shape(0, 0, 0, 0, 0, 0)
+                assert_same_stream(got, want, f"mode={mode} {sql}")
         t.close()
 
 
@@ -220,8 +228,8 @@ def test_streamed_matches_oracle(oracle_mod, engine, per_chunk):
 
 
 @pytest.mark.parametrize("k", range(len(HAND_PROGRAMS)))
-@pytest.mark.parametrize("staged", [0, 1])
-def test_hand_programs_and_or_not(oracle_mod, engine, k, staged):
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_hand_programs_and_or_not(oracle_mod, engine, k, mode):
     """Hand-assembled programs with And, Or and Not (which the code
     generator never emits) on both VMs, over a table with many zeros, NaN and
     signed zeros in its columns."""
@@ -242,7 +250,7 @@ def test_hand_programs_and_or_not(oracle_mod, engine, k, staged):
         want = db.query_ops(skel, vops).columns
         t = vb.Table(engine, TYPES_A)
         t.append(datagen.segments(cols, datagen.SCHEMA_A))
-        engine.set_shape(staged_full=staged)
+        engine.set_shape(full_mode=mode)
         try:
             r = t.query(vb.Program(ops, pc, TYPES_A))
             got = r.download()

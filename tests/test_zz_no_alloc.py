@@ -2,8 +2,8 @@
 scratch is a fixed device array), against the engine's virg_gpu_query on the
 same rows: identical result streams on two calls in a row, the second on a
 smaller segment, so a counter, status word or row count left over from the
-first call would show.  Collected last on purpose; it must also pass alone in
-a fresh process."""
+first call would show, and both against the reference CPU VM (the oracle).
+Collected last on purpose; it must also pass alone in a fresh process."""
 import ctypes
 
 import numpy as np
@@ -43,9 +43,20 @@ def engine_result(engine, cols, prog):
     return out
 
 
-def prealloc_result(torch, cols, prog, capacity):
+def oracle_result(oracle_mod, cols, text):
+    db = oracle_mod.OracleDB()
+    try:
+        db.create_table("test", datagen.SCHEMA_A)
+        db.insert("test", cols["id"], [cols[c] for c, _ in datagen.SCHEMA_A])
+        return db.query(text).columns
+    finally:
+        db.close()
+
+
+def prealloc_result(torch, cols, prog, capacity, default_stream=False):
     """Runs the no-allocation entry point on device copies of `cols`; the
-    caller (this test) owns every device buffer."""
+    caller (this test) owns every device buffer.  default_stream passes a
+    null stream (the legacy default stream)."""
     n = len(cols["id"])
     dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in cols.items()}
     seg = _lib.Segment()
@@ -58,7 +69,7 @@ def prealloc_result(torch, cols, prog, capacity):
                         device="cuda") for j in range(info.nout)]
     ptrs = (ctypes.c_void_p * max(1, info.nout))(*[o.data_ptr() for o in outs])
     rows = ctypes.c_uint64(0)
-    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    stream = None if default_stream else ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     ok = _lib.lib().virg_gpu_query_prealloc(prog.h, ctypes.byref(seg), ptrs, capacity, ctypes.byref(rows),
                                             stream)
     err = None if ok else _lib.lib().virg_gpu_last_error().decode()
@@ -88,7 +99,7 @@ def assert_same(got, want, what):
         assert g.tobytes() == w.tobytes(), f"{what}: column {j} differs"
 
 
-def test_two_calls_in_a_row_match_engine(torch, engine):
+def test_two_calls_in_a_row_match_engine(torch, engine, oracle_mod):
     big = host_columns(300_001, seed=21)
     small = host_columns(70_001, seed=22)
     q1 = config2(40.0, 15.0)
@@ -104,6 +115,16 @@ def test_two_calls_in_a_row_match_engine(torch, engine):
     assert ok, err
     assert n2 == want2[0].shape[0]
     assert_same(got2, want2, "second call")
+    assert_same(got1, oracle_result(oracle_mod, big, q1), "first call against the oracle")
+    assert_same(got2, oracle_result(oracle_mod, small, q2), "second call against the oracle")
+
+
+def test_null_stream(torch, oracle_mod):
+    cols = host_columns(120_000, seed=24)
+    prog = compile_program(CONFIG1)
+    ok, n, got, err = prealloc_result(torch, cols, prog, 120_000, default_stream=True)
+    assert ok, err
+    assert_same(got, oracle_result(oracle_mod, cols, CONFIG1), "null stream")
 
 
 def test_refuses_more_rows_than_its_scratch(torch):
@@ -128,3 +149,9 @@ def test_small_capacity_reports_overflow(torch, engine):
     assert n == need
     # the rows that fit are the first rows of the full result
     assert_same(got, [w[:100] for w in want], "truncated")
+    # an overflowed call leaves nothing behind: the next call with room
+    # returns the whole result
+    ok, n, got, err = prealloc_result(torch, cols, prog, need)
+    assert ok, err
+    assert n == need
+    assert_same(got, want, "after the overflow")

@@ -80,15 +80,16 @@ class Engine:
         return lib().virg_gpu_engine_stream(self.h)
 
     def set_shape(self, threads: int = 0, stage_kb: int = 0, stages: int = 0,
-                  ctas_per_sm: int = 0, chunk_rows: int = 0, staged_full: int = 0) -> None:
+                  ctas_per_sm: int = 0, chunk_rows: int = 0, full_mode: int = 0) -> None:
         """Launch shape of later queries: compute threads per CTA, KB per
-        staging buffer, buffers, CTAs per SM, the chunk bound and whether
-        the full phase stages whole tiles; 0 in a field keeps the automatic
+        staging buffer, buffers, CTAs per SM, the chunk bound and the full
+        phase's mode (0 pick from staged tiles, 1 gather from device memory,
+        2 read staged tiles in place); 0 in a field keeps the automatic
         choice."""
         check(lib().virg_gpu_engine_set_shape(self.h, threads, stage_kb, stages,
                                               ctas_per_sm), "set shape")
         check(lib().virg_gpu_engine_set_chunk_rows(self.h, chunk_rows), "set chunk rows")
-        check(lib().virg_gpu_engine_set_staging(self.h, staged_full), "set staging")
+        check(lib().virg_gpu_engine_set_full_mode(self.h, full_mode), "set full mode")
 
     def device_error(self) -> int:
         e = ctypes.c_uint()

@@ -91,7 +91,7 @@ static bool uses_a(const UOp &u)
 static bool uses_b(const UOp &u) { return u.kind == UK_CMP || u.kind == UK_MATH; }
 static bool writes_d(const UOp &u) { return u.kind == UK_MATH || u.kind == UK_SETCONST || u.kind == UK_COPYCOL; }
 
-void plan_program(const Program &P, ProgPlan &pp, bool allow_gather)
+void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode)
 {
 	memset(&pp, 0, sizeof(pp));
 	bool in_count[kMaxLoads] = {false}, in_proj[kMaxLoads] = {false};
@@ -135,10 +135,11 @@ void plan_program(const Program &P, ProgPlan &pp, bool allow_gather)
 			pp.full_bpr += P.load_stride[i];
 		}
 	}
-	/* the full phase gathers the selected rows' values unless they are
-	 * many bytes per row */
-	if (allow_gather && pp.mode == FM_BITMAP && pp.full_bpr <= kGatherMaxBpr) {
-		pp.mode = FM_GATHER;
+	/* the full phase moves the selected rows' values into each compute
+	 * warp's area (picked from staged tiles, or gathered from device
+	 * memory) unless they are many bytes per row */
+	if (pp.mode == FM_BITMAP && pp.full_bpr <= kGatherMaxBpr && full_mode != 2) {
+		pp.mode = full_mode == 1 ? FM_GATHER : FM_PICK;
 		pp.gather_bpr = pp.full_bpr;
 	}
 	/* selection vectors hold a projection batch's entries, row vectors a
@@ -259,6 +260,19 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 		load_set(d.full_set, P, pp.full_cols, pp.nfull, tf);
 		d.chunk_rows = chunk;
 	}
+	/* FM_PICK: the batch layout of the warp's area (results read it), and
+	 * where the columns sit in a staged tile (the rows are picked there) */
+	LoadSet pick;
+	if (pp.mode == FM_PICK) {
+		load_set(pick, P, pp.full_cols, pp.nfull, 32u * kBatchE);
+		d.gather_n = pick.n;
+		for (uint32_t i = 0; i < pick.n; i++) {
+			d.gather_stride[i] = pick.stride[i];
+			d.gather_off[i] = pick.off[i];
+			d.tile_off[i] = d.full_set.off[i];
+		}
+	}
+	const LoadSet &rset = pp.mode == FM_PICK ? pick : d.full_set;
 	d.full_mode = pp.mode;
 	for (unsigned i = 0; i < kMaxRegs; i++) {
 		d.consts[i] = P.consts[i];
@@ -301,10 +315,10 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 			d.ops_full[k] = OpRec{op_head(P.uops[k]), 0u, 0u, 0u};
 			continue;
 		}
-		d.ops_full[k] = rec(P.uops[k], d.full_set, pp.full_cols, pp.nfull, &bad);
+		d.ops_full[k] = rec(P.uops[k], rset, pp.full_cols, pp.nfull, &bad);
 	}
 	for (uint32_t j = 0; j < P.nout; j++)
-		d.od_out[j] = od(P.out_cls[j], P.out_idx[j], d.full_set, pp.full_cols, pp.nfull, &bad);
+		d.od_out[j] = od(P.out_cls[j], P.out_idx[j], rset, pp.full_cols, pp.nfull, &bad);
 	VGPU_CHECK(!bad, "internal: a result operand is not staged in the full phase");
 	return 1;
 }
@@ -344,13 +358,13 @@ KParams geom_params(const Geom &g)
 }
 
 /* the widest vector areas and staging of a launch's programs */
-static void launch_needs(const std::vector<QueryLaunch> &qs, bool allow_gather, uint32_t *sel, uint32_t *row,
+static void launch_needs(const std::vector<QueryLaunch> &qs, unsigned full_mode, uint32_t *sel, uint32_t *row,
 	uint32_t *gat, uint32_t *bpr)
 {
 	*sel = *row = *gat = *bpr = 0;
 	for (const QueryLaunch &q : qs) {
 		ProgPlan pp;
-		plan_program(*q.prog, pp, allow_gather);
+		plan_program(*q.prog, pp, full_mode);
 		*sel = std::max(*sel, pp.sel_bpr);
 		*row = std::max(*row, pp.row_bpr);
 		*gat = std::max(*gat, pp.gather_bpr);
@@ -361,9 +375,9 @@ static void launch_needs(const std::vector<QueryLaunch> &qs, bool allow_gather, 
 int choose_shape(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, Geom *g)
 {
 	uint32_t sel, row, gat, bpr;
-	launch_needs(qs, !e->pref.staged_full, &sel, &row, &gat, &bpr);
+	launch_needs(qs, e->pref.full_mode, &sel, &row, &gat, &bpr);
 	Shape s;
-	s.staged_full = e->pref.staged_full;
+	s.full_mode = e->pref.full_mode;
 	s.threads = e->pref.threads ? e->pref.threads : 256;
 	s.stage_kb = e->pref.stage_kb ? e->pref.stage_kb : 32;
 	s.stages = e->pref.stages;
@@ -405,7 +419,7 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 	VGPU_CHECK(!qs.empty(), "no queries");
 	if (forced) {
 		uint32_t sel, row, gat, bpr;
-		launch_needs(qs, !forced->staged_full, &sel, &row, &gat, &bpr);
+		launch_needs(qs, forced->full_mode, &sel, &row, &gat, &bpr);
 		VGPU_CHECK(geom_make(*forced, sel, row, gat, e->smem_optin, e->smem_sm, &plan.geom),
 			"shape does not fit shared memory");
 	} else if (!choose_shape(e, qs, &plan.geom)) {
@@ -442,7 +456,7 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		const QueryLaunch &q = qs[i];
 		QDesc &d = hq[i];
 		ProgPlan pp;
-		plan_program(*q.prog, pp, !g.shape.staged_full);
+		plan_program(*q.prog, pp, g.shape.full_mode);
 		if (!desc_fill(d, *q.prog, pp, g, cap))
 			return 0;
 		d.segs = q.d_segs;
@@ -703,11 +717,12 @@ namespace vgpu {
 std::vector<Shape> tune_candidates()
 {
 	std::vector<Shape> c;
-	for (unsigned threads : {256u, 512u})
-		for (unsigned kb : {16u, 24u, 32u, 48u})
-			for (unsigned chunk : {2048u, 4096u, 8192u})
-				c.push_back(Shape{threads, kb, 0, 1, chunk, 0});
-	for (unsigned kb : {24u, 48u})
+	for (unsigned threads : {256u, 320u, 448u})
+		for (unsigned kb : {24u, 32u, 40u, 48u})
+			for (unsigned chunk : {4096u, 8192u})
+				for (unsigned mode : {0u, 2u})
+					c.push_back(Shape{threads, kb, 0, 1, chunk, mode});
+	for (unsigned kb : {16u, 32u})
 		c.push_back(Shape{256, kb, 0, 1, 8192, 1});
 	return c;
 }
@@ -783,7 +798,7 @@ extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 	VGPU_CHECK(e != nullptr, "null engine");
 	if (threads) {
 		Shape s = {threads, 32, 2, 1, 0, 0};
-		VGPU_CHECK(shape_supported(s), "unsupported shape: %u compute threads (128, 256 or 512)", threads);
+		VGPU_CHECK(shape_supported(s), "unsupported shape: %u compute threads (256, 320, 448 or 512)", threads);
 	}
 	VGPU_CHECK(stage_kb <= 192, "stage size %u KB out of range", stage_kb);
 	VGPU_CHECK(stages <= kMaxStages, "at most %u stages", kMaxStages);
@@ -794,10 +809,11 @@ extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 	return 1;
 }
 
-extern "C" int virg_gpu_engine_set_staging(virg_gpu_engine *e, int staged_full)
+extern "C" int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode)
 {
 	VGPU_CHECK(e != nullptr, "null engine");
-	e->pref.staged_full = staged_full ? 1u : 0u;
+	VGPU_CHECK(mode <= 2, "full-phase mode %u: 0 pick, 1 gather, 2 in place", mode);
+	e->pref.full_mode = mode;
 	return 1;
 }
 

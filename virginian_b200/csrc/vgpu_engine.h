@@ -30,7 +30,8 @@ struct Shape {
 	unsigned stages;
 	unsigned ctas_per_sm;  /* 0: as many as fit */
 	unsigned chunk_rows;   /* upper bound on rows per chunk; 0: automatic */
-	unsigned staged_full;  /* 1: stage full tiles even where the full phase could gather */
+	unsigned full_mode;    /* full phase of programs whose results read few bytes per row: 0 picks rows out
+	                        * of staged tiles, 1 gathers them from device memory, 2 reads staged tiles in place */
 	unsigned warps() const { return threads / 32; }
 	unsigned stage_bytes() const { return stage_kb * 1024u; }
 };
@@ -104,7 +105,8 @@ constexpr unsigned kOffBfree = kOffAnn + 8 * kEntries;             /* u64[kMaxSt
 constexpr unsigned kOffCounted = kOffBfree + 8 * kMaxStages;       /* u64[kChunkSlots] */
 constexpr unsigned kOffBased = kOffCounted + 8 * kChunkSlots;      /* u64[kChunkSlots] */
 constexpr unsigned kOffDone = kOffBased + 8 * kChunkSlots;         /* u64[kChunkSlots] */
-constexpr unsigned kOffFlags = kOffDone + 8 * kChunkSlots;         /* u32[8] */
+constexpr unsigned kOffDesc = kOffDone + 8 * kChunkSlots;          /* u64[kChunkSlots]: the slot's descriptor view landed */
+constexpr unsigned kOffFlags = kOffDesc + 8 * kChunkSlots;         /* u32[8] */
 constexpr unsigned kOffFdone = kOffFlags + 32;                     /* u32[kChunkSlots] */
 constexpr unsigned kOffHeld = kOffFdone + 4 * kChunkSlots;         /* u32[kChunkSlots] */
 constexpr unsigned kOffStageInfo = (kOffHeld + 4 * kChunkSlots + 31) / 32 * 32;

@@ -71,6 +71,7 @@ constexpr uint32_t kQNChunks = (uint32_t)offsetof(QDesc, nchunks);
 constexpr uint32_t kQGatherN = (uint32_t)offsetof(QDesc, gather_n);
 constexpr uint32_t kQGatherStride = (uint32_t)offsetof(QDesc, gather_stride);
 constexpr uint32_t kQGatherOff = (uint32_t)offsetof(QDesc, gather_off);
+constexpr uint32_t kQTileOff = (uint32_t)offsetof(QDesc, tile_off);
 static_assert(kQOpsCount % 16 == 0 && kQOpsFull % 16 == 0, "op records are read 16 bytes at a time");
 static_assert(kSlotBitmap % 16 == 0 && kSlotBlockOff % 8 == 0, "slot layout");
 static_assert(kOffStageInfo % 16 == 0 && sizeof(StageInfo) == 32, "stage info is read as two 16-byte words");
@@ -538,15 +539,6 @@ __device__ __forceinline__ void store_rows(uint32_t addr, int lane, const T (&v)
 			SM<T>::st(addr + (uint32_t)(32 * u + lane) * (uint32_t)sizeof(T), v[u]);
 }
 
-/* Ops over 8-byte values run over a group's rows in halves (rows 32 u +
- * lane for u in [h0, h0 + H)), so no op holds more than 16 values of a
- * lane in registers. */
-template <typename T, int U>
-struct Halves {
-	static constexpr int H = sizeof(T) == 8 && U > 8 ? U / 2 : U;
-	static constexpr int N = U / H;
-};
-
 /* an operand seen from row 32 h0 + lane onward */
 __device__ __forceinline__ Opnd shifted(Opnd o, int h0)
 {
@@ -554,107 +546,143 @@ __device__ __forceinline__ Opnd shifted(Opnd o, int h0)
 	return o;
 }
 
-template <typename T, int OP, int U>
-__device__ __forceinline__ void f_cmp(const uint4 &rec, const Bases &b, int lane, RowState &st)
+/* The op handlers of the 4-byte types run inline, fully unrolled over the
+ * lane's U rows; those of the 8-byte and char types run out of line, over
+ * chunks of four rows, with every argument passed by value, so that the
+ * kernel's hot code (the 4-byte paths) stays small enough for the
+ * instruction cache.  A handler computes a row mask (compares and Not) or
+ * writes a register vector (arithmetic and copies); the caller applies the
+ * mask to the row state. */
+
+/* row mask of a compare (OP) or, for OP = -1, of Not (the value is zero) */
+template <typename T, int OP>
+__device__ __forceinline__ bool test_eval(T x, T y)
 {
-	constexpr int H = Halves<T, U>::H;
+	if constexpr (OP < 0)
+		return x == T(0);
+	else
+		return cmp_eval<T, OP>(x, y);
+}
+
+template <typename T, int OP, int U>
+__device__ __forceinline__ uint32_t bits_rows(const uint4 &rec, const Bases &b, int lane)
+{
 	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b);
+	T x[U], y[U];
+	load_rows<T, U>(oa, lane, x);
+	if constexpr (OP >= 0)
+		load_rows<T, U>(ob, lane, y);
 	uint32_t acc[4] = {0u, 0u, 0u, 0u};  /* four independent chains */
 #pragma unroll
-	for (int h = 0; h < Halves<T, U>::N; h++) {
-		T x[H], y[H];
-		load_rows<T, H>(shifted(oa, h * H), lane, x);
-		load_rows<T, H>(shifted(ob, h * H), lane, y);
-#pragma unroll
-		for (int u = 0; u < H; u++)
-			acc[u & 3] |= (uint32_t)cmp_eval<T, OP>(x[u], y[u]) << (h * H + u);
-	}
-	take_jump(st, rec.x, st.active & ((acc[0] | acc[1]) | (acc[2] | acc[3])));
+	for (int u = 0; u < U; u++)
+		acc[u & 3] |= (uint32_t)test_eval<T, OP>(x[u], OP >= 0 ? y[u] : x[u]) << u;
+	return (acc[0] | acc[1]) | (acc[2] | acc[3]);
 }
 
-template <typename T, int U>
-__device__ __forceinline__ void f_not(const uint4 &rec, const Bases &b, int lane, RowState &st)
-{
-	constexpr int H = Halves<T, U>::H;
-	const Opnd oa = opnd<sizeof(T)>(rec.y, b);
-	uint32_t acc[4] = {0u, 0u, 0u, 0u};  /* four independent chains */
-#pragma unroll
-	for (int h = 0; h < Halves<T, U>::N; h++) {
-		T x[H];
-		load_rows<T, H>(shifted(oa, h * H), lane, x);
-#pragma unroll
-		for (int u = 0; u < H; u++)
-			acc[u & 3] |= (uint32_t)(x[u] == T(0)) << (h * H + u);
-	}
-	take_jump(st, rec.x, st.active & ((acc[0] | acc[1]) | (acc[2] | acc[3])));
-}
-
-/* arithmetic into a register vector: active rows only, unless the register
- * has this single definition (then no row that skips it reads it) */
+/* the same over chunks of four rows, a loop the compiler keeps rolled */
 template <typename T, int OP, int U>
-__device__ __forceinline__ void f_math(const uint4 &rec, const Bases &b, int lane, const RowState &st)
+__device__ __forceinline__ uint32_t bits_chunked(const uint4 &rec, const Bases &b, int lane)
 {
-	constexpr int H = Halves<T, U>::H;
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b);
+	uint32_t bits = 0;
+#pragma unroll 1
+	for (int c = 0; c < U / 4; c++) {
+		T x[4], y[4];
+		load_rows<T, 4>(shifted(oa, 4 * c), lane, x);
+		if constexpr (OP >= 0)
+			load_rows<T, 4>(shifted(ob, 4 * c), lane, y);
+#pragma unroll
+		for (int u = 0; u < 4; u++)
+			bits |= (uint32_t)test_eval<T, OP>(x[u], OP >= 0 ? y[u] : x[u]) << (4 * c + u);
+	}
+	return bits;
+}
+
+template <typename T, int U, bool CHUNKED>
+__device__ __forceinline__ uint32_t bits_any(const uint4 &rec, const Bases &b, int lane)
+{
+	const uint32_t h = rec.x;
+#define VGPU_BITS(OP) (CHUNKED ? bits_chunked<T, OP, U>(rec, b, lane) : bits_rows<T, OP, U>(rec, b, lane))
+	if (h & OK_NOT) return VGPU_BITS(-1);
+	if (h_op(h, CO_LT)) return VGPU_BITS(CO_LT);
+	if (h_op(h, CO_GT)) return VGPU_BITS(CO_GT);
+	if (h_op(h, CO_LE)) return VGPU_BITS(CO_LE);
+	if (h_op(h, CO_GE)) return VGPU_BITS(CO_GE);
+	if (h_op(h, CO_EQ)) return VGPU_BITS(CO_EQ);
+	if (h_op(h, CO_NEQ)) return VGPU_BITS(CO_NEQ);
+	if (h_op(h, CO_AND)) return VGPU_BITS(CO_AND);
+	return VGPU_BITS(CO_OR);
+#undef VGPU_BITS
+}
+
+/* arithmetic (OP) or, for OP = -1, a copy of operand a into a register
+ * vector, for the rows in `mask` */
+template <typename T, int OP, int U>
+__device__ __forceinline__ void vec_rows(const uint4 &rec, const Bases &b, int lane, uint32_t mask)
+{
 	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b), od = opnd<sizeof(T)>(rec.w, b);
-	const uint32_t mask = (rec.x & OPH_SINGLE_DEF) ? 0xffffffffu : st.active;
+	T x[U], y[U];
+	load_rows<T, U>(oa, lane, x);
+	if constexpr (OP >= 0) {
+		load_rows<T, U>(ob, lane, y);
 #pragma unroll
-	for (int h = 0; h < Halves<T, U>::N; h++) {
-		T x[H], y[H];
-		load_rows<T, H>(shifted(oa, h * H), lane, x);
-		load_rows<T, H>(shifted(ob, h * H), lane, y);
-#pragma unroll
-		for (int u = 0; u < H; u++)
+		for (int u = 0; u < U; u++)
 			x[u] = Math<T, OP>::eval(x[u], y[u]);
-		store_rows<T, H>(shifted(od, h * H).addr, lane, x, mask >> (h * H));
 	}
+	store_rows<T, U>(od.addr, lane, x, mask);
 }
 
-/* Integer/Float into a register vector: active rows only */
-template <int U>
-__device__ __forceinline__ void f_setconst(const uint4 &rec, const Bases &b, int lane, const RowState &st)
+template <typename T, int OP, int U>
+__device__ __forceinline__ void vec_chunked(const uint4 &rec, const Bases &b, int lane, uint32_t mask)
 {
-	uint32_t v[U];
-	load_rows<uint32_t, U>(opnd<4>(rec.y, b), lane, v);
-	store_rows<uint32_t, U>(opnd<4>(rec.w, b).addr, lane, v, st.active);
-}
-
-/* Column/Rowid into a register vector: every row (the CPU copies the whole
- * block, src/vm/virginia.c:448) */
-template <typename T, int U>
-__device__ __forceinline__ void f_copy(const uint4 &rec, const Bases &b, int lane)
-{
-	constexpr int H = Halves<T, U>::H;
-	const Opnd oa = opnd<sizeof(T)>(rec.y, b), od = opnd<sizeof(T)>(rec.w, b);
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b), od = opnd<sizeof(T)>(rec.w, b);
+#pragma unroll 1
+	for (int c = 0; c < U / 4; c++) {
+		T x[4], y[4];
+		load_rows<T, 4>(shifted(oa, 4 * c), lane, x);
+		if constexpr (OP >= 0) {
+			load_rows<T, 4>(shifted(ob, 4 * c), lane, y);
 #pragma unroll
-	for (int h = 0; h < Halves<T, U>::N; h++) {
-		T x[H];
-		load_rows<T, H>(shifted(oa, h * H), lane, x);
-		store_rows<T, H>(shifted(od, h * H).addr, lane, x, 0xffffffffu);
+			for (int u = 0; u < 4; u++)
+				x[u] = Math<T, OP>::eval(x[u], y[u]);
+		}
+		store_rows<T, 4>(shifted(od, 4 * c).addr, lane, x, mask >> (4 * c));
 	}
 }
 
-template <typename T, int U>
-__device__ __forceinline__ void f_cmp_any(const uint4 &rec, const Bases &b, int lane, RowState &st)
+template <typename T, int U, bool CHUNKED>
+__device__ __forceinline__ void vec_any(const uint4 &rec, const Bases &b, int lane, uint32_t mask)
 {
 	const uint32_t h = rec.x;
-	if (h_op(h, CO_LT)) f_cmp<T, CO_LT, U>(rec, b, lane, st);
-	else if (h_op(h, CO_GT)) f_cmp<T, CO_GT, U>(rec, b, lane, st);
-	else if (h_op(h, CO_LE)) f_cmp<T, CO_LE, U>(rec, b, lane, st);
-	else if (h_op(h, CO_GE)) f_cmp<T, CO_GE, U>(rec, b, lane, st);
-	else if (h_op(h, CO_EQ)) f_cmp<T, CO_EQ, U>(rec, b, lane, st);
-	else if (h_op(h, CO_NEQ)) f_cmp<T, CO_NEQ, U>(rec, b, lane, st);
-	else if (h_op(h, CO_AND)) f_cmp<T, CO_AND, U>(rec, b, lane, st);
-	else f_cmp<T, CO_OR, U>(rec, b, lane, st);
+#define VGPU_VEC(OP) { if (CHUNKED) vec_chunked<T, OP, U>(rec, b, lane, mask); else vec_rows<T, OP, U>(rec, b, lane, mask); return; }
+	if (h & OK_COPY) VGPU_VEC(-1);
+	if (h_op(h, MO_ADD)) VGPU_VEC(MO_ADD);
+	if (h_op(h, MO_SUB)) VGPU_VEC(MO_SUB);
+	if (h_op(h, MO_MUL)) VGPU_VEC(MO_MUL);
+	VGPU_VEC(MO_DIV);
+#undef VGPU_VEC
 }
 
-template <typename T, int U>
-__device__ __forceinline__ void f_math_any(const uint4 &rec, const Bases &b, int lane, const RowState &st)
+/* compares and Not over 8-byte and char values, out of line */
+template <int U>
+__device__ __noinline__ uint32_t bits_rare(uint4 rec, Bases b, int lane)
 {
 	const uint32_t h = rec.x;
-	if (h_op(h, MO_ADD)) f_math<T, MO_ADD, U>(rec, b, lane, st);
-	else if (h_op(h, MO_SUB)) f_math<T, MO_SUB, U>(rec, b, lane, st);
-	else if (h_op(h, MO_MUL)) f_math<T, MO_MUL, U>(rec, b, lane, st);
-	else f_math<T, MO_DIV, U>(rec, b, lane, st);
+	if (h_type(h, VT_DOUBLE)) return bits_any<double, U, true>(rec, b, lane);
+	if (h_type(h, VT_INT64)) return bits_any<long long, U, true>(rec, b, lane);
+	return bits_any<signed char, U, true>(rec, b, lane);
+}
+
+/* arithmetic and copies over 8-byte and char values, out of line */
+template <int U>
+__device__ __noinline__ void vec_rare(uint4 rec, Bases b, int lane, uint32_t mask)
+{
+	const uint32_t h = rec.x;
+	if (h_type(h, VT_DOUBLE)) vec_any<double, U, true>(rec, b, lane, mask);
+	else if (h_type(h, VT_INT64)) vec_any<long long, U, true>(rec, b, lane, mask);
+	else if (h & OK_COPY) {
+		if (h_type(h, VT_CHAR)) vec_chunked<unsigned char, -1, U>(rec, b, lane, mask);
+	} else vec_any<signed char, U, true>(rec, b, lane, mask);
 }
 
 /* one filter op: kind, then type, then operator, each by bit tests */
@@ -671,39 +699,41 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const Bases &b, int 
 				st.pend[s] = 0;
 			}
 	}
-	if (h & OK_CMP) {
-		if (h_type(h, VT_FLOAT)) f_cmp_any<float, U>(rec, b, lane, st);
-		else if (h_type(h, VT_INT)) f_cmp_any<int32_t, U>(rec, b, lane, st);
-		else if (h_type(h, VT_DOUBLE)) f_cmp_any<double, U>(rec, b, lane, st);
-		else if (h_type(h, VT_INT64)) f_cmp_any<long long, U>(rec, b, lane, st);
-		else f_cmp_any<signed char, U>(rec, b, lane, st);
+	if (h & (OK_CMP | OK_NOT)) {
+		uint32_t bits;
+		if (h_type(h, VT_FLOAT)) bits = bits_any<float, U, false>(rec, b, lane);
+		else if (h_type(h, VT_INT)) bits = bits_any<int32_t, U, false>(rec, b, lane);
+		else bits = bits_rare<U>(rec, b, lane);
+		take_jump(st, h, st.active & bits);
 	} else if (h & OK_INVALID) {
 		st.valid &= ~st.active;
-	} else if (h & OK_MATH) {
-		if (h_type(h, VT_FLOAT)) f_math_any<float, U>(rec, b, lane, st);
-		else if (h_type(h, VT_INT)) f_math_any<int32_t, U>(rec, b, lane, st);
-		else if (h_type(h, VT_DOUBLE)) f_math_any<double, U>(rec, b, lane, st);
-		else if (h_type(h, VT_INT64)) f_math_any<long long, U>(rec, b, lane, st);
-		else f_math_any<signed char, U>(rec, b, lane, st);
-	} else if (h & OK_NOT) {
-		if (h_type(h, VT_FLOAT)) f_not<float, U>(rec, b, lane, st);
-		else if (h_type(h, VT_INT)) f_not<int32_t, U>(rec, b, lane, st);
-		else if (h_type(h, VT_DOUBLE)) f_not<double, U>(rec, b, lane, st);
-		else if (h_type(h, VT_INT64)) f_not<long long, U>(rec, b, lane, st);
-		else f_not<signed char, U>(rec, b, lane, st);
+	} else if (h & (OK_MATH | OK_COPY)) {
+		/* arithmetic writes the active rows (every row if this is the
+		 * register's single definition); a Column/Rowid copy writes every
+		 * row (the CPU copies the whole block, src/vm/virginia.c:448) */
+		const uint32_t mask = (h & OK_COPY) || (h & OPH_SINGLE_DEF) ? 0xffffffffu : st.active;
+		if (h & OK_COPY) {
+			if (h_type(h, VT_INT) || h_type(h, VT_FLOAT)) vec_rows<uint32_t, -1, U>(rec, b, lane, mask);
+			else vec_rare<U>(rec, b, lane, mask);
+		} else if (h_type(h, VT_FLOAT)) {
+			vec_any<float, U, false>(rec, b, lane, mask);
+		} else if (h_type(h, VT_INT)) {
+			vec_any<int32_t, U, false>(rec, b, lane, mask);
+		} else {
+			vec_rare<U>(rec, b, lane, mask);
+		}
 	} else if (h & OK_SETCONST) {
-		f_setconst<U>(rec, b, lane, st);
-	} else if (h & OK_COPY) {
-		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) f_copy<unsigned long long, U>(rec, b, lane);
-		else if (h_type(h, VT_CHAR)) f_copy<unsigned char, U>(rec, b, lane);
-		else f_copy<uint32_t, U>(rec, b, lane);
+		/* Integer/Float into a register vector: active rows only */
+		vec_rows<uint32_t, -1, U>(rec, b, lane, st.active);
 	}
 }
 
 /* the filter ops [0, nf) of a record array over one group; returns the
- * lane's validity bits (rows at or past nrows start invalid) */
+ * lane's validity bits (rows at or past nrows start invalid).  Out of line
+ * (one copy for the count phase and the re-filtering full phase), its
+ * arguments by value. */
 template <int U>
-__device__ __forceinline__ uint32_t run_filter(uint32_t ops, uint32_t nf, const Bases &b, uint32_t nrows, int lane)
+__device__ __noinline__ uint32_t run_filter(uint32_t ops, uint32_t nf, Bases b, uint32_t nrows, int lane)
 {
 	RowState st;
 	st.valid = 0;
@@ -773,24 +803,38 @@ __device__ __forceinline__ void p_math_any(const uint4 &rec, const Bases &b, con
 	else p_math<T, MO_DIV>(rec, b, row, act, lane);
 }
 
+/* projection ops over 8-byte and char values, out of line, arguments by
+ * value (rows: the batch's four group rows of this lane) */
+__device__ __noinline__ void project_rare(uint4 rec, Bases b, uint4 rows, uint32_t act, int lane)
+{
+	const uint32_t row[kBatchE] = {rows.x, rows.y, rows.z, rows.w};
+	const uint32_t h = rec.x;
+	if (h & OK_MATH) {
+		if (h_type(h, VT_DOUBLE)) p_math_any<double>(rec, b, row, act, lane);
+		else if (h_type(h, VT_INT64)) p_math_any<long long>(rec, b, row, act, lane);
+		else p_math_any<signed char>(rec, b, row, act, lane);
+	} else if (h & OK_COPY) {
+		if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, b, row, act, lane);
+		else p_copy<unsigned long long>(rec, b, row, act, lane);
+	}
+}
+
 /* one projection op: arithmetic, or a copy (every listed row is active
  * here, so constants and columns are copies) */
 __device__ __forceinline__ void project_op(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
 	uint32_t act, int lane)
 {
+	static_assert(kBatchE == 4, "project_rare passes the batch rows as a uint4");
 	const uint32_t h = rec.x;
-	if (h & OK_MATH) {
-		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, b, row, act, lane);
-		else if (h_type(h, VT_INT)) p_math_any<int32_t>(rec, b, row, act, lane);
-		else if (h_type(h, VT_DOUBLE)) p_math_any<double>(rec, b, row, act, lane);
-		else if (h_type(h, VT_INT64)) p_math_any<long long>(rec, b, row, act, lane);
-		else p_math_any<signed char>(rec, b, row, act, lane);
-	} else if (h & OK_SETCONST) {
+	if (h & OK_SETCONST) {
 		p_copy<uint32_t>(rec, b, row, act, lane);
+	} else if (!(h_type(h, VT_FLOAT) || h_type(h, VT_INT))) {
+		project_rare(rec, b, make_uint4(row[0], row[1], row[2], row[3]), act, lane);
+	} else if (h & OK_MATH) {
+		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, b, row, act, lane);
+		else p_math_any<int32_t>(rec, b, row, act, lane);
 	} else if (h & OK_COPY) {
-		if (h_type(h, VT_INT64) || h_type(h, VT_DOUBLE)) p_copy<unsigned long long>(rec, b, row, act, lane);
-		else if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, b, row, act, lane);
-		else p_copy<uint32_t>(rec, b, row, act, lane);
+		p_copy<uint32_t>(rec, b, row, act, lane);
 	}
 }
 
@@ -809,6 +853,17 @@ __device__ __forceinline__ void p_store(uint32_t od, const Bases &b, const uint3
 	for (int i = 0; i < kBatchE; i++)
 		if ((in >> i) & 1u)
 			out[pos0 + (uint64_t)(32 * i + lane)] = v[i];
+}
+
+/* a result column of 8-byte or char values, out of line, by value */
+__device__ __noinline__ void p_store_rare(uint32_t od, Bases b, uint4 rows, uint32_t in, void *out, uint64_t pos0,
+	uint32_t stride, int lane)
+{
+	const uint32_t row[kBatchE] = {rows.x, rows.y, rows.z, rows.w};
+	if (stride == 8)
+		p_store<unsigned long long>(od, b, row, in, static_cast<unsigned long long *>(out), pos0, lane);
+	else
+		p_store<unsigned char>(od, b, row, in, static_cast<unsigned char *>(out), pos0, lane);
 }
 
 /* ---- groups ------------------------------------------------------------- */
@@ -897,13 +952,59 @@ __device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&gr
 	}
 }
 
+/* FM_PICK: the batch's selected rows of every column the results read,
+ * from the staged tile (its rows from `tile_row0`; entry i at group row
+ * row[i]) into the warp's gather area */
+__device__ __forceinline__ void pick_batch(const Bases &b, uint32_t tile, uint32_t tile_row0,
+	const uint32_t (&row)[kBatchE], int lane)
+{
+	const uint32_t n = lds_u32(b.slot + kQGatherN);
+	for (uint32_t c = 0; c < n; c++) {
+		const uint32_t st = lds_u8(b.slot + kQGatherStride + c);
+		const uint32_t src = tile + lds_u32(b.slot + kQTileOff + 4 * c);
+		const uint32_t dst = b.stage + lds_u32(b.slot + kQGatherOff + 4 * c);
+		if (st == 4) {
+			uint32_t v[kBatchE];
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++)
+				v[i] = lds_u32(src + 4u * (tile_row0 + row[i]));
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++)
+				sts_u32(dst + 4u * (uint32_t)(32 * i + lane), v[i]);
+		} else if (st == 8) {
+			uint64_t v[kBatchE];
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++)
+				v[i] = lds_u64(src + 8u * (tile_row0 + row[i]));
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++)
+				sts_u64(dst + 8u * (uint32_t)(32 * i + lane), v[i]);
+		} else {
+			uint32_t v[kBatchE];
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++)
+				v[i] = lds_u8(src + tile_row0 + row[i]);
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++)
+				sts_u8(dst + (uint32_t)(32 * i + lane), v[i]);
+		}
+	}
+}
+
 /* full phase: one group's selected rows (up to kFullGroup blocks from chunk
  * block blk, nrows rows), in row order, projected and stored at the group's
- * offset; returns false on an output overflow.  With FM_GATHER the staged
- * columns are the batch's gathered values (b.stage is the warp's gather
- * area), indexed by batch entry. */
+ * offset; returns false on an output overflow.
+ *
+ * FM_BITMAP and FM_REFILTER read the staged tile in place (b.stage is the
+ * tile, group rows from b.blk_row0).  FM_PICK and FM_GATHER first move each
+ * batch's selected rows into the warp's gather area (b.stage), where the
+ * results read them by batch entry: FM_PICK from the staged tile at `tile`,
+ * FM_GATHER from device memory.  With FM_PICK and `release` set, the warp
+ * arrives on the entry's release barriers (`release`, and `release2` when
+ * nonzero) once its last batch is picked, and *released says so. */
 __device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32_t blk, uint32_t nrows,
-	uint32_t mode, int lane)
+	uint32_t mode, int lane, uint32_t tile = 0, uint32_t tile_row0 = 0, uint32_t release = 0,
+	uint32_t release2 = 0, bool *released = nullptr)
 {
 	/* lane l holds validity word l of the group (32 rows) */
 	const uint32_t nw = (nrows + 31) / 32;
@@ -969,6 +1070,21 @@ __device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32
 			}
 			gather_batch(b, grow, lane);
 			__syncwarp();
+		} else if (mode == FM_PICK) {
+			pick_batch(b, tile, tile_row0, row, lane);
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++)
+				row[i] = 32u * i + (uint32_t)lane;
+			__syncwarp();
+			if (release && base + 32 * kBatchE >= n) {
+				/* the last batch is picked: the tile is free for this warp */
+				if (lane == 0) {
+					mbar_arrive(release);
+					if (release2)
+						mbar_arrive(release2);
+				}
+				*released = true;
+			}
 		}
 		for (uint32_t k = nf; k < nu; k++)
 			project_op(lds_v4(ops + 16u * k), b, row, act, lane);
@@ -978,13 +1094,11 @@ __device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32
 			const uint32_t stride = lds_u8(b.slot + kQOutStride + j);
 			if (stride == 4)
 				p_store<uint32_t>(od, b, row, in, static_cast<uint32_t *>(out), off + base, lane);
-			else if (stride == 8)
-				p_store<unsigned long long>(od, b, row, in, static_cast<unsigned long long *>(out), off + base, lane);
 			else
-				p_store<unsigned char>(od, b, row, in, static_cast<unsigned char *>(out), off + base, lane);
+				p_store_rare(od, b, make_uint4(row[0], row[1], row[2], row[3]), in, out, off + base, stride, lane);
 		}
-		if (mode == FM_GATHER)
-			__syncwarp();  /* the next batch's gather overwrites this one's values */
+		if (mode == FM_GATHER || mode == FM_PICK)
+			__syncwarp();  /* the next batch overwrites this one's values */
 	}
 	__syncwarp();
 	return ok;
@@ -1122,6 +1236,11 @@ __device__ void lookback_warp(const KParams &kp, unsigned char *smem, int lane)
 		const uint32_t ci = sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * s;
 		if (!lds_u32(ci + offsetof(ChunkInfo, valid)))
 			return;
+		/* the chunk's descriptor view (landed before any count group ran) */
+		if (!mbar_wait(sbase + kOffDesc + 8 * s, (i / kChunkSlots) & 1u, flags)) {
+			abort_cta(kp, flags, DE_STAGE_TIMEOUT);
+			return;
+		}
 		const uint32_t slot = sbase + kSlotArea + s * kSlotBytes;
 		const uint64_t g = lds_u64(ci + offsetof(ChunkInfo, work));
 		const uint32_t rows = lds_u32(ci + offsetof(ChunkInfo, rows));
@@ -1347,7 +1466,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	/* one entry: wait for its ring place (and, if it stages data, for a data
 	 * buffer), announce it, copy this lane's column */
 	auto issue = [&](uint32_t kind, const ProdChunk &c, uint32_t row0, uint32_t nrows, bool last,
-		const LaneCol &col, const unsigned char *src, bool desc, bool staged) -> bool {
+		const LaneCol &col, const unsigned char *src, bool staged) -> bool {
 		const uint32_t s = k % kEntries;
 		const uint32_t full = sbase + kOffFull + 8 * s;
 		const uint32_t bf = staged ? nb % nst : kNoBuf;
@@ -1375,7 +1494,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 				fence_proxy_async_smem();
 			}
 		}
-		const uint32_t tx = __reduce_add_sync(0xffffffffu, bulk) + (desc ? kQDescCopy : 0u);
+		const uint32_t tx = __reduce_add_sync(0xffffffffu, bulk);
 		if (lane == 0) {
 			const uint32_t si = sbase + kOffStageInfo + (uint32_t)sizeof(StageInfo) * s;
 			sts_v4(si, make_uint4(kind, c.slot, c.seq, row0));
@@ -1390,8 +1509,6 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		__syncwarp();
 		if (bulk)
 			bulk_load(data + col.off, src + (size_t)row0 * col.stride, bulk, full);
-		if (desc && lane == 31)
-			bulk_load(sbase + kSlotArea + c.slot * kSlotBytes, kp.queries + c.qi, kQDescCopy, full);
 		k++;
 		if (staged)
 			nb++;
@@ -1402,10 +1519,9 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	 * without data when it gathers, else its full tiles */
 	auto issue_full = [&](const ProdChunk &c) -> bool {
 		if (c.gather)
-			return issue(SK_FULL, c, 0, c.rows, true, c.fc, nullptr, false, false);
+			return issue(SK_FULL, c, 0, c.rows, true, c.fc, nullptr, false);
 		for (uint32_t r = 0; r < c.rows; r += c.full_tile)
-			if (!issue(SK_FULL, c, r, min(c.full_tile, c.rows - r), r + c.full_tile >= c.rows, c.fc, c.fcol, false,
-					true))
+			if (!issue(SK_FULL, c, r, min(c.full_tile, c.rows - r), r + c.full_tile >= c.rows, c.fc, c.fcol, true))
 				return false;
 		return true;
 	};
@@ -1493,7 +1609,7 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 			LaneCol none;
 			none.has = false;
 			none.src = none.stride = none.off = 0;
-			if (!issue(SK_END, e, 0, 0, true, none, nullptr, false, false))
+			if (!issue(SK_END, e, 0, 0, true, none, nullptr, false))
 				failed = true;
 			break;
 		}
@@ -1520,10 +1636,23 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 			sts_u32(held, c.qi);
 		}
 		desc = __shfl_sync(0xffffffffu, desc ? 1 : 0, 0) != 0;
+		/* the slot's descriptor barrier completes once per chunk, when the
+		 * query's descriptor view has landed in the slot (at once if the slot
+		 * holds that query's view already) */
+		const uint32_t dbar = sbase + kOffDesc + 8 * c.slot;
+		if (lane == 0) {
+			if (desc)
+				mbar_arrive_expect_tx(dbar, kQDescCopy);
+			else
+				mbar_arrive(dbar);
+		}
+		__syncwarp();
+		if (desc && lane == 0)
+			bulk_load(sbase + kSlotArea + c.slot * kSlotBytes, kp.queries + c.qi, kQDescCopy, dbar);
 		bool ok = true;
 		for (uint32_t r = 0; ok && r < c.rows; r += c.count_tile)
 			ok = issue(SK_COUNT, c, r, min(c.count_tile, c.rows - r), r + c.count_tile >= c.rows, c.cc, c.ccol,
-				desc && r == 0, true);
+				true);
 		if (ok && npend == kCountAhead)
 			ok = flush_one();
 		if (!ok) {
@@ -1576,6 +1705,16 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 	b.selv = warp_base + kp.sel_off;
 	uint32_t ng = 0;             /* groups of the stages seen so far */
 	uint32_t based_seq = ~0u;    /* the chunk whose offsets this warp waited for */
+	uint32_t desc_seq = ~0u;     /* the chunk whose descriptor view this warp waited for */
+	/* the chunk's descriptor view in its slot: a warp waits for it before it
+	 * first reads the slot for that chunk (the chunk's first count tile need
+	 * not be one this warp waited for) */
+	auto wait_desc = [&](uint32_t slot, uint32_t seq) -> bool {
+		if (desc_seq == seq)
+			return true;
+		desc_seq = seq;
+		return mbar_wait(sbase + kOffDesc + 8 * slot, (seq / kChunkSlots) & 1u, flags);
+	};
 	for (uint32_t k = 0;; k++) {
 		const uint32_t s = k % kEntries;
 		/* the entry's info first: a warp with no group in it releases the
@@ -1595,15 +1734,22 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 			return;
 		}
 		b.slot = sbase + kSlotArea + slot * kSlotBytes;
-		b.stage = buf != kNoBuf ? sbase + kp.stage_area + buf * kp.stage_bytes : gat;
+		const uint32_t tile = buf != kNoBuf ? sbase + kp.stage_area + buf * kp.stage_bytes : 0u;
+		b.stage = buf != kNoBuf ? tile : gat;
+		bool released = false;  /* this warp released the entry already */
 		const uint32_t nblk = (nrows + kBlockRows - 1) / kBlockRows;
 		const uint32_t blk0 = row0 / kBlockRows;
+		if (kind == SK_FULL && !wait_desc(slot, seq)) {
+			if (lane == 0)
+				abort_cta(kp, flags, DE_STAGE_TIMEOUT);
+			return;
+		}
 		const uint32_t mode = kind == SK_FULL ? lds_u32(b.slot + kQFullMode) : FM_BITMAP;
 		const uint32_t G = kind == SK_COUNT || mode == FM_REFILTER ? (uint32_t)kCountGroup : (uint32_t)kFullGroup;
 		const uint32_t ngs = (nblk + G - 1) / G;
 		const uint32_t j0 = ((uint32_t)w + W - ng % W) % W;
 		ng += ngs;
-		if (j0 < ngs && !mbar_wait(sbase + kOffFull + 8 * s, (k / kEntries) & 1u, flags)) {
+		if (j0 < ngs && (!wait_desc(slot, seq) || !mbar_wait(sbase + kOffFull + 8 * s, (k / kEntries) & 1u, flags))) {
 			if (lane == 0)
 				abort_cta(kp, flags, DE_STAGE_TIMEOUT);
 			return;
@@ -1626,12 +1772,21 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 				}
 				based_seq = seq;
 			}
+			/* FM_PICK: a warp with one group in the entry releases the
+			 * tile once it has picked that group's rows */
+			const bool pick1 = mode == FM_PICK && j < ngs && j + W >= ngs;
 			for (; j < ngs; j += W) {
 				const uint32_t r = j * G * kBlockRows;
-				/* staged columns: the group's rows of the tile; gathered
-				 * columns: the batch's entries of the warp's gather area */
-				b.blk_row0 = mode == FM_GATHER ? 0u : r;
-				ok = full_group(b, list, blk0 + j * G, min(G * kBlockRows, nrows - r), mode, lane) && ok;
+				if (mode == FM_PICK || mode == FM_GATHER) {
+					/* results read the warp's gather area by batch entry */
+					b.blk_row0 = 0;
+					b.stage = gat;
+				} else {
+					b.blk_row0 = r;
+				}
+				ok = full_group(b, list, blk0 + j * G, min(G * kBlockRows, nrows - r), mode, lane,
+					tile, r, pick1 ? sbase + kOffEmpty + 8 * s : 0u,
+					pick1 && buf != kNoBuf ? sbase + kOffBfree + 8 * buf : 0u, &released) && ok;
 			}
 		}
 		/* a serving session reports rows beyond capacity in the query's
@@ -1665,9 +1820,11 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					}
 				}
 			}
-			mbar_arrive(sbase + kOffEmpty + 8 * s);
-			if (buf != kNoBuf)
-				mbar_arrive(sbase + kOffBfree + 8 * buf);
+			if (!released) {
+				mbar_arrive(sbase + kOffEmpty + 8 * s);
+				if (buf != kNoBuf)
+					mbar_arrive(sbase + kOffBfree + 8 * buf);
+			}
 			if (last)
 				mbar_arrive(sbase + (kind == SK_COUNT ? kOffCounted : kOffDone) + 8 * slot);
 		}
@@ -1692,6 +1849,7 @@ __global__ void __launch_bounds__(32 * (W + 2), 1) vm_kernel(const KParams kp)
 			mbar_init(sbase + kOffCounted + 8 * q, W);
 			mbar_init(sbase + kOffBased + 8 * q, 1);
 			mbar_init(sbase + kOffDone + 8 * q, W);
+			mbar_init(sbase + kOffDesc + 8 * q, 1);
 			sts_u32(sbase + kOffFdone + 4 * q, 0u);
 			sts_u32(sbase + kOffHeld + 4 * q, ~0u);
 		}
@@ -1731,7 +1889,7 @@ static int occ_t(size_t smem, int *ctas)
 	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, 32 * (W + 2), smem) == cudaSuccess;
 }
 
-#define VGPU_WARPS(X) X(4) X(8) X(16)
+#define VGPU_WARPS(X) X(8) X(10) X(14) X(16)
 
 int shape_supported(const Shape &s)
 {
