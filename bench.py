@@ -243,6 +243,37 @@ def _device_tables(eng, sizes, seed0):
     return tables
 
 
+def _host_tables(eng, sizes, seed0):
+    """Resident tables of the benchmark schema from the seeded host generator
+    (the reference CPU VM rebuilds the same bytes to check the results)."""
+    import virginian_b200 as vb
+    from oracle.digest import host_table
+    from virginian_b200 import datagen
+    types = [t for _, t in datagen.SCHEMA_A]
+    tables = []
+    for i, n in enumerate(sizes):
+        cols = host_table(int(n), seed0, i, threads=min(16, os.cpu_count() or 1))
+        t = vb.Table(eng, types)
+        if n:
+            t.append(datagen.segments(cols, datagen.SCHEMA_A))
+        del cols
+        tables.append(t)
+    return tables
+
+
+def _oracle_pool():
+    """Worker processes (spawned, never forked from the CUDA process) that
+    run the reference CPU VM for the parity checks."""
+    import multiprocessing as mp
+    return mp.get_context("spawn").Pool(max(1, min(16, os.cpu_count() or 1)))
+
+
+def _same(got, want):
+    """digests of one result stream: the same rows and, when there are rows,
+    the same bytes column by column"""
+    return got[0] == want[0] and (got[0] == 0 or tuple(got[1]) == tuple(want[1]))
+
+
 def _queries(n, seed, ntables, layout=None):
     import virginian_b200 as vb
     from virginian_b200 import datagen, querygen, sql as vsql
@@ -261,11 +292,15 @@ def _queries(n, seed, ntables, layout=None):
 def bench_batched(eng, reps=5):
     """256 generated queries over 64 resident tables of log-uniform size in
     [10k, 20M] rows: one persistent graph-replayed launch (autotuned shape)
-    against one launch per query, results compared."""
+    against one launch per query; every batched result compared with the
+    reference CPU VM (virginia_single) on the same table."""
+    import torch
     import virginian_b200 as vb
+    from oracle.digest import digest, table_digests_star
+    hbm, _ = peaks()
     rng = np.random.default_rng(404)
     sizes = np.exp(rng.uniform(np.log(1e4), np.log(2e7), size=64)).astype(np.int64)
-    tables = _device_tables(eng, sizes, 1000)
+    tables = _host_tables(eng, sizes, 1000)
     log("batched: tables ready")
     work = _queries(256, 77, len(tables))
     log("batched: per-query path")
@@ -287,35 +322,60 @@ def bench_batched(eng, reps=5):
         b.add(p, tables[k])
     b.run(graph=True)  # autotunes the shape, captures the graph
     b.wait()
-    times = []
+    stream = torch.cuda.ExternalStream(eng.stream)
+    times, dev_ms = [], []
     for _ in range(reps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
+        ev0.record(stream)
         b.run(graph=True)
+        ev1.record(stream)
         b.wait()
         times.append(time.perf_counter() - t0)
+        ev1.synchronize()
+        dev_ms.append(ev0.elapsed_time(ev1))
     batch_s = statistics.median(times)
+    batch_dev_ms = statistics.median(dev_ms)
     rows_equal = all(b.rows(i) == per_rows[i] for i in range(len(work)))
-    sample = np.random.default_rng(5).choice(len(work), size=24, replace=False)
-    bytes_equal = True
-    for i in sample:
-        q, k, p = work[int(i)]
-        r = tables[k].query(p)
-        a, c = r.download(), b.download(int(i))
-        r.close()
-        bytes_equal = bytes_equal and all(np.array_equal(x.view(np.uint8), y.view(np.uint8)) for x, y in zip(a, c))
+    log("batched: result digests")
+    got = [digest(b.download(i)) for i in range(len(work))]
     shape = b.shape()
     b.close()
     total_rows = int(sizes.sum())
+    alg = sum(int(sizes[k]) * p.info.load_bytes_per_row + got[i][0] * p.info.out_bytes_per_row
+              for i, (q, k, p) in enumerate(work))
     for t in tables:
         t.close()
+    # the reference CPU VM on every (table, query): one task per table,
+    # largest first, in spawned workers while the GPU idles
+    log("batched: reference CPU VM on every query")
+    by_table = {}
+    for i, (q, k, p) in enumerate(work):
+        by_table.setdefault(k, []).append(i)
+    order = sorted(by_table, key=lambda k: -int(sizes[k]))
+    t0 = time.perf_counter()
+    with _oracle_pool() as pool:
+        res = pool.map(table_digests_star, [(int(sizes[k]), 1000, k, [work[i][0] for i in by_table[k]])
+                                            for k in order], chunksize=1)
+    oracle_s = time.perf_counter() - t0
+    mismatch = []
+    for k, digs in zip(order, res):
+        for i, d in zip(by_table[k], digs):
+            if not _same(got[i], d):
+                mismatch.append(i)
     return {"workload": "256 generated queries (predicate trees of depth 1-4, 1-5 result columns) over 64 "
                         "resident tables, rows log-uniform in [1e4, 2e7]",
             "tables": 64, "queries": len(work), "table_rows": total_rows,
             "batched_qps": round(len(work) / batch_s, 1), "per_query_qps": round(len(work) / per_s, 1),
             "speedup": round(per_s / batch_s, 2), "batched_ms": round(batch_s * 1e3, 3),
+            "batched_device_ms": round(batch_dev_ms, 3),
             "per_query_ms": round(per_s * 1e3, 3), "result_rows": int(sum(per_rows)),
-            "rows_equal": bool(rows_equal), "bytes_equal_sample": bool(bytes_equal),
-            "sample_checked": int(len(sample)), "shape": shape,
+            "algorithmic_bytes": int(alg),
+            "batched_gbs": round(alg / (batch_dev_ms / 1e3) / 1e9, 1),
+            "frac_of_hbm": round(alg / (batch_dev_ms / 1e3) / 1e9 / hbm, 3),
+            "rows_equal_per_query_path": bool(rows_equal),
+            "oracle_checked": len(work), "oracle_mismatches": mismatch,
+            "oracle_seconds": round(oracle_s, 1), "shape": shape,
             "launches": {"batched_per_rep": 1, "per_query": len(work)}}
 
 
@@ -342,7 +402,6 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
     _ = r.rows
     r.close()
     out = {}
-    exact = True
     import threading
     for ri, rate in enumerate(rates):
         # the same queries at every rate; only the arrival process differs
@@ -353,7 +412,8 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
         # a client thread consumes results as they complete and releases
         # their memory, while arrivals keep coming
         tickets, lag = [None] * len(chunk), [0.0] * len(chunk)
-        lat, done_at, kept, errors = [0.0] * len(chunk), [0.0] * len(chunk), [], []
+        lat, done_at, errors = [0.0] * len(chunk), [0.0] * len(chunk), []
+        srows = [0] * len(chunk)
         ready = threading.Semaphore(0)
 
         def consume():
@@ -363,11 +423,8 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
                     st = srv.wait(tickets[n], timeout_s=120)
                     lat[n] = lag[n] * 1e3 + st["latency_us"] / 1e3
                     done_at[n] = arrivals[n] + lat[n] / 1e3
-                    # a few results are checked after the timed arrivals
-                    if ri == 0 and n < 6:
-                        kept.append(n)
-                    else:
-                        srv.release(tickets[n])
+                    srows[n] = st["rows"]
+                    srv.release(tickets[n])
             except Exception as ex:  # surfaced after the join
                 errors.append(ex)
 
@@ -386,28 +443,19 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
         if errors:
             raise errors[0]
         serve_span = max(done_at) - arrivals[0]
-        checked = []
-        for n in kept:
-            checked.append((n, srv.download(tickets[n])))
-            srv.release(tickets[n])
-        for n, c in checked:
-            q, k, p = chunk[n]
-            r = tables[k].query(p)
-            a = r.download()
-            r.close()
-            exact = exact and all(np.array_equal(x.view(np.uint8), y.view(np.uint8)) for x, y in zip(a, c))
         # serial: one launch per query, in arrival order
         log(f"serving: serial at rate {rate}")
-        slat = []
+        slat, serial_rows = [], []
         t0 = time.perf_counter()
         for (q, k, p), at in zip(chunk, arrivals):
             while time.perf_counter() - t0 < at:
                 pass
             r = tables[k].query(p)
-            _ = r.rows
+            serial_rows.append(r.rows)
             r.close()
             slat.append((time.perf_counter() - t0 - at) * 1e3)
         serial_span = time.perf_counter() - t0
+        bad_rows = [n for n in range(len(chunk)) if srows[n] != serial_rows[n]]
         out[str(rate)] = {
             "queries": len(chunk), "offered_qps": rate,
             "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
@@ -415,7 +463,45 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
             "serial_p50_ms": round(float(np.percentile(slat, 50)), 3),
             "serial_p99_ms": round(float(np.percentile(slat, 99)), 3),
             "serial_qps": round(len(chunk) / serial_span, 1),
-            "submit_lag_p99_ms": round(float(np.percentile(lag, 99)) * 1e3, 3)}
+            "submit_lag_p99_ms": round(float(np.percentile(lag, 99)) * 1e3, 3),
+            "rows_checked": len(chunk), "rows_mismatch": bad_rows}
+    # the look-back ring: queries back to back until the session's work
+    # numbering has passed the ring's size, then the bytes of the last
+    # results against the one-launch-per-query path
+    log("serving: look-back ring wrap")
+    ring = srv.stats()["status_ring"]
+    inflight, wrap_rows_bad, submitted, last = [], [], 0, []
+    per_rows = {}
+    while submitted < 20000:
+        n = submitted % len(work)
+        q, k, p = work[n]
+        inflight.append((n, srv.submit(p, tables[k])))
+        submitted += 1
+        st = srv.stats()
+        wrapped = st["work_items"] > ring + 200_000
+        while len(inflight) > (0 if wrapped else 48):
+            m, tk = inflight.pop(0)
+            got = srv.download(tk) if wrapped else None
+            rows = srv.wait(tk)["rows"]
+            srv.release(tk)
+            if m not in per_rows:
+                r = tables[work[m][1]].query(work[m][2])
+                per_rows[m] = r.rows
+                r.close()
+            if rows != per_rows[m]:
+                wrap_rows_bad.append(m)
+            if got is not None:
+                last.append((m, got))
+        if wrapped:
+            break
+    ring_work = st["work_items"]
+    exact = True
+    for m, got in last[-8:]:
+        r = tables[work[m][1]].query(work[m][2])
+        a = r.download()
+        r.close()
+        exact = exact and len(a) == len(got) and all(
+            np.array_equal(x.view(np.uint8), y.view(np.uint8)) for x, y in zip(a, got))
     st = srv.stats()
     srv.close()
     total_rows = int(sizes.sum())
@@ -425,7 +511,10 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
                         "Poisson arrivals; latency from arrival to completion seen by the host" %
                         (total_rows * 28 / 1e9),
             "table_rows": total_rows, "result_budget_gb": 20, "rates": out,
-            "mix_equals_alone_sample": bool(exact), "sessions": st["sessions"],
+            "ring_wrap": {"status_ring_words": ring, "session_work_items": ring_work,
+                          "queries": submitted, "rows_mismatch": wrap_rows_bad,
+                          "bytes_checked": min(8, len(last)), "bytes_equal": bool(exact and last)},
+            "sessions": st["sessions"], "restarts": st["restarts"],
             "readmitted": st["readmitted"], "shape": st["shape"]}
 
 
@@ -503,14 +592,18 @@ def bench_streamed(eng, rows=400_000_000, chunk=25_000_000):
 
 
 def run_reference(args):
-    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference's own CPU VM (virginia_multi with every host thread,
+    built from the reference sources) on the headline workload: the same
+    seeded 50M-row table and query, one query per step."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    rows = 1_000_000
+    rows = args.rows
     from oracle import oracle
+    from oracle.digest import host_table
     from virginian_b200 import datagen
-    cols = datagen.table(rows, datagen.SCHEMA_A, seed=0)
+    cols = host_table(rows, 0, 0, threads=min(16, threads))
     c, d = constants(cols, HEADLINE_SEL)
     sql = QUERY.format(c=c, d=d)
     db = oracle.OracleDB()
@@ -518,6 +611,7 @@ def run_reference(args):
     try:
         db.create_table("test", datagen.SCHEMA_A)
         db.insert("test", cols["id"], [cols[x] for x, _ in datagen.SCHEMA_A])
+        del cols
         out_rows = 0
         for i in range(args.warmup + args.steps):
             r = db.query(sql, mode=1, threads=threads, repeat=1)
@@ -534,11 +628,12 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total / len(times) * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/float32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rows_per_step": rows, "query": sql,
-                   "sample": "each step scans a 1M-row sample of the workload's table on the host"},
+        "rows_per_s": round(rows * len(times) / total, 1),
+        "config": {"workload": WORKLOAD, "rows_per_step": rows, "query": sql, "same_config": rows == ROWS,
+                   "result_rows": out_rows},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
                          "kind": "reference",
-                         "sample": f"{rows} rows of the same table and query per step, "
+                         "sample": f"the whole {rows}-row table and the headline query per step, "
                                    "virginia_multi (src/vm/virginia.c) built from the reference sources"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -624,9 +719,20 @@ def run_b200(args):
         dist.all_reduce(t)
         alg_total = float(t.item())
     value = alg_total * args.steps / (ms_max / 1e3) / 1e9
+    rows_per_s = rows * world * args.steps / (ms_max / 1e3)
     kernel_ms = statistics.mean(kt) if kt else None
     hbm, peak_kind = peaks()
     achieved = alg / (kernel_ms / 1e3) / 1e9 if kernel_ms else None
+    from oracle.digest import digest
+    r = table.query(p)
+    head_digest = digest(r.download())
+    r.close()
+    # the read ceiling of the same columns: kernels that only read them
+    ceiling = {}
+    load_cols = [-1] + list(range(len(types)))
+    for name, mode in (("loads_16B", 0), ("bulk_copies", 1)):
+        cms, cbytes = table.read_ceiling(load_cols, mode, 5)
+        ceiling[name] = {"ms": round(cms, 4), "gbs": round(cbytes / (cms / 1e3) / 1e9, 1)}
 
     # selectivity sweep (device-resident)
     log("sweep")
@@ -663,6 +769,7 @@ def run_b200(args):
     e2e_s = time.perf_counter() - t0
     e2e_s = allreduce_max(e2e_s, world)
     assert nrows.value == out_rows
+    e2e_same = _same(digest([o.numpy()[:out_rows] for o in outs]), head_digest)
     e2e_value = alg_total * e2e_steps / e2e_s / 1e9
     h2d = rows * info.load_bytes_per_row
     d2h = out_rows * info.out_bytes_per_row
@@ -700,10 +807,14 @@ def run_b200(args):
                          "peak_kind": peak_kind,
                          "kernel_ms": round(kernel_ms, 4) if kernel_ms else None,
                          "algorithmic_bytes": alg},
+            "rows_per_s": round(rows_per_s, 1),
+            "read_ceiling": dict(ceiling, frac_of_bulk=round(achieved / ceiling["bulk_copies"]["gbs"], 3)
+                                 if achieved else None),
             "sweep": sweep,
             "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                    "ms_per_step": round(e2e_s / e2e_steps * 1e3, 3)},
+                    "ms_per_step": round(e2e_s / e2e_steps * 1e3, 3),
+                    "same_bytes_as_device_path": bool(e2e_same)},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
@@ -723,6 +834,19 @@ def run_b200(args):
                     line[name] = fn(eng)
                 except Exception as ex:  # report, keep the headline line
                     line[name] = {"error": f"{type(ex).__name__}: {ex}"}
+    if rank == 0 and args.parity:
+        # the headline's own result against the reference CPU VM
+        # (virginia_single) on the same table, in a spawned worker
+        log("parity: reference CPU VM on the headline table")
+        from oracle.digest import table_digests_star
+        sql = QUERY.format(c=constants(cols, HEADLINE_SEL)[0], d=constants(cols, HEADLINE_SEL)[1])
+        t0 = time.perf_counter()
+        with _oracle_pool() as pool:
+            want = pool.map(table_digests_star, [(rows, rank, 0, [sql], 8)])[0][0]
+        line["parity"] = {"config2_50M" if rows == ROWS else f"config2_{rows}": _same(head_digest, want),
+                          "rows": want[0], "checked_against": "virginia_single (src/vm/virginia.c) built from "
+                                                              "the reference sources, same table and query",
+                          "seconds": round(time.perf_counter() - t0, 1)}
     if rank == 0:
         print(json.dumps(line))
     eng.close()
@@ -742,6 +866,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--shape", default="", help="threads,stage_kb,stages,ctas_per_sm,chunk_rows: force the launch "
                     "shape of the scan instead of tuning it (for profiling one launch)")
+    ap.add_argument("--no-parity", dest="parity", action="store_false",
+                    help="skip the headline's byte comparison with the reference CPU VM")
     ap.add_argument("--sections", default="batched,serving,streamed",
                     help="workloads besides the headline scan (comma list; empty for none)")
     args = ap.parse_args()

@@ -301,11 +301,10 @@ int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 /* upper bound on the rows of a chunk (the unit a CTA claims and places in
  * the ordered result): a multiple of 256 in [256, 8192], 0 for automatic */
 int virg_gpu_engine_set_chunk_rows(virg_gpu_engine *e, unsigned rows);
-/* how the full phase reads the columns the results need, for programs
- * whose results read at most 32 bytes per row: 0 (default) stages tiles of
- * them and picks each batch's selected rows out of the tile, 1 loads only
- * the selected rows' values straight from device memory, 2 reads the
- * staged tile in place until the rows are stored */
+/* how the full phase reads the columns the results need: 0 (default)
+ * stages tiles of them and reads the selected rows in place, 1 loads only
+ * the selected rows' values straight from device memory (programs whose
+ * results read at most 32 bytes per row) */
 int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode);
 /* record CUDA events around each of the next kernel launches in a ring of
  * `slots` entries (0 turns it off) */
@@ -486,6 +485,10 @@ typedef struct {
 	unsigned long long restarts;     /* sessions that ended by themselves (a
 	                                  * bounded wait ran out); their unfinished
 	                                  * queries ran again in the next session */
+	unsigned long long work_items;   /* work items (query chunks) published to the
+	                                  * running session */
+	unsigned long long status_ring;  /* look-back words of a session's ring; work
+	                                  * item i uses word i mod status_ring */
 } virg_serve_counters;
 
 int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cfg, virg_serve **out);

@@ -84,10 +84,10 @@ def test_query_host_end_to_end(data_a, engine):
 
 
 # (compute threads, stage KB, buffers (0: as many as fit), CTAs per SM, chunk rows, full-phase mode)
-@pytest.mark.parametrize("shape", [(320, 16, 0, 1, 1024, 0), (448, 32, 3, 1, 2048, 2), (256, 16, 0, 1, 8192, 0),
-                                   (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 2), (512, 24, 0, 1, 2048, 0),
-                                   (512, 32, 4, 1, 8192, 2), (256, 8, 0, 1, 256, 0), (256, 24, 0, 1, 4096, 1),
-                                   (320, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1), (256, 8, 0, 1, 256, 2)])
+@pytest.mark.parametrize("shape", [(320, 16, 0, 1, 1024, 0), (448, 32, 3, 1, 2048, 0), (256, 16, 0, 1, 8192, 0),
+                                   (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 0), (512, 24, 0, 1, 2048, 0),
+                                   (512, 32, 4, 1, 8192, 0), (256, 8, 0, 1, 256, 0), (256, 24, 0, 1, 4096, 1),
+                                   (320, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1), (448, 16, 0, 1, 1024, 1)])
 def test_every_launch_shape(data_a, engine, shape):
     db, _, t = data_a
     engine.set_shape(*shape)
@@ -112,7 +112,7 @@ REFILTER = ["select uniformf + normalf5 as s, id from test where uniformf + norm
             "select id, uniformi - normali5 as d, normalf20 from test where uniformi - normali5 < 20 or normalf20 > 30.0"]
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1])
 def test_filter_vectors_in_results(data_a, engine, mode):
     db, _, t = data_a
     engine.set_shape(full_mode=mode)
@@ -166,7 +166,7 @@ def test_int64_and_double_columns(oracle_mod, engine):
                     # 36 result bytes per row: read from the staged tile in place
                     "select id, uniforml, normald, uniformi, uniformf, normalf5, normalf20 from test "
                     "where normali20 > 10 or uniformf < 5.0"]:
-            for mode in (0, 1, 2):
+            for mode in (0, 1):
                 engine.set_shape(full_mode=mode)
                 try:
                     got, want, _ = run_both(db, t, sql, TYPES_B)
@@ -228,7 +228,7 @@ def test_streamed_matches_oracle(oracle_mod, engine, per_chunk):
 
 
 @pytest.mark.parametrize("k", range(len(HAND_PROGRAMS)))
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1])
 def test_hand_programs_and_or_not(oracle_mod, engine, k, mode):
     """Hand-assembled programs with And, Or and Not (which the code
     generator never emits) on both VMs, over a table with many zeros, NaN and

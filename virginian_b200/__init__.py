@@ -83,8 +83,8 @@ class Engine:
                   ctas_per_sm: int = 0, chunk_rows: int = 0, full_mode: int = 0) -> None:
         """Launch shape of later queries: compute threads per CTA, KB per
         staging buffer, buffers, CTAs per SM, the chunk bound and the full
-        phase's mode (0 pick from staged tiles, 1 gather from device memory,
-        2 read staged tiles in place); 0 in a field keeps the automatic
+        phase's mode (0 reads staged tiles in place, 1 gathers the selected
+        rows from device memory); 0 in a field keeps the automatic
         choice."""
         check(lib().virg_gpu_engine_set_shape(self.h, threads, stage_kb, stages,
                                               ctas_per_sm), "set shape")
@@ -208,6 +208,18 @@ class Table:
     @property
     def nbytes(self) -> int:
         return int(lib().virg_gpu_table_bytes(self.h))
+
+    def read_ceiling(self, columns: Sequence[int], mode: int = 0, reps: int = 5) -> Tuple[float, int]:
+        """Device time (ms, best of `reps`) and bytes of a kernel that only
+        reads the given columns (-1: the key) of every segment: mode 0 with
+        16-byte loads, 1-3 with bulk copies into 4, 6 or 2 shared-memory
+        stages.  A measurement aid: the read bandwidth a scan of those
+        columns could reach."""
+        cols = (ctypes.c_int * max(1, len(columns)))(*columns)
+        ms, nbytes = ctypes.c_double(), ctypes.c_ulonglong()
+        check(lib().virg_gpu_table_read_ceiling(self.h, cols, len(columns), mode, reps, ctypes.byref(ms),
+                                                ctypes.byref(nbytes)), "read ceiling")
+        return ms.value, nbytes.value
 
     def query(self, program: Program) -> "Result":
         r = ctypes.c_void_p()
@@ -364,6 +376,7 @@ class Serve:
         return {"sessions": c.sessions, "admitted": c.admitted, "readmitted": c.readmitted,
                 "pending": c.pending, "inflight": c.inflight, "arena_used": c.arena_used,
                 "device_error": c.device_error, "restarts": c.restarts,
+                "work_items": c.work_items, "status_ring": c.status_ring,
                 "shape": {"threads": c.shape[0], "stage_kb": c.shape[1], "stages": c.shape[2],
                           "grid": c.shape[3]}}
 

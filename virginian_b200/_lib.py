@@ -61,7 +61,8 @@ class ServeCounters(ctypes.Structure):
                 ("readmitted", ctypes.c_ulonglong), ("pending", ctypes.c_ulonglong),
                 ("inflight", ctypes.c_ulonglong), ("arena_used", ctypes.c_ulonglong),
                 ("device_error", ctypes.c_uint), ("shape", ctypes.c_uint * 4),
-                ("restarts", ctypes.c_ulonglong)]
+                ("restarts", ctypes.c_ulonglong), ("work_items", ctypes.c_ulonglong),
+                ("status_ring", ctypes.c_ulonglong)]
 
 
 class ProgramInfo(ctypes.Structure):
@@ -102,6 +103,8 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_table_rows": (u64, [vp]),
         "virg_gpu_table_bytes": (u64, [vp]),
         "virg_gpu_table_destroy": (None, [vp]),
+        "virg_gpu_table_read_ceiling": (i, [vp, P(ctypes.c_int), u, u, u, P(ctypes.c_double),
+                                            P(ctypes.c_ulonglong)]),
         "virg_gpu_query": (i, [vp, vp, vp, P(vp)]),
         "virg_gpu_query_tune": (i, [vp, vp, vp, P(u)]),
         "virg_gpu_result_rows": (i, [vp, P(u64)]),

@@ -135,11 +135,11 @@ void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode)
 			pp.full_bpr += P.load_stride[i];
 		}
 	}
-	/* the full phase moves the selected rows' values into each compute
-	 * warp's area (picked from staged tiles, or gathered from device
-	 * memory) unless they are many bytes per row */
-	if (pp.mode == FM_BITMAP && pp.full_bpr <= kGatherMaxBpr && full_mode != 2) {
-		pp.mode = full_mode == 1 ? FM_GATHER : FM_PICK;
+	/* full_mode 1: the full phase gathers the selected rows' values from
+	 * device memory into each compute warp's area, unless they are many
+	 * bytes per row */
+	if (pp.mode == FM_BITMAP && pp.full_bpr <= kGatherMaxBpr && full_mode == 1) {
+		pp.mode = FM_GATHER;
 		pp.gather_bpr = pp.full_bpr;
 	}
 	/* selection vectors hold a projection batch's entries, row vectors a
@@ -260,19 +260,7 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 		load_set(d.full_set, P, pp.full_cols, pp.nfull, tf);
 		d.chunk_rows = chunk;
 	}
-	/* FM_PICK: the batch layout of the warp's area (results read it), and
-	 * where the columns sit in a staged tile (the rows are picked there) */
-	LoadSet pick;
-	if (pp.mode == FM_PICK) {
-		load_set(pick, P, pp.full_cols, pp.nfull, 32u * kBatchE);
-		d.gather_n = pick.n;
-		for (uint32_t i = 0; i < pick.n; i++) {
-			d.gather_stride[i] = pick.stride[i];
-			d.gather_off[i] = pick.off[i];
-			d.tile_off[i] = d.full_set.off[i];
-		}
-	}
-	const LoadSet &rset = pp.mode == FM_PICK ? pick : d.full_set;
+	const LoadSet &rset = d.full_set;
 	d.full_mode = pp.mode;
 	for (unsigned i = 0; i < kMaxRegs; i++) {
 		d.consts[i] = P.consts[i];
@@ -720,8 +708,7 @@ std::vector<Shape> tune_candidates()
 	for (unsigned threads : {256u, 320u, 448u})
 		for (unsigned kb : {24u, 32u, 40u, 48u})
 			for (unsigned chunk : {4096u, 8192u})
-				for (unsigned mode : {0u, 2u})
-					c.push_back(Shape{threads, kb, 0, 1, chunk, mode});
+				c.push_back(Shape{threads, kb, 0, 1, chunk, 0});
 	for (unsigned kb : {16u, 32u})
 		c.push_back(Shape{256, kb, 0, 1, 8192, 1});
 	return c;
@@ -812,7 +799,7 @@ extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 extern "C" int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode)
 {
 	VGPU_CHECK(e != nullptr, "null engine");
-	VGPU_CHECK(mode <= 2, "full-phase mode %u: 0 pick, 1 gather, 2 in place", mode);
+	VGPU_CHECK(mode <= 1, "full-phase mode %u: 0 in place, 1 gather", mode);
 	e->pref.full_mode = mode;
 	return 1;
 }

@@ -110,9 +110,9 @@ struct ProgPlan {
 	uint8_t count_cols[kMaxLoads], full_cols[kMaxLoads];
 	uint32_t ncount, nfull;
 	uint32_t count_bpr, full_bpr;  /* staged bytes per row of each phase */
-	uint32_t mode;                 /* FM_PICK, FM_GATHER, FM_BITMAP or FM_REFILTER */
+	uint32_t mode;                 /* FM_GATHER, FM_BITMAP or FM_REFILTER */
 	uint32_t sel_bpr, row_bpr;     /* register-vector bytes per row */
-	uint32_t gather_bpr;           /* bytes per row in a warp's gather area (FM_PICK, FM_GATHER) */
+	uint32_t gather_bpr;           /* bytes per row in a warp's gather area (FM_GATHER) */
 	uint32_t vec_off[kMaxRegs];    /* offset in the selection or row-vector area */
 };
 
@@ -135,7 +135,8 @@ struct Plan {
 	unsigned grid = 0;
 };
 
-/* full_mode: as Shape::full_mode */
+/* full_mode: as Shape::full_mode (1: gather from device memory where the
+ * program allows it) */
 void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode = 0);
 int geom_make(const Shape &s, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gather_bpr, int smem_block, int smem_sm,
 	Geom *g);

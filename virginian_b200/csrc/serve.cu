@@ -712,6 +712,8 @@ extern "C" int virg_serve_stats(virg_serve *s, virg_serve_counters *c)
 	c->arena_used = s->arena.used;
 	c->device_error = s->device_error;
 	c->restarts = s->restarts;
+	c->work_items = s->work;
+	c->status_ring = kStatusRing;
 	c->shape[0] = s->geom.shape.threads;
 	c->shape[1] = s->geom.shape.stage_kb;
 	c->shape[2] = s->geom.shape.stages;

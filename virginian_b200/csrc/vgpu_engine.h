@@ -30,8 +30,8 @@ struct Shape {
 	unsigned stages;
 	unsigned ctas_per_sm;  /* 0: as many as fit */
 	unsigned chunk_rows;   /* upper bound on rows per chunk; 0: automatic */
-	unsigned full_mode;    /* full phase of programs whose results read few bytes per row: 0 picks rows out
-	                        * of staged tiles, 1 gathers them from device memory, 2 reads staged tiles in place */
+	unsigned full_mode;    /* full phase of programs whose results read few bytes per row: 0 reads staged
+	                        * tiles in place, 1 gathers the selected rows from device memory */
 	unsigned warps() const { return threads / 32; }
 	unsigned stage_bytes() const { return stage_kb * 1024u; }
 };
@@ -95,7 +95,8 @@ struct ChunkInfo {
 	uint64_t work;       /* global work index */
 	uint32_t rows;
 	uint32_t block_base; /* the chunk's first 64-row block in its table */
-	uint32_t pad[2];
+	uint32_t ncount;     /* the chunk's count entries */
+	uint32_t nfull;      /* the chunk's full entries */
 };
 
 constexpr unsigned kOffFull = 0;                                   /* u64[kEntries]: data landed */
@@ -107,9 +108,13 @@ constexpr unsigned kOffBased = kOffCounted + 8 * kChunkSlots;      /* u64[kChunk
 constexpr unsigned kOffDone = kOffBased + 8 * kChunkSlots;         /* u64[kChunkSlots] */
 constexpr unsigned kOffDesc = kOffDone + 8 * kChunkSlots;          /* u64[kChunkSlots]: the slot's descriptor view landed */
 constexpr unsigned kOffFlags = kOffDesc + 8 * kChunkSlots;         /* u32[8] */
-constexpr unsigned kOffFdone = kOffFlags + 32;                     /* u32[kChunkSlots] */
-constexpr unsigned kOffHeld = kOffFdone + 4 * kChunkSlots;         /* u32[kChunkSlots] */
-constexpr unsigned kOffStageInfo = (kOffHeld + 4 * kChunkSlots + 31) / 32 * 32;
+constexpr unsigned kOffCfin = kOffFlags + 32;                      /* u32[kChunkSlots]: count entries finished */
+constexpr unsigned kOffFfin = kOffCfin + 4 * kChunkSlots;          /* u32[kChunkSlots]: full entries finished */
+constexpr unsigned kOffHeld = kOffFfin + 4 * kChunkSlots;          /* u32[kChunkSlots] */
+constexpr unsigned kOffClaim = kOffHeld + 4 * kChunkSlots;         /* u32[kEntries]: entry tag << 16 | units taken */
+constexpr unsigned kOffFin = kOffClaim + 4 * kEntries;             /* u32[kEntries]: units finished */
+constexpr unsigned kOffCur = kOffFin + 4 * kEntries;               /* u32: the entry units are claimed from */
+constexpr unsigned kOffStageInfo = (kOffCur + 4 + 31) / 32 * 32;
 constexpr unsigned kOffChunkInfo = kOffStageInfo + (unsigned)sizeof(StageInfo) * kEntries;
 constexpr unsigned kHdrBytes = (kOffChunkInfo + (unsigned)sizeof(ChunkInfo) * kChunkSlots + 127) / 128 * 128;
 /* flag words */
@@ -124,9 +129,9 @@ constexpr unsigned kSlotBytes = (kSlotColPtr + 8 * kMaxLoads + 127) / 128 * 128;
 constexpr unsigned kSlotArea = kHdrBytes;
 constexpr unsigned kWarpArea = kSlotArea + kChunkSlots * kSlotBytes;
 
-/* a compute warp's private area: the selection list of a full-phase group
- * (a 16-bit group row per entry), selection vectors and gathered columns of
- * a projection batch, row vectors of a count group */
+/* a compute warp's private area: the selection list of a full-phase unit
+ * (a 16-bit row per entry), selection vectors and gathered columns of a
+ * projection batch, row vectors of a count group */
 struct WarpLayout {
 	uint32_t sel_off, gat_off, row_off, bytes;
 };

@@ -154,24 +154,22 @@ constexpr unsigned kMaxChunkRows = 8192;
 constexpr unsigned kMaxChunkBlocks = kMaxChunkRows / kBlockRows;  /* 32: one lane each */
 constexpr unsigned kChunkWords = kMaxChunkRows / 32;
 
-/* how the full phase gets its rows.  FM_PICK, FM_GATHER and FM_BITMAP take
- * the rows' validity from the count phase's bitmap (the results read only
- * columns, constants and vectors computed after the filter):
- *  - FM_PICK stages full tiles of the columns the results read and picks
- *    each batch's selected rows out of the tile into the compute warp's own
- *    area, so a warp releases the tile as soon as it has picked its rows;
+/* how the full phase gets its rows.  FM_BITMAP and FM_GATHER take the rows'
+ * validity from the count phase's bitmap (the results read only columns,
+ * constants and vectors computed after the filter) and split an entry's
+ * selected rows into batches of up to 32 kBatchE rows, each a unit of work:
+ *  - FM_BITMAP stages full tiles of the columns the results read and reads
+ *    the selected rows in place;
  *  - FM_GATHER stages nothing: it loads the selected rows' values straight
- *    from device memory into the warp's area;
- *  - FM_BITMAP (results of many bytes per row) reads the staged tile in
- *    place until its rows are stored.
+ *    from device memory into the compute warp's own area.
  * FM_REFILTER stages full tiles of every column and runs the filter again
- * (the results read register vectors the filter computed). */
+ * over groups of kCountGroup blocks (the results read register vectors the
+ * filter computed). */
 constexpr uint32_t FM_BITMAP = 0;
 constexpr uint32_t FM_REFILTER = 1;
 constexpr uint32_t FM_GATHER = 2;
-constexpr uint32_t FM_PICK = 3;
-/* the largest bytes per row a picking or gathering full phase moves into a
- * compute warp's area */
+/* the largest bytes per row a gathering full phase moves into a compute
+ * warp's area */
 constexpr uint32_t kGatherMaxBpr = 32;
 
 /* the staged columns of one phase: which segment columns, where in a stage */
@@ -196,7 +194,7 @@ struct alignas(16) QDesc {
 	uint32_t nfilter;              /* uops [0, nfilter) are the filter */
 	uint32_t nuops;                /* uops [nfilter, nuops - 1) the projection, then Result */
 	uint32_t nout;
-	uint32_t full_mode;            /* FM_BITMAP or FM_REFILTER */
+	uint32_t full_mode;            /* FM_BITMAP, FM_REFILTER or FM_GATHER */
 	uint32_t chunk_rows;           /* rows per chunk (a multiple of both tile sizes) */
 	uint32_t pad0[3];
 	uint8_t out_stride[kMaxRegs];
@@ -205,14 +203,13 @@ struct alignas(16) QDesc {
 	OpRec ops_count[kMaxOps];
 	OpRec ops_full[kMaxOps];
 	uint32_t od_out[kMaxRegs];     /* result columns, over the full phase's layout */
-	/* FM_PICK and FM_GATHER: the columns the results read (the full set),
-	 * where a batch of them sits in a compute warp's gather area and, for
-	 * FM_PICK, where they sit in a staged full tile */
+	/* FM_GATHER: the columns the results read (the full set) and where a
+	 * batch of them sits in a compute warp's gather area */
 	uint32_t gather_n;
 	uint8_t gather_stride[kMaxLoads];
 	uint8_t pad3[3];
 	uint32_t gather_off[kMaxLoads];
-	uint32_t tile_off[kMaxLoads];
+	uint32_t pad4;
 	void *out_ptr[kMaxRegs];
 	uint64_t capacity;             /* rows each out column can hold */
 	unsigned long long *total_out; /* the query's row count, written with its last chunk's offset */

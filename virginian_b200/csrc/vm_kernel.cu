@@ -71,7 +71,6 @@ constexpr uint32_t kQNChunks = (uint32_t)offsetof(QDesc, nchunks);
 constexpr uint32_t kQGatherN = (uint32_t)offsetof(QDesc, gather_n);
 constexpr uint32_t kQGatherStride = (uint32_t)offsetof(QDesc, gather_stride);
 constexpr uint32_t kQGatherOff = (uint32_t)offsetof(QDesc, gather_off);
-constexpr uint32_t kQTileOff = (uint32_t)offsetof(QDesc, tile_off);
 static_assert(kQOpsCount % 16 == 0 && kQOpsFull % 16 == 0, "op records are read 16 bytes at a time");
 static_assert(kSlotBitmap % 16 == 0 && kSlotBlockOff % 8 == 0, "slot layout");
 static_assert(kOffStageInfo % 16 == 0 && sizeof(StageInfo) == 32, "stage info is read as two 16-byte words");
@@ -952,59 +951,36 @@ __device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&gr
 	}
 }
 
-/* FM_PICK: the batch's selected rows of every column the results read,
- * from the staged tile (its rows from `tile_row0`; entry i at group row
- * row[i]) into the warp's gather area */
-__device__ __forceinline__ void pick_batch(const Bases &b, uint32_t tile, uint32_t tile_row0,
-	const uint32_t (&row)[kBatchE], int lane)
+/* the projection and stores of one batch: entry i of this lane is group
+ * row row[i] (or, when the results read a gather area, batch entry
+ * 32 i + lane); entries in `act` exist, those in `in` fit the output and
+ * are stored at pos0 + their batch entry */
+__device__ __forceinline__ void batch_out(const Bases &b, const uint32_t (&row)[kBatchE], uint32_t act,
+	uint32_t in, uint64_t pos0, int lane)
 {
-	const uint32_t n = lds_u32(b.slot + kQGatherN);
-	for (uint32_t c = 0; c < n; c++) {
-		const uint32_t st = lds_u8(b.slot + kQGatherStride + c);
-		const uint32_t src = tile + lds_u32(b.slot + kQTileOff + 4 * c);
-		const uint32_t dst = b.stage + lds_u32(b.slot + kQGatherOff + 4 * c);
-		if (st == 4) {
-			uint32_t v[kBatchE];
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++)
-				v[i] = lds_u32(src + 4u * (tile_row0 + row[i]));
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++)
-				sts_u32(dst + 4u * (uint32_t)(32 * i + lane), v[i]);
-		} else if (st == 8) {
-			uint64_t v[kBatchE];
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++)
-				v[i] = lds_u64(src + 8u * (tile_row0 + row[i]));
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++)
-				sts_u64(dst + 8u * (uint32_t)(32 * i + lane), v[i]);
-		} else {
-			uint32_t v[kBatchE];
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++)
-				v[i] = lds_u8(src + tile_row0 + row[i]);
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++)
-				sts_u8(dst + (uint32_t)(32 * i + lane), v[i]);
-		}
+	const uint32_t ops = b.slot + kQOpsFull;
+	const uint32_t nf = lds_u32(b.slot + kQNFilter);
+	const uint32_t nu = lds_u32(b.slot + kQNUops) - 1u;
+	const uint32_t nout = lds_u32(b.slot + kQNOut);
+	for (uint32_t k = nf; k < nu; k++)
+		project_op(lds_v4(ops + 16u * k), b, row, act, lane);
+	for (uint32_t j = 0; j < nout; j++) {
+		const uint32_t od = lds_u32(b.slot + kQOdOut + 4 * j);
+		void *out = reinterpret_cast<void *>(lds_u64(b.slot + kQOutPtr + 8 * j));
+		const uint32_t stride = lds_u8(b.slot + kQOutStride + j);
+		if (stride == 4)
+			p_store<uint32_t>(od, b, row, in, static_cast<uint32_t *>(out), pos0, lane);
+		else
+			p_store_rare(od, b, make_uint4(row[0], row[1], row[2], row[3]), in, out, pos0, stride, lane);
 	}
 }
 
-/* full phase: one group's selected rows (up to kFullGroup blocks from chunk
- * block blk, nrows rows), in row order, projected and stored at the group's
- * offset; returns false on an output overflow.
- *
- * FM_BITMAP and FM_REFILTER read the staged tile in place (b.stage is the
- * tile, group rows from b.blk_row0).  FM_PICK and FM_GATHER first move each
- * batch's selected rows into the warp's gather area (b.stage), where the
- * results read them by batch entry: FM_PICK from the staged tile at `tile`,
- * FM_GATHER from device memory.  With FM_PICK and `release` set, the warp
- * arrives on the entry's release barriers (`release`, and `release2` when
- * nonzero) once its last batch is picked, and *released says so. */
-__device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32_t blk, uint32_t nrows,
-	uint32_t mode, int lane, uint32_t tile = 0, uint32_t tile_row0 = 0, uint32_t release = 0,
-	uint32_t release2 = 0, bool *released = nullptr)
+/* FM_REFILTER full phase: one group's selected rows (up to kCountGroup
+ * blocks from chunk block blk, nrows rows), in row order, with the filter
+ * run again for the register vectors the results read; b.stage is the
+ * staged tile and b.blk_row0 the group's first tile row.  Returns false on
+ * an output overflow. */
+__device__ __forceinline__ bool refilter_group(const Bases &b, uint32_t list, uint32_t blk, uint32_t nrows, int lane)
 {
 	/* lane l holds validity word l of the group (32 rows) */
 	const uint32_t nw = (nrows + 31) / 32;
@@ -1020,10 +996,8 @@ __device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32
 	const uint32_t n = __shfl_sync(0xffffffffu, incl, 31);
 	if (n == 0)
 		return true;
-	const uint32_t nf = lds_u32(b.slot + kQNFilter);
-	const uint32_t ops = b.slot + kQOpsFull;
-	if (mode == FM_REFILTER)
-		(void)run_filter<kCountGroup * kBlockRows / 32>(ops, nf, b, nrows, lane);  /* the filter's register vectors */
+	(void)run_filter<kCountGroup * kBlockRows / 32>(b.slot + kQOpsFull, lds_u32(b.slot + kQNFilter), b, nrows,
+		lane);  /* the filter's register vectors */
 	/* the selection list: entry i is the group row of the group's i-th
 	 * selected row; each lane lists its own word's rows */
 	{
@@ -1038,8 +1012,6 @@ __device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32
 	__syncwarp();
 	const uint64_t off = lds_u64(b.slot + kSlotBlockOff + 8u * blk);
 	const uint64_t cap = lds_u64(b.slot + kQCapacity);
-	const uint32_t nu = lds_u32(b.slot + kQNUops) - 1u;
-	const uint32_t nout = lds_u32(b.slot + kQNOut);
 	bool ok = true;
 	for (uint32_t base = 0; base < n; base += 32 * kBatchE) {
 		uint32_t row[kBatchE];
@@ -1059,49 +1031,114 @@ __device__ __forceinline__ bool full_group(const Bases &b, uint32_t list, uint32
 				in |= 1u << i;
 		}
 		ok = ok && act == in;
-		if (mode == FM_GATHER) {
-			/* gathered values are indexed by batch entry; the chunk row
-			 * of entry i is the group's first row plus its group row */
-			uint32_t grow[kBatchE];
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++) {
-				grow[i] = blk * kBlockRows + row[i];
-				row[i] = 32u * i + (uint32_t)lane;
-			}
-			gather_batch(b, grow, lane);
-			__syncwarp();
-		} else if (mode == FM_PICK) {
-			pick_batch(b, tile, tile_row0, row, lane);
-#pragma unroll
-			for (int i = 0; i < kBatchE; i++)
-				row[i] = 32u * i + (uint32_t)lane;
-			__syncwarp();
-			if (release && base + 32 * kBatchE >= n) {
-				/* the last batch is picked: the tile is free for this warp */
-				if (lane == 0) {
-					mbar_arrive(release);
-					if (release2)
-						mbar_arrive(release2);
-				}
-				*released = true;
-			}
-		}
-		for (uint32_t k = nf; k < nu; k++)
-			project_op(lds_v4(ops + 16u * k), b, row, act, lane);
-		for (uint32_t j = 0; j < nout; j++) {
-			const uint32_t od = lds_u32(b.slot + kQOdOut + 4 * j);
-			void *out = reinterpret_cast<void *>(lds_u64(b.slot + kQOutPtr + 8 * j));
-			const uint32_t stride = lds_u8(b.slot + kQOutStride + j);
-			if (stride == 4)
-				p_store<uint32_t>(od, b, row, in, static_cast<uint32_t *>(out), off + base, lane);
-			else
-				p_store_rare(od, b, make_uint4(row[0], row[1], row[2], row[3]), in, out, off + base, stride, lane);
-		}
-		if (mode == FM_GATHER || mode == FM_PICK)
-			__syncwarp();  /* the next batch overwrites this one's values */
+		batch_out(b, row, act, in, off + base, lane);
 	}
 	__syncwarp();
 	return ok;
+}
+
+/* the selected rows of one full entry (chunk blocks [blk0, blk0 + nblk),
+ * up to 32 of them): how many, and the output position of the first */
+__device__ __forceinline__ uint32_t entry_selected(uint32_t slot, uint32_t blk0, uint32_t nblk, uint64_t *off0)
+{
+	const uint64_t first = lds_u64(slot + kSlotBlockOff + 8u * blk0);
+	const uint32_t last = blk0 + nblk - 1;
+	*off0 = first;
+	return (uint32_t)(lds_u64(slot + kSlotBlockOff + 8u * last) + lds_u32(slot + kSlotBlockCnt + 4u * last) - first);
+}
+
+/* FM_BITMAP / FM_GATHER full phase: batch j of an entry's selected rows
+ * (ranks [32 kBatchE j, ...) of the nsel rows of chunk blocks
+ * [blk0, blk0 + nblk), whose first is stored at off0).  The warp lists the
+ * batch's rows from the bitmap, starting at the block that holds its first
+ * rank, then reads them from the staged tile in place (b.stage the tile,
+ * rows counted from its first row) or gathers them from device memory into
+ * the warp's gather area.  Returns false on an output overflow. */
+__device__ __forceinline__ bool full_batch(Bases b, uint32_t list, uint32_t gat, uint32_t blk0, uint32_t nblk,
+	uint32_t j, uint32_t nsel, uint64_t off0, uint32_t mode, int lane)
+{
+	const uint32_t r0 = 32u * kBatchE * j;
+	if (r0 >= nsel)
+		return true;  /* an entry with no selected rows: nothing to do */
+	const uint32_t cnt = min(32u * kBatchE, nsel - r0);
+	/* the block holding rank r0: lane l looks at block blk0 + l */
+	uint32_t bo = 0, bc = 0;
+	if ((uint32_t)lane < nblk) {
+		bo = (uint32_t)(lds_u64(b.slot + kSlotBlockOff + 8u * (blk0 + lane)) - off0);
+		bc = lds_u32(b.slot + kSlotBlockCnt + 4u * (blk0 + lane));
+	}
+	const uint32_t hit = __ballot_sync(0xffffffffu, (uint32_t)lane < nblk && bo <= r0 && r0 < bo + bc);
+	if (hit == 0)
+		return false;  /* counts and offsets disagree: stores nothing, reports an error */
+	const int bsel = __ffs(hit) - 1;
+	uint32_t rank = __shfl_sync(0xffffffffu, bo, bsel);  /* rank of the block's first selected row */
+	/* words of 32 rows from that block on, 32 at a time, until the batch's
+	 * last rank is listed */
+	const uint32_t nwords = 8u * nblk;
+	const uint32_t bm = b.slot + kSlotBitmap + 32u * blk0;
+	for (uint32_t w0 = 8u * (uint32_t)bsel; w0 < nwords && rank < r0 + cnt; w0 += 32) {
+		const uint32_t wi = w0 + (uint32_t)lane;
+		const uint32_t word = wi < nwords ? lds_u32(bm + 4u * wi) : 0u;
+		const uint32_t c = __popc(word);
+		uint32_t incl = c;
+#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+			if (lane >= d)
+				incl += v;
+		}
+		uint32_t rr = rank + incl - c, x = word;
+		if (rr + c > r0 && rr < r0 + cnt) {
+			while (rr < r0) {  /* ranks before the batch */
+				x &= x - 1;
+				rr++;
+			}
+			while (x && rr < r0 + cnt) {
+				const uint32_t bit = __ffs(x) - 1;
+				asm volatile("st.shared.u16 [%0], %1;" ::"r"(list + 2 * (rr - r0)), "h"((uint16_t)(32 * wi + bit))
+					: "memory");
+				rr++;
+				x &= x - 1;
+			}
+		}
+		rank += __shfl_sync(0xffffffffu, incl, 31);
+	}
+	__syncwarp();
+	const uint64_t cap = lds_u64(b.slot + kQCapacity);
+	const uint64_t pos0 = off0 + r0;
+	uint32_t row[kBatchE];
+	uint32_t act = 0, in = 0;
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++) {
+		const uint32_t e = 32 * i + (uint32_t)lane;
+		const bool a = e < cnt;
+		row[i] = 0;
+		if (a) {
+			uint16_t r;
+			asm volatile("ld.shared.u16 %0, [%1];" : "=h"(r) : "r"(list + 2 * e));
+			row[i] = r;
+		}
+		act |= (a ? 1u : 0u) << i;
+		if (a && pos0 + e < cap)
+			in |= 1u << i;
+	}
+	b.blk_row0 = 0;
+	if (mode == FM_GATHER) {
+		/* gathered values are indexed by batch entry; the chunk row of
+		 * entry i is the entry's first row plus its row */
+		uint32_t grow[kBatchE];
+#pragma unroll
+		for (int i = 0; i < kBatchE; i++) {
+			grow[i] = blk0 * kBlockRows + row[i];
+			row[i] = 32u * i + (uint32_t)lane;
+		}
+		b.stage = gat;
+		gather_batch(b, grow, lane);
+		__syncwarp();
+	}
+	batch_out(b, row, act, in, pos0, lane);
+	__syncwarp();  /* the list and gather area are this warp's next batch's */
+	return act == in;
 }
 
 /* ---- ordered placement ------------------------------------------------- */
@@ -1499,6 +1536,12 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 			const uint32_t si = sbase + kOffStageInfo + (uint32_t)sizeof(StageInfo) * s;
 			sts_v4(si, make_uint4(kind, c.slot, c.seq, row0));
 			sts_v4(si + 16, make_uint4(nrows, last ? 1u : 0u, bf, 0u));
+			sts_u32(sbase + kOffFin + 4 * s, 0u);
+			/* the entry's tag, after its info: compute warps claim its
+			 * units from here on */
+			__threadfence_block();
+			asm volatile("st.volatile.shared.u32 [%0], %1;" ::"r"(sbase + kOffClaim + 4 * s), "r"((k & 0xffffu) << 16)
+				: "memory");
 		}
 		__syncwarp();
 		if (lane == 0) {
@@ -1604,8 +1647,11 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 			e.seq = i;
 			e.qi = 0;
 			e.gather = false;
-			if (lane == 0)
+			if (lane == 0) {
 				sts_u32(sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * e.slot + offsetof(ChunkInfo, valid), 0u);
+				/* the look-back warp finds the end in this slot */
+				mbar_arrive(sbase + kOffCounted + 8 * e.slot);
+			}
 			LaneCol none;
 			none.has = false;
 			none.src = none.stride = none.off = 0;
@@ -1630,7 +1676,8 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		if (lane == 0) {
 			const uint32_t ci = sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * c.slot;
 			sts_v4(ci, make_uint4(1u, c.qi, (uint32_t)c.w, 0u));
-			sts_v4(ci + 16, make_uint4(c.rows, c.block_base, 0u, 0u));
+			sts_v4(ci + 16, make_uint4(c.rows, c.block_base, (c.rows + c.count_tile - 1) / c.count_tile,
+				c.gather ? 1u : (c.rows + c.full_tile - 1) / c.full_tile));
 			const uint32_t held = sbase + kOffHeld + 4 * c.slot;
 			desc = lds_u32(held) != c.qi;
 			sts_u32(held, c.qi);
@@ -1681,153 +1728,236 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 
 /* ---- compute warps ------------------------------------------------------- */
 
-/* Every compute warp walks the stages in order.  A stage's blocks form
- * groups (kCountGroup blocks in the count phase; kFullGroup in the full
- * phase, or kCountGroup when it runs the filter again), and the groups of
- * all stages are dealt round-robin over the compute warps (warp w takes the
- * groups whose running number is w mod W), so a stage's groups run in
- * parallel and a warp with nothing in a stage moves on to the next.  After
- * a stage a warp releases it; after a chunk's last count tile it arrives on
- * the chunk's counted barrier; before its first full group of a chunk it
- * waits for the chunk's offsets; after the chunk's last full tile it arrives
- * on the chunk's done barrier (the slot is free once all have). */
+__device__ __forceinline__ uint32_t ldv_u32(uint32_t a)
+{
+	uint32_t v;
+	asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+	return v;
+}
+
+__device__ __forceinline__ void stv_u32(uint32_t a, uint32_t v)
+{
+	asm volatile("st.volatile.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t atom_cas_shared(uint32_t a, uint32_t cmp, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.shared.cas.b32 %0, [%1], %2, %3;" : "=r"(old) : "r"(a), "r"(cmp), "r"(v) : "memory");
+	return old;
+}
+
+/* finish counters: each finisher's release orders its warp's work before
+ * the count, and the last one's acquire makes all of it visible to it (and,
+ * through its barrier arrivals, to the warps that wait on them) */
+__device__ __forceinline__ uint32_t atom_add_acq_rel_shared(uint32_t a, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.acq_rel.cta.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(a), "r"(v) : "memory");
+	return old;
+}
+
+/* Compute warps claim units of work from the entries in ring order: a count
+ * entry's units are its groups of kCountGroup blocks; a full entry's are
+ * batches of up to 32 kBatchE of its selected rows (groups of kCountGroup
+ * blocks when it runs the filter again).  The claim word of an entry holds
+ * the entry's ordinal (low 16 bits, written by the producer when it
+ * announces the entry) and the units taken; a warp takes a unit with a
+ * compare-and-swap on it, the warp that takes an entry's last unit moves the
+ * cursor to the next entry, and the warp that finishes an entry's last unit
+ * releases the entry and its data buffer and, after a chunk's last count or
+ * full entry, arrives on the chunk's counted or done barrier.  So idle warps
+ * always take the oldest work, however uneven an entry's units are, and no
+ * warp waits for another to pass an entry.  A full entry's unit count needs
+ * the chunk's offsets, so a warp waits for them before it counts. */
 template <int W>
 __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int lane)
 {
 	const uint32_t sbase = smem_addr(smem);
 	const uint32_t flags = sbase + kOffFlags;
-	const uint32_t nst = kp.nstages;
 	const uint32_t warp_base = sbase + kWarpArea + (uint32_t)w * kp.warp_bytes;
 	const uint32_t list = warp_base;
 	const uint32_t gat = warp_base + kp.gat_off;
 	Bases b;
 	b.rowv = warp_base + kp.row_off;
 	b.selv = warp_base + kp.sel_off;
-	uint32_t ng = 0;             /* groups of the stages seen so far */
 	uint32_t based_seq = ~0u;    /* the chunk whose offsets this warp waited for */
 	uint32_t desc_seq = ~0u;     /* the chunk whose descriptor view this warp waited for */
 	/* the chunk's descriptor view in its slot: a warp waits for it before it
-	 * first reads the slot for that chunk (the chunk's first count tile need
-	 * not be one this warp waited for) */
+	 * first reads the slot for that chunk */
 	auto wait_desc = [&](uint32_t slot, uint32_t seq) -> bool {
 		if (desc_seq == seq)
 			return true;
 		desc_seq = seq;
 		return mbar_wait(sbase + kOffDesc + 8 * slot, (seq / kChunkSlots) & 1u, flags);
 	};
-	for (uint32_t k = 0;; k++) {
-		const uint32_t s = k % kEntries;
-		/* the entry's info first: a warp with no group in it releases the
-		 * entry without waiting for its data */
-		if (!mbar_wait(sbase + kOffAnn + 8 * s, (k / kEntries) & 1u, flags)) {
+	auto wait_based = [&](uint32_t slot, uint32_t seq) -> bool {
+		if (based_seq == seq)
+			return true;
+		based_seq = seq;
+		return mbar_wait(sbase + kOffBased + 8 * slot, (seq / kChunkSlots) & 1u, flags);
+	};
+	for (;;) {
+		/* ---- claim a unit */
+		uint32_t k = 0, j = 0, n = 0, kind = 0, slot = 0, seq = 0, row0 = 0, nrows = 0, buf = 0, mode = FM_BITMAP;
+		uint32_t nsel = 0;
+		uint64_t off0 = 0;
+		bool fail = false;
+		uint64_t t0 = 0;
+		for (uint32_t spin = 0;; spin++) {
+			/* bounded: a claim that makes no progress for the wait limit
+			 * (or after another warp aborted the CTA) gives up */
+			if ((spin & 255u) == 255u) {
+				const uint64_t now = globaltimer_ns();
+				if (t0 == 0) {
+					t0 = now;
+				} else if (ldv_u32(flags + 4 * kFAbort) ||
+					now - t0 > (uint64_t)lds_u32(flags + 4 * kFWaitMs) * 1000000ull) {
+					fail = true;
+					break;
+				}
+			}
+			uint32_t kk = 0, c = 0;
+			if (lane == 0) {
+				kk = ldv_u32(sbase + kOffCur);
+				c = ldv_u32(sbase + kOffClaim + 4 * (kk % kEntries));
+			}
+			kk = __shfl_sync(0xffffffffu, kk, 0);
+			c = __shfl_sync(0xffffffffu, c, 0);
+			const uint32_t s = kk % kEntries;
+			const uint32_t tag = c >> 16;
+			if (tag != (kk & 0xffffu)) {
+				/* not announced yet (the slot still holds the entry a lap
+				 * earlier), or the cursor moved on meanwhile */
+				if (tag == ((kk - kEntries) & 0xffffu) &&
+					!mbar_wait(sbase + kOffAnn + 8 * s, (kk / kEntries) & 1u, flags)) {
+					fail = true;
+					break;
+				}
+				continue;
+			}
+			__threadfence_block();  /* the entry's info after its tag */
+			const uint32_t sia = sbase + kOffStageInfo + (uint32_t)sizeof(StageInfo) * s;
+			const uint4 s0 = lds_v4(sia), s1 = lds_v4(sia + 16);
+			__threadfence_block();
+			uint32_t c2 = 0;
+			if (lane == 0)
+				c2 = ldv_u32(sbase + kOffClaim + 4 * s);
+			if (__shfl_sync(0xffffffffu, c2, 0) != c)
+				continue;  /* claimed or recycled meanwhile: the info may be torn */
+			kind = s0.x;
+			slot = s0.y;
+			seq = s0.z;
+			row0 = s0.w;
+			nrows = s1.x;
+			buf = s1.z;
+			if (kind == SK_END)
+				return;  /* every unit before the end is claimed */
+			const uint32_t nblk = (nrows + kBlockRows - 1) / kBlockRows;
+			if (kind == SK_COUNT) {
+				n = (nblk + kCountGroup - 1) / kCountGroup;
+			} else {
+				if (!wait_desc(slot, seq) || !wait_based(slot, seq)) {
+					fail = true;
+					break;
+				}
+				b.slot = sbase + kSlotArea + slot * kSlotBytes;
+				mode = lds_u32(b.slot + kQFullMode);
+				if (mode == FM_REFILTER) {
+					n = (nblk + kCountGroup - 1) / kCountGroup;
+				} else {
+					nsel = entry_selected(b.slot, row0 / kBlockRows, nblk, &off0);
+					n = max(1u, (nsel + 32u * kBatchE - 1) / (32u * kBatchE));
+				}
+			}
+			const uint32_t taken = c & 0xffffu;
+			if (taken < n) {
+				uint32_t got = 0;
+				if (lane == 0) {
+					got = atom_cas_shared(sbase + kOffClaim + 4 * s, c, c + 1) == c;
+					if (got && taken + 1 == n)
+						stv_u32(sbase + kOffCur, kk + 1);
+				}
+				if (__shfl_sync(0xffffffffu, got, 0)) {
+					k = kk;
+					j = taken;
+					break;
+				}
+				continue;
+			}
+			/* every unit taken: the last taker is moving the cursor */
+		}
+		if (fail || (kind == SK_COUNT && !wait_desc(slot, seq)) ||
+			!mbar_wait(sbase + kOffFull + 8 * (k % kEntries), (k / kEntries) & 1u, flags)) {
 			if (lane == 0)
 				abort_cta(kp, flags, DE_STAGE_TIMEOUT);
 			return;
 		}
-		const uint32_t sia = sbase + kOffStageInfo + (uint32_t)sizeof(StageInfo) * s;
-		const uint4 s0 = lds_v4(sia), s1 = lds_v4(sia + 16);
-		const uint32_t kind = s0.x, slot = s0.y, seq = s0.z, row0 = s0.w, nrows = s1.x, last = s1.y, buf = s1.z;
-		if (kind == SK_END) {
-			__syncwarp();
-			if (lane == 0)
-				mbar_arrive(sbase + kOffCounted + 8 * slot);
-			return;
-		}
+		/* ---- run it */
 		b.slot = sbase + kSlotArea + slot * kSlotBytes;
 		const uint32_t tile = buf != kNoBuf ? sbase + kp.stage_area + buf * kp.stage_bytes : 0u;
-		b.stage = buf != kNoBuf ? tile : gat;
-		bool released = false;  /* this warp released the entry already */
 		const uint32_t nblk = (nrows + kBlockRows - 1) / kBlockRows;
 		const uint32_t blk0 = row0 / kBlockRows;
-		if (kind == SK_FULL && !wait_desc(slot, seq)) {
-			if (lane == 0)
-				abort_cta(kp, flags, DE_STAGE_TIMEOUT);
-			return;
-		}
-		const uint32_t mode = kind == SK_FULL ? lds_u32(b.slot + kQFullMode) : FM_BITMAP;
-		const uint32_t G = kind == SK_COUNT || mode == FM_REFILTER ? (uint32_t)kCountGroup : (uint32_t)kFullGroup;
-		const uint32_t ngs = (nblk + G - 1) / G;
-		const uint32_t j0 = ((uint32_t)w + W - ng % W) % W;
-		ng += ngs;
-		if (j0 < ngs && (!wait_desc(slot, seq) || !mbar_wait(sbase + kOffFull + 8 * s, (k / kEntries) & 1u, flags))) {
-			if (lane == 0)
-				abort_cta(kp, flags, DE_STAGE_TIMEOUT);
-			return;
-		}
 		bool ok = true;
-		if (kind == SK_COUNT) {
-			for (uint32_t j = j0; j < ngs; j += W) {
-				const uint32_t r = j * kCountGroup * kBlockRows;
-				b.blk_row0 = r;
+		if (kind == SK_COUNT || mode == FM_REFILTER) {
+			const uint32_t r = j * kCountGroup * kBlockRows;
+			b.stage = tile;
+			b.blk_row0 = r;
+			if (kind == SK_COUNT)
 				count_group(b, blk0 + j * kCountGroup, min((uint32_t)kCountGroup, nblk - j * kCountGroup),
 					min((uint32_t)(kCountGroup * kBlockRows), nrows - r), lane);
-			}
+			else
+				ok = refilter_group(b, list, blk0 + j * kCountGroup, min((uint32_t)(kCountGroup * kBlockRows), nrows - r),
+					lane);
 		} else {
-			uint32_t j = j0;
-			if (j < ngs && based_seq != seq) {
-				if (!mbar_wait(sbase + kOffBased + 8 * slot, (seq / kChunkSlots) & 1u, flags)) {
-					if (lane == 0)
-						abort_cta(kp, flags, DE_STAGE_TIMEOUT);
-					return;
-				}
-				based_seq = seq;
-			}
-			/* FM_PICK: a warp with one group in the entry releases the
-			 * tile once it has picked that group's rows */
-			const bool pick1 = mode == FM_PICK && j < ngs && j + W >= ngs;
-			for (; j < ngs; j += W) {
-				const uint32_t r = j * G * kBlockRows;
-				if (mode == FM_PICK || mode == FM_GATHER) {
-					/* results read the warp's gather area by batch entry */
-					b.blk_row0 = 0;
-					b.stage = gat;
-				} else {
-					b.blk_row0 = r;
-				}
-				ok = full_group(b, list, blk0 + j * G, min(G * kBlockRows, nrows - r), mode, lane,
-					tile, r, pick1 ? sbase + kOffEmpty + 8 * s : 0u,
-					pick1 && buf != kNoBuf ? sbase + kOffBfree + 8 * buf : 0u, &released) && ok;
-			}
+			b.stage = tile;
+			ok = full_batch(b, list, gat, blk0, nblk, j, nsel, off0, mode, lane);
 		}
 		/* a serving session reports rows beyond capacity in the query's
 		 * completion record instead */
 		if (!__all_sync(0xffffffffu, ok) && lane == 0 && kp.serve == nullptr)
 			report(kp.error, DE_OUTPUT_OVERFLOW);
-		const bool account = kind == SK_FULL && last && kp.serve != nullptr;
-		if (account)
-			__threadfence();  /* this warp's result rows before the chunk counts as stored */
+		const bool serving_full = kind == SK_FULL && kp.serve != nullptr;
+		if (serving_full)
+			__threadfence();  /* this unit's result rows before the chunk counts as stored */
 		__syncwarp();
-		if (lane == 0) {
-			if (account) {
-				/* the last warp done with the chunk counts it for its query;
-				 * the chunk that completes the query writes its record */
-				unsigned *fd = reinterpret_cast<unsigned *>(smem + kOffFdone) + slot;
-				if (atomicAdd(fd, 1u) == (unsigned)W - 1u) {
-					*fd = 0u;
-					const uint32_t qi = lds_u32(sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * slot +
-						offsetof(ChunkInfo, query));
-					const uint64_t nch = lds_u64(b.slot + kQNChunks);
-					unsigned long long *tot = reinterpret_cast<unsigned long long *>(lds_u64(b.slot + kQTotalOut));
-					__threadfence();
-					const unsigned done = atomicAdd(&kp.done_chunks[qi], 1u) + 1u;
-					if (done == (unsigned)nch) {
+		/* ---- finish it */
+		if (lane == 0 && atom_add_acq_rel_shared(sbase + kOffFin + 4 * (k % kEntries), 1u) + 1u == n) {
+			/* the entry's last unit: its buffer is free, and the chunk's
+			 * phase is done once all its entries of this kind are */
+			if (buf != kNoBuf)
+				mbar_arrive(sbase + kOffBfree + 8 * buf);
+			const uint32_t ci = sbase + kOffChunkInfo + (uint32_t)sizeof(ChunkInfo) * slot;
+			const uint32_t cf = sbase + (kind == SK_COUNT ? kOffCfin : kOffFfin) + 4 * slot;
+			const uint32_t need = lds_u32(ci + (kind == SK_COUNT ? offsetof(ChunkInfo, ncount) : offsetof(ChunkInfo, nfull)));
+			if (atom_add_acq_rel_shared(cf, 1u) + 1u == need) {
+				stv_u32(cf, 0u);
+				if (kind == SK_COUNT) {
+					mbar_arrive(sbase + kOffCounted + 8 * slot);
+				} else {
+					if (serving_full) {
+						/* the chunk that completes its query writes the
+						 * query's completion record */
+						const uint32_t qi = lds_u32(ci + offsetof(ChunkInfo, query));
+						const uint64_t nch = lds_u64(b.slot + kQNChunks);
+						unsigned long long *tot = reinterpret_cast<unsigned long long *>(lds_u64(b.slot + kQTotalOut));
 						__threadfence();
-						const unsigned long long nrow = *reinterpret_cast<volatile unsigned long long *>(tot);
-						volatile ServeRec *r = kp.recs + qi;
-						r->rows = nrow;
-						__threadfence_system();
-						r->seq = (unsigned long long)qi + 1ull;
+						const unsigned done = atomicAdd(&kp.done_chunks[qi], 1u) + 1u;
+						if (done == (unsigned)nch) {
+							__threadfence();
+							const unsigned long long nrow = *reinterpret_cast<volatile unsigned long long *>(tot);
+							volatile ServeRec *r = kp.recs + qi;
+							r->rows = nrow;
+							__threadfence_system();
+							r->seq = (unsigned long long)qi + 1ull;
+						}
 					}
+					mbar_arrive(sbase + kOffDone + 8 * slot);
 				}
 			}
-			if (!released) {
-				mbar_arrive(sbase + kOffEmpty + 8 * s);
-				if (buf != kNoBuf)
-					mbar_arrive(sbase + kOffBfree + 8 * buf);
-			}
-			if (last)
-				mbar_arrive(sbase + (kind == SK_COUNT ? kOffCounted : kOffDone) + 8 * slot);
+			mbar_arrive(sbase + kOffEmpty + 8 * (k % kEntries));
 		}
+		__syncwarp();
 	}
 }
 
@@ -1838,19 +1968,26 @@ __global__ void __launch_bounds__(32 * (W + 2), 1) vm_kernel(const KParams kp)
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	if (tid == 0) {
 		const uint32_t sbase = smem_addr(smem);
+		/* entries, buffers and chunk phases are released once, by the
+		 * warp that finishes their last unit */
 		for (uint32_t s = 0; s < kEntries; s++) {
 			mbar_init(sbase + kOffFull + 8 * s, 1);
-			mbar_init(sbase + kOffEmpty + 8 * s, W);
+			mbar_init(sbase + kOffEmpty + 8 * s, 1);
 			mbar_init(sbase + kOffAnn + 8 * s, 1);
+			/* the slot holds "entry s - kEntries" until entry s is announced */
+			sts_u32(sbase + kOffClaim + 4 * s, ((s - kEntries) & 0xffffu) << 16);
+			sts_u32(sbase + kOffFin + 4 * s, 0u);
 		}
+		sts_u32(sbase + kOffCur, 0u);
 		for (uint32_t s = 0; s < kp.nstages; s++)
-			mbar_init(sbase + kOffBfree + 8 * s, W);
+			mbar_init(sbase + kOffBfree + 8 * s, 1);
 		for (uint32_t q = 0; q < kChunkSlots; q++) {
-			mbar_init(sbase + kOffCounted + 8 * q, W);
+			mbar_init(sbase + kOffCounted + 8 * q, 1);
 			mbar_init(sbase + kOffBased + 8 * q, 1);
-			mbar_init(sbase + kOffDone + 8 * q, W);
+			mbar_init(sbase + kOffDone + 8 * q, 1);
 			mbar_init(sbase + kOffDesc + 8 * q, 1);
-			sts_u32(sbase + kOffFdone + 4 * q, 0u);
+			sts_u32(sbase + kOffCfin + 4 * q, 0u);
+			sts_u32(sbase + kOffFfin + 4 * q, 0u);
 			sts_u32(sbase + kOffHeld + 4 * q, ~0u);
 		}
 		for (int x = 0; x < 8; x++)
