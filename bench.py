@@ -50,6 +50,8 @@ WORKLOAD = ("device-resident filter scan + arithmetic (7-column table, 50M rows 
 TRAFFIC_READ_PER_ROW = 224.154112e6 / 8_000_000
 TRAFFIC_WRITE_PER_RESULT_ROW = 10.263552e6 / 800_581
 SWEEP = [0.001, 0.01, 0.10, 0.50, 0.99]
+# the plain CPU-runnable filter (1M rows)
+CONFIG1 = "SELECT id, uniformi, normali5 FROM test WHERE uniformi > 60 AND normali5 < 0"
 QUERY = ("SELECT id, uniformf + normalf5 * 2.5 AS fsum, normali20 / 3 AS idiv, "
          "uniformi - normali5 AS isub FROM test WHERE uniformf < {c:.6f} OR normalf20 > {d:.6f}")
 
@@ -243,16 +245,18 @@ def _device_tables(eng, sizes, seed0):
     return tables
 
 
-def _host_tables(eng, sizes, seed0):
+def _host_tables(eng, sizes, seed0, table_nos=None):
     """Resident tables of the benchmark schema from the seeded host generator
-    (the reference CPU VM rebuilds the same bytes to check the results)."""
+    (the reference CPU VM rebuilds the same bytes to check the results);
+    table i is generated as table number table_nos[i] (default i)."""
     import virginian_b200 as vb
     from oracle.digest import host_table
     from virginian_b200 import datagen
     types = [t for _, t in datagen.SCHEMA_A]
     tables = []
     for i, n in enumerate(sizes):
-        cols = host_table(int(n), seed0, i, threads=min(16, os.cpu_count() or 1))
+        cols = host_table(int(n), seed0, i if table_nos is None else table_nos[i],
+                          threads=min(16, os.cpu_count() or 1))
         t = vb.Table(eng, types)
         if n:
             t.append(datagen.segments(cols, datagen.SCHEMA_A))
@@ -289,33 +293,42 @@ def _queries(n, seed, ntables, layout=None):
     return out
 
 
-def bench_batched(eng, reps=5):
+def bench_batched(eng, reps=5, world=1, rank=0):
     """256 generated queries over 64 resident tables of log-uniform size in
     [10k, 20M] rows: one persistent graph-replayed launch (autotuned shape)
     against one launch per query; every batched result compared with the
-    reference CPU VM (virginia_single) on the same table."""
+    reference CPU VM (virginia_single) on the same table.  With N ranks each
+    rank holds the tables it owns (virginian_b200.shard.assign_tables) and
+    runs the queries over them; times are the slowest rank's, and the result
+    directory (every query's row count) is one all-reduce."""
     import torch
     import virginian_b200 as vb
     from oracle.digest import digest, table_digests_star
+    from virginian_b200 import shard
     hbm, _ = peaks()
     rng = np.random.default_rng(404)
     sizes = np.exp(rng.uniform(np.log(1e4), np.log(2e7), size=64)).astype(np.int64)
-    tables = _host_tables(eng, sizes, 1000)
+    owner = shard.assign_tables([int(x) for x in sizes], world)
+    mine_t = [k for k in range(len(sizes)) if owner[k] == rank]
+    tables = dict(zip(mine_t, _host_tables(eng, [sizes[k] for k in mine_t], 1000, mine_t)))
     log("batched: tables ready")
-    work = _queries(256, 77, len(tables))
+    all_work = _queries(256, 77, len(sizes))
+    mine = shard.my_queries([k for _, k, _ in all_work], owner, rank)
+    work = [all_work[i] for i in mine]
     log("batched: per-query path")
     # one launch per query (the result count read back after each)
     for q, k, p in work[:8]:
         r = tables[k].query(p)
         _ = r.rows
         r.close()
+    barrier(world)
     t0 = time.perf_counter()
     per_rows = []
     for q, k, p in work:
         r = tables[k].query(p)
         per_rows.append(r.rows)
         r.close()
-    per_s = time.perf_counter() - t0
+    per_s = allreduce_max(time.perf_counter() - t0, world)
     log("batched: batch path")
     b = vb.Batch(eng, autotune=True)
     for q, k, p in work:
@@ -326,14 +339,15 @@ def bench_batched(eng, reps=5):
     times, dev_ms = [], []
     for _ in range(reps):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(world)
         t0 = time.perf_counter()
         ev0.record(stream)
         b.run(graph=True)
         ev1.record(stream)
         b.wait()
-        times.append(time.perf_counter() - t0)
+        times.append(allreduce_max(time.perf_counter() - t0, world))
         ev1.synchronize()
-        dev_ms.append(ev0.elapsed_time(ev1))
+        dev_ms.append(allreduce_max(ev0.elapsed_time(ev1), world))
     batch_s = statistics.median(times)
     batch_dev_ms = statistics.median(dev_ms)
     rows_equal = all(b.rows(i) == per_rows[i] for i in range(len(work)))
@@ -341,11 +355,36 @@ def bench_batched(eng, reps=5):
     got = [digest(b.download(i)) for i in range(len(work))]
     shape = b.shape()
     b.close()
-    total_rows = int(sizes.sum())
-    alg = sum(int(sizes[k]) * p.info.load_bytes_per_row + got[i][0] * p.info.out_bytes_per_row
-              for i, (q, k, p) in enumerate(work))
-    for t in tables:
+    directory = shard.result_directory(len(all_work), mine, [g[0] for g in got],
+                                       device="cuda" if world > 1 else "cpu")
+    alg_local = sum(int(sizes[k]) * p.info.load_bytes_per_row + got[i][0] * p.info.out_bytes_per_row
+                    for i, (q, k, p) in enumerate(work))
+    alg = alg_local
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([float(alg_local)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        alg = int(t.item())
+    for t in tables.values():
         t.close()
+    out = {"workload": "256 generated queries (predicate trees of depth 1-4, 1-5 result columns) over 64 "
+                       "resident tables, rows log-uniform in [1e4, 2e7]" +
+                       ("" if world == 1 else f"; whole tables per rank over {world} ranks"),
+           "tables": 64, "queries": len(all_work), "table_rows": int(sizes.sum()),
+           "batched_qps": round(len(all_work) / batch_s, 1), "per_query_qps": round(len(all_work) / per_s, 1),
+           "speedup": round(per_s / batch_s, 2), "batched_ms": round(batch_s * 1e3, 3),
+           "batched_device_ms": round(batch_dev_ms, 3),
+           "per_query_ms": round(per_s * 1e3, 3), "result_rows": int(sum(directory)),
+           "algorithmic_bytes": int(alg),
+           "batched_gbs": round(alg / (batch_dev_ms / 1e3) / 1e9, 1),
+           "frac_of_hbm": round(alg / (batch_dev_ms / 1e3) / 1e9 / (hbm * world), 3),
+           "rows_equal_per_query_path": bool(rows_equal), "shape": shape,
+           "launches": {"batched_per_rep": 1, "per_query": len(work)}}
+    if world > 1:
+        out["queries_this_rank"] = len(work)
+        out["oracle_checked"] = 0
+        out["oracle_note"] = "checked at one GPU; the per-rank split changes which GPU runs a query, not its bytes"
+        return out
     # the reference CPU VM on every (table, query): one task per table,
     # largest first, in spawned workers while the GPU idles
     log("batched: reference CPU VM on every query")
@@ -357,26 +396,14 @@ def bench_batched(eng, reps=5):
     with _oracle_pool() as pool:
         res = pool.map(table_digests_star, [(int(sizes[k]), 1000, k, [work[i][0] for i in by_table[k]])
                                             for k in order], chunksize=1)
-    oracle_s = time.perf_counter() - t0
     mismatch = []
     for k, digs in zip(order, res):
         for i, d in zip(by_table[k], digs):
             if not _same(got[i], d):
                 mismatch.append(i)
-    return {"workload": "256 generated queries (predicate trees of depth 1-4, 1-5 result columns) over 64 "
-                        "resident tables, rows log-uniform in [1e4, 2e7]",
-            "tables": 64, "queries": len(work), "table_rows": total_rows,
-            "batched_qps": round(len(work) / batch_s, 1), "per_query_qps": round(len(work) / per_s, 1),
-            "speedup": round(per_s / batch_s, 2), "batched_ms": round(batch_s * 1e3, 3),
-            "batched_device_ms": round(batch_dev_ms, 3),
-            "per_query_ms": round(per_s * 1e3, 3), "result_rows": int(sum(per_rows)),
-            "algorithmic_bytes": int(alg),
-            "batched_gbs": round(alg / (batch_dev_ms / 1e3) / 1e9, 1),
-            "frac_of_hbm": round(alg / (batch_dev_ms / 1e3) / 1e9 / hbm, 3),
-            "rows_equal_per_query_path": bool(rows_equal),
-            "oracle_checked": len(work), "oracle_mismatches": mismatch,
-            "oracle_seconds": round(oracle_s, 1), "shape": shape,
-            "launches": {"batched_per_rep": 1, "per_query": len(work)}}
+    out.update({"oracle_checked": len(work), "oracle_mismatches": mismatch,
+                "oracle_seconds": round(time.perf_counter() - t0, 1)})
+    return out
 
 
 def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
@@ -589,6 +616,133 @@ def bench_streamed(eng, rows=400_000_000, chunk=25_000_000):
             "scan_gbs_streamed": round(alg / best["seconds"] / 1e9, 2),
             "resident_kernel_ms": round(kms, 3), "scan_gbs_resident": round(alg / (kms / 1e3) / 1e9, 1),
             "rows_equal": bool(nres == n)}
+
+
+# ---- the reference's own entry points, in child processes -----------------
+
+_DROPIN_CHILD = r"""
+import ctypes, json, sys
+import numpy as np
+sys.path.insert(0, ROOT)
+from virginian_b200 import _lib, datagen
+_lib.lib()                                   # the GPU VM first, RTLD_GLOBAL
+from oracle import oracle as O
+from oracle.digest import host_table
+n, sql, reps = int(sys.argv[1]), sys.argv[2], int(sys.argv[3])
+cols = host_table(n, 41, 0, threads=8)
+db = O.OracleDB(path=O.HOST_LIB, mode=ctypes.RTLD_GLOBAL)
+db.create_table("test", datagen.SCHEMA_A)
+db.insert("test", cols["id"], [cols[c] for c, _ in datagen.SCHEMA_A])
+del cols
+cpu = db.query(sql, mode=0)
+gpu = db.query(sql, mode=2)
+same = (gpu.tablet_rows == cpu.tablet_rows and len(gpu.columns) == len(cpu.columns) and
+        all(a.tobytes() == b.tobytes() for a, b in zip(gpu.columns, cpu.columns)))
+t_cpu = min(db.query(sql, mode=0).seconds for _ in range(reps))
+runs = [db.query(sql, mode=2) for _ in range(reps)]
+best = min(runs, key=lambda r: r.seconds)
+db.close()
+print("JSON " + json.dumps({"rows": n, "result_rows": int(cpu.rows), "result_tablets": len(cpu.tablet_rows),
+                           "same_tablets_and_bytes": bool(same), "virginia_single_s": t_cpu,
+                           "virg_vm_gpu_s": best.seconds, "h2d_s": best.gpu_timing[0],
+                           "kernel_s": best.gpu_timing[1], "d2h_s": best.gpu_timing[2]}))
+"""
+
+_REFGPU_CHILD = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, ROOT)
+from virginian_b200 import datagen
+from oracle import oracle as O
+from oracle.digest import host_table
+n, sql = int(sys.argv[1]), sys.argv[2]
+cols = host_table(n, 31, 0, threads=8)
+db = O.OracleDB(path=O.REFGPU_LIB)
+db.create_table("test", datagen.SCHEMA_A)
+db.insert("test", cols["id"], [cols[c] for c, _ in datagen.SCHEMA_A])
+del cols
+runs = [db.query(sql, mode=2) for _ in range(3)]
+best = min(runs, key=lambda r: r.gpu_timing[1])
+db.close()
+print("JSON " + json.dumps({"rows": n, "result_rows": int(best.rows), "kernel_s": best.gpu_timing[1],
+                           "h2d_s": best.gpu_timing[0], "d2h_s": best.gpu_timing[2]}))
+"""
+
+
+def _child(script, *argv, timeout=900):
+    p = subprocess.run([sys.executable, "-c", "ROOT = %r\n" % ROOT + script] + [str(a) for a in argv],
+                       capture_output=True, text=True, timeout=timeout, cwd=ROOT)
+    lines = [x for x in p.stdout.splitlines() if x.startswith("JSON ")]
+    if p.returncode != 0 or not lines:
+        raise RuntimeError((p.stdout + p.stderr)[-600:])
+    return json.loads(lines[-1][5:])
+
+
+def _headline_sql(n, seed):
+    from oracle.digest import host_table
+    cols = host_table(min(n, 4_000_000), seed, 0, threads=8)
+    c, d = constants(cols, HEADLINE_SEL)
+    return QUERY.format(c=c, d=d)
+
+
+def bench_dropin(eng):
+    """virg_query with the drop-in virg_vm_gpu against virg_query on
+    virginia_single, inside the unmodified reference host library (stock
+    virginian.h: 64 memory tablets of 8 MB, so the larger tables page
+    tablets through the library's own database file), same database and
+    query, result-tablet chains compared tablet by tablet."""
+    out = {}
+    for name, n, sql in (("config1_1M", 1_000_000, None), ("config2_8M", 8_000_000, "h"),
+                         ("config2_50M", 50_000_000, "h")):
+        q = CONFIG1 if sql is None else _headline_sql(n, 41)
+        try:
+            r = _child(_DROPIN_CHILD, n, q, 3)
+            r["speedup"] = round(r["virginia_single_s"] / r["virg_vm_gpu_s"], 2)
+            out[name] = r
+        except Exception as ex:  # report, keep the others
+            out[name] = {"error": f"{type(ex).__name__}: {ex}"}
+    return out
+
+
+def bench_ref_gpu_vm(eng):
+    """The reference's own GPU VM (src/vm/vm_gpu.cu compiled for sm_100a,
+    unordered results) on 8M rows of config 1 and of the headline query:
+    its kernel seconds (vm->timing2, serial transfer mode) next to this
+    VM's kernel time on the same rows resident in HBM."""
+    import virginian_b200 as vb
+    from oracle.digest import host_table
+    from virginian_b200 import datagen, sql as vsql
+    n = 8_000_000
+    types = [t for _, t in datagen.SCHEMA_A]
+    cols = host_table(n, 31, 0, threads=8)
+    t = vb.Table(eng, types)
+    t.append(datagen.segments(cols, datagen.SCHEMA_A))
+    cat = vsql.Catalog()
+    cat.add_table("test", datagen.SCHEMA_A)
+    c, d = constants(cols, HEADLINE_SEL)
+    del cols
+    out = {}
+    for name, q in (("config1", CONFIG1), ("config2_10pct", QUERY.format(c=c, d=d))):
+        comp = cat.compile(q)
+        p = vb.Program(comp.op_list(), comp.pc, types)
+        for _ in range(3):
+            r = t.query(p)
+            rows = r.rows
+            r.close()
+        eng.timing(10)
+        for _ in range(10):
+            r = t.query(p)
+            r.close()
+        ours_ms = statistics.median(eng.kernel_times(10))
+        try:
+            ref = _child(_REFGPU_CHILD, n, q)
+            out[name] = {"rows": n, "result_rows": rows, "ref_kernel_ms": round(ref["kernel_s"] * 1e3, 3),
+                         "ref_result_rows": ref["result_rows"], "kernel_ms": round(ours_ms, 4),
+                         "speedup": round(ref["kernel_s"] * 1e3 / ours_ms, 1)}
+        except Exception as ex:
+            out[name] = {"error": f"{type(ex).__name__}: {ex}", "kernel_ms": round(ours_ms, 4)}
+    t.close()
+    return out
 
 
 def run_reference(args):
@@ -824,16 +978,21 @@ def run_b200(args):
     del keep
     table.close()
     # the other workloads: one GPU, rank 0 (the sharded path covers the scan)
-    if rank == 0 and world == 1:
-        sections = [x for x in args.sections.split(",") if x]
-        for name, fn in (("batched", bench_batched), ("serving", bench_serving),
-                         ("streamed", bench_streamed)):
-            if name in sections:
-                log(name)
-                try:
-                    line[name] = fn(eng)
-                except Exception as ex:  # report, keep the headline line
-                    line[name] = {"error": f"{type(ex).__name__}: {ex}"}
+    # the other workloads: batched on every rank (whole tables per rank);
+    # the others on one GPU, rank 0 (the sharded path covers the scan)
+    sections = [x for x in args.sections.split(",") if x]
+    for name, fn, multi in (("batched", bench_batched, True), ("serving", bench_serving, False),
+                            ("streamed", bench_streamed, False), ("dropin", bench_dropin, False),
+                            ("ref_gpu_vm", bench_ref_gpu_vm, False)):
+        if name not in sections or (world > 1 and not multi):
+            continue
+        log(name)
+        try:
+            res = fn(eng, world=world, rank=rank) if multi else fn(eng)
+        except Exception as ex:  # report, keep the headline line
+            res = {"error": f"{type(ex).__name__}: {ex}"}
+        if rank == 0:
+            line[name] = res
     if rank == 0 and args.parity:
         # the headline's own result against the reference CPU VM
         # (virginia_single) on the same table, in a spawned worker
@@ -868,7 +1027,7 @@ def main():
                     "shape of the scan instead of tuning it (for profiling one launch)")
     ap.add_argument("--no-parity", dest="parity", action="store_false",
                     help="skip the headline's byte comparison with the reference CPU VM")
-    ap.add_argument("--sections", default="batched,serving,streamed",
+    ap.add_argument("--sections", default="batched,serving,streamed,dropin,ref_gpu_vm",
                     help="workloads besides the headline scan (comma list; empty for none)")
     args = ap.parse_args()
     args.shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else ()

@@ -10,6 +10,10 @@ if ROOT not in sys.path:
 
 REF_SRC = os.path.join(os.environ.get("VIRGINIAN_REF", "/root/reference"), "src")
 
+# tests tune in a clean state: no persistent tuned-shape cache unless a test
+# names its own file
+os.environ["VIRGINIAN_B200_TUNE_CACHE"] = ""
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 GPU (sm_100a)")

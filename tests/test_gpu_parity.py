@@ -83,6 +83,29 @@ def test_query_host_end_to_end(data_a, engine):
     assert_same_stream(got, db.query(CONFIG1).columns, "query_host")
 
 
+def test_query_host_pieces_and_chunks(oracle_mod, engine):
+    """End to end over 3.2M rows whose segments are partly back to back in
+    host memory (merged into one copy per column) and partly separate
+    arrays, one of them longer than a staging chunk (split across chunks),
+    with a short segment and an empty one between them; called twice, so
+    the second call reuses the engine's staging ring."""
+    n = 3_200_000
+    db, cols = build_oracle_db(oracle_mod, n, seed=12)
+    try:
+        segs = datagen.segments({k: v[:900_000] for k, v in cols.items()}, datagen.SCHEMA_A, 300_000)
+        rest = {k: np.copy(v[900_000:]) for k, v in cols.items()}
+        segs += datagen.segments({k: v[:7] for k, v in rest.items()}, datagen.SCHEMA_A, 7)
+        segs.append({"rows": 0, "key": rest["id"][:0], "cols": [rest[c][:0] for c, _ in datagen.SCHEMA_A]})
+        segs += datagen.segments({k: np.copy(v[7:]) for k, v in rest.items()}, datagen.SCHEMA_A, n)
+        for sql in (CONFIG1, config2(30.0, 20.0)):
+            p = program(db, sql, TYPES_A)
+            want = db.query(sql).columns
+            for _ in range(2):
+                assert_same_stream(engine.query_host(p, segs), want, f"query_host pieces {sql}")
+    finally:
+        db.close()
+
+
 # (compute threads, stage KB, buffers (0: as many as fit), CTAs per SM, chunk rows, full-phase mode)
 @pytest.mark.parametrize("shape", [(320, 16, 0, 1, 1024, 0), (448, 32, 3, 1, 2048, 0), (256, 16, 0, 1, 8192, 0),
                                    (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 0), (512, 24, 0, 1, 2048, 0),

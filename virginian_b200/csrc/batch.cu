@@ -213,7 +213,7 @@ int autotune(virg_gpu_batch *b)
 		}
 	}
 	VGPU_CHECK(best_shape.threads != 0, "no launch shape fits this batch");
-	e->tuned[key] = best_shape;
+	tune_remember(e, key, best_shape);
 	return build_with(b, &best_shape);
 }
 

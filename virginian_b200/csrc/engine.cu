@@ -148,7 +148,7 @@ void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode)
 	for (uint32_t i = 0; i < P.nvec; i++) {
 		if (P.vec_compact[i]) {
 			pp.vec_off[i] = sel;
-			sel += 32u * kBatchE * P.vec_stride[i];
+			sel += kUnitE * P.vec_stride[i];
 		} else {
 			pp.vec_off[i] = row;
 			row += kCountGroup * kBlockRows * P.vec_stride[i];
@@ -245,7 +245,7 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 		/* one full entry per chunk; the staged columns of a batch are its
 		 * 32 kBatchE gathered entries, in the warp's gather area */
 		const uint32_t gchunk = chunk_cap;
-		load_set(d.full_set, P, pp.full_cols, pp.nfull, 32u * kBatchE);
+		load_set(d.full_set, P, pp.full_cols, pp.nfull, kUnitE);
 		d.full_set.rows = gchunk;
 		d.chunk_rows = gchunk;
 		load_set(d.count_set, P, pp.count_cols, pp.ncount, tile_rows(pp.count_bpr, stage, gchunk));
@@ -613,6 +613,7 @@ extern "C" int virg_gpu_engine_create(int device, virg_gpu_engine **out)
 	e->nsm = prop.multiProcessorCount;
 	e->smem_optin = (int)prop.sharedMemPerBlockOptin;
 	e->smem_sm = (int)prop.sharedMemPerMultiprocessor;
+	e->device_name = prop.name;
 	if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
 		cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
 		cudaMalloc((void **)&e->ctrl, 64) != cudaSuccess || cudaMemset(e->ctrl, 0, 64) != cudaSuccess) {
@@ -625,6 +626,7 @@ extern "C" int virg_gpu_engine_create(int device, virg_gpu_engine **out)
 		uint64_t thr = UINT64_MAX;
 		cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
 	}
+	tune_cache_load(e);
 	*out = e;
 	return 1;
 }
@@ -684,6 +686,7 @@ extern "C" void virg_gpu_engine_destroy(virg_gpu_engine *e)
 	cudaSetDevice(e->device);
 	cudaStreamSynchronize(e->stream);
 	ring_free(e);
+	host_ring_free(e);
 	if (e->status)
 		cudaFree(e->status);
 	if (e->blob)
@@ -757,7 +760,7 @@ extern "C" int virg_gpu_query_tune(virg_gpu_engine *e, const virg_gpu_program *p
 	q.prog = &p->prog;
 	q.nsegs = (uint32_t)t->seg_rows.size();
 	q.seg_rows = t->seg_rows.data();
-	e->tuned[shape_key(std::vector<QueryLaunch>(1, q))] = best_shape;
+	tune_remember(e, shape_key(std::vector<QueryLaunch>(1, q)), best_shape);
 	if (shape4) {
 		shape4[0] = best_shape.threads;
 		shape4[1] = best_shape.stage_kb;
@@ -1097,83 +1100,3 @@ extern "C" void virg_gpu_result_destroy(virg_gpu_result *r)
 	delete r;
 }
 
-/* ---- end to end from host buffers -------------------------------------- */
-
-extern "C" int virg_gpu_query_host(virg_gpu_engine *e, const virg_gpu_program *p,
-	const virg_gpu_segment *segs, unsigned nsegs, void *const *out_cols, uint64_t capacity,
-	uint64_t *out_rows)
-{
-	VGPU_CHECK(e != nullptr && p != nullptr && (segs != nullptr || nsegs == 0) && out_rows != nullptr,
-		"null argument");
-	CUDA_OK(cudaSetDevice(e->device), "set device");
-	const Program &P = p->prog;
-	/* stage only the columns the program reads */
-	virg_gpu_table tmp;
-	tmp.e = e;
-	tmp.schema = p->schema;
-	tmp.transient = true;
-	bool want[kMaxCols] = {false};
-	bool want_key = false;
-	for (unsigned i = 0; i < P.nload; i++) {
-		if (P.load_src[i] == kKeySlot)
-			want_key = true;
-		else
-			want[P.load_src[i]] = true;
-	}
-	for (unsigned s = 0; s < nsegs; s++)
-		if (want_key)
-			VGPU_CHECK(segs[s].key != nullptr || segs[s].rows == 0, "segment %u has no key column", s);
-	std::lock_guard<std::mutex> lk(e->mu);
-	int ok = table_add_segments(&tmp, segs, nsegs, want, want_key, e->stream) && table_sync_desc(&tmp);
-	virg_gpu_result *r = nullptr;
-	if (ok)
-		ok = result_alloc(e, P, tmp.rows, false, 0, &r);
-	if (ok) {
-		QueryLaunch q;
-		q.prog = &P;
-		q.d_segs = tmp.d_segs;
-		q.nsegs = (uint32_t)tmp.segs.size();
-		q.seg_rows = tmp.seg_rows.data();
-		for (unsigned j = 0; j < P.nout; j++)
-			q.out[j] = r->out[j];
-		q.capacity = tmp.rows;
-		q.d_total = r->d_total;
-		q.block_counts = nullptr;
-		std::vector<QueryLaunch> qs(1, q);
-		ok = run_queries(e, qs, nullptr);
-		r->ntiles_zero = (tmp.rows == 0);
-	}
-	uint64_t rows = 0;
-	if (ok)
-		ok = virg_gpu_result_rows(r, &rows);
-	if (ok) {
-		*out_rows = rows;
-		uint64_t n = std::min(rows, capacity);
-		for (unsigned j = 0; j < P.nout && n; j++) {
-			cudaError_t ce = cudaMemcpyAsync(out_cols[j], r->out[j], n * r->stride[j],
-				cudaMemcpyDeviceToHost, e->stream);
-			if (ce != cudaSuccess) {
-				set_error("result copy: %s", cudaGetErrorString(ce));
-				ok = 0;
-			}
-		}
-		if (ok && cudaStreamSynchronize(e->stream) != cudaSuccess) {
-			set_error("result copy sync failed");
-			ok = 0;
-		}
-		if (ok && rows > capacity) {
-			set_error("result has %llu rows, the buffers hold %llu", (unsigned long long)rows,
-				(unsigned long long)capacity);
-			ok = 0;
-		}
-	}
-	if (r)
-		virg_gpu_result_destroy(r);
-	for (void *m : tmp.allocs)
-		cudaFreeAsync(m, e->stream);
-	tmp.allocs.clear();
-	if (tmp.d_segs)
-		cudaFreeAsync(tmp.d_segs, e->stream);
-	tmp.d_segs = nullptr;
-	return ok;
-}

@@ -19,6 +19,19 @@ struct ScratchBuf {
 	size_t cap = 0;
 };
 
+/* the engine's staging ring for rows read from host memory: device buffers
+ * and events kept across calls, grown when a call needs more */
+struct HostRing {
+	static constexpr unsigned kBufs = 3;
+	unsigned char *mem[kBufs] = {};
+	size_t bytes = 0;                    /* each buffer */
+	SegDesc *d_segs[kBufs] = {};
+	size_t seg_cap = 0;                  /* descriptors each buffer holds */
+	cudaEvent_t copied[kBufs] = {}, freed[kBufs] = {}, c0[kBufs] = {}, c1[kBufs] = {};
+	unsigned long long *d_totals = nullptr;  /* running result counts, two alternating words */
+	bool ready = false;
+};
+
 }  // namespace vgpu
 
 struct virg_gpu_engine {
@@ -36,6 +49,7 @@ struct virg_gpu_engine {
 	size_t blob_cap = 0;
 	std::vector<unsigned char> host_blob;
 	std::map<int, vgpu::ScratchBuf> scratch;
+	vgpu::HostRing hring;
 	vgpu::Shape pref = {0, 0, 0, 0, 0, 0};
 	vgpu::Shape last_shape = {0, 0, 0, 0, 0, 0};
 	unsigned last_grid = 0;
@@ -49,6 +63,7 @@ struct virg_gpu_engine {
 	unsigned long long ring_count = 0;
 	/* launch shapes found by autotuning, per program-shape key */
 	std::map<std::string, vgpu::Shape> tuned;
+	std::string device_name;             /* keys the persistent tuned-shape cache */
 	vgpu::Shape force = {0, 0, 0, 0, 0, 0};  /* shape under trial while tuning */
 	std::mutex mu;
 };
@@ -149,6 +164,17 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 KParams plan_params(const Plan &plan, const unsigned char *db, unsigned *counter, uint64_t *status,
 	unsigned *error, uint32_t epoch);
 int run_queries(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, LaunchTiming *timing);
+/* one program over rows in host memory, through the engine's staging ring:
+ * contiguous host rows are merged into pieces, pieces into chunks of at most
+ * chunk_rows rows; each chunk is copied on the copy stream and scanned by
+ * one launch that appends to result r.  The caller holds the engine's lock. */
+int host_pipeline(virg_gpu_engine *e, const Program &P, const virg_gpu_segment *segs, unsigned nsegs,
+	uint64_t chunk_rows, virg_gpu_result *r, virg_gpu_stream_stats *stats);
+void host_ring_free(virg_gpu_engine *e);
+/* the persistent tuned-shape cache: loaded when an engine is created, and
+ * a newly tuned shape recorded in the engine and appended to it */
+void tune_cache_load(virg_gpu_engine *e);
+void tune_remember(virg_gpu_engine *e, const std::string &key, const Shape &s);
 std::string shape_key(const std::vector<QueryLaunch> &qs);
 int read_device_error(virg_gpu_engine *e, unsigned *err);
 const char *device_error_text(unsigned code);

@@ -69,10 +69,18 @@ static_assert(kChunkSlots >= kCountAhead + 2, "slots for the chunks in flight");
 #ifndef VGPU_BATCH_E
 #define VGPU_BATCH_E 4
 #endif
+#ifndef VGPU_UNIT_BATCHES
+#define VGPU_UNIT_BATCHES 1
+#endif
 constexpr unsigned kCountGroup = VGPU_COUNT_GROUP;
 constexpr unsigned kFullGroup = VGPU_FULL_GROUP;
 constexpr unsigned kBatchE = VGPU_BATCH_E;
+/* a full-phase unit: kUnitBatches batches of 32 kBatchE selected rows, each
+ * op run over all of them before the next op */
+constexpr unsigned kUnitBatches = VGPU_UNIT_BATCHES;
+constexpr unsigned kUnitE = 32 * kBatchE * kUnitBatches;
 static_assert(32 * kBatchE <= kCountGroup * kBlockRows, "a batch within a group");
+static_assert(kUnitE <= 2 * kFullGroup * kBlockRows / 2, "a unit's list within the list area");
 
 /* per-stage tile, written by the producer before the stage's data lands */
 struct StageInfo {
@@ -139,8 +147,8 @@ inline WarpLayout warp_layout(unsigned sel_bytes_per_row, unsigned row_bytes_per
 {
 	WarpLayout w;
 	w.sel_off = 2u * kFullGroup * kBlockRows;
-	w.gat_off = w.sel_off + (32u * kBatchE * sel_bytes_per_row + 127u) / 128u * 128u;
-	w.row_off = w.gat_off + (32u * kBatchE * gather_bytes_per_row + 127u) / 128u * 128u;
+	w.gat_off = w.sel_off + (kUnitE * sel_bytes_per_row + 127u) / 128u * 128u;
+	w.row_off = w.gat_off + (kUnitE * gather_bytes_per_row + 127u) / 128u * 128u;
 	w.bytes = w.row_off + (kCountGroup * kBlockRows * row_bytes_per_row + 127u) / 128u * 128u;
 	return w;
 }

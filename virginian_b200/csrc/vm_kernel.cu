@@ -684,6 +684,11 @@ __device__ __noinline__ void vec_rare(uint4 rec, Bases b, int lane, uint32_t mas
 	} else vec_any<signed char, U, true>(rec, b, lane, mask);
 }
 
+#ifndef VGPU_HOT_CHUNKED
+#define VGPU_HOT_CHUNKED 0
+#endif
+constexpr bool kHotChunked = VGPU_HOT_CHUNKED != 0;
+
 /* one filter op: kind, then type, then operator, each by bit tests */
 template <int U>
 __device__ __forceinline__ void filter_op(const uint4 &rec, const Bases &b, int lane, RowState &st)
@@ -700,8 +705,8 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const Bases &b, int 
 	}
 	if (h & (OK_CMP | OK_NOT)) {
 		uint32_t bits;
-		if (h_type(h, VT_FLOAT)) bits = bits_any<float, U, false>(rec, b, lane);
-		else if (h_type(h, VT_INT)) bits = bits_any<int32_t, U, false>(rec, b, lane);
+		if (h_type(h, VT_FLOAT)) bits = bits_any<float, U, kHotChunked>(rec, b, lane);
+		else if (h_type(h, VT_INT)) bits = bits_any<int32_t, U, kHotChunked>(rec, b, lane);
 		else bits = bits_rare<U>(rec, b, lane);
 		take_jump(st, h, st.active & bits);
 	} else if (h & OK_INVALID) {
@@ -712,18 +717,23 @@ __device__ __forceinline__ void filter_op(const uint4 &rec, const Bases &b, int 
 		 * row (the CPU copies the whole block, src/vm/virginia.c:448) */
 		const uint32_t mask = (h & OK_COPY) || (h & OPH_SINGLE_DEF) ? 0xffffffffu : st.active;
 		if (h & OK_COPY) {
-			if (h_type(h, VT_INT) || h_type(h, VT_FLOAT)) vec_rows<uint32_t, -1, U>(rec, b, lane, mask);
-			else vec_rare<U>(rec, b, lane, mask);
+			if (h_type(h, VT_INT) || h_type(h, VT_FLOAT)) {
+				if (kHotChunked) vec_chunked<uint32_t, -1, U>(rec, b, lane, mask);
+				else vec_rows<uint32_t, -1, U>(rec, b, lane, mask);
+			} else {
+				vec_rare<U>(rec, b, lane, mask);
+			}
 		} else if (h_type(h, VT_FLOAT)) {
-			vec_any<float, U, false>(rec, b, lane, mask);
+			vec_any<float, U, kHotChunked>(rec, b, lane, mask);
 		} else if (h_type(h, VT_INT)) {
-			vec_any<int32_t, U, false>(rec, b, lane, mask);
+			vec_any<int32_t, U, kHotChunked>(rec, b, lane, mask);
 		} else {
 			vec_rare<U>(rec, b, lane, mask);
 		}
 	} else if (h & OK_SETCONST) {
 		/* Integer/Float into a register vector: active rows only */
-		vec_rows<uint32_t, -1, U>(rec, b, lane, st.active);
+		if (kHotChunked) vec_chunked<uint32_t, -1, U>(rec, b, lane, st.active);
+		else vec_rows<uint32_t, -1, U>(rec, b, lane, st.active);
 	}
 }
 
@@ -754,115 +764,183 @@ __device__ __noinline__ uint32_t run_filter(uint32_t ops, uint32_t nf, Bases b, 
 	return st.valid;
 }
 
-/* ---- projection: kBatchE selection entries per lane ----------------------
- * A batch is 32 kBatchE entries of a group's selection list; entry i of a
- * lane is batch entry 32 i + lane, at group row row[i].  Register vectors
- * indexed by selection entry use the batch entry. */
+/* ---- projection: the batches of a unit, op by op -------------------------
+ * A unit is kUnitBatches batches of 32 kBatchE selected rows; entry i of
+ * batch s of a lane is unit entry 32 kBatchE s + 32 i + lane, at row
+ * row[s][i] of the staged tile (or the warp's gather area).  Each op runs
+ * over every batch of the unit before the next op, so an op's record is
+ * read and dispatched once per unit.  Register vectors indexed by selection
+ * entry use the unit entry. */
+
+struct UnitRows {
+	uint32_t row[kUnitBatches][kBatchE];
+	uint32_t act[kUnitBatches];  /* entries that exist */
+};
 
 template <typename T, int OP>
-__device__ __forceinline__ void p_math(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
-	uint32_t act, int lane)
+__device__ __forceinline__ void p_math(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
 	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b), od = opnd<sizeof(T)>(rec.w, b);
-	T x[kBatchE], y[kBatchE];
+	T x[kUnitBatches][kBatchE], y[kUnitBatches][kBatchE];
 #pragma unroll
-	for (int i = 0; i < kBatchE; i++) {
-		x[i] = SM<T>::ld(oa.addr + (oa.sel ? (uint32_t)(32 * i + lane) : row[i]) * oa.step);
-		y[i] = SM<T>::ld(ob.addr + (ob.sel ? (uint32_t)(32 * i + lane) : row[i]) * ob.step);
-	}
+	for (int s = 0; s < (int)kUnitBatches; s++)
 #pragma unroll
-	for (int i = 0; i < kBatchE; i++)
-		if ((act >> i) & 1u)
-			SM<T>::st(od.addr + (od.sel ? (uint32_t)(32 * i + lane) : row[i]) * od.step, Math<T, OP>::eval(x[i], y[i]));
+		for (int i = 0; i < kBatchE; i++) {
+			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			x[s][i] = SM<T>::ld(oa.addr + (oa.sel ? e : u.row[s][i]) * oa.step);
+			y[s][i] = SM<T>::ld(ob.addr + (ob.sel ? e : u.row[s][i]) * ob.step);
+		}
+#pragma unroll
+	for (int s = 0; s < (int)kUnitBatches; s++)
+#pragma unroll
+		for (int i = 0; i < kBatchE; i++)
+			if ((u.act[s] >> i) & 1u) {
+				const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+				SM<T>::st(od.addr + (od.sel ? e : u.row[s][i]) * od.step, Math<T, OP>::eval(x[s][i], y[s][i]));
+			}
 }
 
 template <typename T>
-__device__ __forceinline__ void p_copy(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
-	uint32_t act, int lane)
+__device__ __forceinline__ void p_copy(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
 	const Opnd oa = opnd<sizeof(T)>(rec.y, b), od = opnd<sizeof(T)>(rec.w, b);
-	T x[kBatchE];
+	T x[kUnitBatches][kBatchE];
 #pragma unroll
-	for (int i = 0; i < kBatchE; i++)
-		x[i] = SM<T>::ld(oa.addr + (oa.sel ? (uint32_t)(32 * i + lane) : row[i]) * oa.step);
+	for (int s = 0; s < (int)kUnitBatches; s++)
 #pragma unroll
-	for (int i = 0; i < kBatchE; i++)
-		if ((act >> i) & 1u)
-			SM<T>::st(od.addr + (od.sel ? (uint32_t)(32 * i + lane) : row[i]) * od.step, x[i]);
+		for (int i = 0; i < kBatchE; i++) {
+			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			x[s][i] = SM<T>::ld(oa.addr + (oa.sel ? e : u.row[s][i]) * oa.step);
+		}
+#pragma unroll
+	for (int s = 0; s < (int)kUnitBatches; s++)
+#pragma unroll
+		for (int i = 0; i < kBatchE; i++)
+			if ((u.act[s] >> i) & 1u) {
+				const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+				SM<T>::st(od.addr + (od.sel ? e : u.row[s][i]) * od.step, x[s][i]);
+			}
 }
 
 template <typename T>
-__device__ __forceinline__ void p_math_any(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
-	uint32_t act, int lane)
+__device__ __forceinline__ void p_math_any(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
 	const uint32_t h = rec.x;
-	if (h_op(h, MO_ADD)) p_math<T, MO_ADD>(rec, b, row, act, lane);
-	else if (h_op(h, MO_SUB)) p_math<T, MO_SUB>(rec, b, row, act, lane);
-	else if (h_op(h, MO_MUL)) p_math<T, MO_MUL>(rec, b, row, act, lane);
-	else p_math<T, MO_DIV>(rec, b, row, act, lane);
+	if (h_op(h, MO_ADD)) p_math<T, MO_ADD>(rec, b, u, lane);
+	else if (h_op(h, MO_SUB)) p_math<T, MO_SUB>(rec, b, u, lane);
+	else if (h_op(h, MO_MUL)) p_math<T, MO_MUL>(rec, b, u, lane);
+	else p_math<T, MO_DIV>(rec, b, u, lane);
 }
 
-/* projection ops over 8-byte and char values, out of line, arguments by
- * value (rows: the batch's four group rows of this lane) */
-__device__ __noinline__ void project_rare(uint4 rec, Bases b, uint4 rows, uint32_t act, int lane)
+/* one batch of a projection op over 8-byte and char values, out of line,
+ * arguments by value (rows: the batch's four rows of this lane; e0: the
+ * batch's first unit entry) */
+template <typename T, int OP>
+__device__ __forceinline__ void p_math1(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE], uint32_t act,
+	uint32_t e0, int lane)
+{
+	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b), od = opnd<sizeof(T)>(rec.w, b);
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++) {
+		const uint32_t e = e0 + 32u * i + (uint32_t)lane;
+		const T x = SM<T>::ld(oa.addr + (oa.sel ? e : row[i]) * oa.step);
+		if constexpr (OP < 0) {
+			if ((act >> i) & 1u)
+				SM<T>::st(od.addr + (od.sel ? e : row[i]) * od.step, x);
+		} else {
+			const T y = SM<T>::ld(ob.addr + (ob.sel ? e : row[i]) * ob.step);
+			if ((act >> i) & 1u)
+				SM<T>::st(od.addr + (od.sel ? e : row[i]) * od.step, Math<T, OP>::eval(x, y));
+		}
+	}
+}
+
+template <typename T>
+__device__ __forceinline__ void p_math1_any(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
+	uint32_t act, uint32_t e0, int lane)
+{
+	const uint32_t h = rec.x;
+	if (h_op(h, MO_ADD)) p_math1<T, MO_ADD>(rec, b, row, act, e0, lane);
+	else if (h_op(h, MO_SUB)) p_math1<T, MO_SUB>(rec, b, row, act, e0, lane);
+	else if (h_op(h, MO_MUL)) p_math1<T, MO_MUL>(rec, b, row, act, e0, lane);
+	else p_math1<T, MO_DIV>(rec, b, row, act, e0, lane);
+}
+
+__device__ __noinline__ void project_rare(uint4 rec, Bases b, uint4 rows, uint32_t act, uint32_t e0, int lane)
 {
 	const uint32_t row[kBatchE] = {rows.x, rows.y, rows.z, rows.w};
 	const uint32_t h = rec.x;
 	if (h & OK_MATH) {
-		if (h_type(h, VT_DOUBLE)) p_math_any<double>(rec, b, row, act, lane);
-		else if (h_type(h, VT_INT64)) p_math_any<long long>(rec, b, row, act, lane);
-		else p_math_any<signed char>(rec, b, row, act, lane);
+		if (h_type(h, VT_DOUBLE)) p_math1_any<double>(rec, b, row, act, e0, lane);
+		else if (h_type(h, VT_INT64)) p_math1_any<long long>(rec, b, row, act, e0, lane);
+		else p_math1_any<signed char>(rec, b, row, act, e0, lane);
 	} else if (h & OK_COPY) {
-		if (h_type(h, VT_CHAR)) p_copy<unsigned char>(rec, b, row, act, lane);
-		else p_copy<unsigned long long>(rec, b, row, act, lane);
+		if (h_type(h, VT_CHAR)) p_math1<unsigned char, -1>(rec, b, row, act, e0, lane);
+		else p_math1<unsigned long long, -1>(rec, b, row, act, e0, lane);
 	}
 }
 
-/* one projection op: arithmetic, or a copy (every listed row is active
- * here, so constants and columns are copies) */
-__device__ __forceinline__ void project_op(const uint4 &rec, const Bases &b, const uint32_t (&row)[kBatchE],
-	uint32_t act, int lane)
+/* one projection op over the unit: arithmetic, or a copy (every listed row
+ * is active here, so constants and columns are copies) */
+__device__ __forceinline__ void project_op(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
-	static_assert(kBatchE == 4, "project_rare passes the batch rows as a uint4");
+	static_assert(kBatchE == 4, "project_rare passes a batch's rows as a uint4");
 	const uint32_t h = rec.x;
 	if (h & OK_SETCONST) {
-		p_copy<uint32_t>(rec, b, row, act, lane);
+		p_copy<uint32_t>(rec, b, u, lane);
 	} else if (!(h_type(h, VT_FLOAT) || h_type(h, VT_INT))) {
-		project_rare(rec, b, make_uint4(row[0], row[1], row[2], row[3]), act, lane);
+#pragma unroll
+		for (int s = 0; s < (int)kUnitBatches; s++)
+			project_rare(rec, b, make_uint4(u.row[s][0], u.row[s][1], u.row[s][2], u.row[s][3]), u.act[s],
+				32u * kBatchE * s, lane);
 	} else if (h & OK_MATH) {
-		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, b, row, act, lane);
-		else p_math_any<int32_t>(rec, b, row, act, lane);
+		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, b, u, lane);
+		else p_math_any<int32_t>(rec, b, u, lane);
 	} else if (h & OK_COPY) {
-		p_copy<uint32_t>(rec, b, row, act, lane);
+		p_copy<uint32_t>(rec, b, u, lane);
 	}
 }
 
-/* one result column of a batch: entries whose bit is set in `in` are stored
- * at pos0 + their batch entry */
+/* one result column of the unit: entries whose bit is set in in[s] are
+ * stored at pos0 + their unit entry */
 template <typename T>
-__device__ __forceinline__ void p_store(uint32_t od, const Bases &b, const uint32_t (&row)[kBatchE], uint32_t in,
+__device__ __forceinline__ void p_store(uint32_t od, const Bases &b, const UnitRows &u, const uint32_t (&in)[kUnitBatches],
 	T *out, uint64_t pos0, int lane)
 {
 	const Opnd o = opnd<sizeof(T)>(od, b);
-	T v[kBatchE];
+	T v[kUnitBatches][kBatchE];
 #pragma unroll
-	for (int i = 0; i < kBatchE; i++)
-		v[i] = SM<T>::ld(o.addr + (o.sel ? (uint32_t)(32 * i + lane) : row[i]) * o.step);
+	for (int s = 0; s < (int)kUnitBatches; s++)
 #pragma unroll
-	for (int i = 0; i < kBatchE; i++)
-		if ((in >> i) & 1u)
-			out[pos0 + (uint64_t)(32 * i + lane)] = v[i];
+		for (int i = 0; i < kBatchE; i++) {
+			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			v[s][i] = SM<T>::ld(o.addr + (o.sel ? e : u.row[s][i]) * o.step);
+		}
+#pragma unroll
+	for (int s = 0; s < (int)kUnitBatches; s++)
+#pragma unroll
+		for (int i = 0; i < kBatchE; i++)
+			if ((in[s] >> i) & 1u)
+				out[pos0 + (uint64_t)(32u * kBatchE * s + 32u * i + (uint32_t)lane)] = v[s][i];
 }
 
-/* a result column of 8-byte or char values, out of line, by value */
+/* one batch of a result column of 8-byte or char values, out of line, by value */
 __device__ __noinline__ void p_store_rare(uint32_t od, Bases b, uint4 rows, uint32_t in, void *out, uint64_t pos0,
-	uint32_t stride, int lane)
+	uint32_t e0, uint32_t stride, int lane)
 {
 	const uint32_t row[kBatchE] = {rows.x, rows.y, rows.z, rows.w};
-	if (stride == 8)
-		p_store<unsigned long long>(od, b, row, in, static_cast<unsigned long long *>(out), pos0, lane);
-	else
-		p_store<unsigned char>(od, b, row, in, static_cast<unsigned char *>(out), pos0, lane);
+	const Opnd o = stride == 8 ? opnd<8>(od, b) : opnd<1>(od, b);
+#pragma unroll
+	for (int i = 0; i < kBatchE; i++) {
+		const uint32_t e = e0 + 32u * i + (uint32_t)lane;
+		const uint32_t a = o.addr + (o.sel ? e : row[i]) * o.step;
+		if ((in >> i) & 1u) {
+			if (stride == 8)
+				static_cast<unsigned long long *>(out)[pos0 + e] = SM<unsigned long long>::ld(a);
+			else
+				static_cast<unsigned char *>(out)[pos0 + e] = SM<unsigned char>::ld(a);
+		}
+	}
 }
 
 /* ---- groups ------------------------------------------------------------- */
@@ -913,10 +991,10 @@ __device__ __forceinline__ uint64_t ldg_val(const unsigned char *p, uint32_t str
 	return v;
 }
 
-/* FM_GATHER: the batch's selected rows of every gathered column, from
- * device memory into the warp's gather area (batch entry 32 i + lane at
+/* FM_GATHER: one batch's selected rows of every gathered column, from
+ * device memory into the warp's gather area (unit entry e0 + 32 i + lane at
  * row grow[i] of the chunk); four columns' loads in flight at a time */
-__device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&grow)[kBatchE], int lane)
+__device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&grow)[kBatchE], uint32_t e0, int lane)
 {
 	const uint32_t n = lds_u32(b.slot + kQGatherN);
 	for (uint32_t c0 = 0; c0 < n; c0 += 4) {
@@ -939,7 +1017,7 @@ __device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&gr
 				const uint32_t dst = b.stage + lds_u32(b.slot + kQGatherOff + 4 * (c0 + cc));
 #pragma unroll
 				for (int i = 0; i < kBatchE; i++) {
-					const uint32_t a = dst + (uint32_t)(32 * i + lane) * st[cc];
+					const uint32_t a = dst + (e0 + (uint32_t)(32 * i + lane)) * st[cc];
 					if (st[cc] == 4)
 						sts_u32(a, (uint32_t)v[cc][i]);
 					else if (st[cc] == 8)
@@ -951,27 +1029,55 @@ __device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&gr
 	}
 }
 
-/* the projection and stores of one batch: entry i of this lane is group
- * row row[i] (or, when the results read a gather area, batch entry
- * 32 i + lane); entries in `act` exist, those in `in` fit the output and
- * are stored at pos0 + their batch entry */
-__device__ __forceinline__ void batch_out(const Bases &b, const uint32_t (&row)[kBatchE], uint32_t act,
-	uint32_t in, uint64_t pos0, int lane)
+/* the projection and stores of a unit (see UnitRows); entries in in[s]
+ * fit the output and are stored at pos0 + their unit entry */
+__device__ __forceinline__ void unit_out(const Bases &b, const UnitRows &u, const uint32_t (&in)[kUnitBatches],
+	uint64_t pos0, int lane)
 {
 	const uint32_t ops = b.slot + kQOpsFull;
 	const uint32_t nf = lds_u32(b.slot + kQNFilter);
 	const uint32_t nu = lds_u32(b.slot + kQNUops) - 1u;
 	const uint32_t nout = lds_u32(b.slot + kQNOut);
 	for (uint32_t k = nf; k < nu; k++)
-		project_op(lds_v4(ops + 16u * k), b, row, act, lane);
+		project_op(lds_v4(ops + 16u * k), b, u, lane);
 	for (uint32_t j = 0; j < nout; j++) {
 		const uint32_t od = lds_u32(b.slot + kQOdOut + 4 * j);
 		void *out = reinterpret_cast<void *>(lds_u64(b.slot + kQOutPtr + 8 * j));
 		const uint32_t stride = lds_u8(b.slot + kQOutStride + j);
-		if (stride == 4)
-			p_store<uint32_t>(od, b, row, in, static_cast<uint32_t *>(out), pos0, lane);
-		else
-			p_store_rare(od, b, make_uint4(row[0], row[1], row[2], row[3]), in, out, pos0, stride, lane);
+		if (stride == 4) {
+			p_store<uint32_t>(od, b, u, in, static_cast<uint32_t *>(out), pos0, lane);
+		} else {
+#pragma unroll
+			for (int s2 = 0; s2 < (int)kUnitBatches; s2++)
+				p_store_rare(od, b, make_uint4(u.row[s2][0], u.row[s2][1], u.row[s2][2], u.row[s2][3]), in[s2], out,
+					pos0, 32u * kBatchE * s2, stride, lane);
+		}
+	}
+}
+
+/* a unit's rows from its selection list (list entry e: the row of unit
+ * entry e), the first cnt existing; in[s]: those below the output capacity */
+__device__ __forceinline__ void unit_rows(uint32_t list, uint32_t cnt, uint64_t pos0, uint64_t cap, UnitRows &u,
+	uint32_t (&in)[kUnitBatches], int lane)
+{
+#pragma unroll
+	for (int s = 0; s < (int)kUnitBatches; s++) {
+		u.act[s] = 0;
+		in[s] = 0;
+#pragma unroll
+		for (int i = 0; i < kBatchE; i++) {
+			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			const bool a = e < cnt;
+			u.row[s][i] = 0;
+			if (a) {
+				uint16_t r;
+				asm volatile("ld.shared.u16 %0, [%1];" : "=h"(r) : "r"(list + 2 * e));
+				u.row[s][i] = r;
+			}
+			u.act[s] |= (a ? 1u : 0u) << i;
+			if (a && pos0 + e < cap)
+				in[s] |= 1u << i;
+		}
 	}
 }
 
@@ -1013,25 +1119,14 @@ __device__ __forceinline__ bool refilter_group(const Bases &b, uint32_t list, ui
 	const uint64_t off = lds_u64(b.slot + kSlotBlockOff + 8u * blk);
 	const uint64_t cap = lds_u64(b.slot + kQCapacity);
 	bool ok = true;
-	for (uint32_t base = 0; base < n; base += 32 * kBatchE) {
-		uint32_t row[kBatchE];
-		uint32_t act = 0, in = 0;
+	for (uint32_t base = 0; base < n; base += kUnitE) {
+		UnitRows u;
+		uint32_t in[kUnitBatches];
+		unit_rows(list + 2 * base, n - base, off + base, cap, u, in, lane);
 #pragma unroll
-		for (int i = 0; i < kBatchE; i++) {
-			const uint32_t e = base + 32 * i + (uint32_t)lane;
-			const bool a = e < n;
-			row[i] = 0;
-			if (a) {
-				uint16_t r;
-				asm volatile("ld.shared.u16 %0, [%1];" : "=h"(r) : "r"(list + 2 * e));
-				row[i] = r;
-			}
-			act |= (a ? 1u : 0u) << i;
-			if (a && off + e < cap)
-				in |= 1u << i;
-		}
-		ok = ok && act == in;
-		batch_out(b, row, act, in, off + base, lane);
+		for (int s2 = 0; s2 < (int)kUnitBatches; s2++)
+			ok = ok && u.act[s2] == in[s2];
+		unit_out(b, u, in, off + base, lane);
 	}
 	__syncwarp();
 	return ok;
@@ -1047,20 +1142,20 @@ __device__ __forceinline__ uint32_t entry_selected(uint32_t slot, uint32_t blk0,
 	return (uint32_t)(lds_u64(slot + kSlotBlockOff + 8u * last) + lds_u32(slot + kSlotBlockCnt + 4u * last) - first);
 }
 
-/* FM_BITMAP / FM_GATHER full phase: batch j of an entry's selected rows
- * (ranks [32 kBatchE j, ...) of the nsel rows of chunk blocks
+/* FM_BITMAP / FM_GATHER full phase: unit j of an entry's selected rows
+ * (ranks [kUnitE j, ...) of the nsel rows of chunk blocks
  * [blk0, blk0 + nblk), whose first is stored at off0).  The warp lists the
- * batch's rows from the bitmap, starting at the block that holds its first
+ * unit's rows from the bitmap, starting at the block that holds its first
  * rank, then reads them from the staged tile in place (b.stage the tile,
  * rows counted from its first row) or gathers them from device memory into
  * the warp's gather area.  Returns false on an output overflow. */
-__device__ __forceinline__ bool full_batch(Bases b, uint32_t list, uint32_t gat, uint32_t blk0, uint32_t nblk,
+__device__ __forceinline__ bool full_unit(Bases b, uint32_t list, uint32_t gat, uint32_t blk0, uint32_t nblk,
 	uint32_t j, uint32_t nsel, uint64_t off0, uint32_t mode, int lane)
 {
-	const uint32_t r0 = 32u * kBatchE * j;
+	const uint32_t r0 = kUnitE * j;
 	if (r0 >= nsel)
 		return true;  /* an entry with no selected rows: nothing to do */
-	const uint32_t cnt = min(32u * kBatchE, nsel - r0);
+	const uint32_t cnt = min(kUnitE, nsel - r0);
 	/* the block holding rank r0: lane l looks at block blk0 + l */
 	uint32_t bo = 0, bc = 0;
 	if ((uint32_t)lane < nblk) {
@@ -1088,7 +1183,21 @@ __device__ __forceinline__ bool full_batch(Bases b, uint32_t list, uint32_t gat,
 				incl += v;
 		}
 		uint32_t rr = rank + incl - c, x = word;
-		if (rr + c > r0 && rr < r0 + cnt) {
+		const bool part = rr + c > r0 && rr < r0 + cnt;  /* this word holds ranks of the batch */
+		const uint32_t parts = __ballot_sync(0xffffffffu, part);
+		if (__popc(parts) <= 8) {
+			/* dense rows: the batch lies in a few words, so the warp lists
+			 * each of them together, lane j taking bit j */
+			for (uint32_t m = parts; m; m &= m - 1) {
+				const int src = __ffs(m) - 1;
+				const uint32_t wx = __shfl_sync(0xffffffffu, word, src);
+				const uint32_t rx = __shfl_sync(0xffffffffu, rr, src) + __popc(wx & ((1u << lane) - 1u));
+				if (((wx >> lane) & 1u) && rx >= r0 && rx < r0 + cnt)
+					asm volatile("st.shared.u16 [%0], %1;" ::"r"(list + 2 * (rx - r0)),
+						"h"((uint16_t)(32 * (w0 + (uint32_t)src) + (uint32_t)lane)) : "memory");
+			}
+		} else if (part) {
+			/* sparse rows: each lane lists its own word's few rows */
 			while (rr < r0) {  /* ranks before the batch */
 				x &= x - 1;
 				rr++;
@@ -1106,39 +1215,33 @@ __device__ __forceinline__ bool full_batch(Bases b, uint32_t list, uint32_t gat,
 	__syncwarp();
 	const uint64_t cap = lds_u64(b.slot + kQCapacity);
 	const uint64_t pos0 = off0 + r0;
-	uint32_t row[kBatchE];
-	uint32_t act = 0, in = 0;
-#pragma unroll
-	for (int i = 0; i < kBatchE; i++) {
-		const uint32_t e = 32 * i + (uint32_t)lane;
-		const bool a = e < cnt;
-		row[i] = 0;
-		if (a) {
-			uint16_t r;
-			asm volatile("ld.shared.u16 %0, [%1];" : "=h"(r) : "r"(list + 2 * e));
-			row[i] = r;
-		}
-		act |= (a ? 1u : 0u) << i;
-		if (a && pos0 + e < cap)
-			in |= 1u << i;
-	}
+	UnitRows u;
+	uint32_t in[kUnitBatches];
+	unit_rows(list, cnt, pos0, cap, u, in, lane);
 	b.blk_row0 = 0;
 	if (mode == FM_GATHER) {
-		/* gathered values are indexed by batch entry; the chunk row of
-		 * entry i is the entry's first row plus its row */
-		uint32_t grow[kBatchE];
-#pragma unroll
-		for (int i = 0; i < kBatchE; i++) {
-			grow[i] = blk0 * kBlockRows + row[i];
-			row[i] = 32u * i + (uint32_t)lane;
-		}
+		/* gathered values are indexed by unit entry; the chunk row of an
+		 * entry is the entry's first row plus its row */
 		b.stage = gat;
-		gather_batch(b, grow, lane);
+#pragma unroll
+		for (int s2 = 0; s2 < (int)kUnitBatches; s2++) {
+			uint32_t grow[kBatchE];
+#pragma unroll
+			for (int i = 0; i < kBatchE; i++) {
+				grow[i] = blk0 * kBlockRows + u.row[s2][i];
+				u.row[s2][i] = 32u * kBatchE * s2 + 32u * i + (uint32_t)lane;
+			}
+			gather_batch(b, grow, 32u * kBatchE * s2, lane);
+		}
 		__syncwarp();
 	}
-	batch_out(b, row, act, in, pos0, lane);
-	__syncwarp();  /* the list and gather area are this warp's next batch's */
-	return act == in;
+	unit_out(b, u, in, pos0, lane);
+	__syncwarp();  /* the list and gather area are this warp's next unit's */
+	bool ok = true;
+#pragma unroll
+	for (int s2 = 0; s2 < (int)kUnitBatches; s2++)
+		ok = ok && u.act[s2] == in[s2];
+	return ok;
 }
 
 /* ---- ordered placement ------------------------------------------------- */
@@ -1867,7 +1970,7 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					n = (nblk + kCountGroup - 1) / kCountGroup;
 				} else {
 					nsel = entry_selected(b.slot, row0 / kBlockRows, nblk, &off0);
-					n = max(1u, (nsel + 32u * kBatchE - 1) / (32u * kBatchE));
+					n = max(1u, (nsel + kUnitE - 1) / kUnitE);
 				}
 			}
 			const uint32_t taken = c & 0xffffu;
@@ -1911,7 +2014,7 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					lane);
 		} else {
 			b.stage = tile;
-			ok = full_batch(b, list, gat, blk0, nblk, j, nsel, off0, mode, lane);
+			ok = full_unit(b, list, gat, blk0, nblk, j, nsel, off0, mode, lane);
 		}
 		/* a serving session reports rows beyond capacity in the query's
 		 * completion record instead */

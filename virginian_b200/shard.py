@@ -50,3 +50,36 @@ def exchange_counts(n: int, group=None, device: str = "cpu") -> Tuple[int, int]:
     counts = [int(x.item()) for x in out]
     r = dist.get_rank(group)
     return sum(counts[:r]), sum(counts)
+
+
+def assign_tables(table_rows: Sequence[int], world: int) -> List[int]:
+    """Whole tables per rank (the batched and serving workloads): each table
+    has one owner, largest tables first onto the least-loaded rank (ties to
+    the lower rank), so every rank computes the same assignment."""
+    load = [0] * world
+    owner = [0] * len(table_rows)
+    for t in sorted(range(len(table_rows)), key=lambda i: (-int(table_rows[i]), i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[t] = r
+        load[r] += int(table_rows[t])
+    return owner
+
+
+def my_queries(query_tables: Sequence[int], owner: Sequence[int], rank: int) -> List[int]:
+    """The queries a rank runs: those over the tables it owns, in order."""
+    return [q for q, t in enumerate(query_tables) if owner[t] == rank]
+
+
+def result_directory(nq: int, mine: Sequence[int], rows: Sequence[int], group=None,
+                     device: str = "cpu") -> List[int]:
+    """Every query's result row count on every rank: a query's result stays
+    on the rank that ran it (its table's owner), and one all-reduce of the
+    per-query counts tells every rank how long each result is."""
+    import torch
+    import torch.distributed as dist
+    t = torch.zeros(nq, dtype=torch.int64, device=device)
+    for q, n in zip(mine, rows):
+        t[q] = int(n)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(t, group=group)
+    return [int(x) for x in t.cpu().tolist()]
