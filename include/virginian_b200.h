@@ -379,6 +379,12 @@ void virg_gpu_result_destroy(virg_gpu_result *r);
 int virg_gpu_table_read_ceiling(virg_gpu_table *t, const int *cols, unsigned ncols, unsigned mode,
 	unsigned reps, double *ms, unsigned long long *bytes);
 
+/* No counterpart in the reference.  An estimate of the rows a program's
+ * filter keeps in a table: the share of the table's host row sample (runs
+ * of rows taken from segments spread over each append) the filter keeps,
+ * times the table's rows.  Sizes reservations; never used for results. */
+int virg_gpu_table_estimate(const virg_gpu_table *t, const virg_gpu_program *p, uint64_t *rows);
+
 /* end to end: host segments in, host result columns out.  Copies the
  * referenced columns to the device, runs the program and copies the result
  * rows back; out_cols[c] must hold `capacity` rows of result column c. */
@@ -489,12 +495,16 @@ typedef struct {
 	                                  * running session */
 	unsigned long long status_ring;  /* look-back words of a session's ring; work
 	                                  * item i uses word i mod status_ring */
+	unsigned long long sampled;      /* submissions whose reservation came from the
+	                                  * table's row sample */
 } virg_serve_counters;
 
 int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cfg, virg_serve **out);
 /* queue a query; estimated_rows 0 reserves the rows the same program last
- * returned on the same table, plus a quarter, or else the bound (the
- * table's rows); a short reservation is admitted again with the exact rows */
+ * returned on the same table, plus a quarter, else the fraction of the
+ * table's host row sample the program's filter keeps, times its rows, plus
+ * a quarter (else the bound, the table's rows); a short reservation is
+ * admitted again with the exact rows */
 int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_gpu_table *t,
 	uint64_t estimated_rows, uint64_t *ticket);
 /* a query's state; wait_ms < 0 waits for completion, > 0 up to that long.

@@ -198,3 +198,36 @@ def test_result_larger_than_budget_fails_cleanly(setup):
         s.release(t)
     finally:
         s.close()
+
+
+def test_sample_estimates_track_selectivity(oracle_mod):
+    """The host row sample behind serving reservations: the estimate of a
+    filter's rows stays within a few percent of the table's actual share,
+    across selectivities, and a submission without a caller's estimate is
+    sized from it."""
+    import numpy as np
+    from tests.helpers import config2
+    n = 2_000_000
+    cols = datagen.table(n, datagen.SCHEMA_A, seed=61)
+    types = [t for _, t in datagen.SCHEMA_A]
+    cat = sql.Catalog()
+    cat.add_table("test", datagen.SCHEMA_A)
+    with vb.Engine(0) as eng:
+        t = vb.Table(eng, types)
+        t.append(datagen.segments(cols, datagen.SCHEMA_A, 100_000))
+        for c, d in ((1.0, 60.0), (30.0, 20.0), (90.0, -30.0)):
+            comp = cat.compile(config2(c, d))
+            p = vb.Program(comp.op_list(), comp.pc, types)
+            want = int(((cols["uniformf"] < c) | (cols["normalf20"] > d)).sum())
+            est = t.estimate(p)
+            assert abs(est - want) <= 0.05 * n, (c, d, est, want)
+        srv = vb.Serve(eng, result_budget_bytes=1 << 30)
+        comp = cat.compile(config2(30.0, 20.0))
+        p = vb.Program(comp.op_list(), comp.pc, types)
+        tk = srv.submit(p, t)
+        st = srv.wait(tk, timeout_s=60)
+        assert st["rows"] == int(((cols["uniformf"] < 30.0) | (cols["normalf20"] > 20.0)).sum())
+        assert srv.stats()["sampled"] >= 1
+        srv.release(tk)
+        srv.close()
+        t.close()

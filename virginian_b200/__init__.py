@@ -209,6 +209,13 @@ class Table:
     def nbytes(self) -> int:
         return int(lib().virg_gpu_table_bytes(self.h))
 
+    def estimate(self, program: "Program") -> int:
+        """Rows the program's filter keeps in a host sample of this table,
+        scaled to the table (an estimate for sizing reservations)."""
+        n = ctypes.c_uint64()
+        check(lib().virg_gpu_table_estimate(self.h, program.h, ctypes.byref(n)), "table estimate")
+        return n.value
+
     def read_ceiling(self, columns: Sequence[int], mode: int = 0, reps: int = 5) -> Tuple[float, int]:
         """Device time (ms, best of `reps`) and bytes of a kernel that only
         reads the given columns (-1: the key) of every segment: mode 0 with
@@ -376,7 +383,7 @@ class Serve:
         return {"sessions": c.sessions, "admitted": c.admitted, "readmitted": c.readmitted,
                 "pending": c.pending, "inflight": c.inflight, "arena_used": c.arena_used,
                 "device_error": c.device_error, "restarts": c.restarts,
-                "work_items": c.work_items, "status_ring": c.status_ring,
+                "work_items": c.work_items, "status_ring": c.status_ring, "sampled": c.sampled,
                 "shape": {"threads": c.shape[0], "stage_kb": c.shape[1], "stages": c.shape[2],
                           "grid": c.shape[3]}}
 

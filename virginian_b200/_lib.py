@@ -62,7 +62,7 @@ class ServeCounters(ctypes.Structure):
                 ("inflight", ctypes.c_ulonglong), ("arena_used", ctypes.c_ulonglong),
                 ("device_error", ctypes.c_uint), ("shape", ctypes.c_uint * 4),
                 ("restarts", ctypes.c_ulonglong), ("work_items", ctypes.c_ulonglong),
-                ("status_ring", ctypes.c_ulonglong)]
+                ("status_ring", ctypes.c_ulonglong), ("sampled", ctypes.c_ulonglong)]
 
 
 class ProgramInfo(ctypes.Structure):
@@ -103,6 +103,7 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_table_rows": (u64, [vp]),
         "virg_gpu_table_bytes": (u64, [vp]),
         "virg_gpu_table_destroy": (None, [vp]),
+        "virg_gpu_table_estimate": (i, [vp, vp, P(u64)]),
         "virg_gpu_table_read_ceiling": (i, [vp, P(ctypes.c_int), u, u, u, P(ctypes.c_double),
                                             P(ctypes.c_ulonglong)]),
         "virg_gpu_query": (i, [vp, vp, vp, P(vp)]),

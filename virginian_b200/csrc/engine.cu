@@ -947,6 +947,7 @@ extern "C" int virg_gpu_table_append(virg_gpu_table *t, const virg_gpu_segment *
 	if (!table_add_segments(t, segs, nsegs, nullptr, true, t->e->stream))
 		return 0;
 	CUDA_OK(cudaStreamSynchronize(t->e->stream), "table copy");
+	table_sample(t, segs, nsegs);
 	return table_sync_desc(t);
 }
 

@@ -19,6 +19,13 @@ struct ScratchBuf {
 	size_t cap = 0;
 };
 
+/* a host sample of a resident table's rows: runs of consecutive rows from
+ * segments spread over each append, per column (index kKeySlot: the key) */
+struct TableSample {
+	uint32_t rows = 0, runs = 0;
+	std::vector<unsigned char> col[kMaxLoads];
+};
+
 /* the engine's staging ring for rows read from host memory: device buffers
  * and events kept across calls, grown when a call needs more */
 struct HostRing {
@@ -81,6 +88,7 @@ struct virg_gpu_table {
 	uint64_t rows = 0;
 	uint64_t bytes = 0;
 	uint32_t blocks = 0;                 /* 64-row blocks so far */
+	vgpu::TableSample sample;            /* for result-size estimates */
 };
 
 struct virg_gpu_result {
@@ -174,6 +182,10 @@ void host_ring_free(virg_gpu_engine *e);
 /* the persistent tuned-shape cache: loaded when an engine is created, and
  * a newly tuned shape recorded in the engine and appended to it */
 void tune_cache_load(virg_gpu_engine *e);
+/* the table's host sample, extended by appended segments; the fraction of
+ * sample rows a program's filter keeps (negative: no usable sample) */
+void table_sample(virg_gpu_table *t, const virg_gpu_segment *segs, unsigned n);
+double sample_selectivity(const Program &P, const virg_gpu_table *t);
 void tune_remember(virg_gpu_engine *e, const std::string &key, const Shape &s);
 std::string shape_key(const std::vector<QueryLaunch> &qs);
 int read_device_error(virg_gpu_engine *e, unsigned *err);

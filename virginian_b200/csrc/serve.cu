@@ -9,9 +9,11 @@
  *  - admission: queries are admitted in arrival order while the result
  *    arena (the result budget, one device allocation) has room for their
  *    estimated result size and the session has descriptor slots left.  The
- *    estimate is the query's bound, table rows x result bytes per row; a
- *    caller may pass a smaller estimate, and a query whose rows exceed its
- *    reservation is admitted again with exactly its row count;
+ *    estimate is the caller's, else the rows the same program last returned
+ *    on the same table, else the share of the table's host row sample its
+ *    filter keeps (estimate.cpp), each with a margin, else the bound (the
+ *    table's rows); a query whose rows exceed its reservation is admitted
+ *    again with exactly its row count;
  *  - folding in: the scheduler writes the admitted queries' descriptors to
  *    device memory on an upload stream, waits for that copy, then publishes
  *    the new query and work counts through a doorbell word in host-mapped
@@ -185,6 +187,7 @@ struct virg_serve {
 	std::condition_variable cv;  /* completions, for waiters */
 	std::thread sched;
 	std::atomic<bool> quit{false};
+	std::atomic<unsigned long long> sampled{0};  /* submissions estimated from a table sample */
 	std::string fail;
 	/* result rows each (program, table) pair last had, with the table's rows
 	 * then: the default estimate of its next submission */
@@ -602,12 +605,23 @@ extern "C" int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_
 	const uint64_t bound = t->rows;
 	uint64_t est = estimated_rows ? std::min(estimated_rows, bound) : bound;
 	if (!estimated_rows) {
-		/* the selectivity this program last had on this table, with a
+		/* the selectivity this program last had on this table, else the
+		 * fraction of the table's host sample its filter keeps, with a
 		 * margin; a short estimate is admitted again with its exact rows */
-		std::lock_guard<std::mutex> lk(s->mu);
-		auto h = s->history.find({p, t});
-		if (h != s->history.end() && h->second.second == bound)
-			est = std::min<uint64_t>(bound, h->second.first + h->second.first / 4 + 1024);
+		bool known = false;
+		{
+			std::lock_guard<std::mutex> lk(s->mu);
+			auto h = s->history.find({p, t});
+			if (h != s->history.end() && h->second.second == bound) {
+				est = std::min<uint64_t>(bound, h->second.first + h->second.first / 4 + 1024);
+				known = true;
+			}
+		}
+		const double sel = known ? -1.0 : sample_selectivity(P, t);
+		if (sel >= 0.0) {
+			est = std::min<uint64_t>(bound, (uint64_t)(sel * 1.25 * (double)bound) + 4096);
+			s->sampled.fetch_add(1);
+		}
 	}
 	VGPU_CHECK(arena_need(P, est) <= s->cfg.result_budget_bytes,
 		"the query's result reservation (%zu bytes) exceeds the result budget", arena_need(P, est));
@@ -713,6 +727,7 @@ extern "C" int virg_serve_stats(virg_serve *s, virg_serve_counters *c)
 	c->device_error = s->device_error;
 	c->restarts = s->restarts;
 	c->work_items = s->work;
+	c->sampled = s->sampled.load();
 	c->status_ring = kStatusRing;
 	c->shape[0] = s->geom.shape.threads;
 	c->shape[1] = s->geom.shape.stage_kb;

@@ -1900,14 +1900,36 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 		based_seq = seq;
 		return mbar_wait(sbase + kOffBased + 8 * slot, (seq / kChunkSlots) & 1u, flags);
 	};
+	/* the entry of the warp's last unit, kept for the fast claim below */
+	uint32_t k = 0, n = 0, kind = 0, slot = 0, seq = 0, row0 = 0, nrows = 0, buf = 0, mode = FM_BITMAP;
+	uint32_t nsel = 0;
+	uint64_t off0 = 0;
+	bool have = false;
 	for (;;) {
 		/* ---- claim a unit */
-		uint32_t k = 0, j = 0, n = 0, kind = 0, slot = 0, seq = 0, row0 = 0, nrows = 0, buf = 0, mode = FM_BITMAP;
-		uint32_t nsel = 0;
-		uint64_t off0 = 0;
-		bool fail = false;
+		uint32_t j = 0;
+		bool fail = false, fast = false;
 		uint64_t t0 = 0;
-		for (uint32_t spin = 0;; spin++) {
+		if (have) {
+			/* fast path: the next unit of the entry of the warp's last unit.
+			 * The entry's info is still the warp's while its claim word
+			 * carries its tag and units remain (a recycled entry has a new
+			 * tag, so the swap fails) */
+			uint32_t got = 0, taken = 0;
+			if (lane == 0) {
+				const uint32_t cw = sbase + kOffClaim + 4 * (k % kEntries);
+				const uint32_t c = ldv_u32(cw);
+				taken = c & 0xffffu;
+				if ((c >> 16) == (k & 0xffffu) && taken < n) {
+					got = atom_cas_shared(cw, c, c + 1) == c;
+					if (got && taken + 1 == n)
+						stv_u32(sbase + kOffCur, k + 1);
+				}
+			}
+			fast = __shfl_sync(0xffffffffu, got, 0) != 0;
+			j = __shfl_sync(0xffffffffu, taken, 0);
+		}
+		for (uint32_t spin = 0; !fast; spin++) {
 			/* bounded: a claim that makes no progress for the wait limit
 			 * (or after another warp aborted the CTA) gives up */
 			if ((spin & 255u) == 255u) {
@@ -1984,6 +2006,7 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 				if (__shfl_sync(0xffffffffu, got, 0)) {
 					k = kk;
 					j = taken;
+					have = true;
 					break;
 				}
 				continue;
