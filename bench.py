@@ -227,15 +227,17 @@ def _accept_for(cat, types, layout=None):
     return ok
 
 
-def _device_tables(eng, sizes, seed0):
-    """Resident tables of the benchmark schema generated on the GPU."""
+def _device_tables(eng, sizes, seed0, table_nos=None):
+    """Resident tables of the benchmark schema generated on the GPU (table i
+    seeded as table number table_nos[i], default i)."""
     import torch
     import virginian_b200 as vb
     from virginian_b200 import datagen
     types = [t for _, t in datagen.SCHEMA_A]
     tables = []
     for i, n in enumerate(sizes):
-        segs, keep = datagen.device_table(int(n), datagen.SCHEMA_A, seed=seed0 + i)
+        segs, keep = datagen.device_table(int(n), datagen.SCHEMA_A,
+                                          seed=seed0 + (i if table_nos is None else table_nos[i]))
         t = vb.Table(eng, types)
         t.append(segs)
         del segs, keep
@@ -406,19 +408,26 @@ def bench_batched(eng, reps=5, world=1, rank=0):
     return out
 
 
-def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
+def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300, world=1, rank=0):
     """The serving loop over 32 resident tables (~40 GB, 10M-200M rows each):
     Poisson arrivals of generated queries at each rate, latency from arrival
     to completion seen by the host, against serial one-launch-per-query
-    execution of the same arrival sequence."""
+    execution of the same arrival sequence.  With N ranks each rank holds the
+    tables it owns (virginian_b200.shard.assign_tables) and serves the
+    arrivals over them; latencies are pooled over ranks."""
     import virginian_b200 as vb
+    from virginian_b200 import shard
     rng = np.random.default_rng(505)
     raw = np.exp(rng.uniform(np.log(1e7), np.log(2e8), size=32))
     sizes = np.clip(raw * (1.43e9 / raw.sum()), 1e7, 2e8).astype(np.int64)
-    tables = _device_tables(eng, sizes, 2000)
+    owner = shard.assign_tables([int(x) for x in sizes], world)
+    mine_t = [k for k in range(len(sizes)) if owner[k] == rank]
+    tables = dict(zip(mine_t, _device_tables(eng, [sizes[k] for k in mine_t], 2000, mine_t)))
     log("serving: tables ready")
     layout = (32, 16, 48)
-    work = _queries(per_rate, 88, len(tables), layout)
+    all_work = _queries(per_rate, 88, len(sizes), layout)
+    mine = shard.my_queries([k for _, k, _ in all_work], owner, rank)
+    work = [all_work[i] for i in mine]
     srv = vb.Serve(eng, result_budget_bytes=20 << 30, max_load_bytes_per_row=layout[0],
                    max_row_vector_bytes=layout[1], max_sel_vector_bytes=layout[2])
     # warm: one query through each path
@@ -430,12 +439,22 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
     r.close()
     out = {}
     import threading
+
+    def pooled(xs):
+        if world == 1:
+            return list(xs)
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, list(xs))
+        return [x for part in parts for x in part]
+
     for ri, rate in enumerate(rates):
         # the same queries at every rate; only the arrival process differs
-        chunk = work[:per_rate]
+        chunk = work
         log(f"serving: rate {rate}")
-        gaps = np.random.default_rng(600 + ri).exponential(1.0 / rate, size=len(chunk))
-        arrivals = np.cumsum(gaps) - gaps[0]
+        gaps = np.random.default_rng(600 + ri).exponential(1.0 / rate, size=len(all_work))
+        arrivals = (np.cumsum(gaps) - gaps[0])[mine]
+        barrier(world)
         # a client thread consumes results as they complete and releases
         # their memory, while arrivals keep coming
         tickets, lag = [None] * len(chunk), [0.0] * len(chunk)
@@ -469,7 +488,8 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
         th.join()
         if errors:
             raise errors[0]
-        serve_span = max(done_at) - arrivals[0]
+        serve_span = allreduce_max(max(done_at), world)
+        barrier(world)
         # serial: one launch per query, in arrival order
         log(f"serving: serial at rate {rate}")
         slat, serial_rows = [], []
@@ -481,17 +501,26 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
             serial_rows.append(r.rows)
             r.close()
             slat.append((time.perf_counter() - t0 - at) * 1e3)
-        serial_span = time.perf_counter() - t0
-        bad_rows = [n for n in range(len(chunk)) if srows[n] != serial_rows[n]]
+        serial_span = allreduce_max(time.perf_counter() - t0, world)
+        bad_rows = pooled(mine[n] for n in range(len(chunk)) if srows[n] != serial_rows[n])
+        lat, slat, lag = pooled(lat), pooled(slat), pooled(lag)
         out[str(rate)] = {
-            "queries": len(chunk), "offered_qps": rate,
+            "queries": len(all_work), "offered_qps": rate,
             "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-            "sustained_qps": round(len(chunk) / serve_span, 1),
+            "sustained_qps": round(len(all_work) / serve_span, 1),
             "serial_p50_ms": round(float(np.percentile(slat, 50)), 3),
             "serial_p99_ms": round(float(np.percentile(slat, 99)), 3),
-            "serial_qps": round(len(chunk) / serial_span, 1),
+            "serial_qps": round(len(all_work) / serial_span, 1),
             "submit_lag_p99_ms": round(float(np.percentile(lag, 99)) * 1e3, 3),
-            "rows_checked": len(chunk), "rows_mismatch": bad_rows}
+            "rows_checked": len(all_work), "rows_mismatch": bad_rows}
+    if world > 1:
+        st = srv.stats()
+        srv.close()
+        for t in tables.values():
+            t.close()
+        return {"workload": "32 resident tables, generated queries, Poisson arrivals; whole tables per rank "
+                            f"over {world} ranks", "rates": out, "queries_this_rank": len(work),
+                "sessions": st["sessions"], "readmitted": st["readmitted"], "sampled": st["sampled"]}
     # the look-back ring: queries back to back until the session's work
     # numbering has passed the ring's size, then the bytes of the last
     # results against the one-launch-per-query path
@@ -532,7 +561,7 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
     st = srv.stats()
     srv.close()
     total_rows = int(sizes.sum())
-    for t in tables:
+    for t in tables.values():
         t.close()
     return {"workload": "32 resident tables (rows log-uniform in [1e7, 2e8], %.1f GB), generated queries, "
                         "Poisson arrivals; latency from arrival to completion seen by the host" %
@@ -542,7 +571,7 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300):
                           "queries": submitted, "rows_mismatch": wrap_rows_bad,
                           "bytes_checked": min(8, len(last)), "bytes_equal": bool(exact and last)},
             "sessions": st["sessions"], "restarts": st["restarts"],
-            "readmitted": st["readmitted"], "shape": st["shape"]}
+            "readmitted": st["readmitted"], "sampled": st["sampled"], "shape": st["shape"]}
 
 
 STREAM_QUERY = ("SELECT id, uniformi, uniforml, normald FROM test "
@@ -981,7 +1010,7 @@ def run_b200(args):
     # the other workloads: batched on every rank (whole tables per rank);
     # the others on one GPU, rank 0 (the sharded path covers the scan)
     sections = [x for x in args.sections.split(",") if x]
-    for name, fn, multi in (("batched", bench_batched, True), ("serving", bench_serving, False),
+    for name, fn, multi in (("batched", bench_batched, True), ("serving", bench_serving, True),
                             ("streamed", bench_streamed, False), ("dropin", bench_dropin, False),
                             ("ref_gpu_vm", bench_ref_gpu_vm, False)):
         if name not in sections or (world > 1 and not multi):

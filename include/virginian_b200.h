@@ -466,7 +466,7 @@ void virg_gpu_batch_destroy(virg_gpu_batch *b);
 typedef struct {
 	uint64_t result_budget_bytes;    /* device memory for results (0: 20 GB) */
 	unsigned max_queries;            /* queries per kernel session (0: 4096) */
-	unsigned idle_us;                /* end an idle session after this long (0: 2000) */
+	unsigned idle_us;                /* end an idle session after this long (0: 50000) */
 	unsigned max_load_bytes_per_row; /* staged column bytes a program may read (0: 32) */
 	unsigned max_row_vector_bytes;   /* filter register-vector bytes per row (0: 16) */
 	unsigned max_sel_vector_bytes;   /* projection register-vector bytes per row (0: 48) */

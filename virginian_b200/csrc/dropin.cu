@@ -329,7 +329,10 @@ extern "C" int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
 			const unsigned simd_rows = (unsigned)std::min<uint64_t>(64, t->rows - b * 64);
 			virg_tablet_meta *rt = res[0];
 			if (rt->rows + simd_rows >= rt->possible_rows - 300) {
-				/* roll over: the current tablet is complete, so release it */
+				/* roll over: the current tablet is complete, so release it
+				 * once the copies into it have landed */
+				if (cudaStreamSynchronize(e->stream) != cudaSuccess)
+					ok = fail("result copy sync failed");
 				virg_tablet_meta *old = rt;
 				host.allocresult(v, vm, res, res[0]);
 				host.unlock(v, old->id);
@@ -352,6 +355,9 @@ extern "C" int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
 				ok = fail("result tablet overflow");
 				break;
 			}
+			/* result tablets live in pinned host slots (src/init.c:57-58), so
+			 * the copies run asynchronously; the tablet's last copy is waited
+			 * for before it is released or the data tablet is done */
 			for (unsigned j = 0; j < P.nout && run; j++) {
 				char *dst = (char *)rt + rt->fixed_block + rt->fixed_offset[j] +
 					(size_t)P.out_stride[j] * rt->rows;
@@ -360,12 +366,12 @@ extern "C" int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
 						e->stream) != cudaSuccess)
 					ok = fail("result copy failed");
 			}
-			if (cudaStreamSynchronize(e->stream) != cudaSuccess)
-				ok = fail("result copy sync failed");
 			rt->rows += (unsigned)run;
 			done += run;
 			b = b2 - 1;
 		}
+		if (cudaStreamSynchronize(e->stream) != cudaSuccess)
+			ok = fail("result copy sync failed");
 		if (ok && done != total)
 			ok = fail("result row count mismatch");
 		cudaEventRecord(tm.d, e->stream);

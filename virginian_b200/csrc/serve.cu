@@ -199,19 +199,23 @@ namespace {
 int serve_layout(virg_serve *s)
 {
 	virg_gpu_engine *e = s->e;
-	/* eight compute warps, one CTA per SM, the largest data buffers (32 KB
+	/* eight compute warps, one CTA per SM, the largest data buffers (48 KB
 	 * down to 8 KB, each holding a block of the widest staging the session
-	 * admits) of which at least two fit beside the warps' vector areas */
+	 * admits) of which at least two fit beside the warps' vector areas.  The
+	 * session's full phase reads staged tiles in place (no gather area). */
 	const unsigned min_kb = (kBlockRows * s->cfg.max_load_bytes_per_row + 1023) / 1024;
 	bool fit = false;
-	for (unsigned kb : {32u, 24u, 16u, 8u}) {
-		Shape sh = {256, std::max(kb, min_kb), 0, 1, kServeChunkRows, 0};
-		if (geom_make(sh, s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes,
-				std::min<unsigned>(s->cfg.max_load_bytes_per_row, kGatherMaxBpr), e->smem_optin, e->smem_sm,
-				&s->geom)) {
-			fit = true;
-			break;
+	for (unsigned min_stages : {3u, 2u}) {
+		for (unsigned kb : {48u, 40u, 32u, 24u, 16u, 8u}) {
+			Shape sh = {256, std::max(kb, min_kb), 0, 1, kServeChunkRows, 0};
+			if (geom_make(sh, s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes, 0u, e->smem_optin,
+					e->smem_sm, &s->geom) && s->geom.shape.stages >= min_stages) {
+				fit = true;
+				break;
+			}
 		}
+		if (fit)
+			break;
 	}
 	VGPU_CHECK(fit, "serving layout does not fit shared memory (vectors of %u + %u bytes per row)",
 		s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes);
@@ -532,7 +536,7 @@ extern "C" int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cf
 	if (!c.max_queries)
 		c.max_queries = 4096;
 	if (!c.idle_us)
-		c.idle_us = 2000;
+		c.idle_us = 50000;
 	if (!c.max_load_bytes_per_row)
 		c.max_load_bytes_per_row = 32;
 	if (!c.max_row_vector_bytes)
