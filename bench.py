@@ -637,8 +637,8 @@ def bench_streamed(eng, rows=400_000_000, chunk=25_000_000):
     t.close()
     alg = rows * p.info.load_bytes_per_row + n * p.info.out_bytes_per_row
     del host
-    return {"workload": "400M rows of the 9-column schema (%.1f GB) in pinned host memory; %s" %
-                        (rows * 48 / 1e9, STREAM_QUERY),
+    return {"workload": "%dM rows of the 9-column schema (%.1f GB) in pinned host memory; %s" %
+                        (rows // 1_000_000, rows * 48 / 1e9, STREAM_QUERY),
             "rows": rows, "result_rows": int(n), "h2d_bytes": int(best["h2d_bytes"]),
             "seconds": round(best["seconds"], 4),
             "host_link_gbs": round(best["h2d_bytes"] / best["seconds"] / 1e9, 2),
@@ -1017,7 +1017,12 @@ def run_b200(args):
             continue
         log(name)
         try:
-            res = fn(eng, world=world, rank=rank) if multi else fn(eng)
+            if multi:
+                res = fn(eng, world=world, rank=rank)
+            elif name == "streamed":
+                res = fn(eng, rows=args.stream_rows, chunk=min(25_000_000, args.stream_rows))
+            else:
+                res = fn(eng)
         except Exception as ex:  # report, keep the headline line
             res = {"error": f"{type(ex).__name__}: {ex}"}
         if rank == 0:
@@ -1054,6 +1059,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--shape", default="", help="threads,stage_kb,stages,ctas_per_sm,chunk_rows: force the launch "
                     "shape of the scan instead of tuning it (for profiling one launch)")
+    ap.add_argument("--stream-rows", type=int, default=400_000_000,
+                    help="rows of the streamed section's host table (400M: the streamed workload)")
     ap.add_argument("--no-parity", dest="parity", action="store_false",
                     help="skip the headline's byte comparison with the reference CPU VM")
     ap.add_argument("--sections", default="batched,serving,streamed,dropin,ref_gpu_vm",

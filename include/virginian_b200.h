@@ -50,6 +50,7 @@ extern "C" {
 #define VIRG_MAX_COLUMN_NAME 16
 #define VIRG_MAX_TABLE_NAME 32
 #define VIRG_MEM_TABLETS 64
+#define VIRG_TABLET_SIZE (8 * 1024 * 1024)
 #define VIRG_REGS 16
 #define VIRG_GLOBAL_REGS 16
 #define VIRG_OPS 32
@@ -378,6 +379,13 @@ void virg_gpu_result_destroy(virg_gpu_result *r);
  * device time of `reps` launches (ms) and the bytes one launch reads */
 int virg_gpu_table_read_ceiling(virg_gpu_table *t, const int *cols, unsigned ncols, unsigned mode,
 	unsigned reps, double *ms, unsigned long long *bytes);
+
+/* Ingest, replacing the host-slot path src/db/load.c:22-98 for a resident
+ * table: appends every tablet of table `table` of the Virginian database file
+ * at `path` (this build's struct layout) to t, following the tablet chain;
+ * tablets are read into pinned buffers and copied to the device while the
+ * next is read.  *rows receives the rows appended. */
+int virg_gpu_table_load_db(virg_gpu_table *t, const char *path, const char *table, uint64_t *rows);
 
 /* No counterpart in the reference.  An estimate of the rows a program's
  * filter keeps in a table: the share of the table's host row sample (runs

@@ -69,6 +69,16 @@ void orc_close(orc_db *d)
 	free(d);
 }
 
+/* closes the database, which writes every tablet to its file
+ * (src/db/close.c:20-50), and keeps the file; its path goes to path_out */
+int orc_close_keep(orc_db *d, char *path_out, unsigned n)
+{
+	snprintf(path_out, n, "%s", d->path);
+	int ok = virg_close(&d->v) == VIRG_SUCCESS;
+	free(d);
+	return ok;
+}
+
 virginian *orc_virginian(orc_db *d) { return &d->v; }
 
 int orc_create_table(orc_db *d, const char *name, int key_type, unsigned ncols,

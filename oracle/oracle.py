@@ -100,6 +100,8 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.orc_reader_walk.restype = ull
     lib.orc_reader_walk.argtypes = [vp, ctypes.c_char_p, vp, u, ull, ctypes.POINTER(ull)]
     lib.orc_set_gpu_flags.argtypes = [vp, i, i, i]
+    lib.orc_close_keep.restype = i
+    lib.orc_close_keep.argtypes = [vp, ctypes.c_char_p, u]
     lib.orc_testsizes.restype = ctypes.POINTER(ctypes.c_size_t)
     lib.orc_sizeof_vm.restype = u
     lib.orc_sizeof_meta.restype = u
@@ -153,6 +155,15 @@ class OracleDB:
                 os.rmdir(self._tmp)
             except OSError:
                 pass
+
+    def close_keep(self) -> str:
+        """Closes the database, writing every tablet to its file, and keeps
+        the file; returns its path (the caller removes it and its folder)."""
+        buf = ctypes.create_string_buffer(1024)
+        if not self.lib.orc_close_keep(self.h, buf, 1024):
+            raise RuntimeError("virg_close failed")
+        self.h = None
+        return buf.value.decode()
 
     def __enter__(self):
         return self

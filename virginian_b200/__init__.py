@@ -209,6 +209,14 @@ class Table:
     def nbytes(self) -> int:
         return int(lib().virg_gpu_table_bytes(self.h))
 
+    def load_db(self, path: str, table: str) -> int:
+        """Appends every tablet of a table of a Virginian database file (read
+        straight into pinned buffers and copied to the device); returns the
+        rows appended."""
+        n = ctypes.c_uint64()
+        check(lib().virg_gpu_table_load_db(self.h, path.encode(), table.encode(), ctypes.byref(n)), "table load_db")
+        return n.value
+
     def estimate(self, program: "Program") -> int:
         """Rows the program's filter keeps in a host sample of this table,
         scaled to the table (an estimate for sizing reservations)."""

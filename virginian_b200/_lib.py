@@ -104,6 +104,7 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_table_bytes": (u64, [vp]),
         "virg_gpu_table_destroy": (None, [vp]),
         "virg_gpu_table_estimate": (i, [vp, vp, P(u64)]),
+        "virg_gpu_table_load_db": (i, [vp, ctypes.c_char_p, ctypes.c_char_p, P(u64)]),
         "virg_gpu_table_read_ceiling": (i, [vp, P(ctypes.c_int), u, u, u, P(ctypes.c_double),
                                             P(ctypes.c_ulonglong)]),
         "virg_gpu_query": (i, [vp, vp, vp, P(vp)]),

@@ -18,7 +18,7 @@ BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["vm_kernel.cu", "engine.cu", "batch.cu", "stream.cu", "dropin.cu", "noalloc.cu", "serve.cu",
-           "ceiling.cu", "tunecache.cpp", "estimate.cpp", "program.cpp", "sqlc.cpp"]
+           "ceiling.cu", "tunecache.cpp", "estimate.cpp", "ingest.cu", "program.cpp", "sqlc.cpp"]
 EXTRA_SOURCES: List[str] = []
 
 FLAGS = [

@@ -147,7 +147,7 @@ void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode)
 	uint32_t sel = 0, row = 0;
 	for (uint32_t i = 0; i < P.nvec; i++) {
 		if (P.vec_compact[i]) {
-			pp.vec_off[i] = sel;
+			pp.vec_off[i] = sel;  /* re-laid by desc_fill for the launch's unit size */
 			sel += kUnitE * P.vec_stride[i];
 		} else {
 			pp.vec_off[i] = row;
@@ -157,16 +157,15 @@ void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode)
 	}
 }
 
-/* the launch geometry of a shape whose compute warps hold sel_bpr and
- * row_bpr bytes of vectors per row; stages == 0 takes as many stages as fit
- * the shared memory left per CTA */
-int geom_make(const Shape &s0, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gather_bpr, int smem_block, int smem_sm,
-	Geom *g)
+/* geom_make for units of `ub` batches */
+static int geom_make1(const Shape &s0, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gather_bpr, int smem_block,
+	int smem_sm, uint32_t ub, Geom *g)
 {
 	Shape s = s0;
 	VGPU_CHECK(shape_supported(s), "unsupported launch shape: %u compute threads", s.threads);
 	VGPU_CHECK(s.stage_kb >= 1 && s.stage_kb <= 192, "stage size %u KB out of range", s.stage_kb);
-	g->wl = warp_layout(sel_bpr, row_bpr, gather_bpr);
+	g->ub = ub;
+	g->wl = warp_layout(sel_bpr, row_bpr, gather_bpr, ub);
 	g->stage_area = (uint32_t)align_up(kWarpArea + (size_t)s.warps() * g->wl.bytes, 128);
 	const unsigned ctas = s.ctas_per_sm ? s.ctas_per_sm : 1;
 	/* 1 KB of an SM's shared memory is reserved per resident CTA */
@@ -180,6 +179,23 @@ int geom_make(const Shape &s0, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gath
 		return 0;
 	g->shape = s;
 	g->smem = g->stage_area + (size_t)s.stages * s.stage_bytes();
+	return 1;
+}
+
+/* the launch geometry of a shape whose compute warps hold sel_bpr and
+ * row_bpr bytes of vectors per row; stages == 0 takes as many stages as fit
+ * the shared memory left per CTA */
+int geom_make(const Shape &s, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gather_bpr, int smem_block, int smem_sm,
+	Geom *g, uint32_t ub_max)
+{
+	Geom one;
+	if (!geom_make1(s, sel_bpr, row_bpr, gather_bpr, smem_block, smem_sm, 1, &one))
+		return 0;
+	*g = one;
+	Geom two;
+	if (ub_max >= 2 && geom_make1(s, sel_bpr, row_bpr, gather_bpr, smem_block, smem_sm, 2, &two) &&
+		(two.shape.stages >= one.shape.stages || two.shape.stages >= 3))
+		*g = two;
 	return 1;
 }
 
@@ -245,7 +261,7 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 		/* one full entry per chunk; the staged columns of a batch are its
 		 * 32 kBatchE gathered entries, in the warp's gather area */
 		const uint32_t gchunk = chunk_cap;
-		load_set(d.full_set, P, pp.full_cols, pp.nfull, kUnitE);
+		load_set(d.full_set, P, pp.full_cols, pp.nfull, kBatchRows * g.ub);
 		d.full_set.rows = gchunk;
 		d.chunk_rows = gchunk;
 		load_set(d.count_set, P, pp.count_cols, pp.ncount, tile_rows(pp.count_bpr, stage, gchunk));
@@ -269,6 +285,13 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 	d.nfilter = P.nfilter;
 	d.nuops = P.nuops;
 	d.nout = P.nout;
+	/* selection-indexed vectors over the launch's unit size */
+	uint32_t sel_off[kMaxRegs] = {0};
+	for (uint32_t i = 0, at = 0; i < P.nvec; i++)
+		if (P.vec_compact[i]) {
+			sel_off[i] = at;
+			at += kBatchRows * g.ub * P.vec_stride[i];
+		}
 	/* operand descriptors over one phase's layout (bad: a column the phase
 	 * does not stage, never read in that phase) */
 	auto od = [&](uint8_t cls, uint8_t idx, const LoadSet &ls, const uint8_t *cols, uint32_t n, bool *bad) -> uint32_t {
@@ -280,7 +303,7 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 			return OD_STAGE;
 		}
 		if (cls == OC_VEC)
-			return (P.vec_compact[idx] ? OD_SELVEC : OD_ROWVEC) | pp.vec_off[idx];
+			return P.vec_compact[idx] ? (OD_SELVEC | sel_off[idx]) : (OD_ROWVEC | pp.vec_off[idx]);
 		return OD_SCALAR | (uint32_t)(offsetof(QDesc, consts) + idx * 8u);
 	};
 	/* a record over one phase's layout; operand fields the uop does not use
@@ -342,6 +365,7 @@ KParams geom_params(const Geom &g)
 	kp.sel_off = g.wl.sel_off;
 	kp.gat_off = g.wl.gat_off;
 	kp.row_off = g.wl.row_off;
+	kp.unit_batches = g.ub;
 	return kp;
 }
 

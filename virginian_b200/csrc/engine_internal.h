@@ -144,6 +144,7 @@ struct ProgPlan {
 struct Geom {
 	Shape shape;
 	WarpLayout wl;
+	uint32_t ub;                  /* batches a full-phase unit may hold */
 	uint32_t stage_area;
 	size_t smem;
 };
@@ -161,8 +162,10 @@ struct Plan {
 /* full_mode: as Shape::full_mode (1: gather from device memory where the
  * program allows it) */
 void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode = 0);
+/* ub_max: the most batches a full-phase unit may hold (two-batch units are
+ * taken when the warp areas for them leave as many data buffers, or three) */
 int geom_make(const Shape &s, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gather_bpr, int smem_block, int smem_sm,
-	Geom *g);
+	Geom *g, uint32_t ub_max = kUnitBatches);
 int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uint32_t chunk_cap);
 uint64_t chunk_prefix(const uint32_t *seg_rows, uint32_t nsegs, uint32_t chunk_rows, uint32_t *pre);
 KParams geom_params(const Geom &g);

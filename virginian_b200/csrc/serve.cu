@@ -209,7 +209,7 @@ int serve_layout(virg_serve *s)
 		for (unsigned kb : {48u, 40u, 32u, 24u, 16u, 8u}) {
 			Shape sh = {256, std::max(kb, min_kb), 0, 1, kServeChunkRows, 0};
 			if (geom_make(sh, s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes, 0u, e->smem_optin,
-					e->smem_sm, &s->geom) && s->geom.shape.stages >= min_stages) {
+					e->smem_sm, &s->geom, 1) && s->geom.shape.stages >= min_stages) {
 				fit = true;
 				break;
 			}

@@ -69,16 +69,16 @@ static_assert(kChunkSlots >= kCountAhead + 2, "slots for the chunks in flight");
 #ifndef VGPU_BATCH_E
 #define VGPU_BATCH_E 4
 #endif
-#ifndef VGPU_UNIT_BATCHES
-#define VGPU_UNIT_BATCHES 1
-#endif
 constexpr unsigned kCountGroup = VGPU_COUNT_GROUP;
 constexpr unsigned kFullGroup = VGPU_FULL_GROUP;
 constexpr unsigned kBatchE = VGPU_BATCH_E;
-/* a full-phase unit: kUnitBatches batches of 32 kBatchE selected rows, each
- * op run over all of them before the next op */
-constexpr unsigned kUnitBatches = VGPU_UNIT_BATCHES;
-constexpr unsigned kUnitE = 32 * kBatchE * kUnitBatches;
+/* a full-phase unit: one or (at most) kUnitBatches batches of 32 kBatchE
+ * selected rows, each op run over all of them before the next op; a launch
+ * whose warp areas hold two batches' vectors uses two-batch units for
+ * entries with more than one batch of selected rows */
+constexpr unsigned kUnitBatches = 2;
+constexpr unsigned kBatchRows = 32 * kBatchE;
+constexpr unsigned kUnitE = kBatchRows * kUnitBatches;
 static_assert(32 * kBatchE <= kCountGroup * kBlockRows, "a batch within a group");
 static_assert(kUnitE <= 2 * kFullGroup * kBlockRows / 2, "a unit's list within the list area");
 
@@ -143,12 +143,14 @@ constexpr unsigned kWarpArea = kSlotArea + kChunkSlots * kSlotBytes;
 struct WarpLayout {
 	uint32_t sel_off, gat_off, row_off, bytes;
 };
-inline WarpLayout warp_layout(unsigned sel_bytes_per_row, unsigned row_bytes_per_row, unsigned gather_bytes_per_row)
+inline WarpLayout warp_layout(unsigned sel_bytes_per_row, unsigned row_bytes_per_row, unsigned gather_bytes_per_row,
+	unsigned unit_batches)
 {
 	WarpLayout w;
+	const unsigned ue = kBatchRows * unit_batches;
 	w.sel_off = 2u * kFullGroup * kBlockRows;
-	w.gat_off = w.sel_off + (kUnitE * sel_bytes_per_row + 127u) / 128u * 128u;
-	w.row_off = w.gat_off + (kUnitE * gather_bytes_per_row + 127u) / 128u * 128u;
+	w.gat_off = w.sel_off + (ue * sel_bytes_per_row + 127u) / 128u * 128u;
+	w.row_off = w.gat_off + (ue * gather_bytes_per_row + 127u) / 128u * 128u;
 	w.bytes = w.row_off + (kCountGroup * kBlockRows * row_bytes_per_row + 127u) / 128u * 128u;
 	return w;
 }
@@ -185,6 +187,7 @@ struct KParams {
 	uint32_t stage_area;            /* smem offset of buffer 0 */
 	uint32_t warp_bytes;            /* stride between compute warps' areas */
 	uint32_t sel_off, gat_off, row_off;  /* areas within a compute warp's area */
+	uint32_t unit_batches = 1;      /* batches the warp areas hold (1 or kUnitBatches) */
 	/* look-back words: word idx & status_mask, tagged epoch + (idx >> status_shift);
 	 * a launch with a word per work item uses ~0 and 63 (one tag) */
 	unsigned long long status_mask = ~0ull;

@@ -775,61 +775,62 @@ __device__ __noinline__ uint32_t run_filter(uint32_t ops, uint32_t nf, Bases b, 
 struct UnitRows {
 	uint32_t row[kUnitBatches][kBatchE];
 	uint32_t act[kUnitBatches];  /* entries that exist */
+	uint32_t nb;                 /* batches in use (1 or kUnitBatches) */
 };
 
-template <typename T, int OP>
+template <typename T, int OP, int NB>
 __device__ __forceinline__ void p_math(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
 	const Opnd oa = opnd<sizeof(T)>(rec.y, b), ob = opnd<sizeof(T)>(rec.z, b), od = opnd<sizeof(T)>(rec.w, b);
-	T x[kUnitBatches][kBatchE], y[kUnitBatches][kBatchE];
+	T x[NB][kBatchE], y[NB][kBatchE];
 #pragma unroll
-	for (int s = 0; s < (int)kUnitBatches; s++)
+	for (int s = 0; s < NB; s++)
 #pragma unroll
 		for (int i = 0; i < kBatchE; i++) {
-			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			const uint32_t e = kBatchRows * s + 32u * i + (uint32_t)lane;
 			x[s][i] = SM<T>::ld(oa.addr + (oa.sel ? e : u.row[s][i]) * oa.step);
 			y[s][i] = SM<T>::ld(ob.addr + (ob.sel ? e : u.row[s][i]) * ob.step);
 		}
 #pragma unroll
-	for (int s = 0; s < (int)kUnitBatches; s++)
+	for (int s = 0; s < NB; s++)
 #pragma unroll
 		for (int i = 0; i < kBatchE; i++)
 			if ((u.act[s] >> i) & 1u) {
-				const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+				const uint32_t e = kBatchRows * s + 32u * i + (uint32_t)lane;
 				SM<T>::st(od.addr + (od.sel ? e : u.row[s][i]) * od.step, Math<T, OP>::eval(x[s][i], y[s][i]));
 			}
 }
 
-template <typename T>
+template <typename T, int NB>
 __device__ __forceinline__ void p_copy(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
 	const Opnd oa = opnd<sizeof(T)>(rec.y, b), od = opnd<sizeof(T)>(rec.w, b);
-	T x[kUnitBatches][kBatchE];
+	T x[NB][kBatchE];
 #pragma unroll
-	for (int s = 0; s < (int)kUnitBatches; s++)
+	for (int s = 0; s < NB; s++)
 #pragma unroll
 		for (int i = 0; i < kBatchE; i++) {
-			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			const uint32_t e = kBatchRows * s + 32u * i + (uint32_t)lane;
 			x[s][i] = SM<T>::ld(oa.addr + (oa.sel ? e : u.row[s][i]) * oa.step);
 		}
 #pragma unroll
-	for (int s = 0; s < (int)kUnitBatches; s++)
+	for (int s = 0; s < NB; s++)
 #pragma unroll
 		for (int i = 0; i < kBatchE; i++)
 			if ((u.act[s] >> i) & 1u) {
-				const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+				const uint32_t e = kBatchRows * s + 32u * i + (uint32_t)lane;
 				SM<T>::st(od.addr + (od.sel ? e : u.row[s][i]) * od.step, x[s][i]);
 			}
 }
 
-template <typename T>
+template <typename T, int NB>
 __device__ __forceinline__ void p_math_any(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
 	const uint32_t h = rec.x;
-	if (h_op(h, MO_ADD)) p_math<T, MO_ADD>(rec, b, u, lane);
-	else if (h_op(h, MO_SUB)) p_math<T, MO_SUB>(rec, b, u, lane);
-	else if (h_op(h, MO_MUL)) p_math<T, MO_MUL>(rec, b, u, lane);
-	else p_math<T, MO_DIV>(rec, b, u, lane);
+	if (h_op(h, MO_ADD)) p_math<T, MO_ADD, NB>(rec, b, u, lane);
+	else if (h_op(h, MO_SUB)) p_math<T, MO_SUB, NB>(rec, b, u, lane);
+	else if (h_op(h, MO_MUL)) p_math<T, MO_MUL, NB>(rec, b, u, lane);
+	else p_math<T, MO_DIV, NB>(rec, b, u, lane);
 }
 
 /* one batch of a projection op over 8-byte and char values, out of line,
@@ -882,46 +883,47 @@ __device__ __noinline__ void project_rare(uint4 rec, Bases b, uint4 rows, uint32
 
 /* one projection op over the unit: arithmetic, or a copy (every listed row
  * is active here, so constants and columns are copies) */
+template <int NB>
 __device__ __forceinline__ void project_op(const uint4 &rec, const Bases &b, const UnitRows &u, int lane)
 {
 	static_assert(kBatchE == 4, "project_rare passes a batch's rows as a uint4");
 	const uint32_t h = rec.x;
 	if (h & OK_SETCONST) {
-		p_copy<uint32_t>(rec, b, u, lane);
+		p_copy<uint32_t, NB>(rec, b, u, lane);
 	} else if (!(h_type(h, VT_FLOAT) || h_type(h, VT_INT))) {
 #pragma unroll
-		for (int s = 0; s < (int)kUnitBatches; s++)
+		for (int s = 0; s < NB; s++)
 			project_rare(rec, b, make_uint4(u.row[s][0], u.row[s][1], u.row[s][2], u.row[s][3]), u.act[s],
-				32u * kBatchE * s, lane);
+				kBatchRows * s, lane);
 	} else if (h & OK_MATH) {
-		if (h_type(h, VT_FLOAT)) p_math_any<float>(rec, b, u, lane);
-		else p_math_any<int32_t>(rec, b, u, lane);
+		if (h_type(h, VT_FLOAT)) p_math_any<float, NB>(rec, b, u, lane);
+		else p_math_any<int32_t, NB>(rec, b, u, lane);
 	} else if (h & OK_COPY) {
-		p_copy<uint32_t>(rec, b, u, lane);
+		p_copy<uint32_t, NB>(rec, b, u, lane);
 	}
 }
 
 /* one result column of the unit: entries whose bit is set in in[s] are
  * stored at pos0 + their unit entry */
-template <typename T>
+template <typename T, int NB>
 __device__ __forceinline__ void p_store(uint32_t od, const Bases &b, const UnitRows &u, const uint32_t (&in)[kUnitBatches],
 	T *out, uint64_t pos0, int lane)
 {
 	const Opnd o = opnd<sizeof(T)>(od, b);
-	T v[kUnitBatches][kBatchE];
+	T v[NB][kBatchE];
 #pragma unroll
-	for (int s = 0; s < (int)kUnitBatches; s++)
+	for (int s = 0; s < NB; s++)
 #pragma unroll
 		for (int i = 0; i < kBatchE; i++) {
-			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			const uint32_t e = kBatchRows * s + 32u * i + (uint32_t)lane;
 			v[s][i] = SM<T>::ld(o.addr + (o.sel ? e : u.row[s][i]) * o.step);
 		}
 #pragma unroll
-	for (int s = 0; s < (int)kUnitBatches; s++)
+	for (int s = 0; s < NB; s++)
 #pragma unroll
 		for (int i = 0; i < kBatchE; i++)
 			if ((in[s] >> i) & 1u)
-				out[pos0 + (uint64_t)(32u * kBatchE * s + 32u * i + (uint32_t)lane)] = v[s][i];
+				out[pos0 + (uint64_t)(kBatchRows * s + 32u * i + (uint32_t)lane)] = v[s][i];
 }
 
 /* one batch of a result column of 8-byte or char values, out of line, by value */
@@ -1029,9 +1031,10 @@ __device__ __forceinline__ void gather_batch(const Bases &b, const uint32_t (&gr
 	}
 }
 
-/* the projection and stores of a unit (see UnitRows); entries in in[s]
- * fit the output and are stored at pos0 + their unit entry */
-__device__ __forceinline__ void unit_out(const Bases &b, const UnitRows &u, const uint32_t (&in)[kUnitBatches],
+/* the projection and stores of a unit of NB batches (see UnitRows);
+ * entries in in[s] fit the output and are stored at pos0 + their unit entry */
+template <int NB>
+__device__ __forceinline__ void unit_out_n(const Bases &b, const UnitRows &u, const uint32_t (&in)[kUnitBatches],
 	uint64_t pos0, int lane)
 {
 	const uint32_t ops = b.slot + kQOpsFull;
@@ -1039,34 +1042,45 @@ __device__ __forceinline__ void unit_out(const Bases &b, const UnitRows &u, cons
 	const uint32_t nu = lds_u32(b.slot + kQNUops) - 1u;
 	const uint32_t nout = lds_u32(b.slot + kQNOut);
 	for (uint32_t k = nf; k < nu; k++)
-		project_op(lds_v4(ops + 16u * k), b, u, lane);
+		project_op<NB>(lds_v4(ops + 16u * k), b, u, lane);
 	for (uint32_t j = 0; j < nout; j++) {
 		const uint32_t od = lds_u32(b.slot + kQOdOut + 4 * j);
 		void *out = reinterpret_cast<void *>(lds_u64(b.slot + kQOutPtr + 8 * j));
 		const uint32_t stride = lds_u8(b.slot + kQOutStride + j);
 		if (stride == 4) {
-			p_store<uint32_t>(od, b, u, in, static_cast<uint32_t *>(out), pos0, lane);
+			p_store<uint32_t, NB>(od, b, u, in, static_cast<uint32_t *>(out), pos0, lane);
 		} else {
 #pragma unroll
-			for (int s2 = 0; s2 < (int)kUnitBatches; s2++)
+			for (int s2 = 0; s2 < NB; s2++)
 				p_store_rare(od, b, make_uint4(u.row[s2][0], u.row[s2][1], u.row[s2][2], u.row[s2][3]), in[s2], out,
-					pos0, 32u * kBatchE * s2, stride, lane);
+					pos0, kBatchRows * s2, stride, lane);
 		}
 	}
 }
 
-/* a unit's rows from its selection list (list entry e: the row of unit
- * entry e), the first cnt existing; in[s]: those below the output capacity */
-__device__ __forceinline__ void unit_rows(uint32_t list, uint32_t cnt, uint64_t pos0, uint64_t cap, UnitRows &u,
-	uint32_t (&in)[kUnitBatches], int lane)
+__device__ __forceinline__ void unit_out(const Bases &b, const UnitRows &u, const uint32_t (&in)[kUnitBatches],
+	uint64_t pos0, int lane)
 {
+	if (u.nb == 1)
+		unit_out_n<1>(b, u, in, pos0, lane);
+	else
+		unit_out_n<kUnitBatches>(b, u, in, pos0, lane);
+}
+
+/* a unit's rows from its selection list (list entry e: the row of unit
+ * entry e), the first cnt existing (at most kBatchRows nb); in[s]: those
+ * below the output capacity */
+__device__ __forceinline__ void unit_rows(uint32_t list, uint32_t cnt, uint32_t nb, uint64_t pos0, uint64_t cap,
+	UnitRows &u, uint32_t (&in)[kUnitBatches], int lane)
+{
+	u.nb = nb;
 #pragma unroll
 	for (int s = 0; s < (int)kUnitBatches; s++) {
 		u.act[s] = 0;
 		in[s] = 0;
 #pragma unroll
 		for (int i = 0; i < kBatchE; i++) {
-			const uint32_t e = 32u * kBatchE * s + 32u * i + (uint32_t)lane;
+			const uint32_t e = kBatchRows * s + 32u * i + (uint32_t)lane;
 			const bool a = e < cnt;
 			u.row[s][i] = 0;
 			if (a) {
@@ -1086,7 +1100,8 @@ __device__ __forceinline__ void unit_rows(uint32_t list, uint32_t cnt, uint64_t 
  * run again for the register vectors the results read; b.stage is the
  * staged tile and b.blk_row0 the group's first tile row.  Returns false on
  * an output overflow. */
-__device__ __forceinline__ bool refilter_group(const Bases &b, uint32_t list, uint32_t blk, uint32_t nrows, int lane)
+__device__ __forceinline__ bool refilter_group(const Bases &b, uint32_t list, uint32_t blk, uint32_t nrows, uint32_t ub,
+	int lane)
 {
 	/* lane l holds validity word l of the group (32 rows) */
 	const uint32_t nw = (nrows + 31) / 32;
@@ -1119,10 +1134,12 @@ __device__ __forceinline__ bool refilter_group(const Bases &b, uint32_t list, ui
 	const uint64_t off = lds_u64(b.slot + kSlotBlockOff + 8u * blk);
 	const uint64_t cap = lds_u64(b.slot + kQCapacity);
 	bool ok = true;
-	for (uint32_t base = 0; base < n; base += kUnitE) {
+	for (uint32_t base = 0, step = 0; base < n; base += step) {
+		const uint32_t nb = ub > 1 && n - base > kBatchRows ? kUnitBatches : 1u;
+		step = kBatchRows * nb;
 		UnitRows u;
 		uint32_t in[kUnitBatches];
-		unit_rows(list + 2 * base, n - base, off + base, cap, u, in, lane);
+		unit_rows(list + 2 * base, min(n - base, step), nb, off + base, cap, u, in, lane);
 #pragma unroll
 		for (int s2 = 0; s2 < (int)kUnitBatches; s2++)
 			ok = ok && u.act[s2] == in[s2];
@@ -1143,19 +1160,19 @@ __device__ __forceinline__ uint32_t entry_selected(uint32_t slot, uint32_t blk0,
 }
 
 /* FM_BITMAP / FM_GATHER full phase: unit j of an entry's selected rows
- * (ranks [kUnitE j, ...) of the nsel rows of chunk blocks
+ * (ranks [kBatchRows nb j, ...) of the nsel rows of chunk blocks
  * [blk0, blk0 + nblk), whose first is stored at off0).  The warp lists the
  * unit's rows from the bitmap, starting at the block that holds its first
  * rank, then reads them from the staged tile in place (b.stage the tile,
  * rows counted from its first row) or gathers them from device memory into
  * the warp's gather area.  Returns false on an output overflow. */
 __device__ __forceinline__ bool full_unit(Bases b, uint32_t list, uint32_t gat, uint32_t blk0, uint32_t nblk,
-	uint32_t j, uint32_t nsel, uint64_t off0, uint32_t mode, int lane)
+	uint32_t j, uint32_t nb, uint32_t nsel, uint64_t off0, uint32_t mode, int lane)
 {
-	const uint32_t r0 = kUnitE * j;
+	const uint32_t r0 = kBatchRows * nb * j;
 	if (r0 >= nsel)
 		return true;  /* an entry with no selected rows: nothing to do */
-	const uint32_t cnt = min(kUnitE, nsel - r0);
+	const uint32_t cnt = min(kBatchRows * nb, nsel - r0);
 	/* the block holding rank r0: lane l looks at block blk0 + l */
 	uint32_t bo = 0, bc = 0;
 	if ((uint32_t)lane < nblk) {
@@ -1217,7 +1234,7 @@ __device__ __forceinline__ bool full_unit(Bases b, uint32_t list, uint32_t gat, 
 	const uint64_t pos0 = off0 + r0;
 	UnitRows u;
 	uint32_t in[kUnitBatches];
-	unit_rows(list, cnt, pos0, cap, u, in, lane);
+	unit_rows(list, cnt, nb, pos0, cap, u, in, lane);
 	b.blk_row0 = 0;
 	if (mode == FM_GATHER) {
 		/* gathered values are indexed by unit entry; the chunk row of an
@@ -1225,13 +1242,15 @@ __device__ __forceinline__ bool full_unit(Bases b, uint32_t list, uint32_t gat, 
 		b.stage = gat;
 #pragma unroll
 		for (int s2 = 0; s2 < (int)kUnitBatches; s2++) {
+			if ((uint32_t)s2 >= nb)
+				break;
 			uint32_t grow[kBatchE];
 #pragma unroll
 			for (int i = 0; i < kBatchE; i++) {
 				grow[i] = blk0 * kBlockRows + u.row[s2][i];
-				u.row[s2][i] = 32u * kBatchE * s2 + 32u * i + (uint32_t)lane;
+				u.row[s2][i] = kBatchRows * s2 + 32u * i + (uint32_t)lane;
 			}
-			gather_batch(b, grow, 32u * kBatchE * s2, lane);
+			gather_batch(b, grow, kBatchRows * s2, lane);
 		}
 		__syncwarp();
 	}
@@ -1902,7 +1921,7 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 	};
 	/* the entry of the warp's last unit, kept for the fast claim below */
 	uint32_t k = 0, n = 0, kind = 0, slot = 0, seq = 0, row0 = 0, nrows = 0, buf = 0, mode = FM_BITMAP;
-	uint32_t nsel = 0;
+	uint32_t nsel = 0, ub = 1;
 	uint64_t off0 = 0;
 	bool have = false;
 	for (;;) {
@@ -1992,7 +2011,10 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					n = (nblk + kCountGroup - 1) / kCountGroup;
 				} else {
 					nsel = entry_selected(b.slot, row0 / kBlockRows, nblk, &off0);
-					n = max(1u, (nsel + kUnitE - 1) / kUnitE);
+					/* two-batch units for entries with more than a batch of
+					 * rows, where the launch's warp areas hold them */
+					ub = kp.unit_batches > 1 && nsel > kBatchRows ? kUnitBatches : 1u;
+					n = max(1u, (nsel + kBatchRows * ub - 1) / (kBatchRows * ub));
 				}
 			}
 			const uint32_t taken = c & 0xffffu;
@@ -2034,10 +2056,10 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					min((uint32_t)(kCountGroup * kBlockRows), nrows - r), lane);
 			else
 				ok = refilter_group(b, list, blk0 + j * kCountGroup, min((uint32_t)(kCountGroup * kBlockRows), nrows - r),
-					lane);
+					kp.unit_batches, lane);
 		} else {
 			b.stage = tile;
-			ok = full_unit(b, list, gat, blk0, nblk, j, nsel, off0, mode, lane);
+			ok = full_unit(b, list, gat, blk0, nblk, j, ub, nsel, off0, mode, lane);
 		}
 		/* a serving session reports rows beyond capacity in the query's
 		 * completion record instead */
