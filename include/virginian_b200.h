@@ -294,7 +294,7 @@ void *virg_gpu_engine_stream(virg_gpu_engine *e);
 /* device error word set by bounded waits inside kernels (0 = none); reading
  * it synchronises the engine stream and clears it */
 int virg_gpu_engine_check(virg_gpu_engine *e, unsigned *device_error);
-/* launch shape: compute threads per CTA (256, 320, 448 or 512; the CTA adds a
+/* launch shape: compute threads per CTA (128, 256, 320, 448 or 512; the CTA adds a
  * producer and a look-back warp), bytes per staging buffer in KB, number of
  * staging buffers, CTAs per SM; 0 in a field keeps the automatic choice */
 int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,

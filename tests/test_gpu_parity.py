@@ -110,7 +110,8 @@ def test_query_host_pieces_and_chunks(oracle_mod, engine):
 @pytest.mark.parametrize("shape", [(320, 16, 0, 1, 1024, 0), (448, 32, 3, 1, 2048, 0), (256, 16, 0, 1, 8192, 0),
                                    (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 0), (512, 24, 0, 1, 2048, 0),
                                    (512, 32, 4, 1, 8192, 0), (256, 8, 0, 1, 256, 0), (256, 24, 0, 1, 4096, 1),
-                                   (320, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1), (448, 16, 0, 1, 1024, 1)])
+                                   (320, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1), (448, 16, 0, 1, 1024, 1),
+                                   (128, 24, 0, 2, 4096, 0), (128, 32, 0, 2, 8192, 1)])
 def test_every_launch_shape(data_a, engine, shape):
     db, _, t = data_a
     engine.set_shape(*shape)

@@ -738,6 +738,11 @@ std::vector<Shape> tune_candidates()
 				c.push_back(Shape{threads, kb, 0, 1, chunk, 0});
 	for (unsigned kb : {16u, 32u})
 		c.push_back(Shape{256, kb, 0, 1, 8192, 1});
+	/* two CTAs of four compute warps per SM: two producers and look-back
+	 * warps per SM */
+	for (unsigned kb : {24u, 32u})
+		for (unsigned chunk : {4096u, 8192u})
+			c.push_back(Shape{128, kb, 0, 2, chunk, 0});
 	return c;
 }
 }  // namespace vgpu
@@ -812,7 +817,7 @@ extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 	VGPU_CHECK(e != nullptr, "null engine");
 	if (threads) {
 		Shape s = {threads, 32, 2, 1, 0, 0};
-		VGPU_CHECK(shape_supported(s), "unsupported shape: %u compute threads (256, 320, 448 or 512)", threads);
+		VGPU_CHECK(shape_supported(s), "unsupported shape: %u compute threads (128, 256, 320, 448 or 512)", threads);
 	}
 	VGPU_CHECK(stage_kb <= 192, "stage size %u KB out of range", stage_kb);
 	VGPU_CHECK(stages <= kMaxStages, "at most %u stages", kMaxStages);

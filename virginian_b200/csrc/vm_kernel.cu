@@ -1135,7 +1135,7 @@ __device__ __forceinline__ bool refilter_group(const Bases &b, uint32_t list, ui
 	const uint64_t cap = lds_u64(b.slot + kQCapacity);
 	bool ok = true;
 	for (uint32_t base = 0, step = 0; base < n; base += step) {
-		const uint32_t nb = ub > 1 && n - base > kBatchRows ? kUnitBatches : 1u;
+		const uint32_t nb = ub > 1 && n - base >= kUnitE ? kUnitBatches : 1u;
 		step = kBatchRows * nb;
 		UnitRows u;
 		uint32_t in[kUnitBatches];
@@ -2011,9 +2011,11 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					n = (nblk + kCountGroup - 1) / kCountGroup;
 				} else {
 					nsel = entry_selected(b.slot, row0 / kBlockRows, nblk, &off0);
-					/* two-batch units for entries with more than a batch of
-					 * rows, where the launch's warp areas hold them */
-					ub = kp.unit_batches > 1 && nsel > kBatchRows ? kUnitBatches : 1u;
+					/* two-batch units for entries with at least two such
+					 * units of rows (dense entries: the op dispatch is shared
+					 * by twice the rows, and units still run in parallel),
+					 * where the launch's warp areas hold them */
+					ub = kp.unit_batches > 1 && nsel >= 2 * kUnitE ? kUnitBatches : 1u;
 					n = max(1u, (nsel + kBatchRows * ub - 1) / (kBatchRows * ub));
 				}
 			}
@@ -2174,7 +2176,7 @@ static int occ_t(size_t smem, int *ctas)
 	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, 32 * (W + 2), smem) == cudaSuccess;
 }
 
-#define VGPU_WARPS(X) X(8) X(10) X(14) X(16)
+#define VGPU_WARPS(X) X(4) X(8) X(10) X(14) X(16)
 
 int shape_supported(const Shape &s)
 {
