@@ -305,7 +305,11 @@ int virg_gpu_engine_set_chunk_rows(virg_gpu_engine *e, unsigned rows);
 /* how the full phase reads the columns the results need: 0 (default)
  * stages tiles of them and reads the selected rows in place, 1 loads only
  * the selected rows' values straight from device memory (programs whose
- * results read at most 32 bytes per row) */
+ * results read at most 32 bytes per row), 2 runs the projection over every
+ * row of a staged group and stores the rows that pass at their ranks
+ * (programs whose computed values take at most 16 bytes per row; suits
+ * filters that keep most rows).  Programs outside a mode's bounds, and
+ * launches whose shape leaves no room for mode 2, keep mode 0. */
 int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode);
 /* record CUDA events around each of the next kernel launches in a ring of
  * `slots` entries (0 turns it off) */

@@ -76,6 +76,25 @@ def test_config2_selectivity_sweep(data_a, sel):
     assert abs(frac - sel) < max(0.02, sel * 0.2)
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+def test_full_modes_across_selectivity(data_a, engine, mode):
+    """The gathering and dense full phases on the config-2 query at low,
+    middle and high selectivity and on the query suite."""
+    db, cols, t = data_a
+    engine.set_shape(full_mode=mode)
+    try:
+        for sel in (0.01, 0.5, 0.99):
+            q = 1 - (1 - sel) ** 0.5
+            sql = config2(float(np.quantile(cols["uniformf"], q)), float(np.quantile(cols["normalf20"], 1 - q)))
+            got, want, _ = run_both(db, t, sql, TYPES_A)
+            assert_same_stream(got, want, f"mode={mode} {sql}")
+        for sql in SUITE + EXTRA:
+            got, want, _ = run_both(db, t, sql, TYPES_A)
+            assert_same_stream(got, want, f"mode={mode} {sql}")
+    finally:
+        engine.set_shape(0, 0, 0, 0, 0, 0)
+
+
 def test_query_host_end_to_end(data_a, engine):
     db, cols, _ = data_a
     p = program(db, CONFIG1, TYPES_A)
@@ -111,7 +130,8 @@ def test_query_host_pieces_and_chunks(oracle_mod, engine):
                                    (256, 32, 0, 1, 4096, 0), (256, 48, 2, 2, 4096, 0), (512, 24, 0, 1, 2048, 0),
                                    (512, 32, 4, 1, 8192, 0), (256, 8, 0, 1, 256, 0), (256, 24, 0, 1, 4096, 1),
                                    (320, 48, 0, 1, 8192, 1), (256, 8, 0, 1, 256, 1), (448, 16, 0, 1, 1024, 1),
-                                   (128, 24, 0, 2, 4096, 0), (128, 32, 0, 2, 8192, 1)])
+                                   (128, 24, 0, 2, 4096, 0), (128, 32, 0, 2, 8192, 1), (256, 32, 0, 1, 4096, 2),
+                                   (128, 24, 0, 2, 8192, 2), (256, 16, 0, 1, 1024, 2)])
 def test_every_launch_shape(data_a, engine, shape):
     db, _, t = data_a
     engine.set_shape(*shape)
@@ -136,7 +156,7 @@ REFILTER = ["select uniformf + normalf5 as s, id from test where uniformf + norm
             "select id, uniformi - normali5 as d, normalf20 from test where uniformi - normali5 < 20 or normalf20 > 30.0"]
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 def test_filter_vectors_in_results(data_a, engine, mode):
     db, _, t = data_a
     engine.set_shape(full_mode=mode)
@@ -190,7 +210,7 @@ def test_int64_and_double_columns(oracle_mod, engine):
                     # 36 result bytes per row: read from the staged tile in place
                     "select id, uniforml, normald, uniformi, uniformf, normalf5, normalf20 from test "
                     "where normali20 > 10 or uniformf < 5.0"]:
-            for mode in (0, 1):
+            for mode in (0, 1, 2):
                 engine.set_shape(full_mode=mode)
                 try:
                     got, want, _ = run_both(db, t, sql, TYPES_B)
@@ -252,7 +272,7 @@ def test_streamed_matches_oracle(oracle_mod, engine, per_chunk):
 
 
 @pytest.mark.parametrize("k", range(len(HAND_PROGRAMS)))
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 def test_hand_programs_and_or_not(oracle_mod, engine, k, mode):
     """Hand-assembled programs with And, Or and Not (which the code
     generator never emits) on both VMs, over a table with many zeros, NaN and

@@ -137,23 +137,30 @@ void plan_program(const Program &P, ProgPlan &pp, unsigned full_mode)
 	}
 	/* full_mode 1: the full phase gathers the selected rows' values from
 	 * device memory into each compute warp's area, unless they are many
-	 * bytes per row */
+	 * bytes per row; full_mode 2: it runs the projection over whole groups */
 	if (pp.mode == FM_BITMAP && pp.full_bpr <= kGatherMaxBpr && full_mode == 1) {
 		pp.mode = FM_GATHER;
 		pp.gather_bpr = pp.full_bpr;
 	}
+	if (pp.mode == FM_BITMAP && full_mode == 2) {
+		uint32_t dense_row = 0;
+		for (uint32_t i = 0; i < P.nvec; i++)
+			dense_row += P.vec_stride[i];
+		if (dense_row <= kDenseMaxRowBpr)
+			pp.mode = FM_DENSE;
+	}
 	/* selection vectors hold a projection batch's entries, row vectors a
-	 * count group's rows */
+	 * count group's rows (every vector is a row vector in FM_DENSE) */
 	uint32_t sel = 0, row = 0;
 	for (uint32_t i = 0; i < P.nvec; i++) {
-		if (P.vec_compact[i]) {
+		if (P.vec_compact[i] && pp.mode != FM_DENSE) {
 			pp.vec_off[i] = sel;  /* re-laid by desc_fill for the launch's unit size */
 			sel += kUnitE * P.vec_stride[i];
 		} else {
 			pp.vec_off[i] = row;
 			row += kCountGroup * kBlockRows * P.vec_stride[i];
 		}
-		(P.vec_compact[i] ? pp.sel_bpr : pp.row_bpr) += P.vec_stride[i];
+		(P.vec_compact[i] && pp.mode != FM_DENSE ? pp.sel_bpr : pp.row_bpr) += P.vec_stride[i];
 	}
 }
 
@@ -200,11 +207,16 @@ int geom_make(const Shape &s, uint32_t sel_bpr, uint32_t row_bpr, uint32_t gathe
 }
 
 /* a phase's staged columns for tiles of `rows` rows */
-static void load_set(LoadSet &ls, const Program &P, const uint8_t *cols, uint32_t n, uint32_t rows)
+/* (group rows: a staged tile's column is laid out for whole groups of
+ * kCountGroup blocks, since a group's lanes read all of its rows, valid or
+ * not; 0 for a gather area) */
+static void load_set(LoadSet &ls, const Program &P, const uint8_t *cols, uint32_t n, uint32_t rows,
+	uint32_t group_rows = kCountGroup * kBlockRows)
 {
 	memset(&ls, 0, sizeof(ls));
 	ls.n = n;
 	ls.rows = rows;
+	const uint32_t laid = group_rows ? (rows + group_rows - 1) / group_rows * group_rows : rows;
 	uint32_t off = 0;
 	for (uint32_t i = 0; i < n; i++) {
 		const uint32_t slot = cols[i];
@@ -212,7 +224,7 @@ static void load_set(LoadSet &ls, const Program &P, const uint8_t *cols, uint32_
 		ls.stride[i] = P.load_stride[slot];
 		ls.off[i] = off;
 		ls.bytes_per_row += P.load_stride[slot];
-		off += (uint32_t)align_up((size_t)rows * P.load_stride[slot], 128);
+		off += (uint32_t)align_up((size_t)laid * P.load_stride[slot], 128);
 	}
 }
 
@@ -222,7 +234,10 @@ static uint32_t tile_rows(uint32_t bpr, uint32_t stage, uint32_t cap)
 {
 	if (bpr == 0)
 		return cap;
-	return std::min<uint32_t>(cap, stage / bpr / kBlockRows * kBlockRows);
+	/* whole groups of kCountGroup blocks (a tile's columns are laid out for
+	 * whole groups); 0 if not one group fits */
+	constexpr uint32_t kGroupRows = kCountGroup * kBlockRows;
+	return std::min<uint32_t>(cap, stage / bpr / kGroupRows * kGroupRows);
 }
 
 /* the head word of a uop's record (one-hot kind, type and operator) */
@@ -250,23 +265,23 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 	chunk_cap = std::max<uint32_t>(kBlockRows, std::min<uint32_t>(chunk_cap, kMaxChunkRows) / kBlockRows * kBlockRows);
 	const uint32_t tf = tile_rows(pp.full_bpr, stage, chunk_cap);
 	VGPU_CHECK(tf >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the results read",
-		g.shape.stage_kb, kBlockRows, pp.full_bpr);
+		g.shape.stage_kb, kCountGroup * kBlockRows, pp.full_bpr);
 	const uint32_t chunk = std::max(tf, chunk_cap / tf * tf);
 	const uint32_t tc = tile_rows(pp.count_bpr, stage, chunk);
 	VGPU_CHECK(tc >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the filter reads",
-		g.shape.stage_kb, kBlockRows, pp.count_bpr);
+		g.shape.stage_kb, kCountGroup * kBlockRows, pp.count_bpr);
 	d.prog = P;
 	load_set(d.count_set, P, pp.count_cols, pp.ncount, tc);
 	if (pp.mode == FM_GATHER) {
 		/* one full entry per chunk; the staged columns of a batch are its
 		 * 32 kBatchE gathered entries, in the warp's gather area */
 		const uint32_t gchunk = chunk_cap;
-		load_set(d.full_set, P, pp.full_cols, pp.nfull, kBatchRows * g.ub);
+		load_set(d.full_set, P, pp.full_cols, pp.nfull, kBatchRows * g.ub, 0);
 		d.full_set.rows = gchunk;
 		d.chunk_rows = gchunk;
 		load_set(d.count_set, P, pp.count_cols, pp.ncount, tile_rows(pp.count_bpr, stage, gchunk));
 		VGPU_CHECK(d.count_set.rows >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the filter reads",
-			g.shape.stage_kb, kBlockRows, pp.count_bpr);
+			g.shape.stage_kb, kCountGroup * kBlockRows, pp.count_bpr);
 		d.gather_n = d.full_set.n;
 		for (uint32_t i = 0; i < d.full_set.n; i++) {
 			d.gather_stride[i] = d.full_set.stride[i];
@@ -287,8 +302,9 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 	d.nout = P.nout;
 	/* selection-indexed vectors over the launch's unit size */
 	uint32_t sel_off[kMaxRegs] = {0};
+	const bool dense = pp.mode == FM_DENSE;
 	for (uint32_t i = 0, at = 0; i < P.nvec; i++)
-		if (P.vec_compact[i]) {
+		if (P.vec_compact[i] && !dense) {
 			sel_off[i] = at;
 			at += kBatchRows * g.ub * P.vec_stride[i];
 		}
@@ -303,7 +319,7 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 			return OD_STAGE;
 		}
 		if (cls == OC_VEC)
-			return P.vec_compact[idx] ? (OD_SELVEC | sel_off[idx]) : (OD_ROWVEC | pp.vec_off[idx]);
+			return P.vec_compact[idx] && !dense ? (OD_SELVEC | sel_off[idx]) : (OD_ROWVEC | pp.vec_off[idx]);
 		return OD_SCALAR | (uint32_t)(offsetof(QDesc, consts) + idx * 8u);
 	};
 	/* a record over one phase's layout; operand fields the uop does not use
@@ -395,11 +411,19 @@ int choose_shape(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, Geom *g
 	s.stages = e->pref.stages;
 	s.ctas_per_sm = e->pref.ctas_per_sm;
 	s.chunk_rows = e->pref.chunk_rows;
-	/* a stage holds at least one block of the widest phase */
+	/* a stage holds at least one group of kCountGroup blocks of the widest phase */
 	if (!e->pref.stage_kb)
-		s.stage_kb = std::max<unsigned>(s.stage_kb, (kBlockRows * bpr + 1023) / 1024);
+		s.stage_kb = std::max<unsigned>(s.stage_kb, (kCountGroup * kBlockRows * bpr + 1023) / 1024);
 	if (geom_make(s, sel, row, gat, e->smem_optin, e->smem_sm, g))
 		return 1;
+	/* a dense full phase whose row vectors leave no room for two stages
+	 * falls back to the in-place one */
+	if (s.full_mode == 2) {
+		s.full_mode = 0;
+		launch_needs(qs, 0, &sel, &row, &gat, &bpr);
+		if (geom_make(s, sel, row, gat, e->smem_optin, e->smem_sm, g))
+			return 1;
+	}
 	VGPU_FAIL("launch shape (%u threads, %u KB x %u stages, %u CTAs per SM) does not fit shared memory",
 		s.threads, s.stage_kb, s.stages, s.ctas_per_sm);
 }
@@ -735,14 +759,16 @@ std::vector<Shape> tune_candidates()
 	for (unsigned threads : {256u, 320u, 448u})
 		for (unsigned kb : {24u, 32u, 40u, 48u})
 			for (unsigned chunk : {4096u, 8192u})
-				c.push_back(Shape{threads, kb, 0, 1, chunk, 0});
+				for (unsigned mode : {0u, 2u})
+					c.push_back(Shape{threads, kb, 0, 1, chunk, mode});
 	for (unsigned kb : {16u, 32u})
 		c.push_back(Shape{256, kb, 0, 1, 8192, 1});
 	/* two CTAs of four compute warps per SM: two producers and look-back
 	 * warps per SM */
 	for (unsigned kb : {24u, 32u})
 		for (unsigned chunk : {4096u, 8192u})
-			c.push_back(Shape{128, kb, 0, 2, chunk, 0});
+			for (unsigned mode : {0u, 2u})
+				c.push_back(Shape{128, kb, 0, 2, chunk, mode});
 	return c;
 }
 }  // namespace vgpu
@@ -831,7 +857,7 @@ extern "C" int virg_gpu_engine_set_shape(virg_gpu_engine *e, unsigned threads,
 extern "C" int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode)
 {
 	VGPU_CHECK(e != nullptr, "null engine");
-	VGPU_CHECK(mode <= 1, "full-phase mode %u: 0 in place, 1 gather", mode);
+	VGPU_CHECK(mode <= 2, "full-phase mode %u: 0 in place, 1 gather, 2 dense", mode);
 	e->pref.full_mode = mode;
 	return 1;
 }

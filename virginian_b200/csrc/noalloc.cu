@@ -114,7 +114,7 @@ int setup_device(int dev, DeviceSetup *out)
 int pick_geom(const ProgPlan &pp, const DeviceSetup &ds, Geom *g)
 {
 	const uint32_t bpr = std::max(pp.count_bpr, pp.mode == FM_GATHER ? 0u : pp.full_bpr);
-	Shape s = {256, std::max<unsigned>(32, (kBlockRows * bpr + 1023) / 1024), 0, 1, kPreallocChunkRows, 0};
+	Shape s = {256, std::max<unsigned>(32, (kCountGroup * kBlockRows * bpr + 1023) / 1024), 0, 1, kPreallocChunkRows, 0};
 	VGPU_CHECK(geom_make(s, pp.sel_bpr, pp.row_bpr, pp.gather_bpr, ds.smem_block, ds.smem_sm, g),
 		"program needs more shared memory than the device offers");
 	return 1;

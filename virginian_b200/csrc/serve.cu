@@ -200,10 +200,10 @@ int serve_layout(virg_serve *s)
 {
 	virg_gpu_engine *e = s->e;
 	/* eight compute warps, one CTA per SM, the largest data buffers (48 KB
-	 * down to 8 KB, each holding a block of the widest staging the session
+	 * down to 8 KB, each holding a group of blocks of the widest staging the session
 	 * admits) of which at least two fit beside the warps' vector areas.  The
 	 * session's full phase reads staged tiles in place (no gather area). */
-	const unsigned min_kb = (kBlockRows * s->cfg.max_load_bytes_per_row + 1023) / 1024;
+	const unsigned min_kb = (kCountGroup * kBlockRows * s->cfg.max_load_bytes_per_row + 1023) / 1024;
 	bool fit = false;
 	for (unsigned min_stages : {3u, 2u}) {
 		for (unsigned kb : {48u, 40u, 32u, 24u, 16u, 8u}) {

@@ -164,13 +164,22 @@ constexpr unsigned kChunkWords = kMaxChunkRows / 32;
  *    from device memory into the compute warp's own area.
  * FM_REFILTER stages full tiles of every column and runs the filter again
  * over groups of kCountGroup blocks (the results read register vectors the
- * filter computed). */
+ * filter computed).  FM_DENSE stages full tiles and runs the projection over
+ * every row of a group of kCountGroup blocks, as the filter runs (rows held
+ * by lanes, register vectors indexed by row), then stores the valid rows at
+ * their ranks: no selection list and no indirect operand addresses, for
+ * programs whose rows mostly pass the filter (a tuning choice). */
 constexpr uint32_t FM_BITMAP = 0;
 constexpr uint32_t FM_REFILTER = 1;
 constexpr uint32_t FM_GATHER = 2;
+constexpr uint32_t FM_DENSE = 3;
 /* the largest bytes per row a gathering full phase moves into a compute
  * warp's area */
 constexpr uint32_t kGatherMaxBpr = 32;
+/* the largest bytes per row of register vectors a dense full phase keeps
+ * for a whole count group in a compute warp's area (wider programs keep
+ * the in-place full phase) */
+constexpr uint32_t kDenseMaxRowBpr = 16;
 
 /* the staged columns of one phase: which segment columns, where in a stage */
 struct LoadSet {

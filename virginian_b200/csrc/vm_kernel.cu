@@ -1149,6 +1149,94 @@ __device__ __forceinline__ bool refilter_group(const Bases &b, uint32_t list, ui
 	return ok;
 }
 
+/* FM_DENSE: one result column over a group's rows held by lanes (row
+ * 32 u + lane in element u; `mine`: the group's validity word `lane`, so
+ * word u is lane u's); valid rows go to pos0 + their rank among the group's
+ * valid rows (the valid rows of earlier words and of lower lanes in word u);
+ * false if a row falls past cap */
+template <typename T>
+__device__ __forceinline__ bool dense_store(uint32_t od, const Bases &b, uint32_t mine, uint32_t vb, T *out,
+	uint64_t pos0, uint64_t cap, int lane)
+{
+	constexpr int U = kCountGroup * kBlockRows / 32;
+	const Opnd o = opnd<sizeof(T)>(od, b);
+	T v[U];
+	load_rows<T, U>(o, lane, v);
+	const uint32_t below = (1u << lane) - 1u;
+	uint32_t base = 0;
+	bool ok = true;
+#pragma unroll
+	for (int u = 0; u < U; u++) {
+		const uint32_t wu = __shfl_sync(0xffffffffu, mine, u);
+		if ((vb >> u) & 1u) {
+			const uint64_t pos = pos0 + base + __popc(wu & below);
+			if (pos < cap)
+				out[pos] = v[u];
+			else
+				ok = false;
+		}
+		base += __popc(wu);
+	}
+	return ok;
+}
+
+/* 8-byte and char result columns of a dense group, out of line, by value */
+__device__ __noinline__ bool dense_store_rare(uint32_t od, Bases b, uint32_t mine, uint32_t vb, void *out,
+	uint64_t pos0, uint64_t cap, uint32_t stride, int lane)
+{
+	if (stride == 8)
+		return dense_store<unsigned long long>(od, b, mine, vb, static_cast<unsigned long long *>(out), pos0, cap, lane);
+	return dense_store<unsigned char>(od, b, mine, vb, static_cast<unsigned char *>(out), pos0, cap, lane);
+}
+
+/* FM_DENSE full phase: one group (up to kCountGroup blocks from chunk
+ * block blk, nrows rows) with the projection run over every valid row as
+ * vector ops (b.stage the staged tile, b.blk_row0 the group's first tile
+ * row), then each result column's valid rows stored in row order.  Returns
+ * false on an output overflow. */
+__device__ __forceinline__ bool dense_group(const Bases &b, uint32_t blk, uint32_t nrows, int lane)
+{
+	constexpr int U = kCountGroup * kBlockRows / 32;
+	const uint32_t nw = (nrows + 31) / 32;
+	const uint32_t mine = (uint32_t)lane < nw ? lds_u32(b.slot + kSlotBitmap + 32u * blk + 4u * lane) : 0u;
+	uint32_t vb = 0;
+#pragma unroll
+	for (int u = 0; u < U; u++)
+		vb |= ((__shfl_sync(0xffffffffu, mine, u) >> lane) & 1u) << u;
+	if (!__any_sync(0xffffffffu, vb != 0))
+		return true;
+	const uint32_t ops = b.slot + kQOpsFull;
+	const uint32_t nf = lds_u32(b.slot + kQNFilter);
+	const uint32_t nu = lds_u32(b.slot + kQNUops) - 1u;
+	const uint32_t nout = lds_u32(b.slot + kQNOut);
+	for (uint32_t k = nf; k < nu; k++) {
+		const uint4 rec = lds_v4(ops + 16u * k);
+		const uint32_t h = rec.x;
+		if (h & (OK_SETCONST | OK_COPY)) {
+			if (h_type(h, VT_INT) || h_type(h, VT_FLOAT)) vec_rows<uint32_t, -1, U>(rec, b, lane, vb);
+			else vec_rare<U>(rec, b, lane, vb);
+		} else if (h & OK_MATH) {
+			if (h_type(h, VT_FLOAT)) vec_any<float, U, false>(rec, b, lane, vb);
+			else if (h_type(h, VT_INT)) vec_any<int32_t, U, false>(rec, b, lane, vb);
+			else vec_rare<U>(rec, b, lane, vb);
+		}
+	}
+	const uint64_t off = lds_u64(b.slot + kSlotBlockOff + 8u * blk);
+	const uint64_t cap = lds_u64(b.slot + kQCapacity);
+	bool ok = true;
+	for (uint32_t j = 0; j < nout; j++) {
+		const uint32_t od = lds_u32(b.slot + kQOdOut + 4 * j);
+		void *out = reinterpret_cast<void *>(lds_u64(b.slot + kQOutPtr + 8 * j));
+		const uint32_t stride = lds_u8(b.slot + kQOutStride + j);
+		if (stride == 4)
+			ok = dense_store<uint32_t>(od, b, mine, vb, static_cast<uint32_t *>(out), off, cap, lane) && ok;
+		else
+			ok = dense_store_rare(od, b, mine, vb, out, off, cap, stride, lane) && ok;
+	}
+	__syncwarp();
+	return ok;
+}
+
 /* the selected rows of one full entry (chunk blocks [blk0, blk0 + nblk),
  * up to 32 of them): how many, and the output position of the first */
 __device__ __forceinline__ uint32_t entry_selected(uint32_t slot, uint32_t blk0, uint32_t nblk, uint64_t *off0)
@@ -2007,7 +2095,7 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 				}
 				b.slot = sbase + kSlotArea + slot * kSlotBytes;
 				mode = lds_u32(b.slot + kQFullMode);
-				if (mode == FM_REFILTER) {
+				if (mode == FM_REFILTER || mode == FM_DENSE) {
 					n = (nblk + kCountGroup - 1) / kCountGroup;
 				} else {
 					nsel = entry_selected(b.slot, row0 / kBlockRows, nblk, &off0);
@@ -2049,13 +2137,15 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 		const uint32_t nblk = (nrows + kBlockRows - 1) / kBlockRows;
 		const uint32_t blk0 = row0 / kBlockRows;
 		bool ok = true;
-		if (kind == SK_COUNT || mode == FM_REFILTER) {
+		if (kind == SK_COUNT || mode == FM_REFILTER || mode == FM_DENSE) {
 			const uint32_t r = j * kCountGroup * kBlockRows;
 			b.stage = tile;
 			b.blk_row0 = r;
 			if (kind == SK_COUNT)
 				count_group(b, blk0 + j * kCountGroup, min((uint32_t)kCountGroup, nblk - j * kCountGroup),
 					min((uint32_t)(kCountGroup * kBlockRows), nrows - r), lane);
+			else if (mode == FM_DENSE)
+				ok = dense_group(b, blk0 + j * kCountGroup, min((uint32_t)(kCountGroup * kBlockRows), nrows - r), lane);
 			else
 				ok = refilter_group(b, list, blk0 + j * kCountGroup, min((uint32_t)(kCountGroup * kBlockRows), nrows - r),
 					kp.unit_batches, lane);
