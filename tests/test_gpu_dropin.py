@@ -24,7 +24,9 @@ n = int(sys.argv[1])
 cols = datagen.table(n, datagen.SCHEMA_A, seed=21)
 db.create_table("test", datagen.SCHEMA_A)
 db.insert("test", cols["id"], [cols[c] for c, _ in datagen.SCHEMA_A])
-for q in [CONFIG1, config2(20.0, 15.0), "select id, uniformi from test"] + SUITE[:4] + EXTRA[:4]:
+# the last query keeps every row of 28 bytes: several result tablets roll over
+WIDE = "select id, uniformi, normali5, normali20, uniformf, normalf5, normalf20 from test"
+for q in [CONFIG1, config2(20.0, 15.0), "select id, uniformi from test"] + SUITE[:4] + EXTRA[:4] + [WIDE]:
     cpu = db.query(q, mode=0)
     gpu = db.query(q, mode=2)
     assert_same_stream(gpu.columns, cpu.columns, q)
@@ -79,6 +81,14 @@ for q in queries:
     assert_same_stream(gpu.columns, cpu.columns, q)
 lib.virg_gpu_dropin_cache_stats(ctypes.byref(h), ctypes.byref(m), ctypes.byref(b))
 assert m.value > misses_before, (m.value, misses_before)
+# a capacity below two tablets: every tablet evicts the one before it,
+# which the previous tablet's kernel may still be reading
+lib.virg_gpu_dropin_cache(12 << 20)
+for q in queries:
+    cpu = db.query(q, mode=0)
+    gpu = db.query(q, mode=2)
+    assert_same_stream(gpu.columns, cpu.columns, q)
+    assert gpu.tablet_rows == cpu.tablet_rows, (q, gpu.tablet_rows, cpu.tablet_rows)
 lib.virg_gpu_dropin_cache(0)
 lib.virg_gpu_dropin_cache_stats(ctypes.byref(h), ctypes.byref(m), ctypes.byref(b))
 assert b.value == 0, b.value

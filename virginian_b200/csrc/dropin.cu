@@ -10,7 +10,7 @@
  *  2. for each data tablet of the chain, copies the columns the program reads
  *     from the tablet's host slot to HBM, runs the VM kernel (one launch per
  *     tablet; rows come back in original order) and reads back the row count
- *     and the valid-row count of every 64-row block;
+ *     and the valid-row count of every 64-row block, two tablets in flight;
  *  3. replays the single-core CPU VM's result-tablet roll-over rule on those
  *     block counts (src/vm/virginia.c:516-527: roll when
  *     rows + block_rows >= possible_rows - 300) and copies each run of result
@@ -71,6 +71,7 @@ bool resolve(HostApi &h)
 
 std::mutex g_mu;
 virg_gpu_engine *g_engine = nullptr;
+cudaStream_t g_h2d = nullptr;  /* tablet copies, beside the engine's kernel and copy streams */
 
 /* Residency cache of data tablets in HBM (off unless a capacity is set):
  * every column and the key of a tablet, in the engine's device layout,
@@ -99,8 +100,14 @@ void cache_drop(std::map<unsigned, CachedTablet>::iterator it)
 
 /* the tablet's device copy from the cache, or a new one (all columns and the
  * key); nullptr if it cannot be cached (too big, or a copy failed) */
-const CachedTablet *cache_get(const virg_tablet_meta *t, const virg_gpu_schema &schema, cudaStream_t st)
+const CachedTablet *cache_get(const virg_tablet_meta *t, const virg_gpu_schema &schema, cudaStream_t st,
+	cudaStream_t kst)
 {
+	/* a tablet about to be evicted may still be read by a kernel in flight */
+	auto quiesce = [&]() {
+		cudaStreamSynchronize(kst);
+		cudaStreamSynchronize(st);
+	};
 	auto it = g_cache.find(t->id);
 	if (it != g_cache.end()) {
 		if (it->second.rows == t->rows && it->second.slot == (const void *)t) {
@@ -108,6 +115,7 @@ const CachedTablet *cache_get(const virg_tablet_meta *t, const virg_gpu_schema &
 			g_cache_hits++;
 			return &it->second;
 		}
+		quiesce();
 		cache_drop(it);
 	}
 	g_cache_misses++;
@@ -118,6 +126,8 @@ const CachedTablet *cache_get(const virg_tablet_meta *t, const virg_gpu_schema &
 	bytes += (pr * (size_t)t->key_stride + 255) / 256 * 256;
 	if (bytes > g_cache_cap)
 		return nullptr;
+	if (g_cache_bytes + bytes > g_cache_cap && !g_cache.empty())
+		quiesce();
 	while (g_cache_bytes + bytes > g_cache_cap && !g_cache.empty()) {
 		auto lru = g_cache.begin();
 		for (auto i = g_cache.begin(); i != g_cache.end(); ++i)
@@ -164,10 +174,77 @@ int fail(const char *msg)
 	return VIRG_FAIL;
 }
 
-struct Timers {
-	cudaEvent_t a, b, c, d;
+/* One data tablet in flight.  Tablet k's columns are copied in and its
+ * kernel queued before tablet k-1's result rows are spread over the result
+ * tablets, so the host's work on one tablet (reading back its counts,
+ * placing its rows, loading the next tablet into a host slot) overlaps the
+ * device's work on the next.  A pinned buffer per flight carries the
+ * segment descriptor to the device and brings the row total and the
+ * per-block counts back in one wait. */
+struct Flight {
+	virg_gpu_table stage;
+	virg_gpu_result *r = nullptr;
+	uint64_t rows = 0, nblocks = 0;
+	bool busy = false, timed = false;
+	cudaEvent_t a = nullptr, b = nullptr, c0 = nullptr, c = nullptr, counted = nullptr, d0 = nullptr,
+		d1 = nullptr;
+};
+/* pinned buffer layout: SegDesc | u64 total | u8 counts[nblocks] */
+constexpr size_t kPinTotal = (sizeof(SegDesc) + 63) / 64 * 64;
+constexpr size_t kPinCounts = kPinTotal + 64;
+unsigned char *g_pin[2] = {nullptr, nullptr};
+size_t g_pin_cap[2] = {0, 0};
+
+bool pin_reserve(unsigned i, size_t bytes)
+{
+	if (g_pin_cap[i] >= bytes)
+		return true;
+	if (g_pin[i])
+		cudaFreeHost(g_pin[i]);
+	g_pin[i] = nullptr;
+	g_pin_cap[i] = 0;
+	const size_t want = std::max<size_t>(bytes, 64 << 10);
+	if (cudaHostAlloc((void **)&g_pin[i], want, cudaHostAllocDefault) != cudaSuccess) {
+		cudaGetLastError();
+		g_pin[i] = nullptr;
+		return false;
+	}
+	g_pin_cap[i] = want;
+	return true;
+}
+
+struct Times {
 	float h2d = 0, kern = 0, d2h = 0;
 };
+
+/* the stage times of a flight's last tablet, once its copies are done */
+void flight_times(Flight &f, Times &tm)
+{
+	if (!f.timed)
+		return;
+	cudaEventSynchronize(f.d1);
+	float x;
+	if (cudaEventElapsedTime(&x, f.a, f.b) == cudaSuccess)
+		tm.h2d += x;
+	if (cudaEventElapsedTime(&x, f.c0, f.c) == cudaSuccess)
+		tm.kern += x;
+	if (cudaEventElapsedTime(&x, f.d0, f.d1) == cudaSuccess)
+		tm.d2h += x;
+	f.timed = false;
+}
+
+/* release a flight's staged columns (queued after its kernel) */
+void flight_unstage(Flight &f, cudaStream_t st)
+{
+	for (void *m : f.stage.allocs)
+		cudaFreeAsync(m, st);
+	if (f.stage.d_segs)
+		cudaFreeAsync(f.stage.d_segs, st);
+	f.stage.allocs.clear();
+	f.stage.segs.clear();
+	f.stage.seg_rows.clear();
+	f.stage.d_segs = nullptr;
+}
 
 }  // namespace
 
@@ -222,6 +299,10 @@ extern "C" int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
 		return fail(vgpu::last_error());
 	virg_gpu_engine *e = g_engine;
 	cudaSetDevice(e->device);
+	if (!g_h2d && cudaStreamCreateWithFlags(&g_h2d, cudaStreamNonBlocking) != cudaSuccess) {
+		g_h2d = nullptr;
+		return fail("copy stream create failed");
+	}
 
 	/* the table's schema, from its first tablet */
 	virg_gpu_schema schema;
@@ -238,113 +319,78 @@ extern "C" int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
 	if (P.nout > res[0]->fixed_columns)
 		return fail("Result writes more registers than the result tablet has columns");
 
-	Timers tm;
-	cudaEventCreate(&tm.a);
-	cudaEventCreate(&tm.b);
-	cudaEventCreate(&tm.c);
-	cudaEventCreate(&tm.d);
-	int ok = 1;
-	unsigned proced = 0;
-	std::vector<uint8_t> counts;
 	std::lock_guard<std::mutex> elk(e->mu);
+	Flight fl[2];
+	cudaEvent_t roll = nullptr;
+	bool events = cudaEventCreateWithFlags(&roll, cudaEventDisableTiming) == cudaSuccess;
+	for (Flight &f : fl) {
+		for (cudaEvent_t *ev : {&f.a, &f.b, &f.c0, &f.c, &f.d0, &f.d1})
+			events = events && cudaEventCreate(ev) == cudaSuccess;
+		events = events && cudaEventCreateWithFlags(&f.counted, cudaEventDisableTiming) == cudaSuccess;
+		f.stage.e = e;
+		f.stage.schema = schema;
+		f.stage.transient = true;
+	}
+	int ok = events ? 1 : fail("event create failed");
+	Times tm;
+	bool want[VIRG_MAX_COLUMNS] = {false};
+	bool want_key = false;
+	for (unsigned i = 0; i < P.nload; i++) {
+		if (P.load_src[i] == kKeySlot)
+			want_key = true;
+		else
+			want[P.load_src[i]] = true;
+	}
 
-	while (ok) {
-		virg_tablet_meta *t = tab[0];
-		if (t->fixed_columns != schema.ncols) {
-			ok = fail("tablet column layout differs within the table");
-			break;
+	/* spread a finished tablet's ordered rows over result tablets like the
+	 * CPU VM: roll when rows + block_rows >= possible_rows - 300
+	 * (src/vm/virginia.c:516-527), copying each run of rows that stays in
+	 * one result tablet straight from HBM on the copy stream */
+	auto finish = [&](Flight &f) -> int {
+		f.busy = false;
+		if (cudaEventSynchronize(f.counted) != cudaSuccess)
+			return fail("result count read failed");
+		const unsigned char *pin = g_pin[&f - fl];
+		uint64_t total = 0, sum = 0;
+		if (f.rows) {
+			memcpy(&total, pin + kPinTotal, sizeof(total));
+			for (uint64_t b = 0; b < f.nblocks; b++)
+				sum += pin[kPinCounts + b];
 		}
-		/* this tablet's columns, as plain pointers into its host slot */
-		virg_gpu_segment seg;
-		memset(&seg, 0, sizeof(seg));
-		seg.rows = t->rows;
-		seg.key = (const char *)t + t->key_block;
-		for (unsigned c = 0; c < schema.ncols; c++)
-			seg.col[c] = (const char *)t + t->fixed_block + t->fixed_offset[c];
-
-		virg_gpu_table stage;
-		stage.e = e;
-		stage.schema = schema;
-		stage.transient = true;
-		bool want[VIRG_MAX_COLUMNS] = {false};
-		bool want_key = false;
-		for (unsigned i = 0; i < P.nload; i++) {
-			if (P.load_src[i] == kKeySlot)
-				want_key = true;
-			else
-				want[P.load_src[i]] = true;
+		if (sum != total || total > f.rows) {
+			unsigned err = 0;
+			if (read_device_error(e, &err) && err)
+				return fail(device_error_text(err));
+			return fail("result row count mismatch");
 		}
-		cudaEventRecord(tm.a, e->stream);
-		virg_gpu_result *r = nullptr;
-		const uint64_t nblocks = (t->rows + 63) / 64;
-		/* the tablet's columns in HBM: from the residency cache when it is
-		 * on, else copied for this query only */
-		const CachedTablet *ct = g_cache_cap && t->rows ? cache_get(t, schema, e->stream) : nullptr;
-		if (ct) {
-			SegDesc d;
-			memset(&d, 0, sizeof(d));
-			d.rows = t->rows;
-			d.block_base = 0;
-			for (unsigned c = 0; c < kMaxLoads; c++)
-				d.col[c] = ct->col[c];
-			stage.segs.push_back(d);
-			stage.seg_rows.push_back((uint32_t)t->rows);
-			stage.rows = t->rows;
-			stage.blocks = nblocks;
-			stage.dirty = true;
-			ok = table_sync_desc(&stage);
-		} else {
-			ok = table_add_segments(&stage, &seg, 1, want, want_key, e->stream) && table_sync_desc(&stage);
-		}
-		ok = ok && result_alloc(e, P, t->rows, true, nblocks, &r);
-		cudaEventRecord(tm.b, e->stream);
-		if (ok && t->rows) {
-			QueryLaunch q;
-			q.prog = &P;
-			q.d_segs = stage.d_segs;
-			q.nsegs = 1;
-			q.seg_rows = stage.seg_rows.data();
-			for (unsigned j = 0; j < P.nout; j++)
-				q.out[j] = r->out[j];
-			q.capacity = t->rows;
-			q.d_total = r->d_total;
-			q.block_counts = r->block_counts;
-			ok = run_queries(e, std::vector<QueryLaunch>(1, q), nullptr);
-		}
-		cudaEventRecord(tm.c, e->stream);
-		uint64_t total = 0;
-		if (ok && t->rows) {
-			counts.resize(nblocks);
-			ok = virg_gpu_result_rows(r, &total) &&
-				cudaMemcpyAsync(counts.data(), r->block_counts, nblocks, cudaMemcpyDeviceToHost,
-					e->stream) == cudaSuccess &&
-				cudaStreamSynchronize(e->stream) == cudaSuccess;
-			if (!ok && vgpu::last_error()[0])
-				fail(vgpu::last_error());
-		}
-
-		/* distribute the ordered rows over result tablets like the CPU VM */
+		const unsigned char *counts = pin + kPinCounts;
+		cudaStreamWaitEvent(e->copy_stream, f.counted, 0);
+		cudaEventRecord(f.d0, e->copy_stream);
+		int good = 1;
 		uint64_t done = 0;
-		for (uint64_t b = 0; ok && b < nblocks; b++) {
-			const unsigned simd_rows = (unsigned)std::min<uint64_t>(64, t->rows - b * 64);
+		for (uint64_t b = 0; good && b < f.nblocks; b++) {
 			virg_tablet_meta *rt = res[0];
+			const unsigned simd_rows = (unsigned)std::min<uint64_t>(64, f.rows - b * 64);
 			if (rt->rows + simd_rows >= rt->possible_rows - 300) {
 				/* roll over: the current tablet is complete, so release it
 				 * once the copies into it have landed */
-				if (cudaStreamSynchronize(e->stream) != cudaSuccess)
-					ok = fail("result copy sync failed");
+				if (cudaEventRecord(roll, e->copy_stream) != cudaSuccess ||
+					cudaEventSynchronize(roll) != cudaSuccess) {
+					good = fail("result copy sync failed");
+					break;
+				}
 				virg_tablet_meta *old = rt;
 				host.allocresult(v, vm, res, res[0]);
 				host.unlock(v, old->id);
 				rt = res[0];
 			}
-			/* gather this block's rows with the following blocks that stay in
-			 * the same result tablet, then copy the run at once */
+			/* this block's rows with the following blocks that stay in the
+			 * same result tablet, copied as one run */
 			uint64_t run = counts[b];
 			uint64_t b2 = b + 1;
 			unsigned rows_after = rt->rows + counts[b];
-			while (b2 < nblocks) {
-				const unsigned sr = (unsigned)std::min<uint64_t>(64, t->rows - b2 * 64);
+			while (b2 < f.nblocks) {
+				const unsigned sr = (unsigned)std::min<uint64_t>(64, f.rows - b2 * 64);
 				if (rows_after + sr >= rt->possible_rows - 300)
 					break;
 				run += counts[b2];
@@ -352,56 +398,153 @@ extern "C" int virg_vm_gpu(virginian *v, virg_vm *vm, virg_tablet_meta **tab,
 				b2++;
 			}
 			if (rt->rows + run > rt->possible_rows) {
-				ok = fail("result tablet overflow");
+				good = fail("result tablet overflow");
 				break;
 			}
 			/* result tablets live in pinned host slots (src/init.c:57-58), so
-			 * the copies run asynchronously; the tablet's last copy is waited
-			 * for before it is released or the data tablet is done */
+			 * the copies run asynchronously */
 			for (unsigned j = 0; j < P.nout && run; j++) {
 				char *dst = (char *)rt + rt->fixed_block + rt->fixed_offset[j] +
 					(size_t)P.out_stride[j] * rt->rows;
-				const char *src = (const char *)r->out[j] + (size_t)P.out_stride[j] * done;
+				const char *src = (const char *)f.r->out[j] + (size_t)P.out_stride[j] * done;
 				if (cudaMemcpyAsync(dst, src, run * P.out_stride[j], cudaMemcpyDeviceToHost,
-						e->stream) != cudaSuccess)
-					ok = fail("result copy failed");
+						e->copy_stream) != cudaSuccess)
+					good = fail("result copy failed");
 			}
 			rt->rows += (unsigned)run;
 			done += run;
 			b = b2 - 1;
 		}
-		if (cudaStreamSynchronize(e->stream) != cudaSuccess)
-			ok = fail("result copy sync failed");
-		if (ok && done != total)
-			ok = fail("result row count mismatch");
-		cudaEventRecord(tm.d, e->stream);
-		cudaEventSynchronize(tm.d);
-		float f;
-		if (cudaEventElapsedTime(&f, tm.a, tm.b) == cudaSuccess) tm.h2d += f;
-		if (cudaEventElapsedTime(&f, tm.b, tm.c) == cudaSuccess) tm.kern += f;
-		if (cudaEventElapsedTime(&f, tm.c, tm.d) == cudaSuccess) tm.d2h += f;
+		cudaEventRecord(f.d1, e->copy_stream);
+		/* the result buffers are freed on the engine stream after the copies */
+		cudaStreamWaitEvent(e->stream, f.d1, 0);
+		virg_gpu_result_destroy(f.r);
+		f.r = nullptr;
+		f.timed = true;
+		return good;
+	};
 
-		if (r)
-			virg_gpu_result_destroy(r);
-		for (void *m : stage.allocs)
-			cudaFreeAsync(m, e->stream);
-		if (stage.d_segs)
-			cudaFreeAsync(stage.d_segs, e->stream);
-		stage.allocs.clear();
-		stage.d_segs = nullptr;
+	unsigned proced = 0;
+	for (uint64_t k = 0; ok; k++) {
+		virg_tablet_meta *t = tab[0];
+		if (t->fixed_columns != schema.ncols) {
+			ok = fail("tablet column layout differs within the table");
+			break;
+		}
+		Flight &f = fl[k & 1];
+		flight_times(f, tm);
+		f.rows = t->rows;
+		f.nblocks = (t->rows + 63) / 64;
+		if (!pin_reserve((unsigned)(k & 1), kPinCounts + f.nblocks)) {
+			ok = fail("pinned count buffer alloc failed");
+			break;
+		}
+		unsigned char *pin = g_pin[k & 1];
+		/* the tablet's columns in HBM, on the copy-in stream (so they
+		 * overlap the previous tablet's kernel): from the residency cache
+		 * when it is on, else copied from its host slot for this query only */
+		cudaEventRecord(f.a, g_h2d);
+		const CachedTablet *ct = g_cache_cap && t->rows ? cache_get(t, schema, g_h2d, e->stream) : nullptr;
+		SegDesc d;
+		memset(&d, 0, sizeof(d));
+		if (ct) {
+			d.rows = t->rows;
+			for (unsigned c = 0; c < kMaxLoads; c++)
+				d.col[c] = ct->col[c];
+		} else if (t->rows) {
+			virg_gpu_segment seg;
+			memset(&seg, 0, sizeof(seg));
+			seg.rows = t->rows;
+			seg.key = (const char *)t + t->key_block;
+			for (unsigned c = 0; c < schema.ncols; c++)
+				seg.col[c] = (const char *)t + t->fixed_block + t->fixed_offset[c];
+			f.stage.rows = f.stage.blocks = 0;
+			ok = table_add_segments(&f.stage, &seg, 1, want, want_key, g_h2d);
+			if (ok)
+				d = f.stage.segs[0];
+		}
+		if (ok && t->rows) {
+			memcpy(pin, &d, sizeof(d));
+			ok = cudaMallocAsync((void **)&f.stage.d_segs, sizeof(SegDesc), g_h2d) == cudaSuccess &&
+				cudaMemcpyAsync(f.stage.d_segs, pin, sizeof(SegDesc), cudaMemcpyHostToDevice, g_h2d) ==
+					cudaSuccess;
+			if (!ok)
+				fail("segment descriptor copy failed");
+			f.stage.seg_rows.assign(1, (uint32_t)t->rows);
+		}
+		cudaEventRecord(f.b, g_h2d);
+		cudaStreamWaitEvent(e->stream, f.b, 0);
+		ok = ok && result_alloc(e, P, t->rows, true, f.nblocks, &f.r);
+		cudaEventRecord(f.c0, e->stream);
+		if (ok && t->rows) {
+			QueryLaunch q;
+			q.prog = &P;
+			q.d_segs = f.stage.d_segs;
+			q.nsegs = 1;
+			q.seg_rows = f.stage.seg_rows.data();
+			for (unsigned j = 0; j < P.nout; j++)
+				q.out[j] = f.r->out[j];
+			q.capacity = t->rows;
+			q.d_total = f.r->d_total;
+			q.block_counts = f.r->block_counts;
+			ok = run_queries(e, std::vector<QueryLaunch>(1, q), nullptr);
+			if (!ok)
+				fail(vgpu::last_error());
+		}
+		cudaEventRecord(f.c, e->stream);
+		if (ok && t->rows) {
+			ok = cudaMemcpyAsync(pin + kPinTotal, f.r->d_total, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+					e->stream) == cudaSuccess &&
+				cudaMemcpyAsync(pin + kPinCounts, f.r->block_counts, f.nblocks, cudaMemcpyDeviceToHost,
+					e->stream) == cudaSuccess;
+			if (!ok)
+				fail("result count read failed");
+		}
+		cudaEventRecord(f.counted, e->stream);
+		flight_unstage(f, e->stream);
+		f.busy = ok != 0;
+		/* the previous tablet's rows go out while this one runs */
+		Flight &prev = fl[(k + 1) & 1];
+		if (prev.busy && !finish(prev))
+			ok = 0;
 		if (!ok)
 			break;
-
 		proced++;
-		if (t->last_tablet || (num_tablets != 0 && proced >= num_tablets))
+		if (t->last_tablet || (num_tablets != 0 && proced >= num_tablets)) {
+			ok = finish(f);
 			break;
+		}
+		/* the host slot may be reused once its columns are in HBM */
+		if (cudaEventSynchronize(f.b) != cudaSuccess) {
+			ok = fail("tablet copy failed");
+			break;
+		}
 		host.loadnext(v, tab);
 	}
+	cudaStreamSynchronize(g_h2d);
+	cudaStreamSynchronize(e->copy_stream);
 	cudaStreamSynchronize(e->stream);
-	cudaEventDestroy(tm.a);
-	cudaEventDestroy(tm.b);
-	cudaEventDestroy(tm.c);
-	cudaEventDestroy(tm.d);
+	for (Flight &f : fl) {
+		if (f.r)
+			virg_gpu_result_destroy(f.r);
+		f.r = nullptr;
+		flight_unstage(f, e->stream);
+		flight_times(f, tm);
+	}
+	if (ok) {
+		unsigned err = 0;
+		if (!read_device_error(e, &err))
+			ok = fail(vgpu::last_error());
+		else if (err)
+			ok = fail(device_error_text(err));
+	}
+	cudaStreamSynchronize(e->stream);
+	for (Flight &f : fl)
+		for (cudaEvent_t ev : {f.a, f.b, f.c0, f.c, f.counted, f.d0, f.d1})
+			if (ev)
+				cudaEventDestroy(ev);
+	if (roll)
+		cudaEventDestroy(roll);
 	vm->timing1 = tm.h2d / 1000.0f;
 	vm->timing2 = tm.kern / 1000.0f;
 	vm->timing3 = tm.d2h / 1000.0f;
