@@ -424,7 +424,7 @@ def bench_serving(eng, rates=(1000, 10000, 50000), per_rate=300, world=1, rank=0
     mine_t = [k for k in range(len(sizes)) if owner[k] == rank]
     tables = dict(zip(mine_t, _device_tables(eng, [sizes[k] for k in mine_t], 2000, mine_t)))
     log("serving: tables ready")
-    layout = (32, 16, 48)
+    layout = (32, 12, 20)
     all_work = _queries(per_rate, 88, len(sizes), layout)
     mine = shard.my_queries([k for _, k, _ in all_work], owner, rank)
     work = [all_work[i] for i in mine]
@@ -1006,10 +1006,11 @@ def run_b200(args):
             line["cpu_multicore"] = cpu_multi
     del keep
     table.close()
-    # the other workloads: one GPU, rank 0 (the sharded path covers the scan)
-    # the other workloads: batched on every rank (whole tables per rank);
-    # the others on one GPU, rank 0 (the sharded path covers the scan)
+    # the other workloads: batched and serving on every rank (whole tables
+    # per rank); the others on one GPU, rank 0 (the sharded path covers the
+    # scan)
     sections = [x for x in args.sections.split(",") if x]
+    eng.set_shared_scan(args.shared_scan)
     for name, fn, multi in (("batched", bench_batched, True), ("serving", bench_serving, True),
                             ("streamed", bench_streamed, False), ("dropin", bench_dropin, False),
                             ("ref_gpu_vm", bench_ref_gpu_vm, False)):
@@ -1025,6 +1026,8 @@ def run_b200(args):
                 res = fn(eng)
         except Exception as ex:  # report, keep the headline line
             res = {"error": f"{type(ex).__name__}: {ex}"}
+        if name == "batched":
+            res["shared_scan"] = args.shared_scan
         if rank == 0:
             line[name] = res
     if rank == 0 and args.parity:
@@ -1063,6 +1066,8 @@ def main():
                     help="rows of the streamed section's host table (400M: the streamed workload)")
     ap.add_argument("--no-parity", dest="parity", action="store_false",
                     help="skip the headline's byte comparison with the reference CPU VM")
+    ap.add_argument("--no-shared-scan", dest="shared_scan", action="store_false",
+                    help="claim each batched query's chunks in one run (no shared scans)")
     ap.add_argument("--sections", default="batched,serving,streamed,dropin,ref_gpu_vm",
                     help="workloads besides the headline scan (comma list; empty for none)")
     args = ap.parse_args()

@@ -311,6 +311,11 @@ int virg_gpu_engine_set_chunk_rows(virg_gpu_engine *e, unsigned rows);
  * filters that keep most rows).  Programs outside a mode's bounds, and
  * launches whose shape leaves no room for mode 2, keep mode 0. */
 int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode);
+/* shared scans (on by default): in a launch of several queries, the queries
+ * over the same table claim its chunks interleaved, so each chunk's columns
+ * are read from device memory once and from L2 by the others; 0 turns it
+ * off (each query's chunks are claimed in one run, as a single query's) */
+int virg_gpu_engine_set_shared_scan(virg_gpu_engine *e, int enable);
 /* record CUDA events around each of the next kernel launches in a ring of
  * `slots` entries (0 turns it off) */
 int virg_gpu_engine_timing(virg_gpu_engine *e, unsigned slots);
@@ -480,8 +485,8 @@ typedef struct {
 	unsigned max_queries;            /* queries per kernel session (0: 4096) */
 	unsigned idle_us;                /* end an idle session after this long (0: 50000) */
 	unsigned max_load_bytes_per_row; /* staged column bytes a program may read (0: 32) */
-	unsigned max_row_vector_bytes;   /* filter register-vector bytes per row (0: 16) */
-	unsigned max_sel_vector_bytes;   /* projection register-vector bytes per row (0: 48) */
+	unsigned max_row_vector_bytes;   /* filter register-vector bytes per row (0: 12) */
+	unsigned max_sel_vector_bytes;   /* projection register-vector bytes per row (0: 20) */
 	unsigned wait_limit_ms;          /* bound of the kernel's waits (0: 60000) */
 } virg_serve_config;
 

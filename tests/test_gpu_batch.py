@@ -110,3 +110,30 @@ def test_autotuned_batch(setup):
     b2.wait()
     assert b2.shape()["threads"] == shape["threads"]
     b2.close()
+
+
+@pytest.mark.parametrize("chunk_rows", [0, 1024])
+def test_shared_scans_give_the_same_bytes(setup, chunk_rows):
+    """Queries over one table claim its chunks interleaved (a shared scan);
+    with it turned off each query's chunks are claimed in one run.  Both give
+    every query the CPU VM's stream, also with small chunks (many chunks per
+    table, so the interleaved claims cross many CTAs)."""
+    eng, db, cat, tables, work = setup
+    # every table scanned by several queries, empty ones included
+    many = work + [(q, k) for q, k in work[:24]]
+    results = {}
+    try:
+        eng.set_shape(chunk_rows=chunk_rows)
+        for shared in (True, False):
+            eng.set_shared_scan(shared)
+            b = build_batch(eng, cat, tables, many)
+            b.run(graph=False)
+            b.wait()
+            results[shared] = [b.download(s) for s in range(len(many))]
+            b.close()
+    finally:
+        eng.set_shared_scan(True)
+        eng.set_shape(0, 0, 0, 0)
+    for s, (q, k) in enumerate(many):
+        assert_same_stream(results[True][s], results[False][s], f"shared vs one run: {q}")
+        assert_same_stream(results[True][s], db.query(q).columns, q)

@@ -90,6 +90,38 @@ def test_mix_equals_alone_and_oracle(setup):
         s.close()
 
 
+def test_single_queries_of_other_shapes_beside_a_session(setup):
+    """Single queries of other launch shapes (other shared-memory sizes of the
+    same kernel) launched from this thread while the serving thread starts
+    sessions: neither side's launch may fail, and every result stays the
+    query's own."""
+    eng, db, tables, work, alone = setup
+    s = vb.Serve(eng, result_budget_bytes=1 << 30, idle_us=1000)
+    shapes = [(256, 24, 2, 1), (256, 48, 3, 1), (256, 32, 0, 1), (0, 0, 0, 0)]
+    try:
+        for rnd in range(3):
+            tickets = []
+            for i, (q, k, p) in enumerate(work):
+                tickets.append(s.submit(p, tables[k]))
+                eng.set_shape(*shapes[i % len(shapes)])
+                try:
+                    r = tables[k].query(p)
+                    got = r.download()
+                    r.close()
+                finally:
+                    eng.set_shape(0, 0, 0, 0)
+                assert_same_stream(got, alone[i], f"single beside a session: {q}")
+                if i % 5 == 4:
+                    time.sleep(0.003)  # let the session go idle and restart
+            for t, (q, k, p), want in zip(tickets, work, alone):
+                assert_same_stream(s.download(t), want, f"session beside singles: {q}")
+                s.release(t)
+        st = s.stats()
+        assert st["device_error"] == 0 and st["restarts"] == 0
+    finally:
+        s.close()
+
+
 def test_short_estimates_are_admitted_again(setup):
     eng, db, tables, work, alone = setup
     s = vb.Serve(eng, result_budget_bytes=256 << 20)

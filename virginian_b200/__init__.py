@@ -79,13 +79,19 @@ class Engine:
     def stream(self) -> int:
         return lib().virg_gpu_engine_stream(self.h)
 
+    def set_shared_scan(self, enable: bool) -> None:
+        """Shared scans (on by default): in a launch of several queries, the
+        queries over one table claim its chunks interleaved, so a chunk's
+        columns come from device memory once and from L2 for the others."""
+        check(lib().virg_gpu_engine_set_shared_scan(self.h, 1 if enable else 0), "set shared scan")
+
     def set_shape(self, threads: int = 0, stage_kb: int = 0, stages: int = 0,
                   ctas_per_sm: int = 0, chunk_rows: int = 0, full_mode: int = 0) -> None:
         """Launch shape of later queries: compute threads per CTA, KB per
         staging buffer, buffers, CTAs per SM, the chunk bound and the full
         phase's mode (0 reads staged tiles in place, 1 gathers the selected
-        rows from device memory); 0 in a field keeps the automatic
-        choice."""
+        rows from device memory, 2 runs the projection over every row of a
+        staged group); 0 in a field keeps the automatic choice."""
         check(lib().virg_gpu_engine_set_shape(self.h, threads, stage_kb, stages,
                                               ctas_per_sm), "set shape")
         check(lib().virg_gpu_engine_set_chunk_rows(self.h, chunk_rows), "set chunk rows")

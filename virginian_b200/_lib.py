@@ -90,6 +90,7 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         "virg_gpu_engine_set_shape": (i, [vp, u, u, u, u]),
         "virg_gpu_engine_set_chunk_rows": (i, [vp, u]),
         "virg_gpu_engine_set_full_mode": (i, [vp, u]),
+        "virg_gpu_engine_set_shared_scan": (i, [vp, i]),
         "virg_gpu_engine_launches": (ctypes.c_ulonglong, [vp]),
         "virg_gpu_engine_timing": (i, [vp, u]),
         "virg_gpu_engine_kernel_times": (i, [vp, P(ctypes.c_float), u, P(u)]),

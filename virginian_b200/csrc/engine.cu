@@ -10,10 +10,13 @@
  * a multiple of 64 rows plus 16, so a tile of any column is one aligned bulk
  * copy and the 8-byte key-pointer column never crosses the bus.
  *
- * Launch planning.  One launch runs any number of queries: their tiles are
- * numbered query by query, CTAs claim tiles in order, and each query's tiles
- * chain their look-back through the engine's status words, which carry a
- * per-launch epoch so the array never needs clearing between launches.
+ * Launch planning.  One launch runs any number of queries: their chunks are
+ * numbered query by query, CTAs claim chunks in order, and each query's
+ * chunks chain their look-back through the engine's status words, which
+ * carry a per-launch epoch so the array never needs clearing between
+ * launches.  Queries over the same table sit side by side and claim their
+ * chunks interleaved (a shared scan), so each chunk of the table is read
+ * from HBM once and from L2 by the group's other queries.
  */
 #include <algorithm>
 #include <cstring>
@@ -266,7 +269,23 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 	const uint32_t tf = tile_rows(pp.full_bpr, stage, chunk_cap);
 	VGPU_CHECK(tf >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the results read",
 		g.shape.stage_kb, kCountGroup * kBlockRows, pp.full_bpr);
-	const uint32_t chunk = std::max(tf, chunk_cap / tf * tf);
+	/* the chunk: a multiple of the full tile, at most the cap, whose count
+	 * and full tiles fill their data buffers best (a short last tile still
+	 * takes a whole buffer, and every buffer use costs the same issue and
+	 * claim work): the most rows per buffer use, ties to the larger chunk */
+	uint32_t chunk = tf;
+	uint64_t best_num = 0, best_den = 1;
+	for (uint32_t c = tf; c <= std::max(tf, chunk_cap); c += tf) {
+		const uint32_t t = tile_rows(pp.count_bpr, stage, c);
+		if (t < kBlockRows)
+			break;
+		const uint64_t uses = (c + t - 1) / t + (pp.mode == FM_GATHER ? 0u : c / tf);
+		if ((uint64_t)c * best_den >= best_num * uses) {
+			best_num = c;
+			best_den = uses;
+			chunk = c;
+		}
+	}
 	const uint32_t tc = tile_rows(pp.count_bpr, stage, chunk);
 	VGPU_CHECK(tc >= kBlockRows, "a %u KB stage cannot hold %u rows of the %u bytes per row the filter reads",
 		g.shape.stage_kb, kCountGroup * kBlockRows, pp.count_bpr);
@@ -274,8 +293,11 @@ int desc_fill(QDesc &d, const Program &P, const ProgPlan &pp, const Geom &g, uin
 	load_set(d.count_set, P, pp.count_cols, pp.ncount, tc);
 	if (pp.mode == FM_GATHER) {
 		/* one full entry per chunk; the staged columns of a batch are its
-		 * 32 kBatchE gathered entries, in the warp's gather area */
-		const uint32_t gchunk = chunk_cap;
+		 * 32 kBatchE gathered entries, in the warp's gather area.  The
+		 * chunk is a whole number of count tiles, so every count buffer
+		 * use is full */
+		const uint32_t tcap = tile_rows(pp.count_bpr, stage, chunk_cap);
+		const uint32_t gchunk = tcap >= kBlockRows ? std::max(tcap, chunk_cap / tcap * tcap) : chunk_cap;
 		load_set(d.full_set, P, pp.full_cols, pp.nfull, kBatchRows * g.ub, 0);
 		d.full_set.rows = gchunk;
 		d.chunk_rows = gchunk;
@@ -411,9 +433,24 @@ int choose_shape(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, Geom *g
 	s.stages = e->pref.stages;
 	s.ctas_per_sm = e->pref.ctas_per_sm;
 	s.chunk_rows = e->pref.chunk_rows;
-	/* a stage holds at least one group of kCountGroup blocks of the widest phase */
-	if (!e->pref.stage_kb)
-		s.stage_kb = std::max<unsigned>(s.stage_kb, (kCountGroup * kBlockRows * bpr + 1023) / 1024);
+	/* a stage holds at least one group of kCountGroup blocks of the widest
+	 * phase; without a preference, the largest data buffers of which three
+	 * fit beside the warps' areas (fewer, fuller buffer uses per row: each
+	 * use costs the same issue, claim and release work), else the smallest
+	 * size that fits at all */
+	const unsigned min_kb = (kCountGroup * kBlockRows * bpr + 1023) / 1024;
+	if (!e->pref.stage_kb) {
+		s.stage_kb = std::max<unsigned>(32, min_kb);
+		for (unsigned kb : {48u, 40u, 32u, 24u}) {
+			Shape t = s;
+			t.stage_kb = std::max(kb, min_kb);
+			Geom gt;
+			if (geom_make(t, sel, row, gat, e->smem_optin, e->smem_sm, &gt) && gt.shape.stages >= 3) {
+				*g = gt;
+				return 1;
+			}
+		}
+	}
 	if (geom_make(s, sel, row, gat, e->smem_optin, e->smem_sm, g))
 		return 1;
 	/* a dense full phase whose row vectors leave no room for two stages
@@ -439,12 +476,14 @@ size_t plan_blob_bytes(const std::vector<QueryLaunch> &qs, size_t *off_prefix, s
 	return *off_chunks + words * sizeof(uint32_t);
 }
 
-/* the automatic chunk bound: 4096 rows, smaller (down to 1024) when the
- * launch has too few rows to give every CTA a few chunks */
+/* the automatic chunk bound: kMaxChunkRows, smaller (down to 1024) when
+ * the launch has too few rows to give every CTA a few chunks (each query's
+ * chunk is then the multiple of its tiles below the bound that fills its
+ * buffers best) */
 static uint32_t auto_chunk(uint64_t rows, unsigned ctas)
 {
 	const uint64_t want = rows / (4ull * std::max(ctas, 1u));
-	return (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(4096, want / kBlockRows * kBlockRows));
+	return (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(kMaxChunkRows, want / kBlockRows * kBlockRows));
 }
 
 /* descriptor blob: QDesc[nq] | q_work_prefix[nq+1] | seg_chunk_prefix...,
@@ -486,15 +525,47 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 	QDesc *hq = reinterpret_cast<QDesc *>(hb);
 	uint64_t *hprefix = reinterpret_cast<uint64_t *>(hb + off_prefix);
 	uint32_t *hchunks = reinterpret_cast<uint32_t *>(hb + off_chunks);
+	/* descriptors in work-list order: the queries over one table (the same
+	 * segments, chunked alike) side by side as a shared scan whose chunks
+	 * are claimed interleaved (QDesc::grp_size), the groups in the order of
+	 * their first query.  Nothing outside the blob refers to a
+	 * descriptor's place: results, counts and look-back words go through
+	 * its own pointers and work range. */
+	std::vector<QDesc> descs(nq);
+	std::vector<size_t> order;
+	order.reserve(nq);
+	{
+		std::map<std::pair<const void *, uint32_t>, std::vector<size_t>> groups;
+		std::vector<std::pair<const void *, uint32_t>> keys;
+		for (size_t i = 0; i < nq; i++) {
+			const QueryLaunch &q = qs[i];
+			QDesc &d = descs[i];
+			memset(&d, 0, sizeof(d));
+			ProgPlan pp;
+			plan_program(*q.prog, pp, g.shape.full_mode);
+			if (!desc_fill(d, *q.prog, pp, g, cap))
+				return 0;
+			/* a query continuing an earlier launch's result scans alone */
+			const auto key = std::make_pair(e->shared_scan && !q.base_in ? (const void *)q.d_segs : (const void *)&qs[i],
+				d.chunk_rows);
+			auto it = groups.find(key);
+			if (it == groups.end()) {
+				keys.push_back(key);
+				it = groups.emplace(key, std::vector<size_t>()).first;
+			}
+			it->second.push_back(i);
+		}
+		for (const auto &k : keys)
+			for (size_t i : groups[k])
+				order.push_back(i);
+	}
 	uint64_t work = 0;
 	size_t cw = 0;
-	for (size_t i = 0; i < nq; i++) {
+	for (size_t p = 0; p < nq; p++) {
+		const size_t i = order[p];
 		const QueryLaunch &q = qs[i];
-		QDesc &d = hq[i];
-		ProgPlan pp;
-		plan_program(*q.prog, pp, g.shape.full_mode);
-		if (!desc_fill(d, *q.prog, pp, g, cap))
-			return 0;
+		QDesc &d = hq[p];
+		d = descs[i];
 		d.segs = q.d_segs;
 		d.nsegs = q.nsegs;
 		d.seg_chunk_prefix = reinterpret_cast<const uint32_t *>(db + off_chunks + cw * sizeof(uint32_t));
@@ -502,7 +573,7 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		cw += q.nsegs + 1;
 		d.work_first = work;
 		d.nchunks = nch;
-		hprefix[i] = work;
+		hprefix[p] = work;
 		work += nch;
 		for (unsigned j = 0; j < q.prog->nout; j++)
 			d.out_ptr[j] = q.out[j];
@@ -512,6 +583,22 @@ int plan_build(virg_gpu_engine *e, const std::vector<QueryLaunch> &qs, const Sha
 		d.base_in = q.base_in;
 	}
 	hprefix[nq] = work;
+	/* mark the shared scans: runs of two or more descriptors over the same
+	 * segments with the same chunking (so the same number of chunks) */
+	for (size_t p = 0; p < nq;) {
+		size_t r = p + 1;
+		while (r < nq && e->shared_scan && hq[r].segs == hq[p].segs && hq[r].nsegs == hq[p].nsegs &&
+			hq[r].chunk_rows == hq[p].chunk_rows && hq[r].nchunks == hq[p].nchunks && hq[p].nchunks &&
+			!hq[r].base_in && !hq[p].base_in)
+			r++;
+		if (r - p >= 2)
+			for (size_t x = p; x < r; x++) {
+				hq[x].grp_size = (uint32_t)(r - p);
+				hq[x].grp_q0 = (uint32_t)p;
+				hq[x].grp_first = (uint32_t)hq[p].work_first;
+			}
+		p = r;
+	}
 	VGPU_CHECK(work < 0xFFFFFFF0ull, "too many chunks in one launch (%llu)", (unsigned long long)work);
 	plan.work = work;
 	plan.nq = (uint32_t)nq;
@@ -859,6 +946,14 @@ extern "C" int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode)
 	VGPU_CHECK(e != nullptr, "null engine");
 	VGPU_CHECK(mode <= 2, "full-phase mode %u: 0 in place, 1 gather, 2 dense", mode);
 	e->pref.full_mode = mode;
+	return 1;
+}
+
+extern "C" int virg_gpu_engine_set_shared_scan(virg_gpu_engine *e, int enable)
+{
+	VGPU_CHECK(e != nullptr, "null engine");
+	std::lock_guard<std::mutex> lk(e->mu);
+	e->shared_scan = enable != 0;
 	return 1;
 }
 

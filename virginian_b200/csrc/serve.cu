@@ -68,7 +68,7 @@ constexpr uint64_t kSessionWorkLimit = 1ull << 31;
 /* (program, table) pairs whose last result size is remembered */
 constexpr size_t kHistoryLimit = 1 << 16;
 constexpr size_t kChunkPoolWords = 4u << 20;  /* segment chunk prefixes per session */
-constexpr uint32_t kServeChunkRows = 4096;
+constexpr uint32_t kServeChunkRows = kMaxChunkRows;  /* the bound; each query's chunk fills its buffers */
 
 using Clock = std::chrono::steady_clock;
 
@@ -539,10 +539,12 @@ extern "C" int virg_serve_create(virg_gpu_engine *e, const virg_serve_config *cf
 		c.idle_us = 50000;
 	if (!c.max_load_bytes_per_row)
 		c.max_load_bytes_per_row = 32;
+	/* the default vector bounds (12 and 20 bytes per row) leave three
+	 * 40 KB data buffers beside eight compute warps' areas */
 	if (!c.max_row_vector_bytes)
-		c.max_row_vector_bytes = 16;
+		c.max_row_vector_bytes = 12;
 	if (!c.max_sel_vector_bytes)
-		c.max_sel_vector_bytes = 48;
+		c.max_sel_vector_bytes = 20;
 	if (!c.wait_limit_ms)
 		c.wait_limit_ms = 60000;
 	auto fail = [&](const char *what, cudaError_t ce) {

@@ -232,7 +232,15 @@ struct alignas(16) QDesc {
 	const SegDesc *segs;
 	const uint32_t *seg_chunk_prefix;  /* nsegs + 1 entries */
 	uint32_t nsegs;
-	uint32_t pad1[3];
+	/* a shared scan: grp_size queries over the same segments with the same
+	 * chunking (descriptors grp_q0, grp_q0 + 1, ...) hold consecutive places
+	 * in the work list from grp_first on, and their chunks are claimed
+	 * interleaved (claim grp_first + t * grp_size + g is chunk t of query
+	 * grp_q0 + g), so one chunk of the table is read by all of them within
+	 * a few claims; grp_size 0 or 1: claims are work items */
+	uint32_t grp_size;
+	uint32_t grp_q0;
+	uint32_t grp_first;
 	LoadSet count_set, full_set;
 	Program prog;
 };

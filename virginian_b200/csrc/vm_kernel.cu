@@ -1593,6 +1593,7 @@ struct ProdQuery {
 	const uint32_t *chunk_prefix;
 	uint32_t nsegs, qi, seg_hint, chunk_rows;
 	uint32_t count_tile, full_tile;
+	uint32_t grp_size, grp_q0, grp_first;  /* the query's shared scan, if any */
 	bool gather;                  /* the full phase gathers (FM_GATHER) */
 	LaneCol cc, fc;               /* this lane's count and full column */
 	/* the current segment: its chunks [seg_c0, seg_c1) of the query, rows,
@@ -1610,30 +1611,51 @@ struct ProdChunk {
 	const unsigned char *ccol, *fcol;  /* this lane's columns at the chunk's first row */
 };
 
-/* decode work item w with the whole producer warp.  A CTA claims work items
- * in increasing order, so the query and segment searches start at the
- * previous item's. */
-__device__ __forceinline__ void decode_chunk(const KParams &kp, uint32_t w, uint32_t nq, ProdQuery &pq,
+/* the producer's copy of query qi's fields */
+__device__ __forceinline__ void load_query(const KParams &kp, uint32_t qi, ProdQuery &pq, int lane)
+{
+	const QDesc *Q = kp.queries + qi;
+	pq.Q = Q;
+	pq.qi = qi;
+	pq.first = Q->work_first;
+	pq.end = pq.first + Q->nchunks;
+	pq.segs = Q->segs;
+	pq.chunk_prefix = Q->seg_chunk_prefix;
+	pq.nsegs = Q->nsegs;
+	pq.chunk_rows = Q->chunk_rows;
+	pq.count_tile = Q->count_set.rows;
+	pq.full_tile = Q->full_set.rows;
+	pq.grp_size = Q->grp_size;
+	pq.grp_q0 = Q->grp_q0;
+	pq.grp_first = Q->grp_first;
+	pq.gather = Q->full_mode == FM_GATHER;
+	pq.cc = lane_col(Q->count_set, lane);
+	pq.fc = lane_col(Q->full_set, lane);
+	pq.seg_hint = 0;
+	pq.seg = ~0u;
+}
+
+/* decode claim `cl` with the whole producer warp: the work item it names
+ * (itself, or in a shared scan the chunk of one of the group's queries; see
+ * QDesc::grp_size) and that chunk's query, segment and columns.  A CTA's
+ * claims increase, so a search starts at the previous claim's query when it
+ * can; a claim in the previous claim's group needs no search at all. */
+__device__ __forceinline__ void decode_chunk(const KParams &kp, uint32_t cl, uint32_t nq, ProdQuery &pq,
 	ProdChunk &c, int lane)
 {
-	if (pq.Q == nullptr || w >= pq.end) {
-		const uint32_t qi = warp_search(kp.q_work_prefix, pq.Q ? pq.qi : 0u, nq, w, lane);
-		const QDesc *Q = kp.queries + qi;
-		pq.Q = Q;
-		pq.qi = qi;
-		pq.first = Q->work_first;
-		pq.end = pq.first + Q->nchunks;
-		pq.segs = Q->segs;
-		pq.chunk_prefix = Q->seg_chunk_prefix;
-		pq.nsegs = Q->nsegs;
-		pq.chunk_rows = Q->chunk_rows;
-		pq.count_tile = Q->count_set.rows;
-		pq.full_tile = Q->full_set.rows;
-		pq.gather = Q->full_mode == FM_GATHER;
-		pq.cc = lane_col(Q->count_set, lane);
-		pq.fc = lane_col(Q->full_set, lane);
-		pq.seg_hint = 0;
-		pq.seg = ~0u;
+	const bool in_group = pq.Q != nullptr && pq.grp_size > 1 && cl >= pq.grp_first &&
+		cl - pq.grp_first < pq.grp_size * (uint32_t)(pq.end - pq.first);
+	if (!in_group && (pq.Q == nullptr || cl < pq.first || cl >= pq.end)) {
+		const uint32_t lo = pq.Q != nullptr && cl >= pq.first ? pq.qi : 0u;
+		load_query(kp, warp_search(kp.q_work_prefix, lo, nq, cl, lane), pq, lane);
+	}
+	uint32_t w = cl;
+	if (pq.grp_size > 1) {
+		const uint32_t local = cl - pq.grp_first;
+		const uint32_t qi = pq.grp_q0 + local % pq.grp_size;
+		if (qi != pq.qi)
+			load_query(kp, qi, pq, lane);
+		w = (uint32_t)pq.first + local / pq.grp_size;
 	}
 	/* a chunk in the previous chunk's segment needs no load at all */
 	const uint32_t t = (uint32_t)(w - pq.first);
@@ -2246,22 +2268,36 @@ __global__ void __launch_bounds__(32 * (W + 2), 1) vm_kernel(const KParams kp)
 
 /* ---- host-side launcher ------------------------------------------------ */
 
+/* The kernel's dynamic shared-memory bound is always set to the device's
+ * opt-in maximum, never to one launch's size: host threads launching
+ * different shapes of the same kernel (a serving session beside single
+ * queries) would otherwise lower the bound under one another's launches. */
+static int allow_smem(const void *fn)
+{
+	int dev = 0, optin = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess ||
+		cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+		return 0;
+	return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) == cudaSuccess;
+}
+
 template <int W>
 static int launch_t(const KParams &kp, unsigned grid, size_t smem, cudaStream_t stream)
 {
 	auto fn = vm_kernel<W>;
-	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+	if (!allow_smem((const void *)fn))
 		return 0;
-	/* W compute warps, the producer and the look-back warp */
+	/* W compute warps, the producer and the look-back warp; a failed launch
+	 * leaves its error for the caller's message */
 	fn<<<grid, 32 * (W + 2), smem, stream>>>(kp);
-	return cudaGetLastError() == cudaSuccess;
+	return cudaPeekAtLastError() == cudaSuccess;
 }
 
 template <int W>
 static int occ_t(size_t smem, int *ctas)
 {
 	auto fn = vm_kernel<W>;
-	if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+	if (!allow_smem((const void *)fn))
 		return 0;
 	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, 32 * (W + 2), smem) == cudaSuccess;
 }
