@@ -1066,8 +1066,8 @@ def main():
                     help="rows of the streamed section's host table (400M: the streamed workload)")
     ap.add_argument("--no-parity", dest="parity", action="store_false",
                     help="skip the headline's byte comparison with the reference CPU VM")
-    ap.add_argument("--no-shared-scan", dest="shared_scan", action="store_false",
-                    help="claim each batched query's chunks in one run (no shared scans)")
+    ap.add_argument("--shared-scan", action="store_true",
+                    help="batched queries over one table claim its chunks interleaved (shared scans)")
     ap.add_argument("--sections", default="batched,serving,streamed,dropin,ref_gpu_vm",
                     help="workloads besides the headline scan (comma list; empty for none)")
     args = ap.parse_args()

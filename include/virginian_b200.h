@@ -311,10 +311,12 @@ int virg_gpu_engine_set_chunk_rows(virg_gpu_engine *e, unsigned rows);
  * filters that keep most rows).  Programs outside a mode's bounds, and
  * launches whose shape leaves no room for mode 2, keep mode 0. */
 int virg_gpu_engine_set_full_mode(virg_gpu_engine *e, unsigned mode);
-/* shared scans (on by default): in a launch of several queries, the queries
- * over the same table claim its chunks interleaved, so each chunk's columns
- * are read from device memory once and from L2 by the others; 0 turns it
- * off (each query's chunks are claimed in one run, as a single query's) */
+/* shared scans (off by default): in a launch of several queries, the
+ * queries over the same table claim its chunks interleaved, so each chunk's
+ * columns are read from device memory once and from L2 by the others.  Each
+ * claim then usually changes query, which costs the producer a descriptor
+ * load and the chunk slot a descriptor copy; on the bench's batch of 256
+ * generated queries that outweighs the L2 reuse (11.3 ms against 9.5 ms) */
 int virg_gpu_engine_set_shared_scan(virg_gpu_engine *e, int enable);
 /* record CUDA events around each of the next kernel launches in a ring of
  * `slots` entries (0 turns it off) */

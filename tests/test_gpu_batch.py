@@ -132,7 +132,7 @@ def test_shared_scans_give_the_same_bytes(setup, chunk_rows):
             results[shared] = [b.download(s) for s in range(len(many))]
             b.close()
     finally:
-        eng.set_shared_scan(True)
+        eng.set_shared_scan(False)
         eng.set_shape(0, 0, 0, 0)
     for s, (q, k) in enumerate(many):
         assert_same_stream(results[True][s], results[False][s], f"shared vs one run: {q}")

@@ -138,6 +138,47 @@ def test_refuses_more_rows_than_its_scratch(torch):
     assert "at most 67108864 rows" in _lib.lib().virg_gpu_last_error().decode()
 
 
+def test_refuses_host_and_misaligned_columns(torch):
+    """Columns outside the current device's memory, or not 16-byte aligned,
+    are refused on the host before anything is launched."""
+    n = 4096
+    cols = host_columns(n, seed=25)
+    prog = compile_program(CONFIG1)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in cols.items()}
+    outs = [torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(prog.info.nout)]
+    rows = ctypes.c_uint64(0)
+
+    def call(seg, out_ptrs):
+        ptrs = (ctypes.c_void_p * max(1, len(out_ptrs)))(*out_ptrs)
+        ok = _lib.lib().virg_gpu_query_prealloc(prog.h, ctypes.byref(seg), ptrs, n, ctypes.byref(rows), None)
+        return ok, ("" if ok else _lib.lib().virg_gpu_last_error().decode())
+
+    def segment(override=None):
+        seg = _lib.Segment()
+        seg.rows = n
+        seg.key = dev["id"].data_ptr()
+        for c, (name, _) in enumerate(datagen.SCHEMA_A):
+            seg.col[c] = dev[name].data_ptr()
+        if override:
+            for c, p in override.items():
+                seg.col[c] = p
+        return seg
+
+    good = [o.data_ptr() for o in outs]
+    host = np.ascontiguousarray(cols["uniformi"])
+    ci = [name for name, _ in datagen.SCHEMA_A].index("uniformi")
+    ok, err = call(segment({ci: host.ctypes.data}), good)
+    assert not ok and "current device's memory" in err, err
+    ok, err = call(segment({ci: dev["uniformi"].data_ptr() + 4}), good)
+    assert not ok and "16-byte aligned" in err, err
+    host_out = np.empty(n, dtype=np.int32)
+    ok, err = call(segment(), [host_out.ctypes.data] + good[1:])
+    assert not ok and "result columns must be in the current device's memory" in err, err
+    # the same call with its own buffers runs
+    ok, err = call(segment(), good)
+    assert ok, err
+
+
 def test_small_capacity_reports_overflow(torch, engine):
     cols = host_columns(50_000, seed=23)
     prog = compile_program("SELECT id, uniformi FROM test WHERE uniformi > 10")

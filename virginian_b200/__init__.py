@@ -80,7 +80,7 @@ class Engine:
         return lib().virg_gpu_engine_stream(self.h)
 
     def set_shared_scan(self, enable: bool) -> None:
-        """Shared scans (on by default): in a launch of several queries, the
+        """Shared scans (off by default): in a launch of several queries, the
         queries over one table claim its chunks interleaved, so a chunk's
         columns come from device memory once and from L2 for the others."""
         check(lib().virg_gpu_engine_set_shared_scan(self.h, 1 if enable else 0), "set shared scan")

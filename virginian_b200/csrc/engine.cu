@@ -14,9 +14,9 @@
  * numbered query by query, CTAs claim chunks in order, and each query's
  * chunks chain their look-back through the engine's status words, which
  * carry a per-launch epoch so the array never needs clearing between
- * launches.  Queries over the same table sit side by side and claim their
- * chunks interleaved (a shared scan), so each chunk of the table is read
- * from HBM once and from L2 by the group's other queries.
+ * launches.  With shared scans on, queries over the same table sit side by
+ * side and claim their chunks interleaved, so each chunk of the table is
+ * read from HBM once and from L2 by the group's other queries.
  */
 #include <algorithm>
 #include <cstring>

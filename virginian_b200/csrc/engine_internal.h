@@ -72,7 +72,7 @@ struct virg_gpu_engine {
 	std::map<std::string, vgpu::Shape> tuned;
 	std::string device_name;             /* keys the persistent tuned-shape cache */
 	vgpu::Shape force = {0, 0, 0, 0, 0, 0};  /* shape under trial while tuning */
-	bool shared_scan = true;             /* queries over one table claim their chunks interleaved */
+	bool shared_scan = false;            /* queries over one table claim their chunks interleaved */
 	std::mutex mu;
 };
 

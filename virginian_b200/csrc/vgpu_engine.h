@@ -56,21 +56,16 @@ constexpr unsigned kChunkSlots = 6;
 constexpr unsigned kCountAhead = 2;
 static_assert(kChunkSlots >= kCountAhead + 2, "slots for the chunks in flight");
 
-/* blocks a compute warp filters at once (16 rows per lane), blocks of a
- * full-phase group (its selected rows are listed and projected together;
- * kCountGroup when the full phase runs the filter again), and selection
- * entries per lane in a projection batch */
+/* blocks a compute warp filters at once (16 rows per lane; also the rows a
+ * re-filtering or dense full phase takes at once), and selection entries
+ * per lane in a projection batch */
 #ifndef VGPU_COUNT_GROUP
 #define VGPU_COUNT_GROUP 2
-#endif
-#ifndef VGPU_FULL_GROUP
-#define VGPU_FULL_GROUP 4
 #endif
 #ifndef VGPU_BATCH_E
 #define VGPU_BATCH_E 4
 #endif
 constexpr unsigned kCountGroup = VGPU_COUNT_GROUP;
-constexpr unsigned kFullGroup = VGPU_FULL_GROUP;
 constexpr unsigned kBatchE = VGPU_BATCH_E;
 /* a full-phase unit: one or (at most) kUnitBatches batches of 32 kBatchE
  * selected rows, each op run over all of them before the next op; a launch
@@ -79,8 +74,20 @@ constexpr unsigned kBatchE = VGPU_BATCH_E;
 constexpr unsigned kUnitBatches = 2;
 constexpr unsigned kBatchRows = 32 * kBatchE;
 constexpr unsigned kUnitE = kBatchRows * kUnitBatches;
+/* entries with fewer selected rows than this are split into units of half
+ * a batch, so more warps share a sparse tile (0: never, the default: on the
+ * headline query at 10% selectivity, 256 made the kernel 0.718 ms against
+ * 0.570 ms; the per-unit list and dispatch work outweighs the earlier
+ * release of the tile's buffer) */
+#ifndef VGPU_SMALL_UNIT_BELOW
+#define VGPU_SMALL_UNIT_BELOW 0
+#endif
+constexpr unsigned kSmallUnitBelow = VGPU_SMALL_UNIT_BELOW;
 static_assert(32 * kBatchE <= kCountGroup * kBlockRows, "a batch within a group");
-static_assert(kUnitE <= 2 * kFullGroup * kBlockRows / 2, "a unit's list within the list area");
+/* a compute warp's selection list: a 16-bit row per entry, for a
+ * re-filtered group's valid rows or a unit's entries */
+constexpr unsigned kListBytes = 2 * kCountGroup * kBlockRows;
+static_assert(kUnitE * 2 <= kListBytes, "a unit's list within the list area");
 
 /* per-stage tile, written by the producer before the stage's data lands */
 struct StageInfo {
@@ -148,7 +155,7 @@ inline WarpLayout warp_layout(unsigned sel_bytes_per_row, unsigned row_bytes_per
 {
 	WarpLayout w;
 	const unsigned ue = kBatchRows * unit_batches;
-	w.sel_off = 2u * kFullGroup * kBlockRows;
+	w.sel_off = kListBytes;
 	w.gat_off = w.sel_off + (ue * sel_bytes_per_row + 127u) / 128u * 128u;
 	w.row_off = w.gat_off + (ue * gather_bytes_per_row + 127u) / 128u * 128u;
 	w.bytes = w.row_off + (kCountGroup * kBlockRows * row_bytes_per_row + 127u) / 128u * 128u;

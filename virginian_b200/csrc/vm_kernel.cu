@@ -1248,19 +1248,20 @@ __device__ __forceinline__ uint32_t entry_selected(uint32_t slot, uint32_t blk0,
 }
 
 /* FM_BITMAP / FM_GATHER full phase: unit j of an entry's selected rows
- * (ranks [kBatchRows nb j, ...) of the nsel rows of chunk blocks
+ * (ranks [urows j, ...) of the nsel rows of chunk blocks
  * [blk0, blk0 + nblk), whose first is stored at off0).  The warp lists the
  * unit's rows from the bitmap, starting at the block that holds its first
  * rank, then reads them from the staged tile in place (b.stage the tile,
  * rows counted from its first row) or gathers them from device memory into
  * the warp's gather area.  Returns false on an output overflow. */
 __device__ __forceinline__ bool full_unit(Bases b, uint32_t list, uint32_t gat, uint32_t blk0, uint32_t nblk,
-	uint32_t j, uint32_t nb, uint32_t nsel, uint64_t off0, uint32_t mode, int lane)
+	uint32_t j, uint32_t urows, uint32_t nsel, uint64_t off0, uint32_t mode, int lane)
 {
-	const uint32_t r0 = kBatchRows * nb * j;
+	const uint32_t nb = urows > kBatchRows ? kUnitBatches : 1u;
+	const uint32_t r0 = urows * j;
 	if (r0 >= nsel)
 		return true;  /* an entry with no selected rows: nothing to do */
-	const uint32_t cnt = min(kBatchRows * nb, nsel - r0);
+	const uint32_t cnt = min(urows, nsel - r0);
 	/* the block holding rank r0: lane l looks at block blk0 + l */
 	uint32_t bo = 0, bc = 0;
 	if ((uint32_t)lane < nblk) {
@@ -2031,7 +2032,7 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 	};
 	/* the entry of the warp's last unit, kept for the fast claim below */
 	uint32_t k = 0, n = 0, kind = 0, slot = 0, seq = 0, row0 = 0, nrows = 0, buf = 0, mode = FM_BITMAP;
-	uint32_t nsel = 0, ub = 1;
+	uint32_t nsel = 0, urows = kBatchRows;
 	uint64_t off0 = 0;
 	bool have = false;
 	for (;;) {
@@ -2124,9 +2125,11 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					/* two-batch units for entries with at least two such
 					 * units of rows (dense entries: the op dispatch is shared
 					 * by twice the rows, and units still run in parallel),
-					 * where the launch's warp areas hold them */
-					ub = kp.unit_batches > 1 && nsel >= 2 * kUnitE ? kUnitBatches : 1u;
-					n = max(1u, (nsel + kBatchRows * ub - 1) / (kBatchRows * ub));
+					 * where the launch's warp areas hold them; half-batch
+					 * units for sparse entries */
+					urows = kp.unit_batches > 1 && nsel >= 2 * kUnitE ? kUnitE
+						: nsel < kSmallUnitBelow ? kBatchRows / 2 : kBatchRows;
+					n = max(1u, (nsel + urows - 1) / urows);
 				}
 			}
 			const uint32_t taken = c & 0xffffu;
@@ -2173,7 +2176,7 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					kp.unit_batches, lane);
 		} else {
 			b.stage = tile;
-			ok = full_unit(b, list, gat, blk0, nblk, j, ub, nsel, off0, mode, lane);
+			ok = full_unit(b, list, gat, blk0, nblk, j, urows, nsel, off0, mode, lane);
 		}
 		/* a serving session reports rows beyond capacity in the query's
 		 * completion record instead */
