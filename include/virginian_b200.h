@@ -449,13 +449,17 @@ int virg_gpu_query_streamed(virg_gpu_engine *e, const virg_gpu_program *p,
 	const virg_gpu_segment *segs, unsigned nsegs, unsigned segs_per_chunk,
 	virg_gpu_result **out, virg_gpu_stream_stats *stats);
 
-/* Batched persistent execution: every query added to a batch runs in one
- * launch of the VM kernel (chunks of all queries in one ordered work list).
- * A batch owns its descriptors and counters, so virg_gpu_batch_run with
- * use_graph captures the launch in a CUDA graph once and replays it after.
- * With autotune on, the first run times the candidate launch shapes on the
- * batch and caches the fastest in the engine per program-shape key.  Adding
- * a query after a run rebuilds the batch. */
+/* Batched persistent execution: the queries added to a batch run in one
+ * launch of the VM kernel (chunks of all queries in one ordered work list),
+ * or two: a launch's compute warps hold vector areas for its widest
+ * program, so programs too wide for three 48 KB data buffers beside eight
+ * compute warps run in a second launch and leave the others their larger
+ * buffers.  A batch owns its descriptors and counters, so
+ * virg_gpu_batch_run with use_graph captures its launches in a CUDA graph
+ * once and replays it after.  With autotune on, the first run times the
+ * candidate launch shapes for each launch on the batch and caches the
+ * fastest in the engine per program-shape key.  Adding a query after a run
+ * rebuilds the batch. */
 int virg_gpu_batch_create(virg_gpu_engine *e, virg_gpu_batch **out);
 int virg_gpu_batch_add(virg_gpu_batch *b, const virg_gpu_program *p, virg_gpu_table *t,
 	unsigned *slot);
@@ -467,7 +471,8 @@ int virg_gpu_batch_rows(virg_gpu_batch *b, unsigned slot, uint64_t *rows);
 const void *virg_gpu_batch_column(const virg_gpu_batch *b, unsigned slot, unsigned c);
 int virg_gpu_batch_download(virg_gpu_batch *b, unsigned slot, void *const *host_cols,
 	uint64_t first, uint64_t count);
-/* shape4 = {compute threads, stage KB, stages, grid}; work = chunks */
+/* shape4 = {compute threads, stage KB, stages, grid} of the launch with the
+ * most chunks; work = chunks of all launches */
 int virg_gpu_batch_shape(const virg_gpu_batch *b, unsigned *shape4, uint64_t *work);
 void virg_gpu_batch_destroy(virg_gpu_batch *b);
 

@@ -137,3 +137,29 @@ def test_shared_scans_give_the_same_bytes(setup, chunk_rows):
     for s, (q, k) in enumerate(many):
         assert_same_stream(results[True][s], results[False][s], f"shared vs one run: {q}")
         assert_same_stream(results[True][s], db.query(q).columns, q)
+
+
+WIDE_FILTER = ("select id from {t} where uniformi + normali5 > normali20 - uniformi and uniformi * normali5 < 1000 "
+               "and normali20 * 2 > uniformi - 7 and normali5 + normali20 < uniformi * 3")
+MANY_RESULTS = ("select uniformi + normali5 as a, uniformi - normali5 as b, uniformi * normali5 as c, "
+                "normali20 + 1 as d, normali20 * 3 as e, uniformf * 2.0 as f from {t} where uniformi > 20")
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_with_a_wide_program_runs_as_two_launches(setup, graph):
+    """A program whose filter needs more row-vector bytes than three 48 KB
+    data buffers leave room for runs in a second launch of the batch; every
+    query still gets the CPU VM's stream."""
+    eng, db, cat, tables, work = setup
+    many = [(WIDE_FILTER.format(t="t4"), 4), (MANY_RESULTS.format(t="t4"), 4),
+            (WIDE_FILTER.format(t="t6"), 6)] + work[:12] + [(MANY_RESULTS.format(t="t7"), 7)]
+    b = build_batch(eng, cat, tables, many)
+    b.run(graph=graph)
+    b.wait()
+    l0 = eng.launches
+    b.run(graph=graph)
+    b.wait()
+    assert eng.launches - l0 == 2
+    for slot, (q, k) in enumerate(many):
+        assert_same_stream(b.download(slot), db.query(q).columns, q)
+    b.close()

@@ -53,14 +53,22 @@ struct virg_gpu_batch {
 		virg_gpu_result *r;
 	};
 	std::vector<Item> items;
+	/* one launch per part: the programs whose compute warps' vector areas
+	 * leave three 48 KB data buffers, and the others (a launch's areas are
+	 * sized for its widest program, so one wide program would shrink every
+	 * query's buffers) */
+	struct Part {
+		std::vector<size_t> items;
+		Plan plan;
+		unsigned char *d_blob = nullptr;
+		uint64_t *d_status = nullptr;
+	};
+	std::vector<Part> parts;
 	bool built = false;
-	Plan plan;
-	unsigned char *d_blob = nullptr;
-	uint64_t *d_status = nullptr;
-	unsigned *d_ctrl = nullptr;            /* [0] work counter, [1] error */
+	unsigned *d_ctrl = nullptr;            /* per part p: [2p] work counter, [2p + 1] error */
 	unsigned long long *d_totals = nullptr;
 	unsigned long long *h_totals = nullptr;  /* pinned */
-	unsigned *h_err = nullptr;               /* pinned */
+	unsigned *h_ctrl = nullptr;              /* pinned copy of d_ctrl */
 	cudaGraphExec_t gexec = nullptr;
 	cudaEvent_t done = nullptr;
 	bool ran = false;
@@ -82,26 +90,27 @@ void batch_release(virg_gpu_batch *b)
 			virg_gpu_result_destroy(it.r);
 			it.r = nullptr;
 		}
-	if (b->d_blob) cudaFree(b->d_blob);
-	if (b->d_status) cudaFree(b->d_status);
+	for (auto &pt : b->parts) {
+		if (pt.d_blob) cudaFree(pt.d_blob);
+		if (pt.d_status) cudaFree(pt.d_status);
+	}
+	b->parts.clear();
 	if (b->d_ctrl) cudaFree(b->d_ctrl);
 	if (b->d_totals) cudaFree(b->d_totals);
 	if (b->h_totals) cudaFreeHost(b->h_totals);
-	if (b->h_err) cudaFreeHost(b->h_err);
-	b->d_blob = nullptr;
-	b->d_status = nullptr;
+	if (b->h_ctrl) cudaFreeHost(b->h_ctrl);
 	b->d_ctrl = nullptr;
 	b->d_totals = nullptr;
 	b->h_totals = nullptr;
-	b->h_err = nullptr;
+	b->h_ctrl = nullptr;
 	b->built = false;
 	b->ran = false;
 }
 
-std::vector<QueryLaunch> launches_of(virg_gpu_batch *b)
+std::vector<QueryLaunch> launches_of(virg_gpu_batch *b, size_t part)
 {
 	std::vector<QueryLaunch> qs;
-	for (size_t i = 0; i < b->items.size(); i++) {
+	for (size_t i : b->parts[part].items) {
 		auto &it = b->items[i];
 		QueryLaunch q;
 		q.prog = &it.p->prog;
@@ -123,45 +132,69 @@ int issue(virg_gpu_batch *b)
 {
 	virg_gpu_engine *e = b->e;
 	cudaStream_t s = e->stream;
-	const Plan &plan = b->plan;
-	CUDA_OK(cudaMemsetAsync(b->d_ctrl, 0, 2 * sizeof(unsigned), s), "batch counter reset");
+	const size_t np = b->parts.size();
+	CUDA_OK(cudaMemsetAsync(b->d_ctrl, 0, 2 * np * sizeof(unsigned), s), "batch counter reset");
 	CUDA_OK(cudaMemsetAsync(b->d_totals, 0, b->items.size() * sizeof(unsigned long long), s),
 		"batch totals reset");
-	if (plan.work) {
-		CUDA_OK(cudaMemsetAsync(b->d_status, 0, plan.work * sizeof(uint64_t), s), "batch status reset");
-		const KParams kp = plan_params(plan, b->d_blob, b->d_ctrl, b->d_status, b->d_ctrl + 1,
+	for (size_t p = 0; p < np; p++) {
+		const auto &pt = b->parts[p];
+		const Plan &plan = pt.plan;
+		if (!plan.work)
+			continue;
+		CUDA_OK(cudaMemsetAsync(pt.d_status, 0, plan.work * sizeof(uint64_t), s), "batch status reset");
+		const KParams kp = plan_params(plan, pt.d_blob, b->d_ctrl + 2 * p, pt.d_status, b->d_ctrl + 2 * p + 1,
 			kBatchEpoch);
 		if (!launch_vm(plan.geom.shape, kp, plan.grid, plan.geom.smem, s))
 			VGPU_FAIL("batch kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
 	}
 	CUDA_OK(cudaMemcpyAsync(b->h_totals, b->d_totals, b->items.size() * sizeof(unsigned long long),
 		cudaMemcpyDeviceToHost, s), "batch totals read");
-	CUDA_OK(cudaMemcpyAsync(b->h_err, b->d_ctrl + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s),
+	CUDA_OK(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, 2 * np * sizeof(unsigned), cudaMemcpyDeviceToHost, s),
 		"batch error read");
 	return 1;
 }
 
-int build_with(virg_gpu_batch *b, const Shape *forced)
+/* the first part's device error, once the batch's copies have landed */
+unsigned batch_error(const virg_gpu_batch *b)
+{
+	for (size_t p = 0; p < b->parts.size(); p++)
+		if (b->h_ctrl[2 * p + 1])
+			return b->h_ctrl[2 * p + 1];
+	return 0;
+}
+
+/* the part with the most work (its shape is the batch's reported shape) */
+size_t main_part(const virg_gpu_batch *b)
+{
+	size_t m = 0;
+	for (size_t p = 1; p < b->parts.size(); p++)
+		if (b->parts[p].plan.work > b->parts[m].plan.work)
+			m = p;
+	return m;
+}
+
+int build_with(virg_gpu_batch *b, size_t part, const Shape *forced)
 {
 	virg_gpu_engine *e = b->e;
-	std::vector<QueryLaunch> qs = launches_of(b);
+	auto &pt = b->parts[part];
+	std::vector<QueryLaunch> qs = launches_of(b, part);
 	size_t off_prefix, off_chunks;
 	const size_t bytes = plan_blob_bytes(qs, &off_prefix, &off_chunks);
-	if (!b->d_blob)
-		CUDA_OK(cudaMalloc((void **)&b->d_blob, bytes), "batch descriptor alloc");
+	if (!pt.d_blob)
+		CUDA_OK(cudaMalloc((void **)&pt.d_blob, bytes), "batch descriptor alloc");
 	Plan plan;
-	if (!plan_build(e, qs, forced, b->d_blob, plan))
+	if (!plan_build(e, qs, forced, pt.d_blob, plan))
 		return 0;
-	CUDA_OK(cudaMemcpy(b->d_blob, plan.blob.data(), plan.blob.size(), cudaMemcpyHostToDevice),
+	CUDA_OK(cudaMemcpy(pt.d_blob, plan.blob.data(), plan.blob.size(), cudaMemcpyHostToDevice),
 		"batch descriptor copy");
-	if (b->d_status && b->plan.work < plan.work) {
-		cudaFree(b->d_status);
-		b->d_status = nullptr;
+	if (pt.d_status && pt.plan.work < plan.work) {
+		cudaFree(pt.d_status);
+		pt.d_status = nullptr;
 	}
-	if (!b->d_status)
-		CUDA_OK(cudaMalloc((void **)&b->d_status, std::max<uint64_t>(plan.work, 1) * sizeof(uint64_t)),
+	if (!pt.d_status)
+		CUDA_OK(cudaMalloc((void **)&pt.d_status, std::max<uint64_t>(plan.work, 1) * sizeof(uint64_t)),
 			"batch status alloc");
-	b->plan = std::move(plan);
+	pt.plan = std::move(plan);
 	if (b->gexec) {
 		cudaGraphExecDestroy(b->gexec);
 		b->gexec = nullptr;
@@ -184,21 +217,23 @@ float time_once(virg_gpu_batch *b)
 		cudaEventElapsedTime(&ms, a, z);
 	cudaEventDestroy(a);
 	cudaEventDestroy(z);
-	return ok && *b->h_err == 0 ? ms : -1.0f;
+	return ok && batch_error(b) == 0 ? ms : -1.0f;
 }
 
-int autotune(virg_gpu_batch *b)
+/* tune each part in turn (the others at their current shapes), timing the
+ * whole batch; the winner is cached per part's program-shape key */
+int autotune_part(virg_gpu_batch *b, size_t part)
 {
 	virg_gpu_engine *e = b->e;
-	const std::string key = shape_key(launches_of(b));
+	const std::string key = shape_key(launches_of(b, part));
 	auto hit = e->tuned.find(key);
 	if (hit != e->tuned.end())
-		return build_with(b, &hit->second);
+		return build_with(b, part, &hit->second);
 	float best = 1e30f;
 	Shape best_shape = {0, 0, 0, 0, 0, 0};
 	for (const Shape &c : tune_candidates()) {
 		set_error("%s", "");
-		if (!build_with(b, &c))
+		if (!build_with(b, part, &c))
 			continue;  /* does not fit shared memory */
 		float t = 1e30f;
 		for (int rep = 0; rep < 3; rep++) {
@@ -209,12 +244,79 @@ int autotune(virg_gpu_batch *b)
 		}
 		if (t < best) {
 			best = t;
-			best_shape = b->plan.geom.shape;
+			best_shape = b->parts[part].plan.geom.shape;
 		}
 	}
 	VGPU_CHECK(best_shape.threads != 0, "no launch shape fits this batch");
 	tune_remember(e, key, best_shape);
-	return build_with(b, &best_shape);
+	return build_with(b, part, &best_shape);
+}
+
+/* split the items into parts.  A launch's warp areas hold its largest
+ * selection, row and gather vectors (possibly of different programs), so
+ * the first part is the set of programs under a pair of limits (row vector
+ * bytes r, selection vector bytes s) whose combined layout leaves three
+ * 48 KB data buffers beside eight compute warps, chosen to cover the most
+ * table rows; the others form the second part (one part if either is
+ * empty).  Item order is kept within a part. */
+void make_parts(virg_gpu_batch *b)
+{
+	virg_gpu_engine *e = b->e;
+	const size_t n = b->items.size();
+	std::vector<ProgPlan> pp(n);
+	std::vector<uint32_t> rows_opts, sel_opts;
+	for (size_t i = 0; i < n; i++) {
+		plan_program(b->items[i].p->prog, pp[i], e->pref.full_mode);
+		rows_opts.push_back(pp[i].row_bpr);
+		sel_opts.push_back(pp[i].sel_bpr);
+	}
+	std::sort(rows_opts.begin(), rows_opts.end());
+	rows_opts.erase(std::unique(rows_opts.begin(), rows_opts.end()), rows_opts.end());
+	std::sort(sel_opts.begin(), sel_opts.end());
+	sel_opts.erase(std::unique(sel_opts.begin(), sel_opts.end()), sel_opts.end());
+	const Shape s = {256, 48, 3, 1, 0, e->pref.full_mode};
+	auto fits = [&](uint32_t sel, uint32_t row, uint32_t gat) {
+		Geom g;
+		return geom_make(s, sel, row, gat, e->smem_optin, e->smem_sm, &g, 1) != 0;
+	};
+	uint64_t best_w = 0;
+	uint32_t best_r = 0, best_s = 0;
+	bool have = false;
+	for (uint32_t r : rows_opts) {
+		for (auto it = sel_opts.rbegin(); it != sel_opts.rend(); ++it) {
+			uint32_t gat = 0;
+			uint64_t w = 0;
+			for (size_t i = 0; i < n; i++)
+				if (pp[i].row_bpr <= r && pp[i].sel_bpr <= *it) {
+					gat = std::max(gat, pp[i].gather_bpr);
+					w += b->items[i].t->rows + 1;
+				}
+			if (!fits(*it, r, gat))
+				continue;
+			if (!have || w > best_w) {
+				have = true;
+				best_w = w;
+				best_r = r;
+				best_s = *it;
+			}
+			break;  /* the largest selection limit that fits for this r */
+		}
+	}
+	std::vector<size_t> narrow, wide;
+	for (size_t i = 0; i < n; i++)
+		(have && pp[i].row_bpr <= best_r && pp[i].sel_bpr <= best_s ? narrow : wide).push_back(i);
+	set_error("%s", "");
+	b->parts.clear();
+	if (narrow.empty() || wide.empty()) {
+		b->parts.emplace_back();
+		for (size_t i = 0; i < b->items.size(); i++)
+			b->parts.back().items.push_back(i);
+	} else {
+		b->parts.emplace_back();
+		b->parts.back().items = narrow;
+		b->parts.emplace_back();
+		b->parts.back().items = wide;
+	}
 }
 
 }  // namespace
@@ -270,16 +372,22 @@ static int batch_build(virg_gpu_batch *b)
 			return 0;
 	}
 	const size_t nq = b->items.size();
-	CUDA_OK(cudaMalloc((void **)&b->d_ctrl, 2 * sizeof(unsigned)), "batch control alloc");
+	make_parts(b);
+	const size_t np = b->parts.size();
+	CUDA_OK(cudaMalloc((void **)&b->d_ctrl, 2 * np * sizeof(unsigned)), "batch control alloc");
 	CUDA_OK(cudaMalloc((void **)&b->d_totals, nq * sizeof(unsigned long long)), "batch totals alloc");
 	CUDA_OK(cudaHostAlloc((void **)&b->h_totals, nq * sizeof(unsigned long long), cudaHostAllocDefault),
 		"batch pinned totals");
-	CUDA_OK(cudaHostAlloc((void **)&b->h_err, sizeof(unsigned), cudaHostAllocDefault),
-		"batch pinned error");
+	CUDA_OK(cudaHostAlloc((void **)&b->h_ctrl, 2 * np * sizeof(unsigned), cudaHostAllocDefault),
+		"batch pinned control");
 	CUDA_OK(cudaStreamSynchronize(e->stream), "batch result alloc");
-	int ok = b->tune ? autotune(b) : build_with(b, nullptr);
-	if (!ok)
-		return 0;
+	for (size_t p = 0; p < np; p++)
+		if (!build_with(b, p, nullptr))
+			return 0;
+	if (b->tune)
+		for (size_t p = 0; p < np; p++)
+			if (!autotune_part(b, p))
+				return 0;
 	for (size_t i = 0; i < nq; i++)
 		b->items[i].r->d_total = b->d_totals + i;
 	if (!b->done)
@@ -317,10 +425,12 @@ extern "C" int virg_gpu_batch_run(virg_gpu_batch *b, int use_graph)
 		return 0;
 	}
 	CUDA_OK(cudaEventRecord(b->done, s), "batch event record");
-	e->launches += b->plan.work ? 1 : 0;
-	e->last_shape = b->plan.geom.shape;
-	e->last_grid = b->plan.grid;
-	e->last_smem = b->plan.geom.smem;
+	for (const auto &pt : b->parts)
+		e->launches += pt.plan.work ? 1 : 0;
+	const Plan &mp = b->parts[main_part(b)].plan;
+	e->last_shape = mp.geom.shape;
+	e->last_grid = mp.grid;
+	e->last_smem = mp.geom.smem;
 	b->ran = true;
 	return 1;
 }
@@ -329,7 +439,8 @@ extern "C" int virg_gpu_batch_wait(virg_gpu_batch *b)
 {
 	VGPU_CHECK(b != nullptr && b->ran, "batch has not run");
 	CUDA_OK(cudaEventSynchronize(b->done), "batch wait");
-	VGPU_CHECK(*b->h_err == 0, "batch failed on the device: %s", device_error_text(*b->h_err));
+	const unsigned err = batch_error(b);
+	VGPU_CHECK(err == 0, "batch failed on the device: %s", device_error_text(err));
 	for (size_t i = 0; i < b->items.size(); i++) {
 		virg_gpu_result *r = b->items[i].r;
 		r->rows = b->h_totals[i];
@@ -367,14 +478,18 @@ extern "C" int virg_gpu_batch_download(virg_gpu_batch *b, unsigned slot, void *c
 extern "C" int virg_gpu_batch_shape(const virg_gpu_batch *b, unsigned *shape4, uint64_t *work)
 {
 	VGPU_CHECK(b != nullptr && b->built, "batch not built");
+	const Plan &mp = b->parts[main_part(b)].plan;
 	if (shape4) {
-		shape4[0] = b->plan.geom.shape.threads;
-		shape4[1] = b->plan.geom.shape.stage_kb;
-		shape4[2] = b->plan.geom.shape.stages;
-		shape4[3] = b->plan.grid;
+		shape4[0] = mp.geom.shape.threads;
+		shape4[1] = mp.geom.shape.stage_kb;
+		shape4[2] = mp.geom.shape.stages;
+		shape4[3] = mp.grid;
 	}
-	if (work)
-		*work = b->plan.work;
+	if (work) {
+		*work = 0;
+		for (const auto &pt : b->parts)
+			*work += pt.plan.work;
+	}
 	return 1;
 }
 
