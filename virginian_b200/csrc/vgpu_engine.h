@@ -74,15 +74,6 @@ constexpr unsigned kBatchE = VGPU_BATCH_E;
 constexpr unsigned kUnitBatches = 2;
 constexpr unsigned kBatchRows = 32 * kBatchE;
 constexpr unsigned kUnitE = kBatchRows * kUnitBatches;
-/* entries with fewer selected rows than this are split into units of half
- * a batch, so more warps share a sparse tile (0: never, the default: on the
- * headline query at 10% selectivity, 256 made the kernel 0.718 ms against
- * 0.570 ms; the per-unit list and dispatch work outweighs the earlier
- * release of the tile's buffer) */
-#ifndef VGPU_SMALL_UNIT_BELOW
-#define VGPU_SMALL_UNIT_BELOW 0
-#endif
-constexpr unsigned kSmallUnitBelow = VGPU_SMALL_UNIT_BELOW;
 static_assert(32 * kBatchE <= kCountGroup * kBlockRows, "a batch within a group");
 /* a compute warp's selection list: a 16-bit row per entry, for a
  * re-filtered group's valid rows or a unit's entries */

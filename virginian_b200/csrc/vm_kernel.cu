@@ -50,6 +50,11 @@ namespace vgpu {
  * limit (a second by default), far beyond any real wait; look-back polls
  * after 2^24 rounds of 32-256 ns */
 constexpr uint32_t kSuspendHintNs = 20000;
+/* 1: the producer gives a tile the first released data buffer; 0: buffers
+ * in turn */
+#ifndef VGPU_BUF_FREELIST
+#define VGPU_BUF_FREELIST 0
+#endif
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
 /* where the fields the kernel's warps read sit in a slot's descriptor copy */
@@ -1713,6 +1718,11 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 	pq.qi = 0;
 	uint32_t k = 0;   /* entries issued */
 	uint32_t nb = 0;  /* data buffers taken */
+#if VGPU_BUF_FREELIST
+	/* buffer lane's uses so far (lanes below nst): a tile takes whichever
+	 * buffer was released first, not the next in turn */
+	uint32_t buses = 0;
+#endif
 	uint32_t i = 0;   /* chunks set up (and the end) */
 	bool failed = false;
 
@@ -1739,16 +1749,57 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 		const LaneCol &col, const unsigned char *src, bool staged) -> bool {
 		const uint32_t s = k % kEntries;
 		const uint32_t full = sbase + kOffFull + 8 * s;
+#if VGPU_BUF_FREELIST
+		uint32_t bf = kNoBuf;
+#else
 		const uint32_t bf = staged ? nb % nst : kNoBuf;
+#endif
 		int ok = 1;
 		if (lane == 0) {
 			if (k >= kEntries)
 				ok = mbar_wait(sbase + kOffEmpty + 8 * s, ((k / kEntries) - 1) & 1u, flags);
+#if !VGPU_BUF_FREELIST
 			if (ok && staged && nb >= nst)
 				ok = mbar_wait(sbase + kOffBfree + 8 * bf, ((nb / nst) - 1) & 1u, flags);
+#endif
 		}
 		if (!__shfl_sync(0xffffffffu, ok, 0))
 			return false;
+#if VGPU_BUF_FREELIST
+		if (staged) {
+			/* buffer b is free once its releases equal its uses: the phase
+			 * of its last use has completed (or it has none) */
+			uint64_t t0 = 0;
+			for (uint32_t spin = 0;; spin++) {
+				const bool fr = (uint32_t)lane < nst &&
+					(buses == 0 || mbar_test(sbase + kOffBfree + 8 * (uint32_t)lane, (buses - 1) & 1u));
+				const uint32_t m = __ballot_sync(0xffffffffu, fr);
+				if (m) {
+					bf = (uint32_t)(__ffs(m) - 1);
+					break;
+				}
+				if ((spin & 63u) == 63u) {
+					int give_up = 0;
+					if (lane == 0) {
+						const uint64_t now = globaltimer_ns();
+						if (t0 == 0)
+							t0 = now;
+						else {
+							uint32_t ab;
+							asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(ab) : "r"(flags + 4 * kFAbort));
+							if (ab || now - t0 > (uint64_t)lds_u32(flags + 4 * kFWaitMs) * 1000000ull)
+								give_up = 1;
+						}
+					}
+					if (__shfl_sync(0xffffffffu, give_up, 0))
+						return false;
+				}
+				__nanosleep(32);
+			}
+			if ((uint32_t)lane == bf)
+				buses++;
+		}
+#endif
 		const uint32_t data = sbase + kp.stage_area + (staged ? bf : 0u) * kp.stage_bytes;
 		uint32_t bulk = 0;
 		if (staged && col.has && nrows) {
@@ -2125,10 +2176,8 @@ __device__ void compute_warp(const KParams &kp, unsigned char *smem, int w, int 
 					/* two-batch units for entries with at least two such
 					 * units of rows (dense entries: the op dispatch is shared
 					 * by twice the rows, and units still run in parallel),
-					 * where the launch's warp areas hold them; half-batch
-					 * units for sparse entries */
-					urows = kp.unit_batches > 1 && nsel >= 2 * kUnitE ? kUnitE
-						: nsel < kSmallUnitBelow ? kBatchRows / 2 : kBatchRows;
+					 * where the launch's warp areas hold them */
+					urows = kp.unit_batches > 1 && nsel >= 2 * kUnitE ? kUnitE : kBatchRows;
 					n = max(1u, (nsel + urows - 1) / urows);
 				}
 			}
