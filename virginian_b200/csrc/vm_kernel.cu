@@ -22,10 +22,12 @@
  *    the projection ops on the selected rows 32 at a time and store them
  *    at the block's offset (coalesced, original row order).
  *
- * The producer issues a chunk's count phase kCountAhead chunks before its
- * full phase, so a chunk's offset is resolved while the CTA counts the next
- * chunks: no stage waits for another CTA, and a column both phases read is
- * read from HBM once and found in L2 the second time.
+ * The producer takes the data buffer in turn if it is free, else the next
+ * one released (tiles release out of order), and issues a chunk's count
+ * phase kCountAhead chunks before its full phase, so a chunk's offset is
+ * resolved while the CTA counts the next chunks: no stage waits for another
+ * CTA, and a column both phases read is read from HBM once and found in L2
+ * the second time.
  *
  * Each op is one 16-byte record read with one shared-memory load and
  * dispatched by bit tests on its head; operands are read and written by
@@ -50,10 +52,12 @@ namespace vgpu {
  * limit (a second by default), far beyond any real wait; look-back polls
  * after 2^24 rounds of 32-256 ns */
 constexpr uint32_t kSuspendHintNs = 20000;
-/* 1: the producer gives a tile the first released data buffer; 0: buffers
- * in turn */
+/* 1 (default): the producer gives a tile the buffer in turn if it is free,
+ * else the next released one (entries release their buffers out of order:
+ * a count tile keeps its buffer for a dozen groups, a sparse projection
+ * tile for a unit or two); 0: buffers strictly in turn */
 #ifndef VGPU_BUF_FREELIST
-#define VGPU_BUF_FREELIST 0
+#define VGPU_BUF_FREELIST 1
 #endif
 constexpr unsigned kLookbackSpinLimit = 1u << 24;
 
@@ -1768,16 +1772,25 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 #if VGPU_BUF_FREELIST
 		if (staged) {
 			/* buffer b is free once its releases equal its uses: the phase
-			 * of its last use has completed (or it has none) */
+			 * of its last use has completed (or it has none).  The buffer
+			 * in turn if it is free, else the next free one after it; with
+			 * none free, sleep on the one in turn (hardware-suspended,
+			 * woken by its release) and look again */
+			const uint32_t turn = nb % nst;
+			const uint32_t tuses = __shfl_sync(0xffffffffu, buses, (int)turn);
 			uint64_t t0 = 0;
 			for (uint32_t spin = 0;; spin++) {
 				const bool fr = (uint32_t)lane < nst &&
 					(buses == 0 || mbar_test(sbase + kOffBfree + 8 * (uint32_t)lane, (buses - 1) & 1u));
 				const uint32_t m = __ballot_sync(0xffffffffu, fr);
 				if (m) {
-					bf = (uint32_t)(__ffs(m) - 1);
+					const uint32_t after = m & (0xffffffffu << turn);
+					bf = (uint32_t)(__ffs(after ? after : m) - 1);
 					break;
 				}
+				if (lane == 0 && tuses)
+					mbar_try_wait_hint(sbase + kOffBfree + 8 * turn, (tuses - 1) & 1u, 2000);
+				__syncwarp();
 				if ((spin & 63u) == 63u) {
 					int give_up = 0;
 					if (lane == 0) {
@@ -1794,7 +1807,6 @@ __device__ void producer(const KParams &kp, unsigned char *smem, int lane)
 					if (__shfl_sync(0xffffffffu, give_up, 0))
 						return false;
 				}
-				__nanosleep(32);
 			}
 			if ((uint32_t)lane == bf)
 				buses++;
