@@ -46,9 +46,9 @@ WORKLOAD = ("device-resident filter scan + arithmetic (7-column table, 50M rows 
             "10% selectivity)")
 # DRAM bytes of the headline kernel per scanned row and per result row,
 # from ncu (dram__bytes_read.sum, dram__bytes_write.sum) on an 8M-row launch
-# of the same query: 228.83 MB read, 10.36 MB written for 800,581 result rows
-TRAFFIC_READ_PER_ROW = 228.83072e6 / 8_000_000
-TRAFFIC_WRITE_PER_RESULT_ROW = 10.357248e6 / 800_581
+# of the same query: 229.66 MB read, 10.04 MB written for 800,581 result rows
+TRAFFIC_READ_PER_ROW = 229.662976e6 / 8_000_000
+TRAFFIC_WRITE_PER_RESULT_ROW = 10.035456e6 / 800_581
 SWEEP = [0.001, 0.01, 0.10, 0.50, 0.99]
 # the plain CPU-runnable filter (1M rows)
 CONFIG1 = "SELECT id, uniformi, normali5 FROM test WHERE uniformi > 60 AND normali5 < 0"
