@@ -486,7 +486,14 @@ void virg_gpu_batch_destroy(virg_gpu_batch *b);
  * kernel reports each finished query in a completion record.  A query whose
  * rows exceed its estimate is admitted again with its exact row count.
  * Results stay in the result budget's device memory until released.  Tables
- * must not be appended to while queries over them are in flight. */
+ * must not be appended to while queries over them are in flight.  A
+ * session's kernel holds vector areas for the programs it may take: the
+ * bounds below size a wide layout; programs of at most 8 filter-vector and
+ * 20 projection-vector bytes per row also fit a narrow layout with three
+ * 48 KB data buffers, which a session uses while the queries at the head
+ * of the queue fit it (a query that does not ends the session once its
+ * queries are done, and the next session takes the other layout; arrival
+ * order is kept). */
 typedef struct {
 	uint64_t result_budget_bytes;    /* device memory for results (0: 20 GB) */
 	unsigned max_queries;            /* queries per kernel session (0: 4096) */

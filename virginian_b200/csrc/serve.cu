@@ -129,8 +129,16 @@ struct Arena {
 struct virg_serve {
 	virg_gpu_engine *e = nullptr;
 	virg_serve_config cfg{};
-	/* the session's launch geometry (one for every query it takes) */
+	/* the session's launch geometry (one for every query it takes): the
+	 * wide layout holds every program the bounds admit; the narrow one,
+	 * when it has larger data buffers, holds programs with fewer vector
+	 * bytes.  A session runs one of them; a query at the head of the queue
+	 * that the running session's layout does not match ends it once its
+	 * queries are done, and the next session takes the other layout */
 	Geom geom{};
+	Geom geom_wide{}, geom_narrow{};
+	bool have_narrow = false, session_narrow = false;
+	unsigned narrow_row = 0, narrow_sel = 0;
 	unsigned grid = 0;
 	cudaStream_t kstream = nullptr, ustream = nullptr;
 	/* device memory */
@@ -166,6 +174,7 @@ struct virg_serve {
 		int state = 0;  /* 0 pending, 1 in flight, 2 done, 3 failed */
 		std::string error;  /* why it failed */
 		unsigned readmits = 0;
+		bool narrow = false;  /* fits the narrow layout */
 	};
 	std::map<uint64_t, Query> queries;
 	std::deque<uint64_t> pending;
@@ -219,12 +228,40 @@ int serve_layout(virg_serve *s)
 	}
 	VGPU_CHECK(fit, "serving layout does not fit shared memory (vectors of %u + %u bytes per row)",
 		s->cfg.max_sel_vector_bytes, s->cfg.max_row_vector_bytes);
+	s->geom_wide = s->geom;
+	/* the narrow layout: three 48 KB buffers for programs of at most 8
+	 * filter-vector and 20 projection-vector bytes per row (within the
+	 * bounds), if that beats the wide layout's buffers */
+	s->narrow_row = std::min(s->cfg.max_row_vector_bytes, 8u);
+	s->narrow_sel = std::min(s->cfg.max_sel_vector_bytes, 20u);
+	{
+		Shape sh = {256, std::max(48u, min_kb), 3, 1, kServeChunkRows, 0};
+		Geom g;
+		s->have_narrow = sh.stage_kb > s->geom_wide.shape.stage_kb &&
+			geom_make(sh, s->narrow_sel, s->narrow_row, 0u, e->smem_optin, e->smem_sm, &g, 1);
+		if (s->have_narrow) {
+			int n = 0;
+			s->have_narrow = occupancy(g.shape, g.smem, &n) && n >= 1;
+			s->geom_narrow = g;
+		}
+		set_error("%s", "");
+	}
 	int per_sm = 0;
 	if (!occupancy(s->geom.shape, s->geom.smem, &per_sm))
 		VGPU_FAIL("occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
 	VGPU_CHECK(per_sm >= 1, "the serving kernel cannot be resident");
 	s->grid = (unsigned)e->nsm;
 	return 1;
+}
+
+/* does a program fit the narrow layout */
+bool fits_narrow(const virg_serve *s, const Program &P)
+{
+	if (!s->have_narrow)
+		return false;
+	ProgPlan pp;
+	plan_program(P, pp);
+	return pp.row_bpr <= s->narrow_row && pp.sel_bpr <= s->narrow_sel;
 }
 
 /* does a program fit the session's layout */
@@ -256,9 +293,21 @@ uint64_t query_chunks(const virg_gpu_table *t, uint32_t chunk_rows)
 	return chunk_prefix(t->seg_rows.data(), (uint32_t)t->seg_rows.size(), chunk_rows, nullptr);
 }
 
-/* start a session: clear its counters and look-back ring, launch the kernel */
+/* does the query at the head of the queue need the other layout than the
+ * running session's */
+bool head_mismatch(const virg_serve *s)
+{
+	if (!s->have_narrow || s->pending.empty())
+		return false;
+	return s->queries.at(s->pending.front()).narrow != s->session_narrow;
+}
+
+/* start a session: clear its counters and look-back ring, launch the kernel
+ * with the layout the query at the head of the queue needs */
 int session_start(virg_serve *s)
 {
+	s->session_narrow = s->have_narrow && !s->pending.empty() && s->queries.at(s->pending.front()).narrow;
+	s->geom = s->session_narrow ? s->geom_narrow : s->geom_wide;
 	CUDA_OK(cudaMemsetAsync(s->d_ctrl, 0, 2 * sizeof(unsigned), s->kstream), "session reset");
 	CUDA_OK(cudaMemsetAsync(s->d_status, 0, kStatusRing * sizeof(uint64_t), s->kstream), "status reset");
 	CUDA_OK(cudaMemsetAsync(s->d_done, 0, s->cfg.max_queries * sizeof(unsigned), s->kstream), "done reset");
@@ -319,7 +368,7 @@ unsigned admit(virg_serve *s)
 	const uint32_t nq0 = s->nq;
 	uint64_t work = s->work;
 	size_t chunk_words = s->chunk_words;
-	while (!s->pending.empty() && nq0 + batch.size() < s->cfg.max_queries) {
+	while (!s->pending.empty() && nq0 + batch.size() < s->cfg.max_queries && !head_mismatch(s)) {
 		auto &q = s->queries[s->pending.front()];
 		const Program &P = q.p->prog;
 		/* descriptor (its chunking depends on the program's staging) */
@@ -492,7 +541,7 @@ void scheduler(virg_serve *s)
 			/* a session that cannot take the next query ends once drained */
 			if (s->running && !s->pending.empty() && s->inflight.empty() &&
 				(s->nq >= s->cfg.max_queries || s->work >= kSessionWorkLimit / 2 ||
-				 s->chunk_words > kChunkPoolWords / 2)) {
+				 s->chunk_words > kChunkPoolWords / 2 || head_mismatch(s))) {
 				if (!session_stop(s))
 					s->fail = last_error();
 			}
@@ -638,6 +687,7 @@ extern "C" int virg_serve_submit(virg_serve *s, const virg_gpu_program *p, virg_
 	q.p = p;
 	q.t = t;
 	q.estimate_rows = est;
+	q.narrow = fits_narrow(s, P);
 	q.submitted = Clock::now();
 	s->queries.emplace(q.ticket, q);
 	s->pending.push_back(q.ticket);
