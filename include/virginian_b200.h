@@ -451,10 +451,12 @@ int virg_gpu_query_streamed(virg_gpu_engine *e, const virg_gpu_program *p,
 
 /* Batched persistent execution: the queries added to a batch run in one
  * launch of the VM kernel (chunks of all queries in one ordered work list),
- * or two: a launch's compute warps hold vector areas for its widest
+ * or up to three: a launch's compute warps hold vector areas for its widest
  * program, so programs too wide for three 48 KB data buffers beside eight
- * compute warps run in a second launch and leave the others their larger
- * buffers.  A batch owns its descriptors and counters, so
+ * compute warps run in a launch of their own and leave the others their
+ * larger buffers, and of the others those whose table's row sample says
+ * they keep at least half of the rows run apart, so each launch is tuned
+ * for its kind (the dense full phase suits mostly-kept rows).  A batch owns its descriptors and counters, so
  * virg_gpu_batch_run with use_graph captures its launches in a CUDA graph
  * once and replays it after.  With autotune on, the first run times the
  * candidate launch shapes for each launch on the batch and caches the

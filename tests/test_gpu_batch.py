@@ -148,7 +148,8 @@ MANY_RESULTS = ("select uniformi + normali5 as a, uniformi - normali5 as b, unif
 @pytest.mark.parametrize("graph", [False, True])
 def test_batch_with_a_wide_program_runs_as_two_launches(setup, graph):
     """A program whose filter needs more row-vector bytes than three 48 KB
-    data buffers leave room for runs in a second launch of the batch; every
+    data buffers leave room for runs in a launch of its own (besides the
+    launches of the narrow programs, split by sampled selectivity); every
     query still gets the CPU VM's stream."""
     eng, db, cat, tables, work = setup
     many = [(WIDE_FILTER.format(t="t4"), 4), (MANY_RESULTS.format(t="t4"), 4),
@@ -159,7 +160,7 @@ def test_batch_with_a_wide_program_runs_as_two_launches(setup, graph):
     l0 = eng.launches
     b.run(graph=graph)
     b.wait()
-    assert eng.launches - l0 == 2
+    assert eng.launches - l0 in (2, 3)
     for slot, (q, k) in enumerate(many):
         assert_same_stream(b.download(slot), db.query(q).columns, q)
     b.close()

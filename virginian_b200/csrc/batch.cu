@@ -43,6 +43,10 @@ namespace {
  * before every replay, so a fixed epoch is safe */
 constexpr uint32_t kBatchEpoch = kEpochMask;
 
+/* programs whose table sample says they keep at least this share of the
+ * rows form their own part of a batch */
+constexpr double kDensePartSel = 0.5;
+
 }  // namespace
 
 struct virg_gpu_batch {
@@ -302,21 +306,25 @@ void make_parts(virg_gpu_batch *b)
 			break;  /* the largest selection limit that fits for this r */
 		}
 	}
-	std::vector<size_t> narrow, wide;
-	for (size_t i = 0; i < n; i++)
-		(have && pp[i].row_bpr <= best_r && pp[i].sel_bpr <= best_s ? narrow : wide).push_back(i);
+	/* the narrow programs split again by the share of their table's row
+	 * sample their filter keeps: a part of mostly-kept rows can take the
+	 * shape and full-phase mode (dense) that suit it */
+	std::vector<size_t> sparse, dense, wide;
+	for (size_t i = 0; i < n; i++) {
+		if (!(have && pp[i].row_bpr <= best_r && pp[i].sel_bpr <= best_s)) {
+			wide.push_back(i);
+			continue;
+		}
+		const double sel = sample_selectivity(b->items[i].p->prog, b->items[i].t);
+		(sel >= kDensePartSel ? dense : sparse).push_back(i);
+	}
 	set_error("%s", "");
 	b->parts.clear();
-	if (narrow.empty() || wide.empty()) {
-		b->parts.emplace_back();
-		for (size_t i = 0; i < b->items.size(); i++)
-			b->parts.back().items.push_back(i);
-	} else {
-		b->parts.emplace_back();
-		b->parts.back().items = narrow;
-		b->parts.emplace_back();
-		b->parts.back().items = wide;
-	}
+	for (auto *set : {&sparse, &dense, &wide})
+		if (!set->empty()) {
+			b->parts.emplace_back();
+			b->parts.back().items = *set;
+		}
 }
 
 }  // namespace
