@@ -53,7 +53,10 @@ constexpr unsigned kEntries = 16;     /* ring of entries */
 constexpr unsigned kChunkSlots = 6;
 /* chunks whose count phase the producer issues before a chunk's full
  * phase, so the chunk's offset is resolved by the time its full tiles run */
-constexpr unsigned kCountAhead = 2;
+#ifndef VGPU_COUNT_AHEAD
+#define VGPU_COUNT_AHEAD 2
+#endif
+constexpr unsigned kCountAhead = VGPU_COUNT_AHEAD;
 static_assert(kChunkSlots >= kCountAhead + 2, "slots for the chunks in flight");
 
 /* blocks a compute warp filters at once (16 rows per lane; also the rows a
