@@ -751,7 +751,8 @@ extern "C" int virg_gpu_engine_create(int device, virg_gpu_engine **out)
 	e->device_name = prop.name;
 	if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
 		cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-		cudaMalloc((void **)&e->ctrl, 64) != cudaSuccess || cudaMemset(e->ctrl, 0, 64) != cudaSuccess) {
+		cudaMalloc((void **)&e->ctrl, 64) != cudaSuccess || cudaMemset(e->ctrl, 0, 64) != cudaSuccess ||
+		cudaHostAlloc((void **)&e->h_words, 2 * sizeof(unsigned long long), cudaHostAllocDefault) != cudaSuccess) {
 		delete e;
 		VGPU_FAIL("engine setup failed: %s", cudaGetErrorString(cudaGetLastError()));
 	}
@@ -830,6 +831,8 @@ extern "C" void virg_gpu_engine_destroy(virg_gpu_engine *e)
 		if (kv.second.ptr)
 			cudaFree(kv.second.ptr);
 	cudaFree(e->ctrl);
+	if (e->h_words)
+		cudaFreeHost(e->h_words);
 	cudaStreamDestroy(e->stream);
 	cudaStreamDestroy(e->copy_stream);
 	delete e;
@@ -1204,14 +1207,26 @@ extern "C" int virg_gpu_result_rows(virg_gpu_result *r, uint64_t *rows)
 {
 	VGPU_CHECK(r != nullptr && rows != nullptr, "null argument");
 	if (!r->have_rows) {
+		/* the row count and the engine's error word in one pinned copy
+		 * pair and one wait */
 		virg_gpu_engine *e = r->e;
 		unsigned long long h = 0;
-		if (!r->ntiles_zero)
-			CUDA_OK(cudaMemcpyAsync(&h, r->d_total, sizeof(h), cudaMemcpyDeviceToHost, e->stream),
-				"result count read");
 		unsigned err = 0;
-		if (!read_device_error(e, &err))
-			return 0;
+		{
+			std::lock_guard<std::mutex> lk(e->words_mu);
+			e->h_words[0] = 0;
+			e->h_words[1] = 0;
+			if (!r->ntiles_zero)
+				CUDA_OK(cudaMemcpyAsync(&e->h_words[0], r->d_total, sizeof(unsigned long long),
+					cudaMemcpyDeviceToHost, e->stream), "result count read");
+			CUDA_OK(cudaMemcpyAsync(&e->h_words[1], e->ctrl + 1, sizeof(unsigned), cudaMemcpyDeviceToHost,
+				e->stream), "error read");
+			CUDA_OK(cudaStreamSynchronize(e->stream), "stream sync");
+			h = e->h_words[0];
+			err = (unsigned)e->h_words[1];
+		}
+		if (err)
+			CUDA_OK(cudaMemsetAsync(e->ctrl + 1, 0, sizeof(unsigned), e->stream), "error clear");
 		VGPU_CHECK(err == 0, "query failed on the device: %s", device_error_text(err));
 		r->rows = h;
 		r->have_rows = true;

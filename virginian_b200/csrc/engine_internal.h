@@ -49,6 +49,9 @@ struct virg_gpu_engine {
 	cudaStream_t stream = nullptr;       /* launches, descriptor and result copies */
 	cudaStream_t copy_stream = nullptr;  /* streamed tablet uploads */
 	unsigned *ctrl = nullptr;            /* [0] work counter, [1] error word */
+	/* pinned: a result's row count and the error word, read back together */
+	unsigned long long *h_words = nullptr;
+	std::mutex words_mu;
 	uint64_t *status = nullptr;          /* look-back words */
 	size_t status_cap = 0;
 	uint32_t epoch = 0;
